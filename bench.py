@@ -1,0 +1,370 @@
+"""Benchmark: ERI quartets/s on the 21-class McMurchie-Davidson microbenchmark, plus RHF time-to-solution.
+
+Workload (one step): for each of the 21 canonical (s,p,d) angular classes, Q_PER_CLASS = 10^7 random
+shell quartets (contraction 1-3, weights U[0.1,1], exponents log-uniform [0.05,50], centres in a 12-bohr
+box), Cartesian FourC-normalised ERIs written to HBM in chunks of <= 10^6 quartets (output buffer reused).
+Inputs are synthetic and seeded.  Every step reads inputs and writes outputs larger than the 126 MB L2.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+value  = device-resident throughput (quartets/s, all ranks), CUDA events on the launching stream,
+e2e    = the same workload through the C ABI's host-buffer call qcg_eri_batch (pinned host memory,
+         H2D of the quartet list and D2H of every ERI block inside the timed region),
+roofline = the dominant class kernel against the FP64 FMA peak measured here by the library's probe,
+cpu_baseline = the CPU oracle (a port of the reference's arithmetic) on a bounded sample, all host cores.
+--impl reference times the CPU oracle alone (the reference itself cannot be built here).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+Q_PER_CLASS = 10_000_000
+CHUNK = 1_000_000
+NPOOL = 32768
+METRIC = "ERI quartets/s (21 (s,p,d) classes, contraction 1-3, FP64 Cartesian)"
+UNIT = "quartets/s"
+
+
+def class_block(cls):
+    n = [(l + 1) * (l + 2) // 2 for l in cls]
+    return n[0] * n[1] * n[2] * n[3]
+
+
+def class_flops(cls):
+    """Algorithmic FLOPs per primitive quartet (fixed per-class formula, same as the library's)."""
+    from qchem_b200.basis import components
+    la, lb, lc, ld = cls
+    H = lambda n: (n + 1) * (n + 2) * (n + 3) // 6
+
+    def S(l1, l2):
+        return sum((a[0] + b[0] + 1) * (a[1] + b[1] + 1) * (a[2] + b[2] + 1)
+                   for a in components(l1) for b in components(l2))
+
+    L = la + lb + lc + ld
+    nc = lambda l: (l + 1) * (l + 2) // 2
+    return ((20 + 3 * L) + 2 * sum(H(j) for j in range(L + 1)) + 2 * H(la + lb) * S(lc, ld)
+            + 2 * nc(lc) * nc(ld) * S(la, lb) + 2 * nc(la) * nc(lb) * nc(lc) * nc(ld))
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self.t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.t:
+            self.t.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(classes, pool, sample_per_class, threads):
+    """Oracle eri_batch on a bounded sample per class; quartets/s for the full class mix."""
+    from oracle.oracle import OracleBasis
+    from qchem_b200 import workloads as W
+    ob = OracleBasis(pool)
+    t_total = 0.0
+    for k, cls in enumerate(classes):
+        q = W.eri_class_batch(cls, sample_per_class, NPOOL, seed=W.SEED0 + 2500 + k)
+        t0 = time.perf_counter()
+        ob.eri_batch(q, nthreads=threads)
+        dt = time.perf_counter() - t0
+        t_total += dt * (Q_PER_CLASS / sample_per_class)
+    return len(classes) * Q_PER_CLASS / t_total
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the CPU oracle, all host threads, bounded sample per step."""
+    if rank != 0:
+        return
+    from qchem_b200 import workloads as W
+    from oracle.oracle import OracleBasis
+    threads = os.cpu_count() or 1
+    classes = W.quartet_classes()
+    pool = W.shell_pool(NPOOL, seed=W.SEED0 + 2000)
+    ob = OracleBasis(pool)
+    sample = args.ref_sample
+    qs = [W.eri_class_batch(cls, sample, NPOOL, seed=W.SEED0 + 2600 + k) for k, cls in enumerate(classes)]
+    for _ in range(args.warmup):
+        ob.eri_batch(qs[0][:64], nthreads=threads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        for q in qs:
+            ob.eri_batch(q, nthreads=threads)
+        times.append(time.perf_counter() - t0)
+    dt = sum(times)
+    value = len(classes) * sample * args.steps / dt
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "eri_microbenchmark_21_classes", "quartets_per_class_per_step": sample,
+                       "contraction": "1-3", "note": "CPU oracle (port of the reference arithmetic); the reference "
+                                                     "itself cannot be built in this image"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{sample} quartets per class x 21 classes per step"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--quartets-per-class", type=int, default=Q_PER_CLASS)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-extras", action="store_true")
+    ap.add_argument("--ref-sample", type=int, default=2000)
+    ap.add_argument("--cpu-sample", type=int, default=1000)
+    args = ap.parse_args()
+
+    from qchem_b200.parallel import dist_env, max_over_ranks
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from qchem_b200 import api, basis as B, workloads as W
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+    nq_cls = args.quartets_per_class
+    classes = W.quartet_classes()
+    pool = W.shell_pool(NPOOL, seed=W.SEED0 + 2000)
+    eng = api.Engine(pool)
+    eng.set_stream(stream.cuda_stream)
+    nprim = np.array([s.nprim for s in pool], dtype=np.int64)
+
+    # per-rank quartet lists (weak scaling: every rank its own 21 x nq_cls quartets), pinned host + device
+    h_q, d_q, prim_q = [], [], []
+    for k, cls in enumerate(classes):
+        q = W.eri_class_batch(cls, nq_cls, NPOOL, seed=W.SEED0 + 2000 + 97 * rank + k)
+        t = torch.from_numpy(q).pin_memory()
+        h_q.append(t)
+        d_q.append(t.to(dev, non_blocking=True))
+        pr = nprim[q].prod(axis=1)
+        prim_q.append([int(pr[c:c + CHUNK].sum()) for c in range(0, nq_cls, CHUNK)])
+    max_blk = max(class_block(c) for c in classes)
+    d_out = torch.empty(min(CHUNK, nq_cls) * max_blk, dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+
+    def step(events=None):
+        launches = 0
+        for k, cls in enumerate(classes):
+            if events is not None:
+                events[k][0].record(stream)
+            for c0 in range(0, nq_cls, CHUNK):
+                m = min(CHUNK, nq_cls - c0)
+                eng.eri_batch_device(cls, d_q[k].data_ptr() + 16 * c0, m, d_out.data_ptr())
+                launches += 1
+            if events is not None:
+                events[k][1].record(stream)
+        return launches
+
+    peak_tf, _ = api.measure_fp64_peak(20)
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    ev = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in classes]
+          for _ in range(args.steps)]
+    t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t_start.record(stream)
+    launches = 0
+    for s in range(args.steps):
+        launches += step(ev[s])
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms_local = t_start.elapsed_time(t_end)
+    if world > 1:
+        dist.barrier()
+    ms = max_over_ranks(ms_local, dev)
+    total_q = world * len(classes) * nq_cls * args.steps
+    value = total_q / (ms * 1e-3)
+
+    # per-class device time over the timed region -> dominant kernel roofline
+    cls_ms = np.zeros(len(classes))
+    for s in range(args.steps):
+        for k in range(len(classes)):
+            cls_ms[k] += ev[s][k][0].elapsed_time(ev[s][k][1])
+    kdom = int(np.argmax(cls_ms))
+    nlaunch = len(prim_q[kdom])
+    avg_launch_ms = cls_ms[kdom] / (args.steps * nlaunch)
+    flops_per_launch = class_flops(classes[kdom]) * (sum(prim_q[kdom]) / nlaunch)
+    achieved_tf = flops_per_launch / (avg_launch_ms * 1e-3) / 1e12
+    per_class = {"".join("spd"[l] for l in c): {"ms_per_step": cls_ms[k] / args.steps,
+                                                  "tflops": class_flops(c) * sum(prim_q[k]) /
+                                                  (cls_ms[k] / args.steps * 1e-3) / 1e12}
+                 for k, c in enumerate(classes)}
+    traffic = None
+    prof = os.path.join(REPO, "profiles", "dram_traffic.json")
+    if os.path.exists(prof):
+        with open(prof) as f:
+            tr = json.load(f)
+        key = "".join("spd"[l] for l in classes[kdom])
+        if key in tr.get("bytes_per_launch", {}):
+            traffic = tr["bytes_per_launch"][key]
+
+    # end to end through the host-buffer C ABI call (pinned host memory, copies inside the timed region)
+    e2e = None
+    if not args.no_e2e:
+        h_out = torch.empty(min(CHUNK, nq_cls) * max_blk, dtype=torch.float64).pin_memory()
+        eng_h = api.Engine(pool)
+        lib = api.lib()
+        import ctypes
+
+        def e2e_step():
+            h2d = d2h = 0
+            for k, cls in enumerate(classes):
+                for c0 in range(0, nq_cls, CHUNK):
+                    m = min(CHUNK, nq_cls - c0)
+                    qptr = ctypes.cast(h_q[k].data_ptr() + 16 * c0, ctypes.POINTER(ctypes.c_int))
+                    optr = ctypes.cast(h_out.data_ptr(), ctypes.POINTER(ctypes.c_double))
+                    rc = lib.qcg_eri_batch(eng_h._h, *cls, m, qptr, optr)
+                    if rc != 0:
+                        raise api.QcgError(rc, lib.qcg_last_error(eng_h._h).decode())
+                    h2d += 16 * m
+                    d2h += 8 * m * class_block(cls)
+            return h2d, d2h
+
+        e2e_step()
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            h2d, d2h = e2e_step()
+        e2e_s = max_over_ranks(time.perf_counter() - t0, dev)
+        e2e = {"value": total_q / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
+        del h_out
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "eri_microbenchmark_21_classes", "quartets_per_class": nq_cls,
+                       "contraction": "1-3", "exponents": "log-uniform [0.05,50]", "box_bohr": 12,
+                       "shell_pool_per_L": NPOOL, "chunk_quartets": CHUNK,
+                       "l2": "inputs and outputs larger than L2 every step (no flush needed)",
+                       "parallelism": f"dp{world} (independent quartet sets per rank)"},
+            "gpu_launches": launches,
+            "clocks": clk,
+            "roofline": {"bound": "fp64", "achieved": achieved_tf, "peak": peak_tf, "unit": "TFLOP/s",
+                         "frac": achieved_tf / peak_tf, "traffic": traffic,
+                         "kernel": "eri_batch_kernel class " + "".join("spd"[l] for l in classes[kdom]),
+                         "peak_source": "measured here: library DFMA probe (MEASURED_PEAKS.json has no FP64 figure)"},
+            "per_class": per_class,
+            "e2e": e2e}
+
+    if rank == 0 and world == 1:
+        threads = os.cpu_count() or 1
+        cb = cpu_baseline(classes, pool, args.cpu_sample, threads)
+        line["cpu_baseline"] = {"value": cb, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": f"{args.cpu_sample} quartets per class (21 classes), extrapolated to "
+                                          f"{nq_cls} per class"}
+    if rank == 0 and not args.no_extras:
+        line["extras"] = extras(torch, dev)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def extras(torch, dev):
+    """RHF time-to-solution (config-1 water) and one config-3 direct J/K build, GPU vs CPU oracle."""
+    from oracle.oracle import OracleBasis
+    from qchem_b200 import api, basis as B, workloads as W
+    out = {}
+    mol = W.water()
+    sh = B.even_tempered(mol)
+    eng = api.Engine(sh)
+    eng.rhf(mol)   # warm-up (module load, first-launch costs)
+    r = api.Engine(sh).rhf(mol)
+    ro = OracleBasis(sh).rhf(mol, nthreads=os.cpu_count() or 1)
+    out["rhf_water_config1"] = {"energy": r["energy"], "iterations": r["iterations"], "gpu_wall_s": r["wall_s"],
+                                "gpu_fock_ms_total": r["fock_ms"], "oracle_energy": ro["energy"],
+                                "abs_diff_eh": abs(r["energy"] - ro["energy"]), "cpu_oracle_wall_s": ro["wall_s"],
+                                "cpu_threads": os.cpu_count()}
+    mol3 = W.water_cluster()
+    sh3 = B.even_tempered(mol3)
+    D = W.cluster_density(B.nbf(sh3))
+    e3 = api.Engine(sh3)
+    t0 = time.perf_counter()
+    e3.schwarz(1e-10)
+    setup_s = time.perf_counter() - t0
+    J, K, st = e3.fock_jk(D)
+    J, K, st = e3.fock_jk(D)
+    out["fock_jk_config3"] = {"nbf": B.nbf(sh3), "quartets": st.quartets, "ms": st.ms_total,
+                              "tflops_algorithmic": st.flops / (st.ms_eri * 1e-3) / 1e12, "setup_s": setup_s}
+    return out
+
+
+if __name__ == "__main__":
+    main()

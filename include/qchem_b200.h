@@ -1,0 +1,129 @@
+/* qchem_b200.h -- C ABI of the B200 McMurchie-Davidson ERI engine and direct J/K Fock build.
+ *
+ * Drop-in boundary for qchem's molecular Hartree-Fock path (JanReimers/qchem).  Style follows the
+ * reference's flat bridge header pybind/qcb_api.h:14-37: extern "C", an opaque handle, caller-owned
+ * buffers, int status codes, no C++ types across the boundary.
+ *
+ * Each entry point names the reference interface it replaces:
+ *   qcg_basis_create    PG_Cart IrrepBasisSet + PGData::Init (flattened shells, unit-self-overlap norms)
+ *                       src/BasisSet/Molecule/PG_Cart/Imp/IrrepBasisSet.C:60-147,
+ *                       src/BasisSet/Molecule/Evaluators/PG_Cart_MnD/Imp/PGData.C:17-33
+ *   qcg_eri_batch       NR_Evaluator::FourC for whole shell quartets
+ *                       src/BasisSet/Molecule/Evaluators/PG_Cart_MnD/Evaluator.C:1912-1920
+ *   qcg_schwarz         (no reference counterpart: the reference stores full ERI4 blocks; this prepares the
+ *                       screened direct build that replaces them)
+ *   qcg_fock_jk         Orbital_HF_IBS<double>::AccumulateDirect / AccumulateExchange and
+ *                       WholeSystemFock_IBS<double>::MakeAOFock(Dao, exchange)
+ *                       src/BasisSet/Orbital_HF_IBS.C:33-54,75-87; the ERI4 build + contraction they use
+ *                       src/BasisSet/Molecule/IrrepBasisSet.C:138-183, src/BasisSet/Internal/Imp/ERI4.C:10-42
+ *   qcg_one_electron    NR_Evaluator::Overlap / Grad2 / Nuclear   (Evaluator.C:71-76)
+ *   qcg_rhf             Calculation + SCFIterator::Iterate with DIIS  (src/SCFIterator/Imp/SCFIterator.C:283-398)
+ *
+ * Matrices are dense, row-major, nbf x nbf doubles; D is the total RHF density (occupation 2).
+ * J_ab = sum_cd (ab|cd) D_cd and K_ac = sum_bd (ab|cd) D_bd, both UNSCALED (the caller forms
+ * F = H + J - 1/2 K, as HF_HT.C:48-70 does).  The engine is single-stream and not re-entrant per handle.
+ */
+#ifndef QCHEM_B200_H
+#define QCHEM_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct qcg_handle qcg_handle;
+
+enum qcg_status {
+    QCG_OK = 0,
+    QCG_ERR_ARG = 1,         /* invalid argument (null pointer, bad size, L > 2, non-canonical class...) */
+    QCG_ERR_CUDA = 2,        /* a CUDA runtime call failed; see qcg_last_error */
+    QCG_ERR_NONFINITE = 3,   /* NaN/Inf in an input matrix or in a result */
+    QCG_ERR_ASYMMETRIC = 4,  /* density matrix not symmetric */
+    QCG_ERR_ALLOC = 5,       /* device allocation failed or exceeded the handle's memory limit */
+    QCG_ERR_STATE = 6,       /* call order violated (e.g. qcg_fock_jk before qcg_schwarz) */
+    QCG_ERR_NOCONV = 7       /* SCF did not converge within the iteration limit */
+};
+
+/* flags for qcg_fock_jk */
+#define QCG_JK_SKIP_VALIDATION 1   /* do not check D for NaN/Inf and symmetry */
+#define QCG_JK_J_ONLY 2            /* reserved: both J and K are always built */
+
+typedef struct qcg_stats {
+    double ms_total;          /* device time of the whole J/K build (CUDA events) */
+    double ms_eri;            /* device time of the ERI + digestion kernels */
+    long long quartets;       /* shell quartets evaluated after screening */
+    long long prim_quartets;  /* primitive quartets evaluated */
+    double flops;             /* algorithmic FLOPs (fixed per-class formula) of the ERI work */
+} qcg_stats;
+
+typedef struct qcg_scf_params {
+    int max_iter;             /* default 100 */
+    double de_tol;            /* |E_k - E_{k-1}| stop, default 1e-10 Eh */
+    double fd_tol;            /* ||[F',D']|| must also be below this, default 1e-5 (SCFParams MinFD) */
+    double schwarz_thresh;    /* default 1e-10 */
+    int diis_nproj;           /* default 4 */
+    double diis_fdmax;        /* <= 0: Z^2 * 0.1 / 32 (Calculation.C default) */
+    double diis_svtol;        /* default 5e-9 */
+} qcg_scf_params;
+
+typedef struct qcg_scf_result {
+    double energy;            /* total energy incl. nuclear repulsion */
+    double e_nuc;
+    int iterations;
+    int converged;
+    double fd_error;          /* final ||[F',D']|| */
+    double wall_s;            /* host wall time of qcg_rhf */
+    double fock_ms;           /* summed device time of the J/K builds */
+} qcg_scf_result;
+
+/* ---- lifetime -------------------------------------------------------------------------------- */
+/* Shells in basis order.  shell_L[i] in {0,1,2}; primitives of shell i are the next shell_nprim[i]
+ * entries of exps/coefs (raw contraction coefficients: the engine folds the (L,0,0) primitive norm and
+ * renormalises every Cartesian component to unit self-overlap); centres: 3 doubles per shell (bohr). */
+int qcg_basis_create(const int* shell_L, const int* shell_nprim, const double* exps, const double* coefs,
+                     const double* centres, int nshell, qcg_handle** out);
+void qcg_destroy(qcg_handle* h);
+const char* qcg_last_error(const qcg_handle* h);
+int qcg_set_stream(qcg_handle* h, void* cuda_stream);     /* NULL: the handle's own stream */
+int qcg_set_memory_limit(qcg_handle* h, long long bytes); /* cap on device bytes this handle allocates; 0 = none */
+int qcg_nbf(const qcg_handle* h, int* nbf);
+int qcg_nshell(const qcg_handle* h, int* nshell);
+/* per-function normalisation constants ns (1/sqrt of the self-overlap of the coefficient-scaled radial) */
+int qcg_norms(const qcg_handle* h, double* ns);
+
+/* ---- integrals ------------------------------------------------------------------------------- */
+/* Cartesian ERIs of nq shell quartets of ONE canonical class (la>=lb, lc>=ld, (la,lb) >= (lc,ld) in
+ * the order ss<ps<pp<ds<dp<dd).  quartets: 4 int32 shell indices per quartet, whose L must match the
+ * class.  out: nq blocks of nA*nB*nC*nD doubles, row-major [a][b][c][d].  Host buffers. */
+int qcg_eri_batch(qcg_handle* h, int la, int lb, int lc, int ld, long long nq, const int* quartets, double* out);
+/* same with device pointers (no validation of the shell L's; the stream is the handle's) */
+int qcg_eri_batch_device(qcg_handle* h, int la, int lb, int lc, int ld, long long nq, const int* d_quartets,
+                         double* d_out);
+
+/* Schwarz bounds Q_ab = sqrt(max |(ab|ab)|) for every shell pair and the screened quartet lists used by
+ * qcg_fock_jk (quartets with Q_ab Q_cd < thresh are skipped).  Q: optional, nshell*nshell doubles. */
+int qcg_schwarz(qcg_handle* h, double thresh, double* Q);
+
+/* J and K for a total density D.  Host buffers (copies inside). */
+int qcg_fock_jk(qcg_handle* h, const double* D, double* J, double* K, int flags, qcg_stats* stats);
+/* same with device pointers on the handle's stream; results are ready when the stream reaches them */
+int qcg_fock_jk_device(qcg_handle* h, const double* d_D, double* d_J, double* d_K, int flags, qcg_stats* stats);
+
+/* overlap, kinetic (1/2 <grad|grad>) and nuclear attraction, natom nuclei of charge Z at R (3 per atom) */
+int qcg_one_electron(qcg_handle* h, int natom, const double* Z, const double* R, double* S, double* T, double* V);
+
+/* ---- RHF ------------------------------------------------------------------------------------- */
+void qcg_scf_default_params(qcg_scf_params* p);
+/* Closed-shell SCF: core-Hamiltonian guess, Pulay DIIS on the orthonormal-basis Fock matrix, J/K on the
+ * GPU every iteration.  D_out (optional, nbf*nbf) receives the final density. */
+int qcg_rhf(qcg_handle* h, int natom, const double* Z, const double* R, int nelec, const qcg_scf_params* params,
+            qcg_scf_result* result, double* D_out);
+
+/* ---- measurement ----------------------------------------------------------------------------- */
+/* FP64 fused-multiply-add throughput of the current device (TFLOP/s) from a pure-DFMA kernel timed over
+ * `reps` launches: the roofline denominator of the ERI kernels.  No reference counterpart. */
+int qcg_measure_fp64_peak(int reps, double* tflops, double* ms_per_launch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QCHEM_B200_H */

@@ -1,0 +1,306 @@
+"""Python front end of libqchem_b200.so (include/qchem_b200.h), loaded with ctypes.
+
+Two layers:
+  Engine         -- one handle: basis upload, Cartesian ERI batches, Schwarz screening, J/K builds,
+                    one-electron integrals, RHF.
+  OrbitalHFIBS   -- the face qchem's Hartree-Fock code calls, with the reference's method names:
+                    Orbital_HF_IBS<double>::AccumulateDirect / AccumulateExchange (+ ...Both)
+                    (src/BasisSet/Orbital_HF_IBS.C:33-54) and WholeSystemFock_IBS<double>::AODimension /
+                    AddAODensity / MakeAOFock / SliceAOFock (src/BasisSet/Orbital_HF_IBS.C:75-87).
+                    J and K for one density come from ONE fused GPU build, memoised by the density, so the
+                    reference's separate Coulomb and exchange calls with the same D cost one build.
+
+There is no CPU fallback: if the shared library is missing or no CUDA device is usable, constructing an
+Engine raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import hashlib
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import basis as _basis
+
+_LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib", "libqchem_b200.so")
+_lib = None
+
+QCG_OK, QCG_ERR_ARG, QCG_ERR_CUDA, QCG_ERR_NONFINITE, QCG_ERR_ASYMMETRIC, QCG_ERR_ALLOC, QCG_ERR_STATE, \
+    QCG_ERR_NOCONV = range(8)
+QCG_JK_SKIP_VALIDATION = 1
+
+# every symbol include/qchem_b200.h declares
+EXPORTS = ["qcg_basis_create", "qcg_destroy", "qcg_last_error", "qcg_set_stream", "qcg_set_memory_limit", "qcg_nbf",
+           "qcg_nshell", "qcg_norms", "qcg_eri_batch", "qcg_eri_batch_device", "qcg_schwarz", "qcg_fock_jk",
+           "qcg_fock_jk_device", "qcg_one_electron", "qcg_scf_default_params", "qcg_rhf", "qcg_measure_fp64_peak"]
+
+
+class QcgError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"qchem_b200 error {code}: {message}")
+        self.code = code
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("ms_total", ctypes.c_double), ("ms_eri", ctypes.c_double), ("quartets", ctypes.c_longlong),
+                ("prim_quartets", ctypes.c_longlong), ("flops", ctypes.c_double)]
+
+
+class ScfParams(ctypes.Structure):
+    _fields_ = [("max_iter", ctypes.c_int), ("de_tol", ctypes.c_double), ("fd_tol", ctypes.c_double),
+                ("schwarz_thresh", ctypes.c_double), ("diis_nproj", ctypes.c_int), ("diis_fdmax", ctypes.c_double),
+                ("diis_svtol", ctypes.c_double)]
+
+
+class ScfResult(ctypes.Structure):
+    _fields_ = [("energy", ctypes.c_double), ("e_nuc", ctypes.c_double), ("iterations", ctypes.c_int),
+                ("converged", ctypes.c_int), ("fd_error", ctypes.c_double), ("wall_s", ctypes.c_double),
+                ("fock_ms", ctypes.c_double)]
+
+
+def library_path() -> str:
+    return _LIB_PATH
+
+
+def lib():
+    """Load the CUDA library; raises ImportError if it has not been built (no fallback path)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(_LIB_PATH):
+        raise ImportError(f"{_LIB_PATH} not found: build it with `python -m qchem_b200.build`")
+    L = ctypes.CDLL(_LIB_PATH)
+    vp, i32, i64, f64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong, ctypes.c_double
+    P = ctypes.POINTER
+    L.qcg_basis_create.argtypes = [P(i32), P(i32), P(f64), P(f64), P(f64), i32, P(vp)]
+    L.qcg_destroy.argtypes = [vp]
+    L.qcg_destroy.restype = None
+    L.qcg_last_error.argtypes = [vp]
+    L.qcg_last_error.restype = ctypes.c_char_p
+    L.qcg_set_stream.argtypes = [vp, vp]
+    L.qcg_set_memory_limit.argtypes = [vp, i64]
+    L.qcg_nbf.argtypes = [vp, P(i32)]
+    L.qcg_nshell.argtypes = [vp, P(i32)]
+    L.qcg_norms.argtypes = [vp, P(f64)]
+    L.qcg_eri_batch.argtypes = [vp, i32, i32, i32, i32, i64, P(i32), P(f64)]
+    L.qcg_eri_batch_device.argtypes = [vp, i32, i32, i32, i32, i64, vp, vp]
+    L.qcg_schwarz.argtypes = [vp, f64, P(f64)]
+    L.qcg_fock_jk.argtypes = [vp, P(f64), P(f64), P(f64), i32, P(Stats)]
+    L.qcg_fock_jk_device.argtypes = [vp, vp, vp, vp, i32, P(Stats)]
+    L.qcg_one_electron.argtypes = [vp, i32, P(f64), P(f64), P(f64), P(f64), P(f64)]
+    L.qcg_scf_default_params.argtypes = [P(ScfParams)]
+    L.qcg_scf_default_params.restype = None
+    L.qcg_rhf.argtypes = [vp, i32, P(f64), P(f64), i32, P(ScfParams), P(ScfResult), P(f64)]
+    L.qcg_internal_syev.argtypes = [i32, P(f64), P(f64), P(f64)]
+    L.qcg_measure_fp64_peak.argtypes = [i32, P(f64), P(f64)]
+    _lib = L
+    return L
+
+
+def _p(a, t=ctypes.c_double):
+    return a.ctypes.data_as(ctypes.POINTER(t))
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def syev(A: np.ndarray):
+    """The SCF's host eigensolver (exposed for tests)."""
+    A = _f64(A)
+    n = A.shape[0]
+    w, V = np.zeros(n), np.zeros((n, n))
+    rc = lib().qcg_internal_syev(n, _p(A), _p(w), _p(V))
+    if rc != QCG_OK:
+        raise QcgError(rc, "eigensolver failed")
+    return w, V
+
+
+def measure_fp64_peak(reps: int = 20):
+    """(TFLOP/s, ms per launch) of the library's pure-DFMA probe kernel on the current device."""
+    tf, ms = ctypes.c_double(), ctypes.c_double()
+    rc = lib().qcg_measure_fp64_peak(int(reps), ctypes.byref(tf), ctypes.byref(ms))
+    if rc != QCG_OK:
+        raise QcgError(rc, "fp64 peak probe failed")
+    return tf.value, ms.value
+
+
+class Engine:
+    """One basis on the current CUDA device."""
+
+    def __init__(self, shells: Sequence[_basis.Shell]):
+        self.shells = list(shells)
+        L, npr, cen, ex, co = _basis.flatten(self.shells)
+        h = ctypes.c_void_p()
+        rc = lib().qcg_basis_create(_p(L, ctypes.c_int), _p(npr, ctypes.c_int), _p(ex), _p(co), _p(cen),
+                                    len(self.shells), ctypes.byref(h))
+        self._h = h
+        if rc != QCG_OK:
+            msg = lib().qcg_last_error(h).decode() if h.value else "qcg_basis_create failed"
+            self.close()
+            raise QcgError(rc, msg)
+        n = ctypes.c_int()
+        lib().qcg_nbf(self._h, ctypes.byref(n))
+        self.nbf = n.value
+        self.offsets = np.cumsum([0] + [s.nfunc for s in self.shells])[:-1]
+        self._screen = None
+
+    # -- lifetime ------------------------------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().qcg_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != QCG_OK:
+            raise QcgError(rc, lib().qcg_last_error(self._h).decode())
+
+    def set_stream(self, stream_ptr: Optional[int]):
+        self._check(lib().qcg_set_stream(self._h, ctypes.c_void_p(stream_ptr or 0)))
+
+    def set_memory_limit(self, nbytes: int):
+        self._check(lib().qcg_set_memory_limit(self._h, int(nbytes)))
+
+    def norms(self) -> np.ndarray:
+        ns = np.zeros(self.nbf)
+        self._check(lib().qcg_norms(self._h, _p(ns)))
+        return ns
+
+    # -- integrals -----------------------------------------------------------------------------
+    def eri_batch(self, cls, quartets) -> np.ndarray:
+        q = np.ascontiguousarray(quartets, dtype=np.int32)
+        la, lb, lc, ld = cls
+        nf = [(l + 1) * (l + 2) // 2 for l in cls]
+        out = np.zeros((len(q), nf[0] * nf[1] * nf[2] * nf[3]))
+        self._check(lib().qcg_eri_batch(self._h, la, lb, lc, ld, len(q), _p(q, ctypes.c_int), _p(out)))
+        return out
+
+    def eri_batch_device(self, cls, d_quartets_ptr: int, nq: int, d_out_ptr: int):
+        la, lb, lc, ld = cls
+        self._check(lib().qcg_eri_batch_device(self._h, la, lb, lc, ld, int(nq), ctypes.c_void_p(d_quartets_ptr),
+                                               ctypes.c_void_p(d_out_ptr)))
+
+    def schwarz(self, thresh: float = 1e-10) -> np.ndarray:
+        ns = len(self.shells)
+        Q = np.zeros((ns, ns))
+        self._check(lib().qcg_schwarz(self._h, float(thresh), _p(Q)))
+        self._screen = thresh
+        return Q
+
+    def fock_jk(self, D, validate: bool = True):
+        if self._screen is None:
+            self.schwarz()
+        D = _f64(D)
+        if D.shape != (self.nbf, self.nbf):
+            raise QcgError(QCG_ERR_ARG, f"density must be {self.nbf}x{self.nbf}")
+        J, K = np.zeros_like(D), np.zeros_like(D)
+        st = Stats()
+        self._check(lib().qcg_fock_jk(self._h, _p(D), _p(J), _p(K), 0 if validate else QCG_JK_SKIP_VALIDATION,
+                                      ctypes.byref(st)))
+        return J, K, st
+
+    def fock_jk_device(self, d_D: int, d_J: int, d_K: int, validate: bool = False) -> Stats:
+        if self._screen is None:
+            self.schwarz()
+        st = Stats()
+        self._check(lib().qcg_fock_jk_device(self._h, ctypes.c_void_p(d_D), ctypes.c_void_p(d_J), ctypes.c_void_p(d_K),
+                                             0 if validate else QCG_JK_SKIP_VALIDATION, ctypes.byref(st)))
+        return st
+
+    def one_electron(self, mol: _basis.Molecule):
+        n = self.nbf
+        Z = _f64(mol.Z)
+        R = _f64(mol.R).reshape(-1)
+        S, T, V = np.zeros((n, n)), np.zeros((n, n)), np.zeros((n, n))
+        self._check(lib().qcg_one_electron(self._h, len(Z), _p(Z), _p(R), _p(S), _p(T), _p(V)))
+        return S, T, V
+
+    def rhf(self, mol: _basis.Molecule, max_iter=100, de_tol=1e-10, fd_tol=1e-5, schwarz_thresh=1e-10,
+            want_density=False):
+        prm = ScfParams()
+        lib().qcg_scf_default_params(ctypes.byref(prm))
+        prm.max_iter, prm.de_tol, prm.fd_tol, prm.schwarz_thresh = max_iter, de_tol, fd_tol, schwarz_thresh
+        res = ScfResult()
+        Z = _f64(mol.Z)
+        R = _f64(mol.R).reshape(-1)
+        D = np.zeros((self.nbf, self.nbf)) if want_density else None
+        rc = lib().qcg_rhf(self._h, len(Z), _p(Z), _p(R), int(mol.nelec), ctypes.byref(prm), ctypes.byref(res),
+                           _p(D) if D is not None else None)
+        if rc not in (QCG_OK, QCG_ERR_NOCONV):
+            self._check(rc)
+        self._screen = schwarz_thresh
+        out = {"energy": res.energy, "e_nuc": res.e_nuc, "iterations": res.iterations,
+               "converged": bool(res.converged), "fd_error": res.fd_error, "wall_s": res.wall_s,
+               "fock_ms": res.fock_ms}
+        if D is not None:
+            out["D"] = D
+        return out
+
+
+class OrbitalHFIBS:
+    """qchem's HF contraction face over the GPU engine (one irrep: the whole AO basis).
+
+    AccumulateDirect(S, D):    S += J[D],  J_ab = sum_cd (ab|cd) D_cd   (Orbital_HF_IBS.C:36-37)
+    AccumulateExchange(S, D):  S += K[D],  K_ac = sum_bd (ab|cd) D_bd   (unscaled; the caller applies -1/2)
+    MakeAOFock(Dao, exchange): the whole-system J (exchange=False) or K (exchange=True) (Orbital_HF_IBS.C:84)
+    """
+
+    def __init__(self, engine: Engine, schwarz_thresh: float = 1e-10):
+        self.engine = engine
+        self.thresh = schwarz_thresh
+        self._memo_key = None
+        self._memo = None
+        self.builds = 0
+
+    def _jk(self, D):
+        D = _f64(D)
+        if not np.all(np.isfinite(D)):
+            raise QcgError(QCG_ERR_NONFINITE, "density matrix has NaN/Inf entries")
+        key = hashlib.sha1(D.tobytes()).hexdigest()
+        if key != self._memo_key:
+            if self.engine._screen != self.thresh:
+                self.engine.schwarz(self.thresh)
+            J, K, _ = self.engine.fock_jk(D)
+            self._memo_key, self._memo = key, (J, K)
+            self.builds += 1
+        return self._memo
+
+    # Orbital_HF_IBS<double>
+    def AccumulateDirect(self, Sab, Dcd, bs_cd=None):
+        Sab += self._jk(Dcd)[0]
+
+    def AccumulateExchange(self, Sab, Dcd, bs_cd=None):
+        Sab += self._jk(Dcd)[1]
+
+    def AccumulateDirectBoth(self, Ji, Jj, Di, Dj, cd=None):
+        # one irrep: the pair is the diagonal (i == j) block
+        Ji += self._jk(Dj)[0]
+        if Jj is not Ji:
+            Jj += self._jk(Di)[0]
+
+    def AccumulateExchangeBoth(self, Ki, Kj, Di, Dj, cd=None):
+        Ki += self._jk(Dj)[1]
+        if Kj is not Ki:
+            Kj += self._jk(Di)[1]
+
+    # WholeSystemFock_IBS<double>
+    def AODimension(self) -> int:
+        return self.engine.nbf
+
+    def AddAODensity(self, Dao, D):
+        Dao += D
+
+    def MakeAOFock(self, Dao, exchange: bool):
+        J, K = self._jk(Dao)
+        return (K if exchange else J).copy()
+
+    def SliceAOFock(self, Fab, Fao):
+        Fab += Fao

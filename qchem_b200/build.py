@@ -1,0 +1,127 @@
+"""Build libqchem_b200.so (the C ABI of include/qchem_b200.h) for sm_100a, in-tree.
+
+  python -m qchem_b200.build [--force] [-j N]
+
+Steps: generate the per-class MD code (csrc/gen_md.py), compile the 21 class objects plus the
+runtime in parallel with nvcc (-gencode arch=compute_100a,code=sm_100a -lineinfo), link a shared
+library into qchem_b200/_lib/.  Objects are cached in qchem_b200/_build/ keyed by a hash of their
+inputs, so unchanged classes are not recompiled.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import hashlib
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+GEN = os.path.join(CSRC, "gen")
+BUILD = os.path.join(HERE, "_build")
+LIBDIR = os.path.join(HERE, "_lib")
+LIB = os.path.join(LIBDIR, "libqchem_b200.so")
+INCLUDE = os.path.join(os.path.dirname(HERE), "include")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"] + ARCH
+NCLASS = 21
+
+
+def _read(p):
+    with open(p, "rb") as f:
+        return f.read()
+
+
+def _hash(parts):
+    h = hashlib.sha256()
+    for p in parts:
+        h.update(p if isinstance(p, bytes) else p.encode())
+    return h.hexdigest()[:20]
+
+
+def _common_headers():
+    names = ["md_core.cuh", "qcg_internal.h", "eri_kernels.cuh", "boys_table.h"]
+    return [_read(os.path.join(CSRC, n)) for n in names] + [_read(os.path.join(INCLUDE, "qchem_b200.h"))]
+
+
+def _jobs():
+    hdr = _common_headers()
+    jobs = []
+    src = os.path.join(CSRC, "eri_class.cu")
+    for k in range(NCLASS):
+        defs = [f"-DQCG_CLASS={k}"]
+        key = _hash([_read(src), _read(os.path.join(GEN, f"md_class_{k}.cuh"))] + hdr + FLAGS + defs)
+        jobs.append((src, defs, os.path.join(BUILD, f"eri_class_{k}_{key}.o")))
+    for name in ("registry.cu", "fock_kernels.cu", "runtime.cu"):
+        s = os.path.join(CSRC, name)
+        key = _hash([_read(s)] + hdr + FLAGS)
+        jobs.append((s, [], os.path.join(BUILD, f"{name[:-3]}_{key}.o")))
+    return jobs
+
+
+def _compile(job):
+    src, defs, obj = job
+    if os.path.exists(obj):
+        return obj, False
+    tmp = obj + ".tmp.o"
+    cmd = [NVCC] + FLAGS + defs + ["-I", CSRC, "-c", src, "-o", tmp]
+    r = subprocess.run(cmd, capture_output=True, text=True, cwd=CSRC)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed for {os.path.basename(src)} {defs}:\n{r.stderr[-4000:]}")
+    os.replace(tmp, obj)
+    return obj, True
+
+
+def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -> str:
+    sys.path.insert(0, CSRC)
+    try:
+        import gen_md  # noqa: E402
+    finally:
+        sys.path.pop(0)
+    gen_md.main(GEN)
+    if not os.path.exists(os.path.join(CSRC, "boys_table.h")):
+        raise RuntimeError("csrc/boys_table.h is missing (python csrc/gen_boys_table.py regenerates it)")
+    os.makedirs(BUILD, exist_ok=True)
+    os.makedirs(LIBDIR, exist_ok=True)
+    todo = _jobs()
+    if force:
+        for _, _, obj in todo:
+            if os.path.exists(obj):
+                os.remove(obj)
+    # biggest classes first so that the slowest compiles start early
+    todo.sort(key=lambda j: -os.path.getsize(os.path.join(GEN, f"md_class_{j[1][0].split('=')[1]}.cuh"))
+              if j[1] else 0)
+    n = jobs or max(1, os.cpu_count() or 1)
+    built = []
+    with cf.ThreadPoolExecutor(max_workers=n) as ex:
+        for obj, fresh in ex.map(_compile, todo):
+            built.append(obj)
+            if verbose and fresh:
+                print("compiled", os.path.basename(obj), flush=True)
+    objs = [o for _, _, o in todo]
+    key = _hash([os.path.basename(o) for o in sorted(objs)])
+    stamp = LIB + ".key"
+    if force or not os.path.exists(LIB) or not os.path.exists(stamp) or open(stamp).read() != key:
+        tmp = LIB + ".tmp"
+        cmd = [NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objs
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("link failed:\n" + r.stderr[-4000:])
+        os.replace(tmp, LIB)
+        with open(stamp, "w") as f:
+            f.write(key)
+    # drop stale objects of older source versions
+    keep = set(objs)
+    for f in os.listdir(BUILD):
+        p = os.path.join(BUILD, f)
+        if p.endswith(".o") and p not in keep:
+            os.remove(p)
+    return LIB
+
+
+if __name__ == "__main__":
+    j = None
+    if "-j" in sys.argv:
+        j = int(sys.argv[sys.argv.index("-j") + 1])
+    print(build(force="--force" in sys.argv, jobs=j, verbose=True))

@@ -1,0 +1,94 @@
+// eri_class.cu -- instantiates the kernels of ONE quartet class; compiled once per class with
+// -DQCG_CLASS=k (k = X(X+1)/2 + Y for pair classes X >= Y) so that the 21 classes build in parallel.
+#include "eri_kernels.cuh"
+
+#ifndef QCG_CLASS
+#error "compile with -DQCG_CLASS=<0..20>"
+#endif
+
+#define QCG_STR2(x) #x
+#define QCG_STR(x) QCG_STR2(x)
+#define QCG_CAT2(a, b) a##b
+#define QCG_CAT(a, b) QCG_CAT2(a, b)
+#include QCG_STR(gen/QCG_CAT(md_class_, QCG_CLASS).cuh)
+
+namespace qcg {
+
+namespace {
+constexpr int cls_X()
+{
+    int X = 0;
+    while ((X + 1) * (X + 2) / 2 <= QCG_CLASS) ++X;
+    return X;
+}
+constexpr int kX = cls_X();
+constexpr int kY = QCG_CLASS - kX * (kX + 1) / 2;
+
+struct Cls
+{
+    static constexpr int LA = kPairLA[kX], LB = kPairLB[kX], LC = kPairLA[kY], LD = kPairLB[kY];
+    static constexpr bool kRShared = gen::QCG_CAT(kRShared, QCG_CLASS);
+    static constexpr int kRSize = gen::QCG_CAT(kRSize, QCG_CLASS);
+    template <class Sink>
+    static __device__ __forceinline__ void quartet(const PrimPairData& ab, const PrimPairData& cd,
+                                                   const double* __restrict__ bt, double* __restrict__ rs, int stride,
+                                                   Sink& sink)
+    {
+        gen::QCG_CAT(prim_quartet_, QCG_CLASS)(ab, cd, bt, rs, stride, sink);
+    }
+};
+
+// classes whose R table lives in shared memory run 64-thread blocks (per-thread R slice); the others 128
+constexpr int kThreads = Cls::kRShared ? 64 : 128;
+constexpr size_t kSmem = Cls::kRShared ? (size_t)kThreads * Cls::kRSize * sizeof(double) : 0;
+
+template <class KernelPtr>
+void prepare(KernelPtr k)
+{
+    static bool done = false;
+    if (!done && kSmem > 48 * 1024)
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem);
+    done = true;
+}
+
+long long grid_for(long long work, int nsm)
+{
+    long long blocks = (work + kThreads - 1) / kThreads;
+    const long long cap = (long long)nsm * (Cls::kRShared ? 8 : 16);
+    return blocks > cap ? cap : blocks;
+}
+}   // namespace
+
+void QCG_CAT(launch_eri_batch_, QCG_CLASS)(const BasisDev& bs, const int4* q, long long nq, double* out,
+                                           const double* boys, cudaStream_t st, int nsm)
+{
+    if (nq <= 0) return;
+    auto k = eri_batch_kernel<Cls, kThreads>;
+    prepare(k);
+    k<<<(unsigned)grid_for(nq, nsm), kThreads, kSmem, st>>>(bs, q, nq, out, boys);
+}
+
+void QCG_CAT(launch_jk_, QCG_CLASS)(const JKWorkDev& w, const PairListDev& bra, const PairListDev& ket,
+                                    const PrimPairsDev& P, const int* f0, const double* D, double* J, double* K, int n,
+                                    const double* boys, cudaStream_t st, int nsm)
+{
+    if (w.total <= 0) return;
+    auto k = jk_kernel<Cls, kThreads>;
+    prepare(k);
+    k<<<(unsigned)grid_for(w.total, nsm), kThreads, kSmem, st>>>(w, bra, ket, P, f0, D, J, K, n, boys);
+}
+
+// Schwarz diagonals exist only for the diagonal classes (X == Y)
+void QCG_CAT(launch_schwarz_, QCG_CLASS)(const PairListDev& pl, const PrimPairsDev& P, double* Q, const double* boys,
+                                         cudaStream_t st)
+{
+    if constexpr (kX == kY)
+    {
+        if (pl.n <= 0) return;
+        auto k = schwarz_kernel<Cls, kThreads>;
+        prepare(k);
+        k<<<(pl.n + kThreads - 1) / kThreads, kThreads, kSmem, st>>>(pl, P, Q, boys);
+    }
+}
+
+}   // namespace qcg

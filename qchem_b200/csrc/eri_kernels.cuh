@@ -1,0 +1,249 @@
+// eri_kernels.cuh -- class-specialised ERI kernels: Cartesian-ERI batches, Schwarz diagonals and the
+// fused ERI + J/K digestion.  Included by eri_class.cu, which is compiled once per quartet class and
+// supplies Cls::quartet (the generated straight-line primitive-quartet evaluation of that class).
+#pragma once
+#include "md_core.cuh"
+#include "qcg_internal.h"
+
+namespace qcg {
+
+// ------------------------------------------------------------------------------------------------
+// Cartesian ERI batch: out[q][a][b][c][d] = (ab|cd) for quartet q (shell indices), contracted and
+// normalised like qchem's NR_Evaluator::FourC (PG_Cart_MnD/Evaluator.C:1912-1920).
+// ------------------------------------------------------------------------------------------------
+template <int LB, int LC, int LD>
+struct StoreSink
+{
+    double* o;
+    bool first;
+    static constexpr int NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+    __device__ __forceinline__ void ket_begin(int, int) {}
+    __device__ __forceinline__ void ket_end(int, int) {}
+    __device__ __forceinline__ void operator()(int ia, int ib, int ic, int id, double v)
+    {
+        double* p = o + ((ia * NB + ib) * NC + ic) * ND + id;
+        if (first) *p = v;
+        else *p += v;
+    }
+};
+
+__device__ __forceinline__ PrimPairData shell_prim_pair(const BasisDev& bs, int sa, int i, int sb, int j)
+{
+    const int pa = bs.prim0[sa] + i, pb = bs.prim0[sb] + j;
+    return make_prim_pair(bs.alpha[pa], bs.cen[3 * sa], bs.cen[3 * sa + 1], bs.cen[3 * sa + 2], bs.coef[pa],
+                          bs.alpha[pb], bs.cen[3 * sb], bs.cen[3 * sb + 1], bs.cen[3 * sb + 2], bs.coef[pb]);
+}
+
+// dynamic shared memory holding the per-thread R tables of classes with L >= 6
+extern __shared__ double qcg_smem[];
+
+template <class Cls, int THREADS>
+__global__ void __launch_bounds__(THREADS) eri_batch_kernel(BasisDev bs, const int4* __restrict__ quartets,
+                                                            long long nq, double* __restrict__ out,
+                                                            const double* __restrict__ boys_table)
+{
+    constexpr long long BLK = (long long)ncart(Cls::LA) * ncart(Cls::LB) * ncart(Cls::LC) * ncart(Cls::LD);
+    double* rs = qcg_smem + threadIdx.x;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nq; q += (long long)gridDim.x * blockDim.x)
+    {
+        const int4 s = quartets[q];
+        StoreSink<Cls::LB, Cls::LC, Cls::LD> sink{out + q * BLK, true};
+        const int ni = bs.nprim[s.x], nj = bs.nprim[s.y], nk = bs.nprim[s.z], nl = bs.nprim[s.w];
+        for (int i = 0; i < ni; ++i)
+            for (int j = 0; j < nj; ++j)
+            {
+                const PrimPairData ab = shell_prim_pair(bs, s.x, i, s.y, j);
+                for (int k = 0; k < nk; ++k)
+                    for (int l = 0; l < nl; ++l)
+                    {
+                        const PrimPairData cd = shell_prim_pair(bs, s.z, k, s.w, l);
+                        Cls::quartet(ab, cd, boys_table, rs, THREADS, sink);
+                        sink.first = false;
+                    }
+            }
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Pair lists: pair class X holds shell pairs (a,b) with L_a >= L_b, sorted by Schwarz bound
+// descending; the primitive pairs of pair i are P[ppo[i] .. ppo[i]+npp[i]).
+// ------------------------------------------------------------------------------------------------
+__device__ __forceinline__ PrimPairData load_pp(const PrimPairsDev& P, int k)
+{
+    PrimPairData d;
+    d.p = P.p[k];
+    d.Px = P.Px[k]; d.Py = P.Py[k]; d.Pz = P.Pz[k];
+    d.PAx = P.PAx[k]; d.PAy = P.PAy[k]; d.PAz = P.PAz[k];
+    d.PBx = P.PBx[k]; d.PBy = P.PBy[k]; d.PBz = P.PBz[k];
+    d.K = P.K[k];
+    return d;
+}
+
+// Schwarz diagonal: Q_i = sqrt(max_{mu nu} |(mu nu|mu nu)|) for every pair of one diagonal class
+template <int LA, int LB>
+struct DiagSink
+{
+    static constexpr int NB = ncart(LB), NAB = ncart(LA) * ncart(LB);
+    double acc[NAB];
+    __device__ __forceinline__ void ket_begin(int, int) {}
+    __device__ __forceinline__ void ket_end(int, int) {}
+    __device__ __forceinline__ void operator()(int ia, int ib, int ic, int id, double v)
+    {
+        if (ia == ic && ib == id) acc[ia * NB + ib] += v;
+    }
+};
+
+template <class Cls, int THREADS>
+__global__ void __launch_bounds__(THREADS) schwarz_kernel(PairListDev pl, PrimPairsDev P, double* __restrict__ Q,
+                                                          const double* __restrict__ boys_table)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= pl.n) return;
+    double* rs = qcg_smem + threadIdx.x;
+    DiagSink<Cls::LA, Cls::LB> sink;
+#pragma unroll
+    for (int k = 0; k < DiagSink<Cls::LA, Cls::LB>::NAB; ++k) sink.acc[k] = 0.0;
+    const int o = pl.ppo[i], n = pl.npp[i];
+    for (int x = 0; x < n; ++x)
+    {
+        const PrimPairData ab = load_pp(P, o + x);
+        for (int y = 0; y < n; ++y)
+        {
+            const PrimPairData cd = load_pp(P, o + y);
+            Cls::quartet(ab, cd, boys_table, rs, THREADS, sink);
+        }
+    }
+    double m = 0.0;
+#pragma unroll
+    for (int k = 0; k < DiagSink<Cls::LA, Cls::LB>::NAB; ++k) m = fmax(m, fabs(sink.acc[k]));
+    Q[i] = sqrt(m);
+}
+
+// ------------------------------------------------------------------------------------------------
+// Fused ERI + J/K digestion.  For a canonical quartet with weight w = s * (mu nu|la si),
+// s = 1/2^{[a=b]+[c=d]+[ab=cd]}, the eight permutational images reduce to
+//   J'[mu nu] += 2 w D[la si]      J'[la si] += 2 w D[mu nu]
+//   K'[mu la] += w D[nu si]        K'[nu la] += w D[mu si]
+//   K'[mu si] += w D[nu la]        K'[nu si] += w D[mu la]
+// and J = J' + J'^T, K = K' + K'^T afterwards.  Partial sums are kept in registers along the
+// component loops; what leaves the thread goes to the L2-resident J'/K' with red.global.add.f64.
+// ------------------------------------------------------------------------------------------------
+template <int LA, int LB, int LC, int LD>
+struct JKSink
+{
+    static constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD), NAB = NA * NB;
+    const double* __restrict__ D;
+    double* __restrict__ J;
+    double* __restrict__ K;
+    int n, fa, fb, fc, fd;
+    double s;
+    double jab[NAB];
+    double kac[NA], kbc[NB], kad[NA], kbd[NB];
+    double dls, jcd;
+    double dbs[NB], das[NA], dbl[NB], dal[NA];
+
+    __device__ __forceinline__ void init()
+    {
+#pragma unroll
+        for (int k = 0; k < NAB; ++k) jab[k] = 0.0;
+#pragma unroll
+        for (int k = 0; k < NA; ++k) kac[k] = 0.0;
+#pragma unroll
+        for (int k = 0; k < NB; ++k) kbc[k] = 0.0;
+    }
+    __device__ __forceinline__ void ket_begin(int ic, int id)
+    {
+        const int la = fc + ic, si = fd + id;
+        dls = __ldg(D + (size_t)la * n + si);
+        jcd = 0.0;
+#pragma unroll
+        for (int k = 0; k < NA; ++k)
+        {
+            das[k] = __ldg(D + (size_t)(fa + k) * n + si);
+            dal[k] = __ldg(D + (size_t)(fa + k) * n + la);
+            kad[k] = 0.0;
+        }
+#pragma unroll
+        for (int k = 0; k < NB; ++k)
+        {
+            dbs[k] = __ldg(D + (size_t)(fb + k) * n + si);
+            dbl[k] = __ldg(D + (size_t)(fb + k) * n + la);
+            kbd[k] = 0.0;
+        }
+    }
+    __device__ __forceinline__ void operator()(int ia, int ib, int, int, double v)
+    {
+        const double w = s * v;
+        jab[ia * NB + ib] += w * dls;
+        jcd += w * __ldg(D + (size_t)(fa + ia) * n + fb + ib);
+        kac[ia] += w * dbs[ib];
+        kbc[ib] += w * das[ia];
+        kad[ia] += w * dbl[ib];
+        kbd[ib] += w * dal[ia];
+    }
+    __device__ __forceinline__ void ket_end(int ic, int id)
+    {
+        const int la = fc + ic, si = fd + id;
+        atomicAdd(J + (size_t)la * n + si, 2.0 * jcd);
+#pragma unroll
+        for (int k = 0; k < NA; ++k) atomicAdd(K + (size_t)(fa + k) * n + si, kad[k]);
+#pragma unroll
+        for (int k = 0; k < NB; ++k) atomicAdd(K + (size_t)(fb + k) * n + si, kbd[k]);
+        if (id == ND - 1)
+        {
+#pragma unroll
+            for (int k = 0; k < NA; ++k) { atomicAdd(K + (size_t)(fa + k) * n + la, kac[k]); kac[k] = 0.0; }
+#pragma unroll
+            for (int k = 0; k < NB; ++k) { atomicAdd(K + (size_t)(fb + k) * n + la, kbc[k]); kbc[k] = 0.0; }
+        }
+    }
+    __device__ __forceinline__ void finish()
+    {
+#pragma unroll
+        for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+            for (int ib = 0; ib < NB; ++ib) atomicAdd(J + (size_t)(fa + ia) * n + fb + ib, 2.0 * jab[ia * NB + ib]);
+    }
+};
+
+template <class Cls, int THREADS>
+__global__ void __launch_bounds__(THREADS) jk_kernel(JKWorkDev w, PairListDev bra, PairListDev ket, PrimPairsDev P,
+                                                     const int* __restrict__ shell_f0, const double* __restrict__ D,
+                                                     double* __restrict__ J, double* __restrict__ K, int n,
+                                                     const double* __restrict__ boys_table)
+{
+    double* rs = qcg_smem + threadIdx.x;
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < w.total;
+         g += (long long)gridDim.x * blockDim.x)
+    {
+        // bra pair i: offs[i] <= g < offs[i+1]
+        int lo = 0, hi = bra.n;
+        while (hi - lo > 1)
+        {
+            const int mid = (lo + hi) >> 1;
+            if (w.offs[mid] <= g) lo = mid;
+            else hi = mid;
+        }
+        const int i = lo;
+        const int j = (int)(g - w.offs[i]);
+        const int sa = bra.sa[i], sb = bra.sb[i], sc = ket.sa[j], sd = ket.sb[j];
+        JKSink<Cls::LA, Cls::LB, Cls::LC, Cls::LD> sink;
+        sink.D = D; sink.J = J; sink.K = K; sink.n = n;
+        sink.fa = shell_f0[sa]; sink.fb = shell_f0[sb]; sink.fc = shell_f0[sc]; sink.fd = shell_f0[sd];
+        sink.s = (sa == sb ? 0.5 : 1.0) * (sc == sd ? 0.5 : 1.0) * ((w.same_class && i == j) ? 0.5 : 1.0);
+        sink.init();
+        const int oi = bra.ppo[i], ni = bra.npp[i], oj = ket.ppo[j], nj = ket.npp[j];
+        for (int x = 0; x < ni; ++x)
+        {
+            const PrimPairData ab = load_pp(P, oi + x);
+            for (int y = 0; y < nj; ++y)
+            {
+                const PrimPairData cd = load_pp(P, oj + y);
+                Cls::quartet(ab, cd, boys_table, rs, THREADS, sink);
+            }
+        }
+        sink.finish();
+    }
+}
+
+}   // namespace qcg

@@ -1,0 +1,277 @@
+"""Generate straight-line McMurchie-Davidson code for each of the 21 (s,p,d) quartet classes.
+
+For class (LA LB | LC LD) the generated device function evaluates ONE primitive quartet:
+  Boys F_0..F_L -> R^0_{tuv} in place, levels L..0 (registers, or a per-thread slice of shared memory
+  when L >= R_SMEM_MIN_L) -> 1-D Hermite E tables of both pairs (registers) -> for every ket component
+  (c,d): the ket transform X_{tuv} = sum_{h' in supp(cd)} (-1)^{|h'|} E^{cd}_{h'} R_{tuv+h'} with every
+  R value read once per (c,d); then for every bra component (a,b) the factored sum
+  sum_t Ex_t sum_u Ey_u sum_v Ez_v X_{tuv} and the sink call.
+All indices are literals, so nvcc keeps the tables in registers without any constexpr folding work.
+
+Recursions follow qchem: R (Internal/MnD/Imp/RNLM.C:19-68), E (PG_Cart_MnD/Internal/Imp/Hermite2.C:95-139),
+Boys (Internal/Boys/Imp/AuxillaryFJ.C:13-48), prefactor (PG_Cart_MnD/Imp/GaussianRF.C:446-483).
+
+Usage: python gen_md.py <outdir>   (writes md_class_<k>.cuh for k = 0..20)
+"""
+import math
+import os
+import sys
+
+PAIRS = [(0, 0), (1, 0), (1, 1), (2, 0), (2, 1), (2, 2)]
+R_SMEM_MIN_L = 6
+
+
+def classes():
+    out = []
+    for X in range(6):
+        for Y in range(X + 1):
+            out.append(PAIRS[X] + PAIRS[Y])
+    return out
+
+
+def comps(L):
+    return [(L - m - l, l, m) for m in range(L + 1) for l in range(L - m + 1)]
+
+
+def hidx(L, t, u, v):
+    off = 0
+    for tt in range(t):
+        off += (L - tt + 1) * (L - tt + 2) // 2
+    for uu in range(u):
+        off += (L - t - uu + 1)
+    return off + v
+
+
+def nherm(L):
+    return (L + 1) * (L + 2) * (L + 3) // 6
+
+
+def herm_list(L):
+    return [(t, u, v) for t in range(L + 1) for u in range(L + 1 - t) for v in range(L + 1 - t - u)]
+
+
+def inv_sqrt_dfact(k):
+    d = 1.0
+    for x in range(2 * k - 1, 1, -2):
+        d *= x
+    return 1.0 / math.sqrt(d)
+
+
+def comp_norm(c):
+    return inv_sqrt_dfact(c[0]) * inv_sqrt_dfact(c[1]) * inv_sqrt_dfact(c[2])
+
+
+def lit(x):
+    return "%.17g" % x
+
+
+def gen_E(name, LA, LB, PA, PB, a12):
+    """1-D E table of one direction as scalars name_i_j_t, in the build order of Hermite2.C."""
+    out = [f"const double {name}_0_0_0 = 1.0;"]
+
+    def g(i, j, t):
+        return f"{name}_{i}_{j}_{t}"
+
+    def expr(i0, j0, t, P):
+        terms = []
+        if t >= 1:
+            terms.append(f"{g(i0, j0, t - 1)} * {a12}")
+        if t <= i0 + j0:
+            terms.append(f"{g(i0, j0, t)} * {P}")
+        if t + 1 <= i0 + j0:
+            terms.append(f"{g(i0, j0, t + 1)} * {t + 1}.0")
+        return " + ".join(terms)
+
+    for i in range(1, LA + 1):
+        for t in range(0, i + 1):
+            out.append(f"const double {name}_{i}_0_{t} = {expr(i - 1, 0, t, PA)};")
+    for i in range(0, LA + 1):
+        for j in range(1, LB + 1):
+            for t in range(0, i + j + 1):
+                out.append(f"const double {name}_{i}_{j}_{t} = {expr(i, j - 1, t, PB)};")
+    return out
+
+
+CHUNK_OUTPUTS = 216        # classes with more outputs are split into __noinline__ ket-component chunks
+
+
+def e_tables(LA, LB, LC, LD):
+    out = []
+    for dname, la, lb, PA, PB, a12 in (("ebx", LA, LB, "ab.PAx", "ab.PBx", "a12b"),
+                                       ("eby", LA, LB, "ab.PAy", "ab.PBy", "a12b"),
+                                       ("ebz", LA, LB, "ab.PAz", "ab.PBz", "a12b"),
+                                       ("ekx", LC, LD, "cd.PAx", "cd.PBx", "a12k"),
+                                       ("eky", LC, LD, "cd.PAy", "cd.PBy", "a12k"),
+                                       ("ekz", LC, LD, "cd.PAz", "cd.PBz", "a12k")):
+        out.extend(gen_E(dname, la, lb, PA, PB, a12))
+    return out
+
+
+def e_names(prefix, la, lb):
+    names = []
+    for i in range(la + 1):
+        for j in range(lb + 1):
+            for t in range(i + j + 1):
+                names.append(f"{prefix}_{i}_{j}_{t}")
+    return names
+
+
+def r_prologue(L, rsm, w):
+    HL = nherm(L)
+    w("    const double p = ab.p, q = cd.p, pq = p + q;")
+    w("    const double alpha = p * q / pq;")
+    w("    const double X = ab.Px - cd.Px, Y = ab.Py - cd.Py, Z = ab.Pz - cd.Pz;")
+    w(f"    double F[{L + 1}];")
+    w(f"    boys<{L}>(alpha * (X * X + Y * Y + Z * Z), bt, F);")
+    w("    const double m2a = -2.0 * alpha;")
+    w(f"    double pwn[{L + 1}];")
+    w("    pwn[0] = 1.0;")
+    for n in range(1, L + 1):
+        w(f"    pwn[{n}] = pwn[{n - 1}] * m2a;")
+    if rsm:
+        w("#define RR(i) rs[(i) * rstride]")
+    else:
+        w(f"    double Rr[{HL}];")
+        w("#define RR(i) Rr[i]")
+    w(f"    RR(0) = pwn[{L}] * F[{L}];")
+    for n in range(L - 1, -1, -1):
+        for m in range(L - n, 0, -1):
+            for t in range(m, -1, -1):
+                for u in range(m - t, -1, -1):
+                    v = m - t - u
+                    if t > 0:
+                        e = f"X * RR({hidx(L, t - 1, u, v)})"
+                        if t > 1:
+                            e += f" + {t - 1}.0 * RR({hidx(L, t - 2, u, v)})"
+                    elif u > 0:
+                        e = f"Y * RR({hidx(L, 0, u - 1, v)})"
+                        if u > 1:
+                            e += f" + {u - 1}.0 * RR({hidx(L, 0, u - 2, v)})"
+                    else:
+                        e = f"Z * RR({hidx(L, 0, 0, v - 1)})"
+                        if v > 1:
+                            e += f" + {v - 1}.0 * RR({hidx(L, 0, 0, v - 2)})"
+                    w(f"    RR({hidx(L, t, u, v)}) = {e};")
+        w(f"    RR(0) = pwn[{n}] * F[{n}];")
+    w("    const double lambda = 34.986836655249725693 / (p * q * sqrt(pq)) * ab.K * cd.K;")
+    w("    const double a12b = 0.5 / ab.p, a12k = 0.5 / cd.p;")
+
+
+def ket_blocks(LA, LB, LC, LD, cds, w):
+    L = LA + LB + LC + LD
+    LAB = LA + LB
+    A, B, C, D = comps(LA), comps(LB), comps(LC), comps(LD)
+    HAB = herm_list(LAB)
+    NX = len(HAB)
+    for (ic, id_) in cds:
+        c, d = C[ic], D[id_]
+        w(f"    {{ // ket component ({ic},{id_})")
+        w(f"    sink.ket_begin({ic}, {id_});")
+        supp = [(tp, up, vp) for tp in range(c[0] + d[0] + 1) for up in range(c[1] + d[1] + 1)
+                for vp in range(c[2] + d[2] + 1)]
+        for (tp, up, vp) in supp:
+            sgn = "-" if (tp + up + vp) & 1 else ""
+            w(f"    const double s{tp}{up}{vp} = {sgn}ekx_{c[0]}_{d[0]}_{tp} * eky_{c[1]}_{d[1]}_{up} * "
+              f"ekz_{c[2]}_{d[2]}_{vp};")
+        w("    double " + ", ".join(f"x{i} = 0.0" for i in range(NX)) + ";")
+        contrib = {}
+        for h in HAB:
+            for hp in supp:
+                H = hidx(L, h[0] + hp[0], h[1] + hp[1], h[2] + hp[2])
+                contrib.setdefault(H, []).append((hidx(LAB, *h), hp))
+        for H in sorted(contrib):
+            body = " ".join(f"x{xi} = fma(s{hp[0]}{hp[1]}{hp[2]}, r, x{xi});" for (xi, hp) in contrib[H])
+            w(f"    {{ const double r = RR({H}); {body} }}")
+        w(f"    const double lam_cd = lambda * {lit(comp_norm(c) * comp_norm(d))};")
+        for ia, a in enumerate(A):
+            for ib, b in enumerate(B):
+                w("    {")
+                w("      double sx = 0.0;")
+                for t in range(a[0] + b[0] + 1):
+                    w("      { double sy = 0.0;")
+                    for u in range(a[1] + b[1] + 1):
+                        vs = list(range(a[2] + b[2] + 1))
+                        zs = f"ebz_{a[2]}_{b[2]}_0 * x{hidx(LAB, t, u, 0)}"
+                        for v in vs[1:]:
+                            zs = f"fma(ebz_{a[2]}_{b[2]}_{v}, x{hidx(LAB, t, u, v)}, {zs})"
+                        w(f"        sy = fma(eby_{a[1]}_{b[1]}_{u}, {zs}, sy);")
+                    w(f"        sx = fma(ebx_{a[0]}_{b[0]}_{t}, sy, sx); }}")
+                w(f"      sink({ia}, {ib}, {ic}, {id_}, sx * (lam_cd * {lit(comp_norm(a) * comp_norm(b))}));")
+                w("    }")
+        w(f"    sink.ket_end({ic}, {id_});")
+        w("    }")
+
+
+def gen_class(LA, LB, LC, LD, idx):
+    L = LA + LB + LC + LD
+    rsm = L >= R_SMEM_MIN_L
+    A, B, C, D = comps(LA), comps(LB), comps(LC), comps(LD)
+    nab, ncd = len(A) * len(B), len(C) * len(D)
+    all_cds = [(ic, id_) for ic in range(len(C)) for id_ in range(len(D))]
+    chunked = nab * ncd > CHUNK_OUTPUTS
+    o = []
+    w = o.append
+    w(f"// class {idx}: ({'spd'[LA]}{'spd'[LB]}|{'spd'[LC]}{'spd'[LD]}), L = {L}; R table in "
+      f"{'a per-thread slice of shared memory' if rsm else 'registers'}"
+      f"{'; ket components split into __noinline__ chunks' if chunked else ''}")
+    w(f"constexpr bool kRShared{idx} = {'true' if rsm else 'false'};")
+    w(f"constexpr int kRSize{idx} = {nherm(L)};")
+    ebn = e_names("ebx", LA, LB) + e_names("eby", LA, LB) + e_names("ebz", LA, LB)
+    ekn = e_names("ekx", LC, LD) + e_names("eky", LC, LD) + e_names("ekz", LC, LD)
+    chunk_names = []
+    if chunked:
+        per = max(1, CHUNK_OUTPUTS // nab)
+        chunks = [all_cds[i:i + per] for i in range(0, len(all_cds), per)]
+        for ci, cds in enumerate(chunks):
+            fn = f"prim_quartet_{idx}_chunk{ci}"
+            chunk_names.append(fn)
+            w("template <class Sink>")
+            w(f"__device__ __noinline__ void {fn}(const double* __restrict__ rs, const int rstride,")
+            w("    const double* __restrict__ eb, const double* __restrict__ ek, const double lambda, Sink& sink)")
+            w("{")
+            for k, nm in enumerate(ebn):
+                w(f"    const double {nm} = eb[{k}];")
+            for k, nm in enumerate(ekn):
+                w(f"    const double {nm} = ek[{k}];")
+            w("#define RR(i) rs[(i) * rstride]")
+            ket_blocks(LA, LB, LC, LD, cds, w)
+            w("#undef RR")
+            w("}")
+    w("template <class Sink>")
+    w(f"__device__ __forceinline__ void prim_quartet_{idx}(const PrimPairData& ab, const PrimPairData& cd,")
+    w("    const double* __restrict__ bt, double* __restrict__ rs, const int rstride, Sink& sink)")
+    w("{")
+    w("    (void)rs; (void)rstride;")
+    r_prologue(L, rsm, w)
+    for s_ in e_tables(LA, LB, LC, LD):
+        w("    " + s_)
+    if chunked:
+        w(f"    double eb[{len(ebn)}], ek[{len(ekn)}];")
+        for k, nm in enumerate(ebn):
+            w(f"    eb[{k}] = {nm};")
+        for k, nm in enumerate(ekn):
+            w(f"    ek[{k}] = {nm};")
+        for fn in chunk_names:
+            w(f"    {fn}(rs, rstride, eb, ek, lambda, sink);")
+    else:
+        ket_blocks(LA, LB, LC, LD, all_cds, w)
+    w("#undef RR")
+    w("}")
+    return o
+
+
+def main(outdir):
+    os.makedirs(outdir, exist_ok=True)
+    for k, (la, lb, lc, ld) in enumerate(classes()):
+        body = gen_class(la, lb, lc, ld, k)
+        text = ("// generated by gen_md.py -- do not edit\n#pragma once\n#include \"../md_core.cuh\"\n"
+                "namespace qcg {\nnamespace gen {\n" + "\n".join(body) + "\n}  // namespace gen\n}  // namespace qcg\n")
+        path = os.path.join(outdir, f"md_class_{k}.cuh")
+        old = open(path).read() if os.path.exists(path) else None
+        if old != text:
+            with open(path, "w") as f:
+                f.write(text)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(os.path.dirname(os.path.abspath(__file__)), "gen"))

@@ -1,0 +1,61 @@
+// qcg_internal.h -- device-side views and kernel launchers shared by the CUDA translation units.
+// Not part of the public ABI (include/qchem_b200.h is).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace qcg {
+
+// pair classes (la >= lb): 0 ss, 1 ps, 2 pp, 3 ds, 4 dp, 5 dd
+constexpr int kNumPairClasses = 6;
+constexpr int kNumQuartetClasses = 21;   // (X,Y), X >= Y, index X(X+1)/2 + Y
+constexpr int kPairLA[6] = {0, 1, 1, 2, 2, 2};
+constexpr int kPairLB[6] = {0, 0, 1, 0, 1, 2};
+
+// shells as structure of arrays; coef has the (L,0,0) primitive norm and the radial normalisation folded in
+struct BasisDev
+{
+    int nshell;
+    const int* L;
+    const int* nprim;
+    const int* prim0;
+    const double* cen;     // 3 per shell
+    const double* alpha;   // per primitive
+    const double* coef;    // per primitive
+};
+
+// primitive-pair table (all pair classes share one table)
+struct PrimPairsDev
+{
+    const double *p, *Px, *Py, *Pz, *PAx, *PAy, *PAz, *PBx, *PBy, *PBz, *K;
+};
+
+// shell pairs of one pair class, sorted by Schwarz bound descending
+struct PairListDev
+{
+    int n;
+    const int* sa;
+    const int* sb;
+    const int* ppo;
+    const int* npp;
+};
+
+// flattened canonical quartets of one quartet class: bra pair i owns quartets offs[i] .. offs[i+1)
+struct JKWorkDev
+{
+    long long total;
+    const long long* offs;
+    int same_class;
+};
+
+// launchers, one object file per quartet class (eri_class.cu compiled with -DQCG_CLASS=k)
+using EriBatchLauncher = void (*)(const BasisDev&, const int4*, long long, double*, const double*, cudaStream_t, int);
+using JKLauncher = void (*)(const JKWorkDev&, const PairListDev&, const PairListDev&, const PrimPairsDev&, const int*,
+                            const double*, double*, double*, int, const double*, cudaStream_t, int);
+using SchwarzLauncher = void (*)(const PairListDev&, const PrimPairsDev&, double*, const double*, cudaStream_t);
+
+extern const EriBatchLauncher kEriBatchLaunchers[kNumQuartetClasses];
+extern const JKLauncher kJKLaunchers[kNumQuartetClasses];
+extern const SchwarzLauncher kSchwarzLaunchers[kNumPairClasses];
+
+}   // namespace qcg

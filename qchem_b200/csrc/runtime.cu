@@ -1,0 +1,1140 @@
+// runtime.cu -- the C ABI (include/qchem_b200.h): handle, basis upload, pair lists and Schwarz screening,
+// the direct J/K build, Cartesian ERI batches, one-electron integrals and the RHF driver.
+//
+// Host-side work here is setup (once per geometry) and the SCF linear algebra; every integral and the
+// whole J/K build run in the CUDA kernels.  There is no CPU fallback: without a usable device every
+// entry point returns QCG_ERR_CUDA.
+#include <algorithm>
+#include <array>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <deque>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/qchem_b200.h"
+#include "md_core.cuh"
+#include "qcg_internal.h"
+#include "boys_table.h"
+
+namespace qcg {
+void launch_validate(const double* D, int n, double tol, int* flag, cudaStream_t st, int nsm);
+void launch_symmetrize(const double* Jp, const double* Kp, double* J, double* K, int n, int* flag, cudaStream_t st,
+                       int nsm);
+void launch_one_electron(const BasisDev& bs, const int* f0, int n, int natom, const double* Z, const double* R,
+                         double* S, double* T, double* V, const double* boys, cudaStream_t st, int nsm);
+void launch_dfma_peak(double* out, int blocks, int threads, int iters, cudaStream_t st);
+}   // namespace qcg
+
+using namespace qcg;
+
+namespace {
+
+struct Error
+{
+    int code;
+    std::string msg;
+};
+
+#define CK(call)                                                                                                  \
+    do {                                                                                                          \
+        cudaError_t e_ = (call);                                                                                  \
+        if (e_ != cudaSuccess) throw Error{QCG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)};   \
+    } while (0)
+
+constexpr int kMaxL = 2;
+const double kPi = 3.14159265358979323846;
+
+int pair_class(int la, int lb)   // la >= lb
+{
+    return la * (la + 1) / 2 + lb;
+}
+
+// algorithmic FLOPs per primitive quartet (fixed per-class formula):
+// (20+3L) + 2 sum_{j<=L} H(j) + 2 H(Lab) S(cd) + 2 nc nd S(ab) + 2 na nb nc nd
+double class_flops(int la, int lb, int lc, int ld)
+{
+    auto H = [](int n) { return (n + 1) * (n + 2) * (n + 3) / 6; };
+    auto comps = [](int L) {
+        std::vector<std::array<int, 3>> c;
+        for (int m = 0; m <= L; ++m)
+            for (int l = 0; l <= L - m; ++l) c.push_back({L - m - l, l, m});
+        return c;
+    };
+    auto S = [&](int l1, int l2) {
+        long t = 0;
+        for (auto a : comps(l1))
+            for (auto b : comps(l2)) t += (long)(a[0] + b[0] + 1) * (a[1] + b[1] + 1) * (a[2] + b[2] + 1);
+        return (double)t;
+    };
+    const int L = la + lb + lc + ld;
+    double f = 20 + 3 * L;
+    for (int j = 0; j <= L; ++j) f += 2 * H(j);
+    f += 2.0 * H(la + lb) * S(lc, ld) + 2.0 * ncart(lc) * ncart(ld) * S(la, lb) +
+         2.0 * ncart(la) * ncart(lb) * ncart(lc) * ncart(ld);
+    return f;
+}
+
+struct DevBuf
+{
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+}   // namespace
+
+struct qcg_handle
+{
+    int device = 0;
+    int nsm = 148;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    std::string last_error;
+    long long mem_limit = 0, mem_used = 0;
+    std::vector<DevBuf> allocs;
+
+    // basis (host)
+    int nshell = 0, nbf = 0;
+    std::vector<int> L, nprim, prim0, f0;
+    std::vector<double> cen, alpha, coef, ns;
+
+    // basis (device)
+    BasisDev bs{};
+    double* d_boys = nullptr;
+    int* d_f0 = nullptr;
+
+    // pair lists and screening
+    bool screened = false;
+    double thresh = 0;
+    std::vector<int> pl_sa[kNumPairClasses], pl_sb[kNumPairClasses], pl_ppo[kNumPairClasses], pl_npp[kNumPairClasses];
+    std::vector<double> pl_Q[kNumPairClasses];
+    PairListDev pl_dev[kNumPairClasses]{};
+    PrimPairsDev pp_dev{};
+    JKWorkDev work[kNumQuartetClasses]{};
+    long long work_quartets = 0, work_prim_quartets = 0;
+    double work_flops = 0;
+    std::vector<double> Qfull;
+
+    // J/K buffers
+    double *d_D = nullptr, *d_Jp = nullptr, *d_Kp = nullptr, *d_J = nullptr, *d_K = nullptr;
+    int* d_flag = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
+
+    template <class T>
+    T* alloc(size_t count)
+    {
+        const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+        if (mem_limit > 0 && mem_used + (long long)bytes > mem_limit)
+            throw Error{QCG_ERR_ALLOC, "device memory limit of " + std::to_string(mem_limit) + " bytes exceeded"};
+        void* p = nullptr;
+        cudaError_t e = cudaMalloc(&p, bytes);
+        if (e != cudaSuccess) throw Error{QCG_ERR_ALLOC, std::string("cudaMalloc: ") + cudaGetErrorString(e)};
+        allocs.push_back({p, bytes});
+        mem_used += bytes;
+        return (T*)p;
+    }
+    void release(void* p)
+    {
+        for (size_t i = 0; i < allocs.size(); ++i)
+            if (allocs[i].p == p)
+            {
+                cudaFree(p);
+                mem_used -= allocs[i].bytes;
+                allocs.erase(allocs.begin() + i);
+                return;
+            }
+    }
+    template <class T>
+    T* upload(const std::vector<T>& v)
+    {
+        T* d = alloc<T>(v.size());
+        if (!v.empty()) CK(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, stream));
+        return d;
+    }
+    ~qcg_handle()
+    {
+        for (auto& a : allocs) cudaFree(a.p);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (ev2) cudaEventDestroy(ev2);
+        if (own_stream) cudaStreamDestroy(own_stream);
+    }
+};
+
+namespace {
+
+template <class F>
+int guarded(qcg_handle* h, F&& f)
+{
+    try
+    {
+        f();
+        if (h) h->last_error.clear();
+        return QCG_OK;
+    }
+    catch (const Error& e)
+    {
+        if (h) h->last_error = e.msg;
+        return e.code;
+    }
+    catch (const std::exception& e)
+    {
+        if (h) h->last_error = e.what();
+        return QCG_ERR_ARG;
+    }
+}
+
+void require(bool ok, const std::string& msg, int code = QCG_ERR_ARG)
+{
+    if (!ok) throw Error{code, msg};
+}
+
+double dfact(int i)
+{
+    double r = 1;
+    for (int k = i; k > 1; k -= 2) r *= k;
+    return r;
+}
+
+// GetNormalization(Polarization(L,0,0)) of one primitive (PG_Cart_MnD/Imp/GaussianRF.C:512-521)
+double prim_norm(double a, int L)
+{
+    const double s = std::pow(kPi / (2 * a), 1.5);
+    return std::sqrt(std::pow(4 * a, L) / (s * dfact(2 * L - 1)));
+}
+
+// ------------------------------------------------------------------------------------------------
+// Symmetric eigensolver, A = V diag(w) V^T with ascending w (row-major n x n):
+//   1. Householder reduction to tridiagonal T = Q^T A Q, one reflector per column,
+//   2. implicit symmetric QR steps with a Wilkinson shift on T (bulge chasing with Givens rotations),
+//      rotations accumulated into V = Q G_1^T G_2^T ...
+// ------------------------------------------------------------------------------------------------
+void syev(int n, const double* Ain, double* w, double* V)
+{
+    std::vector<double> T(Ain, Ain + (size_t)n * n), Q((size_t)n * n, 0.0), v(n), pv(n), wv(n);
+    auto t = [&](int i, int j) -> double& { return T[(size_t)i * n + j]; };
+    auto q = [&](int i, int j) -> double& { return Q[(size_t)i * n + j]; };
+    for (int i = 0; i < n; ++i) q(i, i) = 1.0;
+    for (int k = 0; k + 2 < n; ++k)
+    {
+        // reflector H = I - beta v v^T mapping x = T[k+1:, k] onto alpha e_1
+        double xn = 0.0;
+        for (int i = k + 1; i < n; ++i) xn += t(i, k) * t(i, k);
+        xn = std::sqrt(xn);
+        if (xn == 0.0) continue;
+        const double alpha = t(k + 1, k) > 0 ? -xn : xn;
+        for (int i = k + 1; i < n; ++i) v[i] = t(i, k);
+        v[k + 1] -= alpha;
+        double vv = 0.0;
+        for (int i = k + 1; i < n; ++i) vv += v[i] * v[i];
+        if (vv == 0.0) continue;
+        const double beta = 2.0 / vv;
+        // trailing block update: A <- A - v w^T - w v^T with p = beta A v, w = p - (beta p.v / 2) v
+        double pdv = 0.0;
+        for (int i = k + 1; i < n; ++i)
+        {
+            double s = 0.0;
+            for (int j = k + 1; j < n; ++j) s += t(i, j) * v[j];
+            pv[i] = beta * s;
+            pdv += pv[i] * v[i];
+        }
+        for (int i = k + 1; i < n; ++i) wv[i] = pv[i] - 0.5 * beta * pdv * v[i];
+        for (int i = k + 1; i < n; ++i)
+            for (int j = k + 1; j < n; ++j) t(i, j) -= v[i] * wv[j] + wv[i] * v[j];
+        t(k + 1, k) = t(k, k + 1) = alpha;
+        for (int i = k + 2; i < n; ++i) t(i, k) = t(k, i) = 0.0;
+        // Q <- Q H
+        for (int r = 0; r < n; ++r)
+        {
+            double s = 0.0;
+            for (int j = k + 1; j < n; ++j) s += q(r, j) * v[j];
+            s *= beta;
+            for (int j = k + 1; j < n; ++j) q(r, j) -= s * v[j];
+        }
+    }
+    // rotation G on (k,k+1): T <- G T G^T, Q <- Q G^T, G = [[c, s], [-s, c]]
+    auto rotate = [&](int k, double c, double s, int lo, int hi) {
+        for (int j = lo; j <= hi; ++j)
+        {
+            const double a = t(k, j), b = t(k + 1, j);
+            t(k, j) = c * a + s * b;
+            t(k + 1, j) = -s * a + c * b;
+        }
+        for (int i = lo; i <= hi; ++i)
+        {
+            const double a = t(i, k), b = t(i, k + 1);
+            t(i, k) = c * a + s * b;
+            t(i, k + 1) = -s * a + c * b;
+        }
+        for (int r = 0; r < n; ++r)
+        {
+            const double a = q(r, k), b = q(r, k + 1);
+            q(r, k) = c * a + s * b;
+            q(r, k + 1) = -s * a + c * b;
+        }
+    };
+    const double eps = 1e-15;
+    int m = n - 1, steps = 0;
+    while (m > 0)
+    {
+        if (std::fabs(t(m, m - 1)) <= eps * (std::fabs(t(m, m)) + std::fabs(t(m - 1, m - 1))))
+        {
+            t(m, m - 1) = t(m - 1, m) = 0.0;
+            --m;
+            continue;
+        }
+        int l = m - 1;
+        while (l > 0 && std::fabs(t(l, l - 1)) > eps * (std::fabs(t(l, l)) + std::fabs(t(l - 1, l - 1)))) --l;
+        if (++steps > 60 * n) throw Error{QCG_ERR_NOCONV, "eigensolver did not converge"};
+        // Wilkinson shift from the trailing 2x2 of the block
+        const double a = t(m - 1, m - 1), b = t(m, m - 1), c2 = t(m, m);
+        const double delta = 0.5 * (a - c2);
+        const double mu = delta == 0.0 ? c2 - std::fabs(b)
+                                       : c2 - b * b / (delta + (delta > 0 ? 1.0 : -1.0) * std::hypot(delta, b));
+        double x = t(l, l) - mu, z = t(l + 1, l);
+        for (int k = l; k < m; ++k)
+        {
+            const double r = std::hypot(x, z);
+            const double c = r == 0.0 ? 1.0 : x / r, s = r == 0.0 ? 0.0 : z / r;
+            rotate(k, c, s, std::max(l, k - 1), std::min(m, k + 2));
+            if (k + 1 < m)
+            {
+                x = t(k + 1, k);
+                z = t(k + 2, k);
+            }
+        }
+    }
+    std::vector<int> idx(n);
+    std::iota(idx.begin(), idx.end(), 0);
+    std::sort(idx.begin(), idx.end(), [&](int x, int y) { return t(x, x) < t(y, y); });
+    for (int j = 0; j < n; ++j)
+    {
+        w[j] = t(idx[j], idx[j]);
+        for (int r = 0; r < n; ++r) V[(size_t)r * n + j] = q(r, idx[j]);
+    }
+}
+
+// C = op(A) op(B), n x n, row-major
+void gemm(int n, const double* A, bool ta, const double* B, bool tb, double* C)
+{
+    std::vector<double> At, Bt;
+    const double* a = A;
+    const double* b = B;
+    if (ta)
+    {
+        At.resize((size_t)n * n);
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j) At[(size_t)i * n + j] = A[(size_t)j * n + i];
+        a = At.data();
+    }
+    if (!tb)
+    {
+        Bt.resize((size_t)n * n);
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j) Bt[(size_t)i * n + j] = B[(size_t)j * n + i];
+        b = Bt.data();
+    }
+    // C_ij = sum_k a_ik bT_jk
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j)
+        {
+            const double* ai = a + (size_t)i * n;
+            const double* bj = b + (size_t)j * n;
+            double s = 0.0;
+            for (int k = 0; k < n; ++k) s += ai[k] * bj[k];
+            C[(size_t)i * n + j] = s;
+        }
+}
+
+std::vector<double> solve_dense(int n, std::vector<double> A, std::vector<double> b)
+{
+    for (int c = 0; c < n; ++c)
+    {
+        int piv = c;
+        for (int r = c + 1; r < n; ++r)
+            if (std::fabs(A[r * n + c]) > std::fabs(A[piv * n + c])) piv = r;
+        if (piv != c)
+        {
+            for (int k = 0; k < n; ++k) std::swap(A[c * n + k], A[piv * n + k]);
+            std::swap(b[c], b[piv]);
+        }
+        if (A[c * n + c] == 0.0) throw Error{QCG_ERR_NOCONV, "singular DIIS system"};
+        for (int r = c + 1; r < n; ++r)
+        {
+            const double f = A[r * n + c] / A[c * n + c];
+            for (int k = c; k < n; ++k) A[r * n + k] -= f * A[c * n + k];
+            b[r] -= f * b[c];
+        }
+    }
+    std::vector<double> x(n);
+    for (int r = n - 1; r >= 0; --r)
+    {
+        double s = b[r];
+        for (int k = r + 1; k < n; ++k) s -= A[r * n + k] * x[k];
+        x[r] = s / A[r * n + r];
+    }
+    return x;
+}
+
+void ensure_jk_buffers(qcg_handle* h)
+{
+    if (h->d_Jp) return;
+    const size_t nn = (size_t)h->nbf * h->nbf;
+    h->d_D = h->alloc<double>(nn);
+    h->d_Jp = h->alloc<double>(nn);
+    h->d_Kp = h->alloc<double>(nn);
+    h->d_J = h->alloc<double>(nn);
+    h->d_K = h->alloc<double>(nn);
+    h->d_flag = h->alloc<int>(1);
+}
+
+// ------------------------------------------------------------------------------------------------
+// pair lists, Schwarz bounds and screened work lists
+// ------------------------------------------------------------------------------------------------
+void build_screening(qcg_handle* h, double thresh)
+{
+    // shell pairs per class, (a,b) with L_a > L_b, or L_a == L_b and a >= b
+    std::vector<int> sa[kNumPairClasses], sb[kNumPairClasses];
+    for (int a = 0; a < h->nshell; ++a)
+        for (int b = 0; b <= a; ++b)
+        {
+            int x = a, y = b;
+            if (h->L[y] > h->L[x]) std::swap(x, y);
+            const int pc = pair_class(h->L[x], h->L[y]);
+            sa[pc].push_back(x);
+            sb[pc].push_back(y);
+        }
+    // primitive pairs in class order (unsorted), then Schwarz
+    struct PP
+    {
+        double p, Px, Py, Pz, PAx, PAy, PAz, PBx, PBy, PBz, K;
+    };
+    auto make_pp = [&](int a, int i, int b, int j) {
+        const int pa = h->prim0[a] + i, pb = h->prim0[b] + j;
+        const double al = h->alpha[pa], be = h->alpha[pb];
+        const double* A = &h->cen[3 * a];
+        const double* B = &h->cen[3 * b];
+        PP d;
+        d.p = al + be;
+        const double ip = 1.0 / d.p;
+        d.Px = (al * A[0] + be * B[0]) * ip;
+        d.Py = (al * A[1] + be * B[1]) * ip;
+        d.Pz = (al * A[2] + be * B[2]) * ip;
+        d.PAx = d.Px - A[0]; d.PAy = d.Py - A[1]; d.PAz = d.Pz - A[2];
+        d.PBx = d.Px - B[0]; d.PBy = d.Py - B[1]; d.PBz = d.Pz - B[2];
+        const double r2 = (A[0] - B[0]) * (A[0] - B[0]) + (A[1] - B[1]) * (A[1] - B[1]) + (A[2] - B[2]) * (A[2] - B[2]);
+        d.K = h->coef[pa] * h->coef[pb] * std::exp(-al * be * ip * r2);
+        return d;
+    };
+    auto build_pp = [&](const std::vector<int>* A_, const std::vector<int>* B_, std::vector<PP>& pp,
+                        std::vector<int>* ppo, std::vector<int>* npp) {
+        pp.clear();
+        for (int c = 0; c < kNumPairClasses; ++c)
+        {
+            ppo[c].resize(A_[c].size());
+            npp[c].resize(A_[c].size());
+            for (size_t k = 0; k < A_[c].size(); ++k)
+            {
+                const int a = A_[c][k], b = B_[c][k];
+                ppo[c][k] = (int)pp.size();
+                npp[c][k] = h->nprim[a] * h->nprim[b];
+                for (int i = 0; i < h->nprim[a]; ++i)
+                    for (int j = 0; j < h->nprim[b]; ++j) pp.push_back(make_pp(a, i, b, j));
+            }
+        }
+    };
+    auto upload_pp = [&](const std::vector<PP>& pp) {
+        std::vector<double> f[11];
+        for (auto& x : pp)
+        {
+            const double v[11] = {x.p, x.Px, x.Py, x.Pz, x.PAx, x.PAy, x.PAz, x.PBx, x.PBy, x.PBz, x.K};
+            for (int k = 0; k < 11; ++k) f[k].push_back(v[k]);
+        }
+        double* d[11];
+        for (int k = 0; k < 11; ++k) d[k] = h->upload(f[k]);
+        PrimPairsDev P{d[0], d[1], d[2], d[3], d[4], d[5], d[6], d[7], d[8], d[9], d[10]};
+        return P;
+    };
+    std::vector<PP> pp;
+    std::vector<int> ppo[kNumPairClasses], npp[kNumPairClasses];
+    build_pp(sa, sb, pp, ppo, npp);
+    PrimPairsDev P0 = upload_pp(pp);
+    std::vector<double> Qc[kNumPairClasses];
+    std::vector<void*> tmp;
+    for (int c = 0; c < kNumPairClasses; ++c)
+    {
+        const int n = (int)sa[c].size();
+        Qc[c].assign(n, 0.0);
+        if (n == 0) continue;
+        int* dsa = h->upload(sa[c]);
+        int* dsb = h->upload(sb[c]);
+        int* dppo = h->upload(ppo[c]);
+        int* dnpp = h->upload(npp[c]);
+        double* dQ = h->alloc<double>(n);
+        PairListDev pl{n, dsa, dsb, dppo, dnpp};
+        kSchwarzLaunchers[c](pl, P0, dQ, h->d_boys, h->stream);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(Qc[c].data(), dQ, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        tmp.insert(tmp.end(), {dsa, dsb, dppo, dnpp, dQ});
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    for (void* p : tmp) h->release(p);
+    for (const double* p : {P0.p, P0.Px, P0.Py, P0.Pz, P0.PAx, P0.PAy, P0.PAz, P0.PBx, P0.PBy, P0.PBz, P0.K})
+        h->release((void*)p);
+    // full Q matrix for callers
+    h->Qfull.assign((size_t)h->nshell * h->nshell, 0.0);
+    for (int c = 0; c < kNumPairClasses; ++c)
+        for (size_t k = 0; k < sa[c].size(); ++k)
+        {
+            if (!std::isfinite(Qc[c][k])) throw Error{QCG_ERR_NONFINITE, "non-finite Schwarz bound"};
+            h->Qfull[(size_t)sa[c][k] * h->nshell + sb[c][k]] = Qc[c][k];
+            h->Qfull[(size_t)sb[c][k] * h->nshell + sa[c][k]] = Qc[c][k];
+        }
+    // sort each class by Q descending, rebuild primitive pairs in that order
+    for (int c = 0; c < kNumPairClasses; ++c)
+    {
+        const size_t n = sa[c].size();
+        std::vector<size_t> ord(n);
+        std::iota(ord.begin(), ord.end(), 0);
+        std::stable_sort(ord.begin(), ord.end(), [&](size_t x, size_t y) { return Qc[c][x] > Qc[c][y]; });
+        h->pl_sa[c].resize(n);
+        h->pl_sb[c].resize(n);
+        h->pl_Q[c].resize(n);
+        for (size_t k = 0; k < n; ++k)
+        {
+            h->pl_sa[c][k] = sa[c][ord[k]];
+            h->pl_sb[c][k] = sb[c][ord[k]];
+            h->pl_Q[c][k] = Qc[c][ord[k]];
+        }
+    }
+    build_pp(h->pl_sa, h->pl_sb, pp, h->pl_ppo, h->pl_npp);
+    h->pp_dev = upload_pp(pp);
+    for (int c = 0; c < kNumPairClasses; ++c)
+    {
+        const int n = (int)h->pl_sa[c].size();
+        h->pl_dev[c] = PairListDev{n, h->upload(h->pl_sa[c]), h->upload(h->pl_sb[c]), h->upload(h->pl_ppo[c]),
+                                   h->upload(h->pl_npp[c])};
+    }
+    // work lists: bra pair i of class X against the prefix of class Y with Q_i Q_j >= thresh
+    h->work_quartets = 0;
+    h->work_prim_quartets = 0;
+    h->work_flops = 0;
+    for (int X = 0; X < kNumPairClasses; ++X)
+        for (int Y = 0; Y <= X; ++Y)
+        {
+            const int k = X * (X + 1) / 2 + Y;
+            const auto& qx = h->pl_Q[X];
+            const auto& qy = h->pl_Q[Y];
+            std::vector<long long> offs(qx.size() + 1, 0);
+            // prefix sums of ket primitive-pair counts for the primitive-quartet tally
+            std::vector<long long> nppy(qy.size() + 1, 0);
+            for (size_t j = 0; j < qy.size(); ++j) nppy[j + 1] = nppy[j] + h->pl_npp[Y][j];
+            long long pq = 0;
+            for (size_t i = 0; i < qx.size(); ++i)
+            {
+                long long cnt = 0;
+                if (qx[i] > 0)
+                {
+                    const double need = thresh / qx[i];
+                    // qy descending: count of entries >= need
+                    cnt = std::upper_bound(qy.begin(), qy.end(), need, [](double v, double e) { return v > e; }) -
+                          qy.begin();
+                    // entries exactly equal to need pass too (upper_bound with > keeps ties in front)
+                }
+                if (X == Y) cnt = std::min<long long>(cnt, (long long)i + 1);
+                offs[i + 1] = offs[i] + cnt;
+                pq += (long long)h->pl_npp[X][i] * nppy[cnt];
+            }
+            h->work[k].total = offs.back();
+            h->work[k].offs = h->upload(offs);
+            h->work[k].same_class = (X == Y);
+            h->work_quartets += offs.back();
+            h->work_prim_quartets += pq;
+            h->work_flops += (double)pq * class_flops(kPairLA[X], kPairLB[X], kPairLA[Y], kPairLB[Y]);
+        }
+    CK(cudaStreamSynchronize(h->stream));
+    h->thresh = thresh;
+    h->screened = true;
+}
+
+void jk_device(qcg_handle* h, const double* dD, double* dJ, double* dK, int flags, qcg_stats* stats)
+{
+    require(h->screened, "qcg_schwarz must be called before qcg_fock_jk", QCG_ERR_STATE);
+    ensure_jk_buffers(h);
+    const int n = h->nbf;
+    const size_t nn = (size_t)n * n;
+    if (!h->ev0)
+    {
+        CK(cudaEventCreate(&h->ev0));
+        CK(cudaEventCreate(&h->ev1));
+        CK(cudaEventCreate(&h->ev2));
+    }
+    CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
+    if (!(flags & QCG_JK_SKIP_VALIDATION))
+    {
+        launch_validate(dD, n, 1e-10, h->d_flag, h->stream, h->nsm);
+        int flag = 0;
+        CK(cudaMemcpyAsync(&flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        if (flag & 1) throw Error{QCG_ERR_NONFINITE, "density matrix has NaN/Inf entries"};
+        if (flag & 2) throw Error{QCG_ERR_ASYMMETRIC, "density matrix is not symmetric"};
+    }
+    CK(cudaEventRecord(h->ev0, h->stream));
+    CK(cudaMemsetAsync(h->d_Jp, 0, nn * sizeof(double), h->stream));
+    CK(cudaMemsetAsync(h->d_Kp, 0, nn * sizeof(double), h->stream));
+    CK(cudaEventRecord(h->ev1, h->stream));
+    // heaviest classes first so that the short ones fill the tail
+    for (int k = kNumQuartetClasses - 1; k >= 0; --k)
+    {
+        int X = 0;
+        while ((X + 1) * (X + 2) / 2 <= k) ++X;
+        const int Y = k - X * (X + 1) / 2;
+        kJKLaunchers[k](h->work[k], h->pl_dev[X], h->pl_dev[Y], h->pp_dev, h->d_f0, dD, h->d_Jp, h->d_Kp, n, h->d_boys,
+                        h->stream, h->nsm);
+    }
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(h->ev2, h->stream));
+    launch_symmetrize(h->d_Jp, h->d_Kp, dJ, dK, n, h->d_flag, h->stream, h->nsm);
+    CK(cudaGetLastError());
+    if (stats)
+    {
+        CK(cudaEventSynchronize(h->ev2));
+        float a = 0, b = 0;
+        CK(cudaEventElapsedTime(&a, h->ev0, h->ev2));
+        CK(cudaEventElapsedTime(&b, h->ev1, h->ev2));
+        stats->ms_total = a;
+        stats->ms_eri = b;
+        stats->quartets = h->work_quartets;
+        stats->prim_quartets = h->work_prim_quartets;
+        stats->flops = h->work_flops;
+    }
+}
+
+int class_index(int la, int lb, int lc, int ld)
+{
+    if (la < lb || lc < ld || la > kMaxL || lc > kMaxL || lb < 0 || ld < 0) return -1;
+    const int X = pair_class(la, lb), Y = pair_class(lc, ld);
+    if (X < Y) return -1;
+    return X * (X + 1) / 2 + Y;
+}
+
+}   // namespace
+
+// =================================================================================================
+// C ABI
+// =================================================================================================
+extern "C" {
+
+int qcg_basis_create(const int* shell_L, const int* shell_nprim, const double* exps, const double* coefs,
+                     const double* centres, int nshell, qcg_handle** out)
+{
+    if (!out) return QCG_ERR_ARG;
+    *out = nullptr;
+    qcg_handle* h = new qcg_handle;
+    int rc = guarded(h, [&] {
+        require(shell_L && shell_nprim && exps && coefs && centres, "null argument");
+        require(nshell > 0, "nshell must be positive");
+        h->nshell = nshell;
+        int np = 0;
+        for (int s = 0; s < nshell; ++s)
+        {
+            require(shell_L[s] >= 0 && shell_L[s] <= kMaxL, "shell L must be 0, 1 or 2");
+            require(shell_nprim[s] >= 1, "shell_nprim must be >= 1");
+            for (int x = 0; x < 3; ++x) require(std::isfinite(centres[3 * s + x]), "non-finite centre", QCG_ERR_NONFINITE);
+            h->L.push_back(shell_L[s]);
+            h->nprim.push_back(shell_nprim[s]);
+            h->prim0.push_back(np);
+            h->f0.push_back(h->nbf);
+            h->nbf += ncart(shell_L[s]);
+            for (int i = 0; i < shell_nprim[s]; ++i)
+            {
+                const double a = exps[np + i], c = coefs[np + i];
+                require(std::isfinite(a) && a > 0, "exponents must be finite and positive");
+                require(std::isfinite(c), "non-finite contraction coefficient", QCG_ERR_NONFINITE);
+                h->alpha.push_back(a);
+                h->coef.push_back(c * prim_norm(a, shell_L[s]));
+            }
+            np += shell_nprim[s];
+            for (int x = 0; x < 3; ++x) h->cen.push_back(centres[3 * s + x]);
+        }
+        // radial normalisation: unit self-overlap of the (L,0,...) component up to the component factor
+        // prod (2n_x-1)!!, which the kernels apply per component (PGData.C:17-33)
+        for (int s = 0; s < nshell; ++s)
+        {
+            double ss = 0.0;
+            const int Ls = h->L[s];
+            for (int i = 0; i < h->nprim[s]; ++i)
+                for (int j = 0; j < h->nprim[s]; ++j)
+                {
+                    const double p = h->alpha[h->prim0[s] + i] + h->alpha[h->prim0[s] + j];
+                    ss += h->coef[h->prim0[s] + i] * h->coef[h->prim0[s] + j] * std::pow(kPi / p, 1.5) / std::pow(2 * p, Ls);
+                }
+            require(ss > 0, "shell with zero self-overlap");
+            const double nrad = 1.0 / std::sqrt(ss);
+            for (int i = 0; i < h->nprim[s]; ++i) h->coef[h->prim0[s] + i] *= nrad;
+            for (int k = 0; k < ncart(Ls); ++k)
+                h->ns.push_back(nrad * comp_norm(Ls, k));
+        }
+        CK(cudaGetDevice(&h->device));
+        cudaDeviceProp prop;
+        CK(cudaGetDeviceProperties(&prop, h->device));
+        h->nsm = prop.multiProcessorCount;
+        CK(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
+        h->stream = h->own_stream;
+        h->d_boys = h->alloc<double>(121 * 23);
+        CK(cudaMemcpyAsync(h->d_boys, kBoysTable, sizeof(kBoysTable), cudaMemcpyHostToDevice, h->stream));
+        h->bs.nshell = nshell;
+        h->bs.L = h->upload(h->L);
+        h->bs.nprim = h->upload(h->nprim);
+        h->bs.prim0 = h->upload(h->prim0);
+        h->bs.cen = h->upload(h->cen);
+        h->bs.alpha = h->upload(h->alpha);
+        h->bs.coef = h->upload(h->coef);
+        h->d_f0 = h->upload(h->f0);
+        CK(cudaStreamSynchronize(h->stream));
+    });
+    if (rc != QCG_OK)
+    {
+        // keep the handle so that the caller can read the message, then it must be destroyed
+        *out = h;
+        return rc;
+    }
+    *out = h;
+    return QCG_OK;
+}
+
+void qcg_destroy(qcg_handle* h) { delete h; }
+
+const char* qcg_last_error(const qcg_handle* h) { return h ? h->last_error.c_str() : "null handle"; }
+
+int qcg_set_stream(qcg_handle* h, void* s)
+{
+    if (!h) return QCG_ERR_ARG;
+    h->stream = s ? (cudaStream_t)s : h->own_stream;
+    return QCG_OK;
+}
+
+int qcg_set_memory_limit(qcg_handle* h, long long bytes)
+{
+    if (!h || bytes < 0) return QCG_ERR_ARG;
+    h->mem_limit = bytes;
+    return QCG_OK;
+}
+
+int qcg_nbf(const qcg_handle* h, int* n)
+{
+    if (!h || !n) return QCG_ERR_ARG;
+    *n = h->nbf;
+    return QCG_OK;
+}
+
+int qcg_nshell(const qcg_handle* h, int* n)
+{
+    if (!h || !n) return QCG_ERR_ARG;
+    *n = h->nshell;
+    return QCG_OK;
+}
+
+int qcg_norms(const qcg_handle* h, double* ns)
+{
+    if (!h || !ns) return QCG_ERR_ARG;
+    std::copy(h->ns.begin(), h->ns.end(), ns);
+    return QCG_OK;
+}
+
+int qcg_eri_batch_device(qcg_handle* h, int la, int lb, int lc, int ld, long long nq, const int* d_quartets,
+                         double* d_out)
+{
+    if (!h) return QCG_ERR_ARG;
+    return guarded(h, [&] {
+        const int k = class_index(la, lb, lc, ld);
+        require(k >= 0, "non-canonical or unsupported angular class");
+        require(nq >= 0, "negative quartet count");
+        if (nq == 0) return;
+        require(d_quartets && d_out, "null argument");
+        kEriBatchLaunchers[k](h->bs, (const int4*)d_quartets, nq, d_out, h->d_boys, h->stream, h->nsm);
+        CK(cudaGetLastError());
+    });
+}
+
+int qcg_eri_batch(qcg_handle* h, int la, int lb, int lc, int ld, long long nq, const int* quartets, double* out)
+{
+    if (!h) return QCG_ERR_ARG;
+    return guarded(h, [&] {
+        const int k = class_index(la, lb, lc, ld);
+        require(k >= 0, "non-canonical or unsupported angular class");
+        require(nq >= 0, "negative quartet count");
+        if (nq == 0) return;
+        require(quartets && out, "null argument");
+        const int Ls[4] = {la, lb, lc, ld};
+        for (long long q = 0; q < nq; ++q)
+            for (int x = 0; x < 4; ++x)
+            {
+                const int s = quartets[4 * q + x];
+                require(s >= 0 && s < h->nshell, "shell index out of range");
+                require(h->L[s] == Ls[x], "shell angular momentum does not match the class");
+            }
+        const long long blk = (long long)ncart(la) * ncart(lb) * ncart(lc) * ncart(ld);
+        // bounded device footprint: chunks of at most 2^27 output doubles (1 GiB)
+        const long long chunk = std::max<long long>(1, std::min<long long>(nq, (1LL << 27) / blk));
+        int* dq = h->alloc<int>(4 * chunk);
+        double* dout = h->alloc<double>(chunk * blk);
+        try
+        {
+            for (long long q0 = 0; q0 < nq; q0 += chunk)
+            {
+                const long long m = std::min(chunk, nq - q0);
+                CK(cudaMemcpyAsync(dq, quartets + 4 * q0, 4 * m * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+                kEriBatchLaunchers[k](h->bs, (const int4*)dq, m, dout, h->d_boys, h->stream, h->nsm);
+                CK(cudaGetLastError());
+                CK(cudaMemcpyAsync(out + q0 * blk, dout, m * blk * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+            }
+            CK(cudaStreamSynchronize(h->stream));
+        }
+        catch (...)
+        {
+            h->release(dq);
+            h->release(dout);
+            throw;
+        }
+        h->release(dq);
+        h->release(dout);
+    });
+}
+
+int qcg_schwarz(qcg_handle* h, double thresh, double* Q)
+{
+    if (!h) return QCG_ERR_ARG;
+    return guarded(h, [&] {
+        require(std::isfinite(thresh) && thresh >= 0, "threshold must be finite and non-negative");
+        if (!h->screened || h->thresh != thresh)
+        {
+            // drop previous screening state (device buffers of pair lists and work lists)
+            if (h->screened)
+            {
+                for (int c = 0; c < kNumPairClasses; ++c)
+                    for (const void* p : {(const void*)h->pl_dev[c].sa, (const void*)h->pl_dev[c].sb,
+                                          (const void*)h->pl_dev[c].ppo, (const void*)h->pl_dev[c].npp})
+                        h->release((void*)p);
+                const PrimPairsDev& P = h->pp_dev;
+                for (const double* p : {P.p, P.Px, P.Py, P.Pz, P.PAx, P.PAy, P.PAz, P.PBx, P.PBy, P.PBz, P.K})
+                    h->release((void*)p);
+                for (int k = 0; k < kNumQuartetClasses; ++k) h->release((void*)h->work[k].offs);
+                h->screened = false;
+            }
+            build_screening(h, thresh);
+        }
+        if (Q) std::copy(h->Qfull.begin(), h->Qfull.end(), Q);
+    });
+}
+
+int qcg_fock_jk_device(qcg_handle* h, const double* d_D, double* d_J, double* d_K, int flags, qcg_stats* stats)
+{
+    if (!h) return QCG_ERR_ARG;
+    return guarded(h, [&] {
+        require(d_D && d_J && d_K, "null argument");
+        jk_device(h, d_D, d_J, d_K, flags, stats);
+    });
+}
+
+int qcg_fock_jk(qcg_handle* h, const double* D, double* J, double* K, int flags, qcg_stats* stats)
+{
+    if (!h) return QCG_ERR_ARG;
+    return guarded(h, [&] {
+        require(D && J && K, "null argument");
+        const int n = h->nbf;
+        const size_t nn = (size_t)n * n;
+        if (!(flags & QCG_JK_SKIP_VALIDATION))
+        {
+            for (size_t k = 0; k < nn; ++k)
+                if (!std::isfinite(D[k])) throw Error{QCG_ERR_NONFINITE, "density matrix has NaN/Inf entries"};
+            for (int i = 0; i < n; ++i)
+                for (int j = i + 1; j < n; ++j)
+                {
+                    const double a = D[(size_t)i * n + j], b = D[(size_t)j * n + i];
+                    if (std::fabs(a - b) > 1e-10 * (1.0 + std::fabs(a)))
+                        throw Error{QCG_ERR_ASYMMETRIC, "density matrix is not symmetric"};
+                }
+        }
+        require(h->screened, "qcg_schwarz must be called before qcg_fock_jk", QCG_ERR_STATE);
+        ensure_jk_buffers(h);
+        CK(cudaMemcpyAsync(h->d_D, D, nn * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        jk_device(h, h->d_D, h->d_J, h->d_K, flags | QCG_JK_SKIP_VALIDATION, stats);
+        CK(cudaMemcpyAsync(J, h->d_J, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(K, h->d_K, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        int flag = 0;
+        CK(cudaMemcpyAsync(&flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        if (flag & 1) throw Error{QCG_ERR_NONFINITE, "non-finite J/K result"};
+    });
+}
+
+int qcg_one_electron(qcg_handle* h, int natom, const double* Z, const double* R, double* S, double* T, double* V)
+{
+    if (!h) return QCG_ERR_ARG;
+    return guarded(h, [&] {
+        require(natom >= 0 && (natom == 0 || (Z && R)) && S && T && V, "bad argument");
+        const int n = h->nbf;
+        const size_t nn = (size_t)n * n;
+        std::vector<double> z(Z, Z + natom), r(R, R + 3 * natom);
+        for (double x : r) require(std::isfinite(x), "non-finite nuclear position", QCG_ERR_NONFINITE);
+        double* dZ = h->upload(z);
+        double* dR = h->upload(r);
+        double* dS = h->alloc<double>(nn);
+        double* dT = h->alloc<double>(nn);
+        double* dV = h->alloc<double>(nn);
+        launch_one_electron(h->bs, h->d_f0, n, natom, dZ, dR, dS, dT, dV, h->d_boys, h->stream, h->nsm);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpyAsync(S, dS, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(T, dT, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(V, dV, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+        for (void* p : {(void*)dZ, (void*)dR, (void*)dS, (void*)dT, (void*)dV}) h->release(p);
+        if (e != cudaSuccess) throw Error{QCG_ERR_CUDA, std::string("one-electron integrals: ") + cudaGetErrorString(e)};
+    });
+}
+
+void qcg_scf_default_params(qcg_scf_params* p)
+{
+    if (!p) return;
+    p->max_iter = 100;
+    p->de_tol = 1e-10;
+    p->fd_tol = 1e-5;
+    p->schwarz_thresh = 1e-10;
+    p->diis_nproj = 4;
+    p->diis_fdmax = 0.0;
+    p->diis_svtol = 5e-9;
+}
+
+// Closed-shell SCF (SCFIterator.C:283-362 loop; DIIS gating/pruning per SCFAcceleratorDIIS.C:35-238)
+int qcg_rhf(qcg_handle* h, int natom, const double* Z, const double* R, int nelec, const qcg_scf_params* params,
+            qcg_scf_result* result, double* D_out)
+{
+    if (!h) return QCG_ERR_ARG;
+    bool converged = false;
+    int rc = guarded(h, [&] {
+        auto t0 = std::chrono::steady_clock::now();
+        qcg_scf_params prm;
+        qcg_scf_default_params(&prm);
+        if (params) prm = *params;
+        require(result != nullptr, "null result");
+        require(natom > 0 && Z && R, "bad nuclei");
+        require(nelec > 0 && nelec % 2 == 0, "closed-shell RHF needs a positive even electron count");
+        const int n = h->nbf, nocc = nelec / 2;
+        require(nocc <= n, "more occupied orbitals than basis functions");
+        const size_t nn = (size_t)n * n;
+        double Ztot = 0, Enn = 0;
+        for (int i = 0; i < natom; ++i)
+        {
+            Ztot += Z[i];
+            for (int j = 0; j < i; ++j)
+            {
+                double d2 = 0;
+                for (int x = 0; x < 3; ++x) d2 += (R[3 * i + x] - R[3 * j + x]) * (R[3 * i + x] - R[3 * j + x]);
+                Enn += Z[i] * Z[j] / std::sqrt(d2);
+            }
+        }
+        const double fdmax = prm.diis_fdmax > 0 ? prm.diis_fdmax : Ztot * Ztot * 0.1 / 32;
+        std::vector<double> S(nn), T(nn), V(nn), H(nn);
+        {
+            int e = qcg_one_electron(h, natom, Z, R, S.data(), T.data(), V.data());
+            if (e != QCG_OK) throw Error{e, h->last_error};
+        }
+        for (size_t k = 0; k < nn; ++k) H[k] = T[k] + V[k];
+        {
+            int e = qcg_schwarz(h, prm.schwarz_thresh, nullptr);
+            if (e != QCG_OK) throw Error{e, h->last_error};
+        }
+        ensure_jk_buffers(h);
+        // canonical orthogonalisation X = U s^{-1/2}
+        std::vector<double> sw(n), U(nn), X(nn);
+        syev(n, S.data(), sw.data(), U.data());
+        require(sw[0] > 0, "overlap matrix is not positive definite");
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j) X[(size_t)i * n + j] = U[(size_t)i * n + j] / std::sqrt(sw[j]);
+        std::vector<double> tmp(nn), Fp(nn), Dp(nn, 0.0), D(nn), Up(nn), w(n);
+        auto ortho = [&](const std::vector<double>& F, std::vector<double>& out) {
+            gemm(n, F.data(), false, X.data(), false, tmp.data());
+            gemm(n, X.data(), true, tmp.data(), false, out.data());
+        };
+        auto diag_fill = [&](const std::vector<double>& F) {
+            syev(n, F.data(), w.data(), Up.data());
+            for (int i = 0; i < n; ++i)
+                for (int j = 0; j < n; ++j)
+                {
+                    double s = 0;
+                    for (int k = 0; k < nocc; ++k) s += Up[(size_t)i * n + k] * Up[(size_t)j * n + k];
+                    Dp[(size_t)i * n + j] = 2 * s;
+                }
+            gemm(n, X.data(), false, Dp.data(), false, tmp.data());
+            gemm(n, tmp.data(), false, X.data(), true, D.data());
+            // exact symmetry for the validation in the J/K build
+            for (int i = 0; i < n; ++i)
+                for (int j = i + 1; j < n; ++j)
+                {
+                    const double a = 0.5 * (D[(size_t)i * n + j] + D[(size_t)j * n + i]);
+                    D[(size_t)i * n + j] = D[(size_t)j * n + i] = a;
+                }
+        };
+        ortho(H, Fp);
+        diag_fill(Fp);   // core guess
+        std::deque<std::vector<double>> Es, Fps;
+        std::vector<double> J(nn), K(nn), F(nn), Err(nn), a(nn), b(nn);
+        double E = 0, Eold = 0, En = 0, fock_ms = 0;
+        int it;
+        for (it = 1; it <= prm.max_iter; ++it)
+        {
+            qcg_stats st{};
+            CK(cudaMemcpyAsync(h->d_D, D.data(), nn * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+            jk_device(h, h->d_D, h->d_J, h->d_K, QCG_JK_SKIP_VALIDATION, &st);
+            CK(cudaMemcpyAsync(J.data(), h->d_J, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaMemcpyAsync(K.data(), h->d_K, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+            fock_ms += st.ms_total;
+            double e = 0;
+            for (size_t k = 0; k < nn; ++k)
+            {
+                F[k] = H[k] + J[k] - 0.5 * K[k];
+                e += D[k] * (H[k] + F[k]);
+            }
+            E = 0.5 * e + Enn;
+            if (!std::isfinite(E)) throw Error{QCG_ERR_NONFINITE, "non-finite SCF energy"};
+            ortho(F, Fp);
+            gemm(n, Fp.data(), false, Dp.data(), false, a.data());
+            gemm(n, Dp.data(), false, Fp.data(), false, b.data());
+            En = 0;
+            for (size_t k = 0; k < nn; ++k)
+            {
+                Err[k] = a[k] - b[k];
+                En += Err[k] * Err[k];
+            }
+            En = std::sqrt(En);
+            if (it > 1 && std::fabs(E - Eold) < prm.de_tol && En < prm.fd_tol)
+            {
+                converged = true;
+                break;
+            }
+            Eold = E;
+            std::vector<double> Fuse = Fp;
+            if (En != 0.0 && En <= fdmax)
+            {
+                Es.push_back(Err);
+                Fps.push_back(Fp);
+                if ((int)Es.size() > prm.diis_nproj)
+                {
+                    Es.pop_front();
+                    Fps.pop_front();
+                }
+                auto bordered = [&]() {
+                    const int m = (int)Es.size();
+                    std::vector<double> B((m + 1) * (m + 1), 0.0);
+                    for (int i = 0; i < m; ++i)
+                    {
+                        B[i * (m + 1) + m] = B[m * (m + 1) + i] = 1.0;
+                        for (int j = i; j < m; ++j)
+                        {
+                            double s = 0;
+                            for (size_t k = 0; k < nn; ++k) s += Es[i][k] * Es[j][k];
+                            B[i * (m + 1) + j] = B[j * (m + 1) + i] = s;
+                        }
+                    }
+                    return B;
+                };
+                auto minsv = [&](const std::vector<double>& B) {
+                    const int m1 = (int)std::lround(std::sqrt((double)B.size()));
+                    std::vector<double> ev(m1), vv(B.size());
+                    syev(m1, B.data(), ev.data(), vv.data());
+                    double mn = 1e300;
+                    for (double x : ev) mn = std::min(mn, std::fabs(x));
+                    return mn;
+                };
+                if (Es.size() >= 2)
+                {
+                    auto B = bordered();
+                    while (Es.size() >= 2 && minsv(B) < prm.diis_svtol)
+                    {
+                        Es.pop_front();
+                        Fps.pop_front();
+                        B = bordered();
+                    }
+                    const int m = (int)Es.size();
+                    if (m >= 2)
+                    {
+                        std::vector<double> rhs(m + 1, 0.0);
+                        rhs[m] = 1.0;
+                        auto c = solve_dense(m + 1, B, rhs);
+                        std::fill(Fuse.begin(), Fuse.end(), 0.0);
+                        for (int i = 0; i < m; ++i)
+                            for (size_t k = 0; k < nn; ++k) Fuse[k] += c[i] * Fps[i][k];
+                    }
+                }
+            }
+            diag_fill(Fuse);
+        }
+        result->energy = E;
+        result->e_nuc = Enn;
+        result->iterations = std::min(it, prm.max_iter);
+        result->converged = converged ? 1 : 0;
+        result->fd_error = En;
+        result->fock_ms = fock_ms;
+        result->wall_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (D_out) std::copy(D.begin(), D.end(), D_out);
+    });
+    if (rc == QCG_OK && !converged) return QCG_ERR_NOCONV;
+    return rc;
+}
+
+// FP64 FMA peak of the current device: TFLOP/s of a pure-DFMA kernel over `reps` timed launches.
+int qcg_measure_fp64_peak(int reps, double* tflops, double* ms_per_launch)
+{
+    if (!tflops || reps <= 0) return QCG_ERR_ARG;
+    try
+    {
+        int dev = 0, nsm = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        double* out = nullptr;
+        CK(cudaMalloc(&out, sizeof(double)));
+        cudaEvent_t a, b;
+        CK(cudaEventCreate(&a));
+        CK(cudaEventCreate(&b));
+        const int blocks = nsm * 8, threads = 256, iters = 2048;
+        launch_dfma_peak(out, blocks, threads, iters, nullptr);   // warm-up
+        CK(cudaEventRecord(a, nullptr));
+        for (int r = 0; r < reps; ++r) launch_dfma_peak(out, blocks, threads, iters, nullptr);
+        CK(cudaEventRecord(b, nullptr));
+        CK(cudaEventSynchronize(b));
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, a, b));
+        const double flops = 2.0 * 8 * 16 * (double)iters * threads * blocks * reps;
+        *tflops = flops / (ms * 1e-3) / 1e12;
+        if (ms_per_launch) *ms_per_launch = ms / reps;
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        cudaFree(out);
+        return QCG_OK;
+    }
+    catch (const Error& e)
+    {
+        return e.code;
+    }
+}
+
+// test hook: the host eigensolver used by the SCF (not part of the public header)
+int qcg_internal_syev(int n, const double* A, double* w, double* V)
+{
+    try
+    {
+        syev(n, A, w, V);
+        return QCG_OK;
+    }
+    catch (const Error& e)
+    {
+        return e.code;
+    }
+}
+
+}   // extern "C"

@@ -1,0 +1,192 @@
+"""GPU parity: the CUDA path through the C ABI against the CPU oracle on the same seeded inputs.
+
+Tolerances (fixed by the task): Cartesian ERIs 1e-12 absolute, Fock (J, K) matrices 1e-10 absolute,
+converged SCF energies 1e-8 Eh.
+"""
+import numpy as np
+import pytest
+
+from qchem_b200 import api, basis as B, workloads as W
+from tests.conftest import molecule_from
+
+pytestmark = pytest.mark.gpu
+
+ERI_TOL = 1e-12
+FOCK_TOL = 1e-10
+E_TOL = 1e-8
+
+
+@pytest.fixture(scope="module")
+def pool():
+    shells = W.shell_pool(64, seed=W.SEED0 + 2000)
+    return shells
+
+
+@pytest.fixture(scope="module")
+def pool_engines(pool, oracle_mod):
+    return api.Engine(pool), oracle_mod.OracleBasis(pool)
+
+
+@pytest.mark.parametrize("k", range(21))
+def test_eri_batch_class(k, pool_engines):
+    eng, ob = pool_engines
+    cls = W.quartet_classes()[k]
+    q = W.eri_class_batch(cls, 200, 64, seed=W.SEED0 + 2000 + k)
+    got = eng.eri_batch(cls, q)
+    ref = ob.eri_batch(q)
+    assert got.shape == ref.shape
+    assert np.all(np.isfinite(got))
+    err = np.abs(got - ref).max()
+    assert err <= ERI_TOL, f"class {cls}: max abs error {err:.3e} (max |eri| {np.abs(ref).max():.3e})"
+
+
+def test_eri_batch_matches_fourc_elements(pool_engines):
+    """Spot-check single elements against the reference's per-component route (FourC)."""
+    eng, ob = pool_engines
+    cls = (2, 1, 1, 1)
+    q = W.eri_class_batch(cls, 3, 64, seed=7)
+    got = eng.eri_batch(cls, q)
+    for qi, (a, b, c, d) in enumerate(q):
+        fa, fb, fc, fd = (int(ob.offsets[s]) for s in (a, b, c, d))
+        blk = got[qi].reshape(6, 3, 3, 3)
+        for ia, ib, ic, id_ in [(0, 0, 0, 0), (5, 2, 1, 0), (3, 1, 2, 2)]:
+            ref = ob.fourc(fa + ia, fb + ib, fc + ic, fd + id_)
+            assert abs(blk[ia, ib, ic, id_] - ref) <= ERI_TOL
+
+
+def test_norms_match_reference_convention(pool, pool_engines):
+    eng, ob = pool_engines
+    np.testing.assert_allclose(eng.norms(), ob.norms(), rtol=1e-13, atol=0)
+
+
+def test_schwarz_water(oracle_mod):
+    sh = B.even_tempered(W.water())
+    eng, ob = api.Engine(sh), oracle_mod.OracleBasis(sh)
+    np.testing.assert_allclose(eng.schwarz(1e-10), ob.schwarz(), rtol=1e-11, atol=1e-13)
+
+
+def _jk_case(shells, D, oracle_mod, thresh=1e-10):
+    eng, ob = api.Engine(shells), oracle_mod.OracleBasis(shells)
+    eng.schwarz(thresh)
+    J, K, st = eng.fock_jk(D)
+    Jr, Kr, cnt = ob.jk_direct(D, thresh=thresh)
+    assert st.quartets == cnt
+    return J, K, Jr, Kr
+
+
+def test_jk_water_config1(oracle_mod):
+    mol = W.water()
+    sh = B.even_tempered(mol)
+    D = oracle_mod.OracleBasis(sh).rhf(mol)["D"]
+    J, K, Jr, Kr = _jk_case(sh, D, oracle_mod)
+    assert np.abs(J - Jr).max() <= FOCK_TOL
+    assert np.abs(K - Kr).max() <= FOCK_TOL
+    assert np.abs(J - J.T).max() == 0.0 and np.abs(K - K.T).max() == 0.0
+
+
+def test_jk_water_dzvp_contracted(oracle_mod, anchors, dzvp_text):
+    mol = molecule_from(anchors["water"])
+    sh = B.read_gaussian94(dzvp_text, mol)
+    n = B.nbf(sh)
+    rng = np.random.default_rng(11)
+    Q, _ = np.linalg.qr(rng.normal(size=(n, 5)))
+    D = 2 * Q @ Q.T
+    J, K, Jr, Kr = _jk_case(sh, D, oracle_mod)
+    assert np.abs(J - Jr).max() <= FOCK_TOL
+    assert np.abs(K - Kr).max() <= FOCK_TOL
+
+
+def test_jk_small_cluster(oracle_mod):
+    mol = W.water_cluster(nx=2, ny=2, nz=1, seed=W.SEED0 + 3100)
+    sh = B.even_tempered(mol)
+    D = W.cluster_density(B.nbf(sh), nocc=20, seed=W.SEED0 + 3101)
+    J, K, Jr, Kr = _jk_case(sh, D, oracle_mod)
+    assert np.abs(J - Jr).max() <= FOCK_TOL
+    assert np.abs(K - Kr).max() <= FOCK_TOL
+
+
+def test_jk_no_screening_matches_eri4(oracle_mod):
+    """Threshold 0: every canonical quartet; compare with the reference's ERI4 supermatrix route."""
+    mol = W.water()
+    sh = B.even_tempered(mol)
+    n = B.nbf(sh)
+    rng = np.random.default_rng(5)
+    Q, _ = np.linalg.qr(rng.normal(size=(n, 5)))
+    D = 2 * Q @ Q.T
+    eng = api.Engine(sh)
+    eng.schwarz(0.0)
+    J, K, st = eng.fock_jk(D)
+    Jr, Kr = oracle_mod.OracleBasis(sh).jk_eri4(D)
+    assert st.quartets == 435 * 436 // 2
+    assert np.abs(J - Jr).max() <= FOCK_TOL
+    assert np.abs(K - Kr).max() <= FOCK_TOL
+
+
+def test_one_electron_water_dzvp(oracle_mod, anchors, dzvp_text):
+    mol = molecule_from(anchors["water"])
+    sh = B.read_gaussian94(dzvp_text, mol)
+    eng, ob = api.Engine(sh), oracle_mod.OracleBasis(sh)
+    for got, ref in zip(eng.one_electron(mol), ob.one_electron(mol)):
+        assert np.abs(got - ref).max() <= 1e-12
+
+
+def test_rhf_config1_energy(oracle_mod):
+    mol = W.water()
+    sh = B.even_tempered(mol)
+    r = api.Engine(sh).rhf(mol)
+    ro = oracle_mod.OracleBasis(sh).rhf(mol)
+    assert r["converged"]
+    assert abs(r["energy"] - ro["energy"]) <= E_TOL
+
+
+@pytest.mark.parametrize("name", ["water", "n2"])
+def test_rhf_dzvp_anchor(name, anchors, dzvp_text, oracle_mod):
+    a = anchors[name]
+    mol = molecule_from(a)
+    sh = B.read_gaussian94(dzvp_text, mol)
+    r = api.Engine(sh).rhf(mol)
+    assert r["converged"]
+    assert abs((r["energy"] - a["energy"]) / a["energy"]) < a["rel_tol"]
+    ro = oracle_mod.OracleBasis(sh).rhf(mol)
+    assert abs(r["energy"] - ro["energy"]) <= E_TOL
+
+
+def test_rigid_motion_invariance():
+    """Rotating and translating the molecule leaves the RHF energy unchanged (IntegrationTests/M_Sym.C:139-141)."""
+    mol = W.water()
+    e0 = api.Engine(B.even_tempered(mol)).rhf(mol)["energy"]
+    th = 0.7
+    Rz = np.array([[np.cos(th), -np.sin(th), 0], [np.sin(th), np.cos(th), 0], [0, 0, 1]])
+    mol2 = B.Molecule(mol.Z, mol.R @ Rz.T + np.array([0.3, -1.2, 2.5]))
+    e1 = api.Engine(B.even_tempered(mol2)).rhf(mol2)["energy"]
+    assert abs(e0 - e1) < 1e-8
+
+
+def test_orbital_hf_ibs_face_fuses_j_and_k(oracle_mod):
+    mol = W.water()
+    sh = B.even_tempered(mol)
+    D = oracle_mod.OracleBasis(sh).rhf(mol)["D"]
+    ibs = api.OrbitalHFIBS(api.Engine(sh))
+    Sj = np.zeros_like(D)
+    Sk = np.zeros_like(D)
+    ibs.AccumulateDirect(Sj, D)
+    ibs.AccumulateExchange(Sk, D)
+    assert ibs.builds == 1
+    Jr, Kr, _ = oracle_mod.OracleBasis(sh).jk_direct(D)
+    assert np.abs(Sj - Jr).max() <= FOCK_TOL and np.abs(Sk - Kr).max() <= FOCK_TOL
+    Dao = np.zeros_like(D)
+    ibs.AddAODensity(Dao, D)
+    F = np.zeros_like(D)
+    ibs.SliceAOFock(F, ibs.MakeAOFock(Dao, exchange=True))
+    assert ibs.builds == 1 and np.abs(F - Kr).max() <= FOCK_TOL
+    assert ibs.AODimension() == B.nbf(sh)
+
+
+def test_jk_deterministic_to_rounding(oracle_mod):
+    mol = W.water()
+    sh = B.even_tempered(mol)
+    D = oracle_mod.OracleBasis(sh).rhf(mol)["D"]
+    eng = api.Engine(sh)
+    J1, K1, _ = eng.fock_jk(D)
+    J2, K2, _ = eng.fock_jk(D)
+    assert np.abs(J1 - J2).max() <= 1e-13 and np.abs(K1 - K2).max() <= 1e-13
