@@ -190,7 +190,8 @@ def main():
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     dev = torch.device("cuda", local)
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream(device=dev)   # every kernel and every timing event of the run on this stream
+    torch.cuda.set_stream(stream)
     nq_cls = args.quartets_per_class
     classes = W.quartet_classes()
     pool = W.shell_pool(NPOOL, seed=W.SEED0 + 2000)

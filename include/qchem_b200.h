@@ -83,7 +83,9 @@ int qcg_basis_create(const int* shell_L, const int* shell_nprim, const double* e
                      const double* centres, int nshell, qcg_handle** out);
 void qcg_destroy(qcg_handle* h);
 const char* qcg_last_error(const qcg_handle* h);
-int qcg_set_stream(qcg_handle* h, void* cuda_stream);     /* NULL: the handle's own stream */
+/* stream for all later work of this handle; NULL is the CUDA default (legacy) stream.  A new handle
+ * starts on its own non-blocking stream. */
+int qcg_set_stream(qcg_handle* h, void* cuda_stream);
 int qcg_set_memory_limit(qcg_handle* h, long long bytes); /* cap on device bytes this handle allocates; 0 = none */
 int qcg_nbf(const qcg_handle* h, int* nbf);
 int qcg_nshell(const qcg_handle* h, int* nshell);

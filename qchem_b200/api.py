@@ -163,8 +163,9 @@ class Engine:
         if rc != QCG_OK:
             raise QcgError(rc, lib().qcg_last_error(self._h).decode())
 
-    def set_stream(self, stream_ptr: Optional[int]):
-        self._check(lib().qcg_set_stream(self._h, ctypes.c_void_p(stream_ptr or 0)))
+    def set_stream(self, stream_ptr: int):
+        """All later work of this engine goes to CUDA stream `stream_ptr` (0 = the legacy default stream)."""
+        self._check(lib().qcg_set_stream(self._h, ctypes.c_void_p(int(stream_ptr))))
 
     def set_memory_limit(self, nbytes: int):
         self._check(lib().qcg_set_memory_limit(self._h, int(nbytes)))

@@ -40,22 +40,23 @@ def _hash(parts):
     return h.hexdigest()[:20]
 
 
-def _common_headers():
-    names = ["md_core.cuh", "qcg_internal.h", "eri_kernels.cuh", "boys_table.h"]
-    return [_read(os.path.join(CSRC, n)) for n in names] + [_read(os.path.join(INCLUDE, "qchem_b200.h"))]
+def _headers(names):
+    return [_read(os.path.join(CSRC, n)) for n in names]
 
 
 def _jobs():
-    hdr = _common_headers()
+    core = _headers(["md_core.cuh", "qcg_internal.h"])
     jobs = []
     src = os.path.join(CSRC, "eri_class.cu")
     for k in range(NCLASS):
         defs = [f"-DQCG_CLASS={k}"]
-        key = _hash([_read(src), _read(os.path.join(GEN, f"md_class_{k}.cuh"))] + hdr + FLAGS + defs)
+        key = _hash([_read(src), _read(os.path.join(GEN, f"md_class_{k}.cuh"))] + core
+                    + _headers(["eri_kernels.cuh"]) + FLAGS + defs)
         jobs.append((src, defs, os.path.join(BUILD, f"eri_class_{k}_{key}.o")))
+    extra = {"runtime.cu": _headers(["boys_table.h"]) + [_read(os.path.join(INCLUDE, "qchem_b200.h"))]}
     for name in ("registry.cu", "fock_kernels.cu", "runtime.cu"):
         s = os.path.join(CSRC, name)
-        key = _hash([_read(s)] + hdr + FLAGS)
+        key = _hash([_read(s)] + core + extra.get(name, []) + FLAGS)
         jobs.append((s, [], os.path.join(BUILD, f"{name[:-3]}_{key}.o")))
     return jobs
 

@@ -713,7 +713,7 @@ const char* qcg_last_error(const qcg_handle* h) { return h ? h->last_error.c_str
 int qcg_set_stream(qcg_handle* h, void* s)
 {
     if (!h) return QCG_ERR_ARG;
-    h->stream = s ? (cudaStream_t)s : h->own_stream;
+    h->stream = (cudaStream_t)s;   // NULL is the CUDA default (legacy) stream
     return QCG_OK;
 }
 
