@@ -110,6 +110,17 @@ int qcg_fock_jk(qcg_handle* h, const double* D, double* J, double* K, int flags,
 /* same with device pointers on the handle's stream; results are ready when the stream reaches them */
 int qcg_fock_jk_device(qcg_handle* h, const double* d_D, double* d_J, double* d_K, int flags, qcg_stats* stats);
 
+/* The J/K build of qcg_fock_jk_device for callers that must not allocate device memory once their setup
+ * is done -- for example a host program whose device memory is owned by its own pool allocator, or one
+ * that runs under a device-memory budget fixed at startup.  This call performs no cudaMalloc, cudaFree or
+ * other allocating call: its J'/K' accumulators live in a file-scope device array of the library, sized
+ * for at most 512 basis functions (larger bases are rejected with QCG_ERR_ARG).  qcg_basis_create and
+ * qcg_schwarz, which do allocate, must have run before.  The first call on a device looks up the array's
+ * device address; make that first call before any stream capture.  All calls share the one array (it
+ * keeps the last call's contents and is cleared at the start of each call), so calls that overlap on the
+ * GPU race: issue them in order on one stream.  No validation of D.  Has no counterpart in the reference. */
+int qcg_fock_jk_device_noalloc(qcg_handle* h, const double* d_D, double* d_J, double* d_K);
+
 /* overlap, kinetic (1/2 <grad|grad>) and nuclear attraction, natom nuclei of charge Z at R (3 per atom) */
 int qcg_one_electron(qcg_handle* h, int natom, const double* Z, const double* R, double* S, double* T, double* V);
 

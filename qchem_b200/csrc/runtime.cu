@@ -1087,6 +1087,67 @@ int qcg_rhf(qcg_handle* h, int natom, const double* Z, const double* R, int nele
     return rc;
 }
 
+// ------------------------------------------------------------------------------------------------
+// J/K build that allocates nothing.  Its J'/K' accumulators and result flag live in this file-scope
+// device array (every GPU that loads the library holds it until the process exits).  Host code must not
+// hand the array's name to a kernel: on the host it is only a stand-in, so the device address is looked
+// up once per device with cudaGetSymbolAddress and cached.
+// ------------------------------------------------------------------------------------------------
+constexpr int kNoAllocMaxNbf = 512;
+constexpr size_t kNoAllocScratchDoubles = 2 * (size_t)kNoAllocMaxNbf * kNoAllocMaxNbf + 32;
+static __device__ __align__(256) double qcg_noalloc_scratch[kNoAllocScratchDoubles];
+
+namespace {
+constexpr int kNoAllocMaxDevices = 64;
+double* g_noalloc_scratch[kNoAllocMaxDevices] = {};
+
+double* noalloc_scratch_for(int device)
+{
+    require(device >= 0 && device < kNoAllocMaxDevices, "device index out of range");
+    if (!g_noalloc_scratch[device])
+    {
+        int cur = -1;
+        CK(cudaGetDevice(&cur));
+        require(cur == device, "the handle's device must be the current device", QCG_ERR_STATE);
+        void* p = nullptr;
+        CK(cudaGetSymbolAddress(&p, qcg_noalloc_scratch));
+        g_noalloc_scratch[device] = (double*)p;
+    }
+    return g_noalloc_scratch[device];
+}
+}   // namespace
+
+extern "C" int qcg_fock_jk_device_noalloc(qcg_handle* h, const double* d_D, double* d_J, double* d_K)
+{
+    if (!h) return QCG_ERR_ARG;
+    return guarded(h, [&] {
+        require(d_D && d_J && d_K, "null argument");
+        require(h->nbf <= kNoAllocMaxNbf,
+                "qcg_fock_jk_device_noalloc supports at most " + std::to_string(kNoAllocMaxNbf) +
+                    " basis functions (this basis has " + std::to_string(h->nbf) + ")");
+        require(h->screened, "qcg_schwarz must be called before qcg_fock_jk_device_noalloc", QCG_ERR_STATE);
+        double* scratch = noalloc_scratch_for(h->device);
+        const int n = h->nbf;
+        const size_t nn = (size_t)n * n;
+        double* Jp = scratch;
+        double* Kp = scratch + nn;
+        int* flag = (int*)(scratch + 2 * nn);
+        // the array keeps the previous call's contents: the accumulators must start from zero
+        CK(cudaMemsetAsync(scratch, 0, (2 * nn + 1) * sizeof(double), h->stream));
+        for (int k = kNumQuartetClasses - 1; k >= 0; --k)
+        {
+            int X = 0;
+            while ((X + 1) * (X + 2) / 2 <= k) ++X;
+            const int Y = k - X * (X + 1) / 2;
+            kJKLaunchers[k](h->work[k], h->pl_dev[X], h->pl_dev[Y], h->pp_dev, h->d_f0, d_D, Jp, Kp, n, h->d_boys,
+                            h->stream, h->nsm);
+        }
+        CK(cudaGetLastError());
+        launch_symmetrize(Jp, Kp, d_J, d_K, n, flag, h->stream, h->nsm);
+        CK(cudaGetLastError());
+    });
+}
+
 // FP64 FMA peak of the current device: TFLOP/s of a pure-DFMA kernel over `reps` timed launches.
 int qcg_measure_fp64_peak(int reps, double* tflops, double* ms_per_launch)
 {

@@ -1,0 +1,65 @@
+"""qcg_fock_jk_device_noalloc: the J/K build for callers that must not allocate device memory after setup
+(a host program whose device memory belongs to its own pool allocator, or one held to a fixed budget).
+
+The entry point keeps its accumulators in a fixed device array of the library instead of allocating.  This
+test calls it through the C ABI and checks it against the allocating entry point qcg_fock_jk_device, twice
+in a row (the array keeps the previous call's contents, so the second call also checks that it is cleared).
+The handle's device-memory cap is set below what it already holds while the entry point runs, so any
+allocation attempt through the handle would fail the call.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from qchem_b200 import api, basis as B, workloads as W
+
+pytestmark = pytest.mark.gpu
+
+FOCK_TOL = 1e-10   # the J/K tolerance used by the other GPU tests
+
+
+def _entry():
+    L = api.lib()
+    f = L.qcg_fock_jk_device_noalloc
+    f.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    f.restype = ctypes.c_int
+    return f
+
+
+def test_noalloc_matches_allocating_entry_point_twice():
+    import torch
+    f = _entry()
+    mol = W.water()
+    eng = api.Engine(B.even_tempered(mol))
+    eng.schwarz(1e-10)
+    n = eng.nbf
+    rng = np.random.default_rng(21)
+    Q, _ = np.linalg.qr(rng.normal(size=(n, 5)))
+    D = torch.tensor(2 * Q @ Q.T, device="cuda", dtype=torch.float64)
+    J_ref, K_ref = torch.empty_like(D), torch.empty_like(D)
+    eng.fock_jk_device(D.data_ptr(), J_ref.data_ptr(), K_ref.data_ptr())
+    torch.cuda.synchronize()
+    eng.set_memory_limit(1)   # below current use: any allocation through the handle would now fail
+    try:
+        for _ in range(2):
+            J, K = torch.full_like(D, np.nan), torch.full_like(D, np.nan)
+            rc = f(eng._h, ctypes.c_void_p(D.data_ptr()), ctypes.c_void_p(J.data_ptr()), ctypes.c_void_p(K.data_ptr()))
+            torch.cuda.synchronize()
+            assert rc == api.QCG_OK, api.lib().qcg_last_error(eng._h).decode()
+            assert torch.abs(J - J_ref).max().item() <= FOCK_TOL
+            assert torch.abs(K - K_ref).max().item() <= FOCK_TOL
+    finally:
+        eng.set_memory_limit(0)
+
+
+def test_noalloc_rejects_bases_above_the_limit():
+    import torch
+    f = _entry()
+    mol = W.water_cluster(nx=3, ny=3, nz=1, seed=W.SEED0 + 3200)   # 9 waters, 513 functions
+    eng = api.Engine(B.even_tempered(mol))
+    assert eng.nbf > 512
+    D = torch.zeros((eng.nbf, eng.nbf), device="cuda", dtype=torch.float64)
+    rc = f(eng._h, ctypes.c_void_p(D.data_ptr()), ctypes.c_void_p(D.data_ptr()), ctypes.c_void_p(D.data_ptr()))
+    assert rc == api.QCG_ERR_ARG
+    assert "at most 512" in api.lib().qcg_last_error(eng._h).decode()
