@@ -59,13 +59,13 @@ long long grid_for(long long work, int nsm)
 }
 }   // namespace
 
-void QCG_CAT(launch_eri_batch_, QCG_CLASS)(const BasisDev& bs, const int4* q, long long nq, double* out,
-                                           const double* boys, cudaStream_t st, int nsm)
+void QCG_CAT(launch_eri_batch_, QCG_CLASS)(const BasisDev& bs, const int4* q, const int* order, long long nq,
+                                           double* out, const double* boys, cudaStream_t st, int nsm)
 {
     if (nq <= 0) return;
     auto k = eri_batch_kernel<Cls, kThreads>;
     prepare(k);
-    k<<<(unsigned)grid_for(nq, nsm), kThreads, kSmem, st>>>(bs, q, nq, out, boys);
+    k<<<(unsigned)grid_for(nq, nsm), kThreads, kSmem, st>>>(bs, q, order, nq, out, boys);
 }
 
 void QCG_CAT(launch_jk_, QCG_CLASS)(const JKWorkDev& w, const PairListDev& bra, const PairListDev& ket,

@@ -11,19 +11,19 @@ namespace qcg {
 // Cartesian ERI batch: out[q][a][b][c][d] = (ab|cd) for quartet q (shell indices), contracted and
 // normalised like qchem's NR_Evaluator::FourC (PG_Cart_MnD/Evaluator.C:1912-1920).
 // ------------------------------------------------------------------------------------------------
+// accumulates every primitive quartet into the (zeroed) output block with fire-and-forget L2 reductions:
+// the thread never reads the block back, so no loads are hoisted into registers around the ERI code
 template <int LB, int LC, int LD>
 struct StoreSink
 {
+    static constexpr bool kByValue = true;
     double* o;
-    bool first;
     static constexpr int NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
     __device__ __forceinline__ void ket_begin(int, int) {}
     __device__ __forceinline__ void ket_end(int, int) {}
     __device__ __forceinline__ void operator()(int ia, int ib, int ic, int id, double v)
     {
-        double* p = o + ((ia * NB + ib) * NC + ic) * ND + id;
-        if (first) *p = v;
-        else *p += v;
+        atomicAdd(o + ((ia * NB + ib) * NC + ic) * ND + id, v);
     }
 };
 
@@ -37,30 +37,32 @@ __device__ __forceinline__ PrimPairData shell_prim_pair(const BasisDev& bs, int 
 // dynamic shared memory holding the per-thread R tables of classes with L >= 6
 extern __shared__ double qcg_smem[];
 
+// Quartets are visited through `order` (a permutation grouping equal contraction patterns, so that the
+// lanes of a warp run the same primitive loops); each writes its own output block.
 template <class Cls, int THREADS>
 __global__ void __launch_bounds__(THREADS) eri_batch_kernel(BasisDev bs, const int4* __restrict__ quartets,
-                                                            long long nq, double* __restrict__ out,
+                                                            const int* __restrict__ order, long long nq,
+                                                            double* __restrict__ out,
                                                             const double* __restrict__ boys_table)
 {
     constexpr long long BLK = (long long)ncart(Cls::LA) * ncart(Cls::LB) * ncart(Cls::LC) * ncart(Cls::LD);
     double* rs = qcg_smem + threadIdx.x;
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nq; q += (long long)gridDim.x * blockDim.x)
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < nq; g += (long long)gridDim.x * blockDim.x)
     {
+        const long long q = order ? order[g] : g;
         const int4 s = quartets[q];
-        StoreSink<Cls::LB, Cls::LC, Cls::LD> sink{out + q * BLK, true};
+        double* o = out + q * BLK;
+        for (int k = 0; k < (int)BLK; ++k) o[k] = 0.0;
+        StoreSink<Cls::LB, Cls::LC, Cls::LD> sink{o};
         const int ni = bs.nprim[s.x], nj = bs.nprim[s.y], nk = bs.nprim[s.z], nl = bs.nprim[s.w];
-        for (int i = 0; i < ni; ++i)
-            for (int j = 0; j < nj; ++j)
-            {
-                const PrimPairData ab = shell_prim_pair(bs, s.x, i, s.y, j);
-                for (int k = 0; k < nk; ++k)
-                    for (int l = 0; l < nl; ++l)
-                    {
-                        const PrimPairData cd = shell_prim_pair(bs, s.z, k, s.w, l);
-                        Cls::quartet(ab, cd, boys_table, rs, THREADS, sink);
-                        sink.first = false;
-                    }
-            }
+        const int nket = nk * nl, ntot = ni * nj * nket;
+        for (int x = 0; x < ntot; ++x)
+        {
+            const int ij = x / nket, kl = x - ij * nket;
+            const PrimPairData ab = shell_prim_pair(bs, s.x, ij / nj, s.y, ij % nj);
+            const PrimPairData cd = shell_prim_pair(bs, s.z, kl / nl, s.w, kl % nl);
+            Cls::quartet(ab, cd, boys_table, rs, THREADS, sink);
+        }
     }
 }
 

@@ -1,5 +1,7 @@
 // fock_kernels.cu -- the small kernels around the J/K build: density validation, J'/K' symmetrisation,
 // and the one-electron integrals (overlap, kinetic, nuclear attraction) of the RHF Hamiltonian.
+#include <algorithm>
+
 #include "md_core.cuh"
 #include "qcg_internal.h"
 
@@ -36,6 +38,65 @@ __global__ void symmetrize_kernel(const double* __restrict__ Jp, const double* _
         K[k] = kv;
         if (!isfinite(jv) || !isfinite(kv)) atomicOr(flag, 1);
     }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Grouping of an ERI batch by contraction pattern (counting sort over 256 buckets): the batch kernels
+// then visit quartets with equal primitive-loop shapes in the same warp.
+// ------------------------------------------------------------------------------------------------
+// contraction-pattern key of every quartet (primitive counts up to 4 per shell; larger ones share a bucket)
+__global__ void pattern_key_kernel(BasisDev bs, const int4* __restrict__ quartets, long long nq,
+                                   unsigned char* __restrict__ key, int* __restrict__ hist)
+{
+    __shared__ int h[256];
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) h[i] = 0;
+    __syncthreads();
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nq; q += (long long)gridDim.x * blockDim.x)
+    {
+        const int4 s = quartets[q];
+        const int a = min(bs.nprim[s.x], 4) - 1, b = min(bs.nprim[s.y], 4) - 1, c = min(bs.nprim[s.z], 4) - 1,
+                  d = min(bs.nprim[s.w], 4) - 1;
+        const int k = ((a * 4 + b) * 4 + c) * 4 + d;
+        key[q] = (unsigned char)k;
+        atomicAdd(&h[k], 1);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 256; i += blockDim.x)
+        if (h[i]) atomicAdd(&hist[i], h[i]);
+}
+
+// exclusive scan of the 256 bucket counts (one block of 256 threads)
+__global__ void pattern_scan_kernel(const int* __restrict__ hist, int* __restrict__ cursor)
+{
+    __shared__ int v[256];
+    const int t = threadIdx.x;
+    v[t] = hist[t];
+    __syncthreads();
+    for (int off = 1; off < 256; off <<= 1)
+    {
+        const int x = t >= off ? v[t - off] : 0;
+        __syncthreads();
+        v[t] += x;
+        __syncthreads();
+    }
+    cursor[t] = v[t] - hist[t];
+}
+
+__global__ void pattern_scatter_kernel(const unsigned char* __restrict__ key, long long nq, int* __restrict__ cursor,
+                                       int* __restrict__ order)
+{
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nq; q += (long long)gridDim.x * blockDim.x)
+        order[atomicAdd(&cursor[key[q]], 1)] = (int)q;
+}
+
+void launch_pattern_sort(const BasisDev& bs, const int4* quartets, long long nq, unsigned char* key, int* hist,
+                         int* cursor, int* order, cudaStream_t st, int nsm)
+{
+    cudaMemsetAsync(hist, 0, 256 * sizeof(int), st);
+    const long long blocks = std::min<long long>((nq + 255) / 256, (long long)nsm * 8);
+    pattern_key_kernel<<<(unsigned)blocks, 256, 0, st>>>(bs, quartets, nq, key, hist);
+    pattern_scan_kernel<<<1, 256, 0, st>>>(hist, cursor);
+    pattern_scatter_kernel<<<(unsigned)blocks, 256, 0, st>>>(key, nq, cursor, order);
 }
 
 void launch_validate(const double* D, int n, double tol, int* flag, cudaStream_t st, int nsm)

@@ -92,7 +92,8 @@ def gen_E(name, LA, LB, PA, PB, a12):
     return out
 
 
-CHUNK_OUTPUTS = 216        # classes with more outputs are split into __noinline__ ket-component chunks
+CHUNK_ABOVE = 100          # classes with more outputs than this are split into __noinline__ chunks ...
+CHUNK_OUTPUTS = 72         # ... of at most this many outputs (keeps each chunk's live set in registers)
 
 
 def e_tables(LA, LB, LC, LD):
@@ -204,11 +205,13 @@ def ket_blocks(LA, LB, LC, LD, cds, w):
 
 def gen_class(LA, LB, LC, LD, idx):
     L = LA + LB + LC + LD
-    rsm = L >= R_SMEM_MIN_L
     A, B, C, D = comps(LA), comps(LB), comps(LC), comps(LD)
     nab, ncd = len(A) * len(B), len(C) * len(D)
     all_cds = [(ic, id_) for ic in range(len(C)) for id_ in range(len(D))]
-    chunked = nab * ncd > CHUNK_OUTPUTS
+    chunked = nab * ncd > CHUNK_ABOVE
+    # chunk functions read R through the per-thread shared-memory slice, so chunked classes keep R there
+    rsm = L >= R_SMEM_MIN_L or chunked
+    assert rsm or not chunked
     o = []
     w = o.append
     w(f"// class {idx}: ({'spd'[LA]}{'spd'[LB]}|{'spd'[LC]}{'spd'[LD]}), L = {L}; R table in "
@@ -216,8 +219,6 @@ def gen_class(LA, LB, LC, LD, idx):
       f"{'; ket components split into __noinline__ chunks' if chunked else ''}")
     w(f"constexpr bool kRShared{idx} = {'true' if rsm else 'false'};")
     w(f"constexpr int kRSize{idx} = {nherm(L)};")
-    ebn = e_names("ebx", LA, LB) + e_names("eby", LA, LB) + e_names("ebz", LA, LB)
-    ekn = e_names("ekx", LC, LD) + e_names("eky", LC, LD) + e_names("ekz", LC, LD)
     chunk_names = []
     if chunked:
         per = max(1, CHUNK_OUTPUTS // nab)
@@ -225,14 +226,20 @@ def gen_class(LA, LB, LC, LD, idx):
         for ci, cds in enumerate(chunks):
             fn = f"prim_quartet_{idx}_chunk{ci}"
             chunk_names.append(fn)
+            # each chunk rebuilds the 1-D E tables from the pair scalars (cheaper than reloading them)
             w("template <class Sink>")
             w(f"__device__ __noinline__ void {fn}(const double* __restrict__ rs, const int rstride,")
-            w("    const double* __restrict__ eb, const double* __restrict__ ek, const double lambda, Sink& sink)")
+            w("    const double a12b, const double bPAx, const double bPAy, const double bPAz, const double bPBx,")
+            w("    const double bPBy, const double bPBz, const double a12k, const double kPAx, const double kPAy,")
+            w("    const double kPAz, const double kPBx, const double kPBy, const double kPBz, const double lambda,")
+            w("    typename SinkArg<Sink>::type sink)")
             w("{")
-            for k, nm in enumerate(ebn):
-                w(f"    const double {nm} = eb[{k}];")
-            for k, nm in enumerate(ekn):
-                w(f"    const double {nm} = ek[{k}];")
+            for s_ in e_tables(LA, LB, LC, LD):
+                s_ = (s_.replace("ab.PAx", "bPAx").replace("ab.PAy", "bPAy").replace("ab.PAz", "bPAz")
+                      .replace("ab.PBx", "bPBx").replace("ab.PBy", "bPBy").replace("ab.PBz", "bPBz")
+                      .replace("cd.PAx", "kPAx").replace("cd.PAy", "kPAy").replace("cd.PAz", "kPAz")
+                      .replace("cd.PBx", "kPBx").replace("cd.PBy", "kPBy").replace("cd.PBz", "kPBz"))
+                w("    " + s_)
             w("#define RR(i) rs[(i) * rstride]")
             ket_blocks(LA, LB, LC, LD, cds, w)
             w("#undef RR")
@@ -243,17 +250,13 @@ def gen_class(LA, LB, LC, LD, idx):
     w("{")
     w("    (void)rs; (void)rstride;")
     r_prologue(L, rsm, w)
-    for s_ in e_tables(LA, LB, LC, LD):
-        w("    " + s_)
     if chunked:
-        w(f"    double eb[{len(ebn)}], ek[{len(ekn)}];")
-        for k, nm in enumerate(ebn):
-            w(f"    eb[{k}] = {nm};")
-        for k, nm in enumerate(ekn):
-            w(f"    ek[{k}] = {nm};")
         for fn in chunk_names:
-            w(f"    {fn}(rs, rstride, eb, ek, lambda, sink);")
+            w(f"    {fn}<Sink>(rs, rstride, a12b, ab.PAx, ab.PAy, ab.PAz, ab.PBx, ab.PBy, ab.PBz, a12k, cd.PAx, cd.PAy, "
+              f"cd.PAz, cd.PBx, cd.PBy, cd.PBz, lambda, sink);")
     else:
+        for s_ in e_tables(LA, LB, LC, LD):
+            w("    " + s_)
         ket_blocks(LA, LB, LC, LD, all_cds, w)
     w("#undef RR")
     w("}")

@@ -148,4 +148,17 @@ __device__ __forceinline__ PrimPairData make_prim_pair(double a, double ax, doub
     return d;
 }
 
+// how a sink is handed to a __noinline__ chunk function: by reference unless the sink says it is a
+// stateless value (a pointer wrapper), which then travels in registers
+template <class Sink, class = void>
+struct SinkArg
+{
+    using type = Sink&;
+};
+template <class Sink>
+struct SinkArg<Sink, decltype((void)Sink::kByValue)>
+{
+    using type = Sink;
+};
+
 }   // namespace qcg

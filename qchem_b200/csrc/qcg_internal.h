@@ -49,12 +49,17 @@ struct JKWorkDev
 };
 
 // launchers, one object file per quartet class (eri_class.cu compiled with -DQCG_CLASS=k)
-using EriBatchLauncher = void (*)(const BasisDev&, const int4*, long long, double*, const double*, cudaStream_t, int);
+using EriBatchLauncher = void (*)(const BasisDev&, const int4*, const int*, long long, double*, const double*,
+                                  cudaStream_t, int);
 using JKLauncher = void (*)(const JKWorkDev&, const PairListDev&, const PairListDev&, const PrimPairsDev&, const int*,
                             const double*, double*, double*, int, const double*, cudaStream_t, int);
 using SchwarzLauncher = void (*)(const PairListDev&, const PrimPairsDev&, double*, const double*, cudaStream_t);
 
 extern const EriBatchLauncher kEriBatchLaunchers[kNumQuartetClasses];
+
+// counting sort of a quartet batch by contraction pattern -> order (a permutation of 0..nq-1)
+void launch_pattern_sort(const BasisDev& bs, const int4* quartets, long long nq, unsigned char* key, int* hist,
+                         int* cursor, int* order, cudaStream_t st, int nsm);
 extern const JKLauncher kJKLaunchers[kNumQuartetClasses];
 extern const SchwarzLauncher kSchwarzLaunchers[kNumPairClasses];
 

@@ -4,7 +4,8 @@
 namespace qcg {
 
 #define QCG_DECL(k)                                                                                          \
-    void launch_eri_batch_##k(const BasisDev&, const int4*, long long, double*, const double*, cudaStream_t, int); \
+    void launch_eri_batch_##k(const BasisDev&, const int4*, const int*, long long, double*, const double*,          \
+                              cudaStream_t, int);                                                                   \
     void launch_jk_##k(const JKWorkDev&, const PairListDev&, const PairListDev&, const PrimPairsDev&, const int*,    \
                        const double*, double*, double*, int, const double*, cudaStream_t, int);                      \
     void launch_schwarz_##k(const PairListDev&, const PrimPairsDev&, double*, const double*, cudaStream_t);

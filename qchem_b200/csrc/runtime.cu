@@ -118,6 +118,11 @@ struct qcg_handle
     double work_flops = 0;
     std::vector<double> Qfull;
 
+    // ERI-batch scratch: contraction-pattern keys, bucket counters and the visiting order (grow only)
+    long long sort_cap = 0;
+    unsigned char* d_key = nullptr;
+    int *d_order = nullptr, *d_hist = nullptr, *d_cursor = nullptr;
+
     // J/K buffers
     double *d_D = nullptr, *d_Jp = nullptr, *d_Kp = nullptr, *d_J = nullptr, *d_K = nullptr;
     int* d_flag = nullptr;
@@ -613,6 +618,24 @@ void jk_device(qcg_handle* h, const double* dD, double* dJ, double* dK, int flag
     }
 }
 
+// grouped visiting order of a batch (returns the device permutation)
+const int* batch_order(qcg_handle* h, const int* d_quartets, long long nq)
+{
+    require(nq <= 0x7fffffffLL, "at most 2^31-1 quartets per batch");
+    if (nq > h->sort_cap)
+    {
+        if (h->d_key) { h->release(h->d_key); h->release(h->d_order); }
+        if (!h->d_hist) { h->d_hist = h->alloc<int>(256); h->d_cursor = h->alloc<int>(256); }
+        h->d_key = h->alloc<unsigned char>(nq);
+        h->d_order = h->alloc<int>(nq);
+        h->sort_cap = nq;
+    }
+    launch_pattern_sort(h->bs, (const int4*)d_quartets, nq, h->d_key, h->d_hist, h->d_cursor, h->d_order, h->stream,
+                        h->nsm);
+    CK(cudaGetLastError());
+    return h->d_order;
+}
+
 int class_index(int la, int lb, int lc, int ld)
 {
     if (la < lb || lc < ld || la > kMaxL || lc > kMaxL || lb < 0 || ld < 0) return -1;
@@ -755,7 +778,8 @@ int qcg_eri_batch_device(qcg_handle* h, int la, int lb, int lc, int ld, long lon
         require(nq >= 0, "negative quartet count");
         if (nq == 0) return;
         require(d_quartets && d_out, "null argument");
-        kEriBatchLaunchers[k](h->bs, (const int4*)d_quartets, nq, d_out, h->d_boys, h->stream, h->nsm);
+        const int* order = batch_order(h, d_quartets, nq);
+        kEriBatchLaunchers[k](h->bs, (const int4*)d_quartets, order, nq, d_out, h->d_boys, h->stream, h->nsm);
         CK(cudaGetLastError());
     });
 }
@@ -788,7 +812,8 @@ int qcg_eri_batch(qcg_handle* h, int la, int lb, int lc, int ld, long long nq, c
             {
                 const long long m = std::min(chunk, nq - q0);
                 CK(cudaMemcpyAsync(dq, quartets + 4 * q0, 4 * m * sizeof(int), cudaMemcpyHostToDevice, h->stream));
-                kEriBatchLaunchers[k](h->bs, (const int4*)dq, m, dout, h->d_boys, h->stream, h->nsm);
+                const int* order = batch_order(h, dq, m);
+                kEriBatchLaunchers[k](h->bs, (const int4*)dq, order, m, dout, h->d_boys, h->stream, h->nsm);
                 CK(cudaGetLastError());
                 CK(cudaMemcpyAsync(out + q0 * blk, dout, m * blk * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
             }
