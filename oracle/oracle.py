@@ -37,6 +37,8 @@ def lib():
         L.orc_jk_direct.argtypes = [vp, P(f64), P(f64), P(f64), f64, i32]
         L.orc_jk_direct.restype = i64
         L.orc_jk_eri4.argtypes = [vp, P(f64), P(f64), P(f64)]
+        L.orc_jk_direct_shard.argtypes = [vp, P(f64), P(f64), P(f64), f64, i32, i32, i32]
+        L.orc_jk_direct_shard.restype = i64
         L.orc_rhf.argtypes = [vp, i32, P(f64), P(f64), i32, i32, f64, f64, i32, i32, P(f64), P(i32), P(f64),
                               P(f64)]
         L.orc_rhf.restype = i32
@@ -122,6 +124,14 @@ class OracleBasis:
         J, K = np.zeros((n, n)), np.zeros((n, n))
         cnt = lib().orc_jk_direct(self.h, _p(D), _p(J), _p(K), float(thresh), int(nthreads))
         return J, K, cnt
+
+    def jk_direct_shard(self, D, rank, world, thresh=1e-10, nthreads=0):
+        """Share of one rank in a world-way split of the bra shell pairs (ij % world == rank)."""
+        n = self.nbf
+        D = np.ascontiguousarray(D, dtype=np.float64)
+        J, K = np.zeros((n, n)), np.zeros((n, n))
+        lib().orc_jk_direct_shard(self.h, _p(D), _p(J), _p(K), float(thresh), int(nthreads), int(rank), int(world))
+        return J, K
 
     def jk_eri4(self, D):
         n = self.nbf

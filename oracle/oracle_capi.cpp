@@ -166,8 +166,10 @@ void digest(const Basis& bs, int sa, int sb, int sc, int sd, const double* v, do
                 }
 }
 
+// rank/world: this call evaluates only bra shell pairs ij with ij % world == rank (a multi-rank share);
+// the sum over all ranks is the full build
 long long jk_direct(const Basis& bs, const std::vector<double>& Q, const double* D, double* Jout, double* Kout,
-                    double thresh, int nthreads)
+                    double thresh, int nthreads, int rank = 0, int world = 1)
 {
     const int ns = bs.shells.size(), n = bs.nbf;
     std::vector<std::pair<int, int>> pairs;
@@ -183,6 +185,7 @@ long long jk_direct(const Basis& bs, const std::vector<double>& Q, const double*
 #pragma omp for schedule(dynamic, 1)
         for (long long ij = np - 1; ij >= 0; --ij)
         {
+            if (ij % world != rank) continue;
             auto [a, b] = pairs[ij];
             for (long long kl = 0; kl <= ij; ++kl)
             {
@@ -406,6 +409,13 @@ long long orc_jk_direct(void* h, const double* D, double* J, double* K, double t
     auto* o = (OBasis*)h;
     if (o->Q.empty()) o->Q = schwarz(o->bs);
     return jk_direct(o->bs, o->Q, D, J, K, thresh, nthreads);
+}
+long long orc_jk_direct_shard(void* h, const double* D, double* J, double* K, double thresh, int nthreads, int rank,
+                              int world)
+{
+    auto* o = (OBasis*)h;
+    if (o->Q.empty()) o->Q = schwarz(o->bs);
+    return jk_direct(o->bs, o->Q, D, J, K, thresh, nthreads, rank, world);
 }
 void orc_jk_eri4(void* h, const double* D, double* J, double* K)
 {
