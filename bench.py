@@ -173,7 +173,12 @@ def main():
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--ref-sample", type=int, default=2000)
     ap.add_argument("--cpu-sample", type=int, default=1000)
+    ap.add_argument("--workload", default="eri", choices=["eri", "fock_config3", "rhf_config1"],
+                    help="eri: the headline ERI microbenchmark; fock_config3: one direct J/K build of the "
+                         "32-water cluster per step; rhf_config1: one water RHF to convergence per step")
     args = ap.parse_args()
+    if args.workload != "eri":
+        return run_secondary(args)
 
     from qchem_b200.parallel import dist_env, max_over_ranks
     rank, world, local = dist_env()
@@ -336,6 +341,74 @@ def main():
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def run_secondary(args):
+    """Secondary workloads on one GPU: the config-3 Fock build or the config-1 RHF, each as a step."""
+    import torch
+    from qchem_b200 import api, basis as B, workloads as W
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    peak_tf, _ = api.measure_fp64_peak(20)
+    if args.workload == "fock_config3":
+        mol = W.water_cluster()
+        sh = B.even_tempered(mol)
+        eng = api.Engine(sh)
+        eng.set_stream(stream.cuda_stream)
+        eng.schwarz(1e-10)
+        Dh = W.cluster_density(B.nbf(sh))
+        D = torch.tensor(Dh, device="cuda")
+        J, K = torch.empty_like(D), torch.empty_like(D)
+        for _ in range(args.warmup):
+            st = eng.fock_jk_device(D.data_ptr(), J.data_ptr(), K.data_ptr())
+        torch.cuda.synchronize()
+        clocks = ClockSampler(0)
+        clocks.start()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            st = eng.fock_jk_device(D.data_ptr(), J.data_ptr(), K.data_ptr())
+        e1.record(stream)
+        torch.cuda.synchronize()
+        clk = clocks.stop()
+        ms = e0.elapsed_time(e1) / args.steps
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            eng.fock_jk(Dh)
+        e2e_s = (time.perf_counter() - t0) / args.steps
+        n = B.nbf(sh)
+        tf = st.flops / (ms * 1e-3) / 1e12
+        line = {"metric": "direct J/K Fock build, shell quartets/s (32-water cluster, N=1824)",
+                "value": st.quartets / (ms * 1e-3), "unit": "quartets/s", "n_gpus": 1, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": "fock_jk_water32_even_tempered", "nbf": n, "schwarz": 1e-10,
+                           "quartets": st.quartets, "prim_quartets": st.prim_quartets},
+                "gpu_launches": 24 * args.steps, "clocks": clk,
+                "roofline": {"bound": "fp64", "achieved": tf, "peak": peak_tf, "unit": "TFLOP/s", "frac": tf / peak_tf,
+                             "traffic": None, "kernel": "jk_kernel (all classes)",
+                             "peak_source": "measured here: library DFMA probe"},
+                "e2e": {"value": st.quartets / e2e_s, "unit": "quartets/s", "h2d_bytes_per_step": 8 * n * n,
+                        "d2h_bytes_per_step": 16 * n * n}}
+    else:
+        mol = W.water()
+        sh = B.even_tempered(mol)
+        for _ in range(args.warmup):
+            api.Engine(sh).rhf(mol)
+        walls, res = [], None
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            res = api.Engine(sh).rhf(mol)
+            walls.append(time.perf_counter() - t0)
+        wall = sum(walls) / len(walls)
+        line = {"metric": "RHF time-to-solution (water, even-tempered 57 functions, dE < 1e-10)", "value": wall,
+                "unit": "s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall,
+                "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "config": {"workload": "rhf_water_config1", "energy": res["energy"],
+                                                 "iterations": res["iterations"], "fock_ms": res["fock_ms"]},
+                "e2e": {"value": wall, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
 
 
 def extras(torch, dev):

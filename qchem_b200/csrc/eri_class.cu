@@ -28,13 +28,14 @@ struct Cls
 {
     static constexpr int LA = kPairLA[kX], LB = kPairLB[kX], LC = kPairLA[kY], LD = kPairLB[kY];
     static constexpr bool kRShared = gen::QCG_CAT(kRShared, QCG_CLASS);
+    static constexpr bool kChunked = gen::QCG_CAT(kChunked, QCG_CLASS);
     static constexpr int kRSize = gen::QCG_CAT(kRSize, QCG_CLASS);
-    template <class Sink>
+    template <class Sink, bool LOCKSTEP = false>
     static __device__ __forceinline__ void quartet(const PrimPairData& ab, const PrimPairData& cd,
                                                    const double* __restrict__ bt, double* __restrict__ rs, int stride,
                                                    Sink& sink)
     {
-        gen::QCG_CAT(prim_quartet_, QCG_CLASS)(ab, cd, bt, rs, stride, sink);
+        gen::QCG_CAT(prim_quartet_, QCG_CLASS)<Sink, LOCKSTEP>(ab, cd, bt, rs, stride, sink);
     }
 };
 
@@ -59,13 +60,36 @@ long long grid_for(long long work, int nsm)
 }
 }   // namespace
 
+// chunked classes: 128-thread blocks in lock step (one chunk of code in flight per block)
+constexpr int kLockThreads = 128;
+constexpr size_t kLockSmem = (size_t)kLockThreads * Cls::kRSize * sizeof(double);
+
+// lock step measured faster for every chunked class except (dd|dd), whose 169 KB per 128-thread block
+// leaves no room for a second block (ERI microbenchmark, 10^6 quartets per class)
+constexpr bool kUseLockstep = Cls::kChunked && QCG_CLASS != 20;
+
 void QCG_CAT(launch_eri_batch_, QCG_CLASS)(const BasisDev& bs, const int4* q, const int* order, long long nq,
                                            double* out, const double* boys, cudaStream_t st, int nsm)
 {
     if (nq <= 0) return;
-    auto k = eri_batch_kernel<Cls, kThreads>;
-    prepare(k);
-    k<<<(unsigned)grid_for(nq, nsm), kThreads, kSmem, st>>>(bs, q, order, nq, out, boys);
+    if constexpr (kUseLockstep)
+    {
+        auto k = eri_batch_lockstep_kernel<Cls, kLockThreads>;
+        static bool done = false;
+        if (!done && kLockSmem > 48 * 1024)
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLockSmem);
+        done = true;
+        long long blocks = (nq + kLockThreads - 1) / kLockThreads;
+        const long long cap = (long long)nsm * 2;
+        if (blocks > cap) blocks = cap;
+        k<<<(unsigned)blocks, kLockThreads, kLockSmem, st>>>(bs, q, order, nq, out, boys);
+    }
+    else
+    {
+        auto k = eri_batch_kernel<Cls, kThreads>;
+        prepare(k);
+        k<<<(unsigned)grid_for(nq, nsm), kThreads, kSmem, st>>>(bs, q, order, nq, out, boys);
+    }
 }
 
 void QCG_CAT(launch_jk_, QCG_CLASS)(const JKWorkDev& w, const PairListDev& bra, const PairListDev& ket,

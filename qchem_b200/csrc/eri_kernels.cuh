@@ -34,7 +34,23 @@ __device__ __forceinline__ PrimPairData shell_prim_pair(const BasisDev& bs, int 
                           bs.alpha[pb], bs.cen[3 * sb], bs.cen[3 * sb + 1], bs.cen[3 * sb + 2], bs.coef[pb]);
 }
 
-// dynamic shared memory holding the per-thread R tables of classes with L >= 6
+// the same with a per-thread switch: lanes that only keep a block in step write nothing
+template <int LB, int LC, int LD>
+struct MaskedStoreSink
+{
+    static constexpr bool kByValue = true;
+    double* o;
+    bool active;
+    static constexpr int NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+    __device__ __forceinline__ void ket_begin(int, int) {}
+    __device__ __forceinline__ void ket_end(int, int) {}
+    __device__ __forceinline__ void operator()(int ia, int ib, int ic, int id, double v)
+    {
+        if (active) atomicAdd(o + ((ia * NB + ib) * NC + ic) * ND + id, v);
+    }
+};
+
+// dynamic shared memory holding the per-thread R tables of classes with L >= 6 or chunked code
 extern __shared__ double qcg_smem[];
 
 // Quartets are visited through `order` (a permutation grouping equal contraction patterns, so that the
@@ -62,6 +78,51 @@ __global__ void __launch_bounds__(THREADS) eri_batch_kernel(BasisDev bs, const i
             const PrimPairData ab = shell_prim_pair(bs, s.x, ij / nj, s.y, ij % nj);
             const PrimPairData cd = shell_prim_pair(bs, s.z, kl / nl, s.w, kl % nl);
             Cls::quartet(ab, cd, boys_table, rs, THREADS, sink);
+        }
+    }
+}
+
+// Block-synchronous variant for the classes whose code is split into chunks: the block takes the sorted
+// quartets in rounds of THREADS, every thread runs the block's largest primitive count (surplus
+// iterations are masked), so all threads reach every barrier inside Cls::quartet<..., true> and the
+// block's warps walk the chunk code together.
+template <class Cls, int THREADS>
+__global__ void __launch_bounds__(THREADS) eri_batch_lockstep_kernel(BasisDev bs, const int4* __restrict__ quartets,
+                                                                     const int* __restrict__ order, long long nq,
+                                                                     double* __restrict__ out,
+                                                                     const double* __restrict__ boys_table)
+{
+    constexpr long long BLK = (long long)ncart(Cls::LA) * ncart(Cls::LB) * ncart(Cls::LC) * ncart(Cls::LD);
+    __shared__ int s_nmax;
+    double* rs = qcg_smem + threadIdx.x;
+    for (long long base = (long long)blockIdx.x * THREADS; base < nq; base += (long long)gridDim.x * THREADS)
+    {
+        const long long g = base + threadIdx.x;
+        const bool valid = g < nq;
+        const long long gq = valid ? g : base;   // idle lanes shadow the round's first quartet
+        const long long q = order ? order[gq] : gq;
+        const int4 s = quartets[q];
+        double* o = out + q * BLK;
+        if (valid)
+            for (int k = 0; k < (int)BLK; ++k) o[k] = 0.0;
+        const int ni = bs.nprim[s.x], nj = bs.nprim[s.y], nk = bs.nprim[s.z], nl = bs.nprim[s.w];
+        const int nket = nk * nl, ntot = ni * nj * nket;
+        if (threadIdx.x == 0) s_nmax = 0;
+        __syncthreads();
+        atomicMax(&s_nmax, ntot);
+        __syncthreads();
+        const int nmax = s_nmax;
+        __syncthreads();
+        MaskedStoreSink<Cls::LB, Cls::LC, Cls::LD> sink{o, false};
+        for (int x = 0; x < nmax; ++x)
+        {
+            const int xx = x < ntot ? x : 0;
+            sink.active = valid && x < ntot;
+            const int ij = xx / nket, kl = xx - ij * nket;
+            const PrimPairData ab = shell_prim_pair(bs, s.x, ij / nj, s.y, ij % nj);
+            const PrimPairData cd = shell_prim_pair(bs, s.z, kl / nl, s.w, kl % nl);
+            Cls::template quartet<MaskedStoreSink<Cls::LB, Cls::LC, Cls::LD>, true>(ab, cd, boys_table, rs, THREADS,
+                                                                                   sink);
         }
     }
 }

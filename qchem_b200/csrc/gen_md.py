@@ -218,6 +218,7 @@ def gen_class(LA, LB, LC, LD, idx):
       f"{'a per-thread slice of shared memory' if rsm else 'registers'}"
       f"{'; ket components split into __noinline__ chunks' if chunked else ''}")
     w(f"constexpr bool kRShared{idx} = {'true' if rsm else 'false'};")
+    w(f"constexpr bool kChunked{idx} = {'true' if chunked else 'false'};")
     w(f"constexpr int kRSize{idx} = {nherm(L)};")
     chunk_names = []
     if chunked:
@@ -244,7 +245,10 @@ def gen_class(LA, LB, LC, LD, idx):
             ket_blocks(LA, LB, LC, LD, cds, w)
             w("#undef RR")
             w("}")
-    w("template <class Sink>")
+    # LOCKSTEP: the caller guarantees that every thread of the block executes this call (block-uniform
+    # control flow); the barriers then keep the block's warps on the same chunk, so that the instruction
+    # working set is one chunk rather than the whole class
+    w("template <class Sink, bool LOCKSTEP = false>")
     w(f"__device__ __forceinline__ void prim_quartet_{idx}(const PrimPairData& ab, const PrimPairData& cd,")
     w("    const double* __restrict__ bt, double* __restrict__ rs, const int rstride, Sink& sink)")
     w("{")
@@ -252,6 +256,7 @@ def gen_class(LA, LB, LC, LD, idx):
     r_prologue(L, rsm, w)
     if chunked:
         for fn in chunk_names:
+            w("    if constexpr (LOCKSTEP) __syncthreads();")
             w(f"    {fn}<Sink>(rs, rstride, a12b, ab.PAx, ab.PAy, ab.PAz, ab.PBx, ab.PBy, ab.PBz, a12k, cd.PAx, cd.PAy, "
               f"cd.PAz, cd.PBx, cd.PBy, cd.PBz, lambda, sink);")
     else:
