@@ -1,0 +1,107 @@
+// qchem_b200.hpp -- header-only C++ adapter over the C ABI (qchem_b200.h) for qchem's HF contraction face.
+//
+// qcg::FockEngine owns one qcg_handle and answers the two questions qchem's Hartree-Fock code asks of a
+// basis with the WholeSystemFock_IBS<double> face (src/BasisSet/Orbital_HF_IBS.C:75-87):
+//   MakeAOFock(Dao, exchange=false) -> J[Dao],  MakeAOFock(Dao, exchange=true) -> K[Dao]
+// and the Orbital_HF_IBS<double> contraction face (src/BasisSet/Orbital_HF_IBS.C:33-54) for a basis that is
+// one irrep: AccumulateDirect(S, D) adds J[D], AccumulateExchange(S, D) adds K[D].  qchem calls the
+// Coulomb and the exchange face separately with the same density (Vee then Vxc, HF_HT.C:48-70); the
+// engine builds J and K together in one GPU pass and keeps them for the density it last saw, so the
+// second call costs nothing.  Status codes from the C ABI become qcg::Error exceptions here, the way the
+// reference's own substrate throws std::runtime_error (Internal/Imp/Orbital_ERI4_IBS.C:19-32).
+#pragma once
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "qchem_b200.h"
+
+namespace qcg {
+
+struct Error : std::runtime_error
+{
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error("qchem_b200: " + m), code(c) {}
+};
+
+// One shell in basis order: angular momentum 0..2, centre (bohr), exponents and raw contraction coefficients.
+struct ShellSpec
+{
+    int L;
+    double centre[3];
+    std::vector<double> exps, coefs;
+};
+
+class FockEngine
+{
+public:
+    explicit FockEngine(const std::vector<ShellSpec>& shells, double schwarz_thresh = 1e-10)
+    {
+        std::vector<int> L, np;
+        std::vector<double> ex, co, cen;
+        for (const auto& s : shells)
+        {
+            L.push_back(s.L);
+            np.push_back((int)s.exps.size());
+            ex.insert(ex.end(), s.exps.begin(), s.exps.end());
+            co.insert(co.end(), s.coefs.begin(), s.coefs.end());
+            cen.insert(cen.end(), s.centre, s.centre + 3);
+        }
+        int rc = qcg_basis_create(L.data(), np.data(), ex.data(), co.data(), cen.data(), (int)shells.size(), &h_);
+        if (rc != QCG_OK)
+        {
+            std::string msg = h_ ? qcg_last_error(h_) : "qcg_basis_create failed";
+            qcg_destroy(h_);
+            h_ = nullptr;
+            throw Error(rc, msg);
+        }
+        check(qcg_nbf(h_, &n_));
+        check(qcg_schwarz(h_, schwarz_thresh, nullptr));
+    }
+    ~FockEngine() { qcg_destroy(h_); }
+    FockEngine(const FockEngine&) = delete;
+    FockEngine& operator=(const FockEngine&) = delete;
+
+    size_t AODimension() const { return (size_t)n_; }
+
+    // J (exchange=false) or K (exchange=true) of a dense row-major n x n density into out (n x n)
+    void MakeAOFock(const double* Dao, bool exchange, double* out)
+    {
+        build(Dao);
+        const std::vector<double>& X = exchange ? K_ : J_;
+        std::memcpy(out, X.data(), X.size() * sizeof(double));
+    }
+    // S += J[D] and S += K[D] (qchem's AccumulateDirect / AccumulateExchange for a single-irrep basis)
+    void AccumulateDirect(double* S, const double* D) { add(S, D, false); }
+    void AccumulateExchange(double* S, const double* D) { add(S, D, true); }
+
+    qcg_handle* handle() { return h_; }
+
+private:
+    void check(int rc)
+    {
+        if (rc != QCG_OK) throw Error(rc, qcg_last_error(h_));
+    }
+    void build(const double* D)
+    {
+        const size_t nn = (size_t)n_ * n_;
+        if (D_.size() == nn && std::memcmp(D_.data(), D, nn * sizeof(double)) == 0) return;   // same density
+        J_.resize(nn);
+        K_.resize(nn);
+        check(qcg_fock_jk(h_, D, J_.data(), K_.data(), 0, nullptr));
+        D_.assign(D, D + nn);
+    }
+    void add(double* S, const double* D, bool exchange)
+    {
+        build(D);
+        const std::vector<double>& X = exchange ? K_ : J_;
+        for (size_t k = 0; k < X.size(); ++k) S[k] += X[k];
+    }
+
+    qcg_handle* h_ = nullptr;
+    int n_ = 0;
+    std::vector<double> D_, J_, K_;
+};
+
+}   // namespace qcg

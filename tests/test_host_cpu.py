@@ -174,3 +174,22 @@ def test_two_rank_jk_reduction_matches_single_build(oracle_mod):
         assert p.exitcode == 0
     assert t == 2.0
     assert np.abs(J - Jr).max() < 1e-12 and np.abs(K - Kr).max() < 1e-12
+
+
+def test_cpp_adapter_builds_and_fails_loudly_without_a_device(tmp_path):
+    """include/qchem_b200.hpp compiles against the C ABI; without a GPU its constructor throws QCG_ERR_CUDA."""
+    import shutil
+    import subprocess
+    import torch
+    if shutil.which("g++") is None:
+        pytest.skip("no g++")
+    src = tmp_path / "t.cpp"
+    src.write_text('#include "qchem_b200.hpp"\nint main(){std::vector<qcg::ShellSpec> s{{0,{0,0,0},{1.0},{1.0}}};\n'
+                   'try { qcg::FockEngine e(s); return e.AODimension() == 1 ? 0 : 3; }\n'
+                   'catch (const qcg::Error& err) { return err.code == QCG_ERR_CUDA ? 10 : 11; }}\n')
+    libdir = os.path.dirname(api.library_path())
+    exe = tmp_path / "t"
+    subprocess.run(["g++", "-std=c++17", "-I", os.path.join(REPO, "include"), str(src), "-L", libdir, "-lqchem_b200",
+                    f"-Wl,-rpath,{libdir}", "-o", str(exe)], check=True)
+    rc = subprocess.run([str(exe)]).returncode
+    assert rc == (0 if torch.cuda.is_available() else 10)
