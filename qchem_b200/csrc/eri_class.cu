@@ -99,7 +99,11 @@ void QCG_CAT(launch_jk_, QCG_CLASS)(const JKWorkDev& w, const PairListDev& bra, 
     if (w.total <= 0) return;
     auto k = jk_kernel<Cls, kThreads>;
     prepare(k);
-    k<<<(unsigned)grid_for(w.total, nsm), kThreads, kSmem, st>>>(w, bra, ket, P, f0, D, J, K, n, boys);
+    // quartets per lane run: enough threads for the whole GPU first, longer runs only for large builds
+    long long run = w.total / ((long long)nsm * 1024);
+    run = run < 1 ? 1 : (run > 8 ? 8 : run);
+    const long long work = (w.total + run - 1) / run;
+    k<<<(unsigned)grid_for(work, nsm), kThreads, kSmem, st>>>(w, bra, ket, P, f0, D, J, K, n, boys, (int)run);
 }
 
 // Schwarz diagonals exist only for the diagonal classes (X == Y)

@@ -205,8 +205,11 @@ struct JKSink
     double dls, jcd;
     double dbs[NB], das[NA], dbl[NB], dal[NA];
 
-    __device__ __forceinline__ void init()
+    // a new bra pair: J'[a b] partial sums start from zero
+    __device__ __forceinline__ void set_bra(int fa_, int fb_)
     {
+        fa = fa_;
+        fb = fb_;
 #pragma unroll
         for (int k = 0; k < NAB; ++k) jab[k] = 0.0;
 #pragma unroll
@@ -260,25 +263,38 @@ struct JKSink
             for (int k = 0; k < NB; ++k) { atomicAdd(K + (size_t)(fb + k) * n + la, kbc[k]); kbc[k] = 0.0; }
         }
     }
-    __device__ __forceinline__ void finish()
+    // the bra pair is done (or the lane's run ends): flush J'[a b]
+    __device__ __forceinline__ void flush_bra()
     {
 #pragma unroll
         for (int ia = 0; ia < NA; ++ia)
 #pragma unroll
-            for (int ib = 0; ib < NB; ++ib) atomicAdd(J + (size_t)(fa + ia) * n + fb + ib, 2.0 * jab[ia * NB + ib]);
+            for (int ib = 0; ib < NB; ++ib)
+            {
+                const double x = jab[ia * NB + ib];
+                if (x != 0.0) atomicAdd(J + (size_t)(fa + ia) * n + fb + ib, 2.0 * x);
+            }
     }
 };
 
+// Each lane walks RUN quartets spaced one warp apart (g = base + lane + 32 k), so consecutive quartets of a
+// lane usually share the bra pair: the bra pair is found by one binary search per run and then advanced,
+// and the bra-side J' sums stay in registers until the bra pair changes.  RUN is chosen by the launcher
+// from the class's quartet count (1 for small molecules, where parallelism matters more).
 template <class Cls, int THREADS>
 __global__ void __launch_bounds__(THREADS) jk_kernel(JKWorkDev w, PairListDev bra, PairListDev ket, PrimPairsDev P,
                                                      const int* __restrict__ shell_f0, const double* __restrict__ D,
                                                      double* __restrict__ J, double* __restrict__ K, int n,
-                                                     const double* __restrict__ boys_table)
+                                                     const double* __restrict__ boys_table, int RUN)
 {
     double* rs = qcg_smem + threadIdx.x;
-    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < w.total;
-         g += (long long)gridDim.x * blockDim.x)
+    const int lane = threadIdx.x & 31;
+    const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const long long nwarp = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long base = warp * 32 * RUN; base < w.total; base += nwarp * 32 * RUN)
     {
+        long long g = base + lane;
+        if (g >= w.total) continue;
         // bra pair i: offs[i] <= g < offs[i+1]
         int lo = 0, hi = bra.n;
         while (hi - lo > 1)
@@ -287,25 +303,43 @@ __global__ void __launch_bounds__(THREADS) jk_kernel(JKWorkDev w, PairListDev br
             if (w.offs[mid] <= g) lo = mid;
             else hi = mid;
         }
-        const int i = lo;
-        const int j = (int)(g - w.offs[i]);
-        const int sa = bra.sa[i], sb = bra.sb[i], sc = ket.sa[j], sd = ket.sb[j];
+        int i = lo;
+        long long next = w.offs[i + 1];
         JKSink<Cls::LA, Cls::LB, Cls::LC, Cls::LD> sink;
         sink.D = D; sink.J = J; sink.K = K; sink.n = n;
-        sink.fa = shell_f0[sa]; sink.fb = shell_f0[sb]; sink.fc = shell_f0[sc]; sink.fd = shell_f0[sd];
-        sink.s = (sa == sb ? 0.5 : 1.0) * (sc == sd ? 0.5 : 1.0) * ((w.same_class && i == j) ? 0.5 : 1.0);
-        sink.init();
-        const int oi = bra.ppo[i], ni = bra.npp[i], oj = ket.ppo[j], nj = ket.npp[j];
-        for (int x = 0; x < ni; ++x)
+        int sa = bra.sa[i], sb = bra.sb[i];
+        sink.set_bra(shell_f0[sa], shell_f0[sb]);
+        for (int r = 0; r < RUN && g < w.total; ++r, g += 32)
         {
-            const PrimPairData ab = load_pp(P, oi + x);
-            for (int y = 0; y < nj; ++y)
+            if (g >= next)
             {
-                const PrimPairData cd = load_pp(P, oj + y);
-                Cls::quartet(ab, cd, boys_table, rs, THREADS, sink);
+                sink.flush_bra();
+                do
+                {
+                    ++i;
+                    next = w.offs[i + 1];
+                } while (g >= next);
+                sa = bra.sa[i];
+                sb = bra.sb[i];
+                sink.set_bra(shell_f0[sa], shell_f0[sb]);
+            }
+            const int j = (int)(g - w.offs[i]);
+            const int sc = ket.sa[j], sd = ket.sb[j];
+            sink.fc = shell_f0[sc];
+            sink.fd = shell_f0[sd];
+            sink.s = (sa == sb ? 0.5 : 1.0) * (sc == sd ? 0.5 : 1.0) * ((w.same_class && i == j) ? 0.5 : 1.0);
+            const int oi = bra.ppo[i], ni = bra.npp[i], oj = ket.ppo[j], nj = ket.npp[j];
+            for (int x = 0; x < ni; ++x)
+            {
+                const PrimPairData ab = load_pp(P, oi + x);
+                for (int y = 0; y < nj; ++y)
+                {
+                    const PrimPairData cd = load_pp(P, oj + y);
+                    Cls::quartet(ab, cd, boys_table, rs, THREADS, sink);
+                }
             }
         }
-        sink.finish();
+        sink.flush_bra();
     }
 }
 

@@ -127,6 +127,11 @@ struct qcg_handle
     double *d_D = nullptr, *d_Jp = nullptr, *d_Kp = nullptr, *d_J = nullptr, *d_K = nullptr;
     int* d_flag = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
+    // side streams for the class kernels of one build (fork after the accumulators are zeroed, join before
+    // the symmetrisation), so that classes with few quartets run side by side
+    static constexpr int kSide = 6;
+    cudaStream_t side[kSide] = {};
+    cudaEvent_t fork = nullptr, join[kSide] = {};
 
     template <class T>
     T* alloc(size_t count)
@@ -165,6 +170,12 @@ struct qcg_handle
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (ev2) cudaEventDestroy(ev2);
+        if (fork) cudaEventDestroy(fork);
+        for (int k = 0; k < kSide; ++k)
+        {
+            if (join[k]) cudaEventDestroy(join[k]);
+            if (side[k]) cudaStreamDestroy(side[k]);
+        }
         if (own_stream) cudaStreamDestroy(own_stream);
     }
 };
@@ -591,16 +602,35 @@ void jk_device(qcg_handle* h, const double* dD, double* dJ, double* dK, int flag
     CK(cudaMemsetAsync(h->d_Jp, 0, nn * sizeof(double), h->stream));
     CK(cudaMemsetAsync(h->d_Kp, 0, nn * sizeof(double), h->stream));
     CK(cudaEventRecord(h->ev1, h->stream));
-    // heaviest classes first so that the short ones fill the tail
+    if (!h->fork)
+    {
+        CK(cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming));
+        for (int s = 0; s < qcg_handle::kSide; ++s)
+        {
+            CK(cudaStreamCreateWithFlags(&h->side[s], cudaStreamNonBlocking));
+            CK(cudaEventCreateWithFlags(&h->join[s], cudaEventDisableTiming));
+        }
+    }
+    CK(cudaEventRecord(h->fork, h->stream));
+    for (int s = 0; s < qcg_handle::kSide; ++s) CK(cudaStreamWaitEvent(h->side[s], h->fork, 0));
+    // heaviest classes first so that the short ones fill the tail; classes spread over the side streams
+    int slot = 0;
     for (int k = kNumQuartetClasses - 1; k >= 0; --k)
     {
+        if (h->work[k].total <= 0) continue;
         int X = 0;
         while ((X + 1) * (X + 2) / 2 <= k) ++X;
         const int Y = k - X * (X + 1) / 2;
         kJKLaunchers[k](h->work[k], h->pl_dev[X], h->pl_dev[Y], h->pp_dev, h->d_f0, dD, h->d_Jp, h->d_Kp, n, h->d_boys,
-                        h->stream, h->nsm);
+                        h->side[slot], h->nsm);
+        slot = (slot + 1) % qcg_handle::kSide;
     }
     CK(cudaGetLastError());
+    for (int s = 0; s < qcg_handle::kSide; ++s)
+    {
+        CK(cudaEventRecord(h->join[s], h->side[s]));
+        CK(cudaStreamWaitEvent(h->stream, h->join[s], 0));
+    }
     CK(cudaEventRecord(h->ev2, h->stream));
     launch_symmetrize(h->d_Jp, h->d_Kp, dJ, dK, n, h->d_flag, h->stream, h->nsm);
     CK(cudaGetLastError());
