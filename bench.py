@@ -392,21 +392,43 @@ def run_secondary(args):
                 "e2e": {"value": st.quartets / e2e_s, "unit": "quartets/s", "h2d_bytes_per_step": 8 * n * n,
                         "d2h_bytes_per_step": 16 * n * n}}
     else:
+        def solve(mol, sh, steps, warmup, **kw):
+            for _ in range(warmup):
+                api.Engine(sh).rhf(mol, **kw)
+            walls, res = [], None
+            for _ in range(steps):
+                t0 = time.perf_counter()
+                res = api.Engine(sh).rhf(mol, **kw)
+                walls.append(time.perf_counter() - t0)
+            return sum(walls) / len(walls), res
+
         mol = W.water()
         sh = B.even_tempered(mol)
-        for _ in range(args.warmup):
-            api.Engine(sh).rhf(mol)
-        walls, res = [], None
-        for _ in range(args.steps):
-            t0 = time.perf_counter()
-            res = api.Engine(sh).rhf(mol)
-            walls.append(time.perf_counter() - t0)
-        wall = sum(walls) / len(walls)
-        line = {"metric": "RHF time-to-solution (water, even-tempered 57 functions, dE < 1e-10)", "value": wall,
-                "unit": "s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall,
-                "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic", "config": {"workload": "rhf_water_config1", "energy": res["energy"],
-                                                 "iterations": res["iterations"], "fock_ms": res["fock_ms"]},
+        wall, res = solve(mol, sh, args.steps, args.warmup)
+        wall_c, res_c = solve(mol, sh, args.steps, 1, incremental=True)
+        # where the Fock build dominates: 8 waters (2x2x2 jittered grid of 6.5 bohr), 456 functions
+        mol8 = W.water_cluster(nx=2, ny=2, nz=2, spacing=6.5, seed=W.SEED0 + 3400)
+        sh8 = B.even_tempered(mol8)
+        w8, r8 = solve(mol8, sh8, 1, 0)
+        w8c, r8c = solve(mol8, sh8, 1, 0, incremental=True)
+        line = {"metric": "RHF time-to-solution (water, even-tempered 57 functions, dE < 1e-10), plain FP64 GPU",
+                "value": wall, "unit": "s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1e3 * wall, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64", "data": "synthetic",
+                "config": {"workload": "rhf_water_config1", "energy": res["energy"], "iterations": res["iterations"],
+                           "fock_ms": res["fock_ms"]},
+                "chosen_form": {"water_config1": {"wall_s": wall_c, "energy": res_c["energy"],
+                                                  "abs_diff_vs_plain_eh": abs(res_c["energy"] - res["energy"]),
+                                                  "full_builds": res_c["full_builds"],
+                                                  "incremental_builds": res_c["incremental_builds"],
+                                                  "speedup_vs_plain": wall / wall_c},
+                                "water8_456fn": {"plain_wall_s": w8, "chosen_wall_s": w8c,
+                                                 "plain_energy": r8["energy"], "chosen_energy": r8c["energy"],
+                                                 "abs_diff_eh": abs(r8c["energy"] - r8["energy"]),
+                                                 "plain_fock_ms": r8["fock_ms"], "chosen_fock_ms": r8c["fock_ms"],
+                                                 "iterations": [r8["iterations"], r8c["iterations"]],
+                                                 "converged": [r8["converged"], r8c["converged"]],
+                                                 "speedup_vs_plain": w8 / w8c}},
                 "e2e": {"value": wall, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 

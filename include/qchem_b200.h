@@ -63,6 +63,13 @@ typedef struct qcg_scf_params {
     int diis_nproj;           /* default 4 */
     double diis_fdmax;        /* <= 0: Z^2 * 0.1 / 32 (Calculation.C default) */
     double diis_svtol;        /* default 5e-9 */
+    int incremental;          /* 0 (default): full FP64 J/K every iteration.  1: after a full build, build
+                                 J[D_k - D_k-1], K[...] with density-weighted Schwarz screening and add them
+                                 to the previous J, K; full rebuild every rebuild_every iterations and once
+                                 more on convergence (the reported energy is from a full build) */
+    double inc_thresh;        /* skip a quartet of an incremental build when Q_ab Q_cd max|dD| < inc_thresh
+                                 (default 1e-11) */
+    int rebuild_every;        /* default 8 */
 } qcg_scf_params;
 
 typedef struct qcg_scf_result {
@@ -73,6 +80,8 @@ typedef struct qcg_scf_result {
     double fd_error;          /* final ||[F',D']|| */
     double wall_s;            /* host wall time of qcg_rhf */
     double fock_ms;           /* summed device time of the J/K builds */
+    int full_builds;          /* J/K builds from the full density */
+    int incremental_builds;   /* J/K builds from a density difference */
 } qcg_scf_result;
 
 /* ---- lifetime -------------------------------------------------------------------------------- */

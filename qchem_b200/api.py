@@ -51,13 +51,14 @@ class Stats(ctypes.Structure):
 class ScfParams(ctypes.Structure):
     _fields_ = [("max_iter", ctypes.c_int), ("de_tol", ctypes.c_double), ("fd_tol", ctypes.c_double),
                 ("schwarz_thresh", ctypes.c_double), ("diis_nproj", ctypes.c_int), ("diis_fdmax", ctypes.c_double),
-                ("diis_svtol", ctypes.c_double)]
+                ("diis_svtol", ctypes.c_double), ("incremental", ctypes.c_int), ("inc_thresh", ctypes.c_double),
+                ("rebuild_every", ctypes.c_int)]
 
 
 class ScfResult(ctypes.Structure):
     _fields_ = [("energy", ctypes.c_double), ("e_nuc", ctypes.c_double), ("iterations", ctypes.c_int),
                 ("converged", ctypes.c_int), ("fd_error", ctypes.c_double), ("wall_s", ctypes.c_double),
-                ("fock_ms", ctypes.c_double)]
+                ("fock_ms", ctypes.c_double), ("full_builds", ctypes.c_int), ("incremental_builds", ctypes.c_int)]
 
 
 def library_path() -> str:
@@ -225,10 +226,13 @@ class Engine:
         return S, T, V
 
     def rhf(self, mol: _basis.Molecule, max_iter=100, de_tol=1e-10, fd_tol=1e-5, schwarz_thresh=1e-10,
-            want_density=False):
+            want_density=False, incremental=False, inc_thresh=1e-11, rebuild_every=8):
+        """RHF to convergence.  incremental=True: density-difference J/K builds with density-weighted
+        screening between full builds (the energy on exit is always from a full build)."""
         prm = ScfParams()
         lib().qcg_scf_default_params(ctypes.byref(prm))
         prm.max_iter, prm.de_tol, prm.fd_tol, prm.schwarz_thresh = max_iter, de_tol, fd_tol, schwarz_thresh
+        prm.incremental, prm.inc_thresh, prm.rebuild_every = int(incremental), float(inc_thresh), int(rebuild_every)
         res = ScfResult()
         Z = _f64(mol.Z)
         R = _f64(mol.R).reshape(-1)
@@ -240,7 +244,7 @@ class Engine:
         self._screen = schwarz_thresh
         out = {"energy": res.energy, "e_nuc": res.e_nuc, "iterations": res.iterations,
                "converged": bool(res.converged), "fd_error": res.fd_error, "wall_s": res.wall_s,
-               "fock_ms": res.fock_ms}
+               "fock_ms": res.fock_ms, "full_builds": res.full_builds, "incremental_builds": res.incremental_builds}
         if D is not None:
             out["D"] = D
         return out

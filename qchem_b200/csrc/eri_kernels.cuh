@@ -325,6 +325,15 @@ __global__ void __launch_bounds__(THREADS) jk_kernel(JKWorkDev w, PairListDev br
             }
             const int j = (int)(g - w.offs[i]);
             const int sc = ket.sa[j], sd = ket.sb[j];
+            if (w.dmax)
+            {
+                const double* M = w.dmax;
+                const int ns = w.nshell;
+                double m = fmax(M[sa * ns + sb], M[sc * ns + sd]);
+                m = fmax(m, fmax(M[sa * ns + sc], M[sa * ns + sd]));
+                m = fmax(m, fmax(M[sb * ns + sc], M[sb * ns + sd]));
+                if (bra.Q[i] * ket.Q[j] * m < w.dthr) continue;
+            }
             sink.fc = shell_f0[sc];
             sink.fd = shell_f0[sd];
             sink.s = (sa == sb ? 0.5 : 1.0) * (sc == sd ? 0.5 : 1.0) * ((w.same_class && i == j) ? 0.5 : 1.0);

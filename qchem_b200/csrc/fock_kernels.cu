@@ -99,6 +99,28 @@ void launch_pattern_sort(const BasisDev& bs, const int4* quartets, long long nq,
     pattern_scatter_kernel<<<(unsigned)blocks, 256, 0, st>>>(key, nq, cursor, order);
 }
 
+// dmax[a*nshell+b] = max |D_mu nu| over mu in shell a, nu in shell b
+__global__ void block_max_kernel(const double* __restrict__ D, const int* __restrict__ f0, const int* __restrict__ L,
+                                 int nshell, int n, double* __restrict__ dmax)
+{
+    const long long total = (long long)nshell * nshell;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total; k += (long long)gridDim.x * blockDim.x)
+    {
+        const int a = (int)(k / nshell), b = (int)(k % nshell);
+        const int na = (L[a] + 1) * (L[a] + 2) / 2, nb = (L[b] + 1) * (L[b] + 2) / 2;
+        double m = 0.0;
+        for (int i = 0; i < na; ++i)
+            for (int j = 0; j < nb; ++j) m = fmax(m, fabs(D[(long long)(f0[a] + i) * n + f0[b] + j]));
+        dmax[k] = m;
+    }
+}
+
+void launch_block_max(const double* D, const int* shell_f0, const int* shell_L, int nshell, int n, double* dmax,
+                      cudaStream_t st, int nsm)
+{
+    block_max_kernel<<<nsm * 4, 256, 0, st>>>(D, shell_f0, shell_L, nshell, n, dmax);
+}
+
 void launch_validate(const double* D, int n, double tol, int* flag, cudaStream_t st, int nsm)
 {
     validate_density_kernel<<<nsm * 4, 256, 0, st>>>(D, n, tol, flag);

@@ -38,6 +38,7 @@ struct PairListDev
     const int* sb;
     const int* ppo;
     const int* npp;
+    const double* Q;   // Schwarz bound of each pair (same order)
 };
 
 // flattened canonical quartets of one quartet class: bra pair i owns quartets offs[i] .. offs[i+1)
@@ -46,7 +47,15 @@ struct JKWorkDev
     long long total;
     const long long* offs;
     int same_class;
+    // density screening of an incremental build: skip a quartet when
+    // Q_ab Q_cd max(|D| over its six digestion blocks) < dthr; dmax[a*nshell+b] = max |D| of block (a,b)
+    const double* dmax;
+    int nshell;
+    double dthr;
 };
+
+void launch_block_max(const double* D, const int* shell_f0, const int* shell_L, int nshell, int n, double* dmax,
+                      cudaStream_t st, int nsm);
 
 // launchers, one object file per quartet class (eri_class.cu compiled with -DQCG_CLASS=k)
 using EriBatchLauncher = void (*)(const BasisDev&, const int4*, const int*, long long, double*, const double*,

@@ -490,7 +490,7 @@ void build_screening(qcg_handle* h, double thresh)
         int* dppo = h->upload(ppo[c]);
         int* dnpp = h->upload(npp[c]);
         double* dQ = h->alloc<double>(n);
-        PairListDev pl{n, dsa, dsb, dppo, dnpp};
+        PairListDev pl{n, dsa, dsb, dppo, dnpp, nullptr};
         kSchwarzLaunchers[c](pl, P0, dQ, h->d_boys, h->stream);
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(Qc[c].data(), dQ, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
@@ -532,7 +532,7 @@ void build_screening(qcg_handle* h, double thresh)
     {
         const int n = (int)h->pl_sa[c].size();
         h->pl_dev[c] = PairListDev{n, h->upload(h->pl_sa[c]), h->upload(h->pl_sb[c]), h->upload(h->pl_ppo[c]),
-                                   h->upload(h->pl_npp[c])};
+                                   h->upload(h->pl_npp[c]), h->upload(h->pl_Q[c])};
     }
     // work lists: bra pair i of class X against the prefix of class Y with Q_i Q_j >= thresh
     h->work_quartets = 0;
@@ -576,7 +576,8 @@ void build_screening(qcg_handle* h, double thresh)
     h->screened = true;
 }
 
-void jk_device(qcg_handle* h, const double* dD, double* dJ, double* dK, int flags, qcg_stats* stats)
+void jk_device(qcg_handle* h, const double* dD, double* dJ, double* dK, int flags, qcg_stats* stats,
+               const double* dmax = nullptr, double dthr = 0.0)
 {
     require(h->screened, "qcg_schwarz must be called before qcg_fock_jk", QCG_ERR_STATE);
     ensure_jk_buffers(h);
@@ -621,7 +622,11 @@ void jk_device(qcg_handle* h, const double* dD, double* dJ, double* dK, int flag
         int X = 0;
         while ((X + 1) * (X + 2) / 2 <= k) ++X;
         const int Y = k - X * (X + 1) / 2;
-        kJKLaunchers[k](h->work[k], h->pl_dev[X], h->pl_dev[Y], h->pp_dev, h->d_f0, dD, h->d_Jp, h->d_Kp, n, h->d_boys,
+        JKWorkDev wk = h->work[k];
+        wk.dmax = dmax;
+        wk.nshell = h->nshell;
+        wk.dthr = dthr;
+        kJKLaunchers[k](wk, h->pl_dev[X], h->pl_dev[Y], h->pp_dev, h->d_f0, dD, h->d_Jp, h->d_Kp, n, h->d_boys,
                         h->side[slot], h->nsm);
         slot = (slot + 1) % qcg_handle::kSide;
     }
@@ -872,7 +877,8 @@ int qcg_schwarz(qcg_handle* h, double thresh, double* Q)
             {
                 for (int c = 0; c < kNumPairClasses; ++c)
                     for (const void* p : {(const void*)h->pl_dev[c].sa, (const void*)h->pl_dev[c].sb,
-                                          (const void*)h->pl_dev[c].ppo, (const void*)h->pl_dev[c].npp})
+                                          (const void*)h->pl_dev[c].ppo, (const void*)h->pl_dev[c].npp,
+                                          (const void*)h->pl_dev[c].Q})
                         h->release((void*)p);
                 const PrimPairsDev& P = h->pp_dev;
                 for (const double* p : {P.p, P.Px, P.Py, P.Pz, P.PAx, P.PAy, P.PAz, P.PBx, P.PBy, P.PBz, P.K})
@@ -962,6 +968,9 @@ void qcg_scf_default_params(qcg_scf_params* p)
     p->diis_nproj = 4;
     p->diis_fdmax = 0.0;
     p->diis_svtol = 5e-9;
+    p->incremental = 0;
+    p->inc_thresh = 1e-11;
+    p->rebuild_every = 8;
 }
 
 // Closed-shell SCF (SCFIterator.C:283-362 loop; DIIS gating/pruning per SCFAcceleratorDIIS.C:35-238)
@@ -1038,17 +1047,47 @@ int qcg_rhf(qcg_handle* h, int natom, const double* Z, const double* R, int nele
         diag_fill(Fp);   // core guess
         std::deque<std::vector<double>> Es, Fps;
         std::vector<double> J(nn), K(nn), F(nn), Err(nn), a(nn), b(nn);
+        std::vector<double> Dprev, Jprev, Kprev, dD(nn);
         double E = 0, Eold = 0, En = 0, fock_ms = 0;
+        const bool inc = prm.incremental != 0;
+        int since_full = 0, nfull = 0, ninc = 0;
+        bool force_full = true;
+        double* d_dmax = nullptr;
+        if (inc) d_dmax = h->alloc<double>((size_t)h->nshell * h->nshell);
         int it;
         for (it = 1; it <= prm.max_iter; ++it)
         {
             qcg_stats st{};
-            CK(cudaMemcpyAsync(h->d_D, D.data(), nn * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-            jk_device(h, h->d_D, h->d_J, h->d_K, QCG_JK_SKIP_VALIDATION, &st);
+            const bool full = !inc || force_full || since_full >= prm.rebuild_every;
+            if (full)
+            {
+                CK(cudaMemcpyAsync(h->d_D, D.data(), nn * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+                jk_device(h, h->d_D, h->d_J, h->d_K, QCG_JK_SKIP_VALIDATION, &st);
+            }
+            else
+            {
+                for (size_t k = 0; k < nn; ++k) dD[k] = D[k] - Dprev[k];
+                CK(cudaMemcpyAsync(h->d_D, dD.data(), nn * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+                launch_block_max(h->d_D, h->d_f0, h->bs.L, h->nshell, n, d_dmax, h->stream, h->nsm);
+                jk_device(h, h->d_D, h->d_J, h->d_K, QCG_JK_SKIP_VALIDATION, &st, d_dmax, prm.inc_thresh);
+            }
             CK(cudaMemcpyAsync(J.data(), h->d_J, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
             CK(cudaMemcpyAsync(K.data(), h->d_K, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
             CK(cudaStreamSynchronize(h->stream));
             fock_ms += st.ms_total;
+            if (full)
+            {
+                since_full = 0;
+                force_full = false;
+                ++nfull;
+            }
+            else
+            {
+                for (size_t k = 0; k < nn; ++k) { J[k] += Jprev[k]; K[k] += Kprev[k]; }
+                ++since_full;
+                ++ninc;
+            }
+            if (inc) { Dprev = D; Jprev = J; Kprev = K; }
             double e = 0;
             for (size_t k = 0; k < nn; ++k)
             {
@@ -1069,8 +1108,13 @@ int qcg_rhf(qcg_handle* h, int natom, const double* Z, const double* R, int nele
             En = std::sqrt(En);
             if (it > 1 && std::fabs(E - Eold) < prm.de_tol && En < prm.fd_tol)
             {
-                converged = true;
-                break;
+                if (!full)
+                    force_full = true;   // confirm on a full build before stopping
+                else
+                {
+                    converged = true;
+                    break;
+                }
             }
             Eold = E;
             std::vector<double> Fuse = Fp;
@@ -1135,6 +1179,9 @@ int qcg_rhf(qcg_handle* h, int natom, const double* Z, const double* R, int nele
         result->converged = converged ? 1 : 0;
         result->fd_error = En;
         result->fock_ms = fock_ms;
+        result->full_builds = nfull;
+        result->incremental_builds = ninc;
+        if (d_dmax) h->release(d_dmax);
         result->wall_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         if (D_out) std::copy(D.begin(), D.end(), D_out);
     });
