@@ -171,6 +171,7 @@ def main():
     ap.add_argument("--quartets-per-class", type=int, default=Q_PER_CLASS)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extras", action="store_true")
+    ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--ref-sample", type=int, default=2000)
     ap.add_argument("--cpu-sample", type=int, default=1000)
     ap.add_argument("--workload", default="eri", choices=["eri", "fock_config3", "rhf_config1"],
@@ -217,14 +218,15 @@ def main():
     d_out = torch.empty(min(CHUNK, nq_cls) * max_blk, dtype=torch.float64, device=dev)
     torch.cuda.synchronize()
 
-    def step(events=None):
+    def step(events=None, fp32=False, out=None):
         launches = 0
+        out = d_out if out is None else out
         for k, cls in enumerate(classes):
             if events is not None:
                 events[k][0].record(stream)
             for c0 in range(0, nq_cls, CHUNK):
                 m = min(CHUNK, nq_cls - c0)
-                eng.eri_batch_device(cls, d_q[k].data_ptr() + 16 * c0, m, d_out.data_ptr())
+                eng.eri_batch_device(cls, d_q[k].data_ptr() + 16 * c0, m, out.data_ptr(), fp32=fp32)
                 launches += 1
             if events is not None:
                 events[k][1].record(stream)
@@ -328,6 +330,8 @@ def main():
             "per_class": per_class,
             "e2e": e2e}
 
+    if rank == 0 and not args.no_fp32:
+        line["fp32"] = fp32_pass(torch, stream, eng, classes, d_q, prim_q, step, args)
     if rank == 0 and world == 1:
         threads = os.cpu_count() or 1
         cb = cpu_baseline(classes, pool, args.cpu_sample, threads)
@@ -341,6 +345,55 @@ def main():
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def fp32_pass(torch, stream, eng, classes, d_q, prim_q, step, args):
+    """The same workload with FP32 evaluation (float output): throughput, roofline against the FP32 FMA
+    peak, and the FP32 error against FP64 on the first 20000 quartets of every class (reported, not gated)."""
+    from qchem_b200 import api
+    nq_cls = args.quartets_per_class
+    max_blk = max(class_block(c) for c in classes)
+    d_out32 = torch.empty(min(CHUNK, nq_cls) * max_blk, dtype=torch.float32, device=d_q[0].device)
+    peak32, _ = api.measure_fp32_peak(20)
+    step(fp32=True, out=d_out32)
+    torch.cuda.synchronize()
+    ev = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in classes]
+          for _ in range(args.steps)]
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for s in range(args.steps):
+        step(ev[s], fp32=True, out=d_out32)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1)
+    cls_ms = np.zeros(len(classes))
+    for s in range(args.steps):
+        for k in range(len(classes)):
+            cls_ms[k] += ev[s][k][0].elapsed_time(ev[s][k][1])
+    kdom = int(np.argmax(cls_ms))
+    tf = {k: class_flops(c) * sum(prim_q[k]) / (cls_ms[k] / args.steps * 1e-3) / 1e12 for k, c in enumerate(classes)}
+    # accuracy sample
+    m = min(20000, nq_cls)
+    errs = {}
+    a64 = torch.empty(m * max_blk, dtype=torch.float64, device=d_q[0].device)
+    a32 = torch.empty(m * max_blk, dtype=torch.float32, device=d_q[0].device)
+    for k, cls in enumerate(classes):
+        n = m * class_block(cls)
+        eng.eri_batch_device(cls, d_q[k].data_ptr(), m, a64.data_ptr())
+        eng.eri_batch_device(cls, d_q[k].data_ptr(), m, a32.data_ptr(), fp32=True)
+        x, y = a64[:n], a32[:n].double()
+        scale = float(x.abs().max())
+        errs["".join("spd"[l] for l in cls)] = {"max_abs": float((x - y).abs().max()),
+                                                 "max_abs_over_max_eri": float((x - y).abs().max()) / scale}
+    torch.cuda.synchronize()
+    key = "".join("spd"[l] for l in classes[kdom])
+    return {"value": len(classes) * nq_cls * args.steps / (ms * 1e-3), "unit": UNIT, "dtype": "f32",
+            "ms_per_step": ms / args.steps,
+            "roofline": {"bound": "fp32", "achieved": tf[kdom], "peak": peak32, "unit": "TFLOP/s",
+                         "frac": tf[kdom] / peak32, "kernel": "eri_batch_kernel<float> class " + key,
+                         "peak_source": "measured here: library FFMA probe"},
+            "per_class_tflops": {"".join("spd"[l] for l in c): tf[k] for k, c in enumerate(classes)},
+            "error_vs_fp64": errs}
 
 
 def run_secondary(args):
@@ -402,15 +455,16 @@ def run_secondary(args):
                 walls.append(time.perf_counter() - t0)
             return sum(walls) / len(walls), res
 
+        chosen = dict(incremental=True, fp32_early=True)
         mol = W.water()
         sh = B.even_tempered(mol)
         wall, res = solve(mol, sh, args.steps, args.warmup)
-        wall_c, res_c = solve(mol, sh, args.steps, 1, incremental=True)
+        wall_c, res_c = solve(mol, sh, args.steps, 1, **chosen)
         # where the Fock build dominates: 8 waters (2x2x2 jittered grid of 6.5 bohr), 456 functions
         mol8 = W.water_cluster(nx=2, ny=2, nz=2, spacing=6.5, seed=W.SEED0 + 3400)
         sh8 = B.even_tempered(mol8)
         w8, r8 = solve(mol8, sh8, 1, 0)
-        w8c, r8c = solve(mol8, sh8, 1, 0, incremental=True)
+        w8c, r8c = solve(mol8, sh8, 1, 0, **chosen)
         line = {"metric": "RHF time-to-solution (water, even-tempered 57 functions, dE < 1e-10), plain FP64 GPU",
                 "value": wall, "unit": "s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": 1e3 * wall, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
@@ -421,6 +475,8 @@ def run_secondary(args):
                                                   "abs_diff_vs_plain_eh": abs(res_c["energy"] - res["energy"]),
                                                   "full_builds": res_c["full_builds"],
                                                   "incremental_builds": res_c["incremental_builds"],
+                                                  "fp32_builds": res_c["fp32_builds"],
+                                                  "iterations": [res["iterations"], res_c["iterations"]],
                                                   "speedup_vs_plain": wall / wall_c},
                                 "water8_456fn": {"plain_wall_s": w8, "chosen_wall_s": w8c,
                                                  "plain_energy": r8["energy"], "chosen_energy": r8c["energy"],

@@ -46,6 +46,7 @@ enum qcg_status {
 /* flags for qcg_fock_jk */
 #define QCG_JK_SKIP_VALIDATION 1   /* do not check D for NaN/Inf and symmetry */
 #define QCG_JK_J_ONLY 2            /* reserved: both J and K are always built */
+#define QCG_JK_FP32 4              /* evaluate every quartet in FP32 (accumulation into J and K stays FP64) */
 
 typedef struct qcg_stats {
     double ms_total;          /* device time of the whole J/K build (CUDA events) */
@@ -70,6 +71,15 @@ typedef struct qcg_scf_params {
     double inc_thresh;        /* skip a quartet of an incremental build when Q_ab Q_cd max|dD| < inc_thresh
                                  (default 1e-11) */
     int rebuild_every;        /* default 8 */
+    int fp32_early;           /* 1: until the DIIS error first falls below fp32_switch, quartets whose density-
+                                 weighted bound Q_ab Q_cd max|D| is below fp32_scale * (previous DIIS error) are
+                                 evaluated in FP32 (FP64 accumulation, FP64 Boys below T = 12), then a full FP64
+                                 rebuild; default 0 */
+    double fp32_switch;       /* default 1e-5 */
+    double fp32_scale;        /* <= 0 (default): 1e-4 / (3e-7 nbf^2), i.e. the worst-case FP32 error of a Fock
+                                 element (nbf^2 quartets of relative error 3e-7) at 1e-4 of the DIIS error */
+    double fp32_below;        /* after the switch, quartets whose bound is below this stay FP32; default 0 */
+    const double* D_guess;    /* optional initial total density, nbf*nbf (NULL: core-Hamiltonian guess) */
 } qcg_scf_params;
 
 typedef struct qcg_scf_result {
@@ -82,6 +92,7 @@ typedef struct qcg_scf_result {
     double fock_ms;           /* summed device time of the J/K builds */
     int full_builds;          /* J/K builds from the full density */
     int incremental_builds;   /* J/K builds from a density difference */
+    int fp32_builds;          /* J/K builds in which quartets below a bound were evaluated in FP32 */
 } qcg_scf_result;
 
 /* ---- lifetime -------------------------------------------------------------------------------- */
@@ -109,6 +120,12 @@ int qcg_eri_batch(qcg_handle* h, int la, int lb, int lc, int ld, long long nq, c
 /* same with device pointers (no validation of the shell L's; the stream is the handle's) */
 int qcg_eri_batch_device(qcg_handle* h, int la, int lb, int lc, int ld, long long nq, const int* d_quartets,
                          double* d_out);
+/* FP32 forms of the two batch calls: the same integrals evaluated in FP32 arithmetic (pair data, Boys
+ * argument, prefactor and Boys below T = 12 in FP64, rounded once) with float output.  No reference
+ * counterpart (the reference is FP64 only). */
+int qcg_eri_batch_f32(qcg_handle* h, int la, int lb, int lc, int ld, long long nq, const int* quartets, float* out);
+int qcg_eri_batch_device_f32(qcg_handle* h, int la, int lb, int lc, int ld, long long nq, const int* d_quartets,
+                             float* d_out);
 
 /* Schwarz bounds Q_ab = sqrt(max |(ab|ab)|) for every shell pair and the screened quartet lists used by
  * qcg_fock_jk (quartets with Q_ab Q_cd < thresh are skipped).  Q: optional, nshell*nshell doubles. */
@@ -118,6 +135,11 @@ int qcg_schwarz(qcg_handle* h, double thresh, double* Q);
 int qcg_fock_jk(qcg_handle* h, const double* D, double* J, double* K, int flags, qcg_stats* stats);
 /* same with device pointers on the handle's stream; results are ready when the stream reaches them */
 int qcg_fock_jk_device(qcg_handle* h, const double* d_D, double* d_J, double* d_K, int flags, qcg_stats* stats);
+/* Mixed precision for later qcg_fock_jk / qcg_fock_jk_device calls: quartets whose density-weighted
+ * Schwarz bound Q_ab Q_cd max|D| (max over the six D blocks the quartet touches) is below `bound` are
+ * evaluated in FP32 (accumulated in FP64), the rest in FP64.  0 (the default) keeps every quartet FP64.
+ * No reference counterpart. */
+int qcg_set_fp32_bound(qcg_handle* h, double bound);
 
 /* The J/K build of qcg_fock_jk_device for callers that must not allocate device memory once their setup
  * is done -- for example a host program whose device memory is owned by its own pool allocator, or one
@@ -144,6 +166,8 @@ int qcg_rhf(qcg_handle* h, int natom, const double* Z, const double* R, int nele
 /* FP64 fused-multiply-add throughput of the current device (TFLOP/s) from a pure-DFMA kernel timed over
  * `reps` launches: the roofline denominator of the ERI kernels.  No reference counterpart. */
 int qcg_measure_fp64_peak(int reps, double* tflops, double* ms_per_launch);
+/* the same for FP32 fused multiply-adds: the roofline denominator of the FP32 ERI kernels */
+int qcg_measure_fp32_peak(int reps, double* tflops, double* ms_per_launch);
 
 #ifdef __cplusplus
 }

@@ -30,11 +30,14 @@ _lib = None
 QCG_OK, QCG_ERR_ARG, QCG_ERR_CUDA, QCG_ERR_NONFINITE, QCG_ERR_ASYMMETRIC, QCG_ERR_ALLOC, QCG_ERR_STATE, \
     QCG_ERR_NOCONV = range(8)
 QCG_JK_SKIP_VALIDATION = 1
+QCG_JK_FP32 = 4
 
 # every symbol include/qchem_b200.h declares
 EXPORTS = ["qcg_basis_create", "qcg_destroy", "qcg_last_error", "qcg_set_stream", "qcg_set_memory_limit", "qcg_nbf",
            "qcg_nshell", "qcg_norms", "qcg_eri_batch", "qcg_eri_batch_device", "qcg_schwarz", "qcg_fock_jk",
-           "qcg_fock_jk_device", "qcg_one_electron", "qcg_scf_default_params", "qcg_rhf", "qcg_measure_fp64_peak"]
+           "qcg_fock_jk_device", "qcg_one_electron", "qcg_scf_default_params", "qcg_rhf", "qcg_measure_fp64_peak",
+           "qcg_fock_jk_device_noalloc", "qcg_eri_batch_f32", "qcg_eri_batch_device_f32", "qcg_set_fp32_bound",
+           "qcg_measure_fp32_peak"]
 
 
 class QcgError(RuntimeError):
@@ -52,13 +55,16 @@ class ScfParams(ctypes.Structure):
     _fields_ = [("max_iter", ctypes.c_int), ("de_tol", ctypes.c_double), ("fd_tol", ctypes.c_double),
                 ("schwarz_thresh", ctypes.c_double), ("diis_nproj", ctypes.c_int), ("diis_fdmax", ctypes.c_double),
                 ("diis_svtol", ctypes.c_double), ("incremental", ctypes.c_int), ("inc_thresh", ctypes.c_double),
-                ("rebuild_every", ctypes.c_int)]
+                ("rebuild_every", ctypes.c_int), ("fp32_early", ctypes.c_int), ("fp32_switch", ctypes.c_double),
+                ("fp32_scale", ctypes.c_double), ("fp32_below", ctypes.c_double),
+                ("D_guess", ctypes.POINTER(ctypes.c_double))]
 
 
 class ScfResult(ctypes.Structure):
     _fields_ = [("energy", ctypes.c_double), ("e_nuc", ctypes.c_double), ("iterations", ctypes.c_int),
                 ("converged", ctypes.c_int), ("fd_error", ctypes.c_double), ("wall_s", ctypes.c_double),
-                ("fock_ms", ctypes.c_double), ("full_builds", ctypes.c_int), ("incremental_builds", ctypes.c_int)]
+                ("fock_ms", ctypes.c_double), ("full_builds", ctypes.c_int), ("incremental_builds", ctypes.c_int),
+                ("fp32_builds", ctypes.c_int)]
 
 
 def library_path() -> str:
@@ -87,6 +93,9 @@ def lib():
     L.qcg_norms.argtypes = [vp, P(f64)]
     L.qcg_eri_batch.argtypes = [vp, i32, i32, i32, i32, i64, P(i32), P(f64)]
     L.qcg_eri_batch_device.argtypes = [vp, i32, i32, i32, i32, i64, vp, vp]
+    L.qcg_eri_batch_f32.argtypes = [vp, i32, i32, i32, i32, i64, P(i32), P(ctypes.c_float)]
+    L.qcg_eri_batch_device_f32.argtypes = [vp, i32, i32, i32, i32, i64, vp, vp]
+    L.qcg_set_fp32_bound.argtypes = [vp, f64]
     L.qcg_schwarz.argtypes = [vp, f64, P(f64)]
     L.qcg_fock_jk.argtypes = [vp, P(f64), P(f64), P(f64), i32, P(Stats)]
     L.qcg_fock_jk_device.argtypes = [vp, vp, vp, vp, i32, P(Stats)]
@@ -96,6 +105,7 @@ def lib():
     L.qcg_rhf.argtypes = [vp, i32, P(f64), P(f64), i32, P(ScfParams), P(ScfResult), P(f64)]
     L.qcg_internal_syev.argtypes = [i32, P(f64), P(f64), P(f64)]
     L.qcg_measure_fp64_peak.argtypes = [i32, P(f64), P(f64)]
+    L.qcg_measure_fp32_peak.argtypes = [i32, P(f64), P(f64)]
     _lib = L
     return L
 
@@ -125,6 +135,15 @@ def measure_fp64_peak(reps: int = 20):
     rc = lib().qcg_measure_fp64_peak(int(reps), ctypes.byref(tf), ctypes.byref(ms))
     if rc != QCG_OK:
         raise QcgError(rc, "fp64 peak probe failed")
+    return tf.value, ms.value
+
+
+def measure_fp32_peak(reps: int = 20):
+    """(TFLOP/s, ms per launch) of the library's pure-FFMA probe kernel on the current device."""
+    tf, ms = ctypes.c_double(), ctypes.c_double()
+    rc = lib().qcg_measure_fp32_peak(int(reps), ctypes.byref(tf), ctypes.byref(ms))
+    if rc != QCG_OK:
+        raise QcgError(rc, "fp32 peak probe failed")
     return tf.value, ms.value
 
 
@@ -177,18 +196,27 @@ class Engine:
         return ns
 
     # -- integrals -----------------------------------------------------------------------------
-    def eri_batch(self, cls, quartets) -> np.ndarray:
+    def eri_batch(self, cls, quartets, fp32: bool = False) -> np.ndarray:
+        """Cartesian ERI blocks of one class; fp32=True evaluates them in FP32 (float32 output)."""
         q = np.ascontiguousarray(quartets, dtype=np.int32)
         la, lb, lc, ld = cls
         nf = [(l + 1) * (l + 2) // 2 for l in cls]
-        out = np.zeros((len(q), nf[0] * nf[1] * nf[2] * nf[3]))
-        self._check(lib().qcg_eri_batch(self._h, la, lb, lc, ld, len(q), _p(q, ctypes.c_int), _p(out)))
+        out = np.zeros((len(q), nf[0] * nf[1] * nf[2] * nf[3]), dtype=np.float32 if fp32 else np.float64)
+        if fp32:
+            self._check(lib().qcg_eri_batch_f32(self._h, la, lb, lc, ld, len(q), _p(q, ctypes.c_int),
+                                                _p(out, ctypes.c_float)))
+        else:
+            self._check(lib().qcg_eri_batch(self._h, la, lb, lc, ld, len(q), _p(q, ctypes.c_int), _p(out)))
         return out
 
-    def eri_batch_device(self, cls, d_quartets_ptr: int, nq: int, d_out_ptr: int):
+    def eri_batch_device(self, cls, d_quartets_ptr: int, nq: int, d_out_ptr: int, fp32: bool = False):
         la, lb, lc, ld = cls
-        self._check(lib().qcg_eri_batch_device(self._h, la, lb, lc, ld, int(nq), ctypes.c_void_p(d_quartets_ptr),
-                                               ctypes.c_void_p(d_out_ptr)))
+        f = lib().qcg_eri_batch_device_f32 if fp32 else lib().qcg_eri_batch_device
+        self._check(f(self._h, la, lb, lc, ld, int(nq), ctypes.c_void_p(d_quartets_ptr), ctypes.c_void_p(d_out_ptr)))
+
+    def set_fp32_bound(self, bound: float):
+        """Later J/K builds evaluate quartets with Q_ab Q_cd < bound in FP32 (FP64 accumulation)."""
+        self._check(lib().qcg_set_fp32_bound(self._h, float(bound)))
 
     def schwarz(self, thresh: float = 1e-10) -> np.ndarray:
         ns = len(self.shells)
@@ -197,7 +225,8 @@ class Engine:
         self._screen = thresh
         return Q
 
-    def fock_jk(self, D, validate: bool = True):
+    def fock_jk(self, D, validate: bool = True, fp32: bool = False):
+        """J[D], K[D] (unscaled) and the build's Stats; fp32=True evaluates every quartet in FP32."""
         if self._screen is None:
             self.schwarz()
         D = _f64(D)
@@ -205,16 +234,17 @@ class Engine:
             raise QcgError(QCG_ERR_ARG, f"density must be {self.nbf}x{self.nbf}")
         J, K = np.zeros_like(D), np.zeros_like(D)
         st = Stats()
-        self._check(lib().qcg_fock_jk(self._h, _p(D), _p(J), _p(K), 0 if validate else QCG_JK_SKIP_VALIDATION,
-                                      ctypes.byref(st)))
+        flags = (0 if validate else QCG_JK_SKIP_VALIDATION) | (QCG_JK_FP32 if fp32 else 0)
+        self._check(lib().qcg_fock_jk(self._h, _p(D), _p(J), _p(K), flags, ctypes.byref(st)))
         return J, K, st
 
-    def fock_jk_device(self, d_D: int, d_J: int, d_K: int, validate: bool = False) -> Stats:
+    def fock_jk_device(self, d_D: int, d_J: int, d_K: int, validate: bool = False, fp32: bool = False) -> Stats:
         if self._screen is None:
             self.schwarz()
         st = Stats()
+        flags = (0 if validate else QCG_JK_SKIP_VALIDATION) | (QCG_JK_FP32 if fp32 else 0)
         self._check(lib().qcg_fock_jk_device(self._h, ctypes.c_void_p(d_D), ctypes.c_void_p(d_J), ctypes.c_void_p(d_K),
-                                             0 if validate else QCG_JK_SKIP_VALIDATION, ctypes.byref(st)))
+                                             flags, ctypes.byref(st)))
         return st
 
     def one_electron(self, mol: _basis.Molecule):
@@ -226,13 +256,25 @@ class Engine:
         return S, T, V
 
     def rhf(self, mol: _basis.Molecule, max_iter=100, de_tol=1e-10, fd_tol=1e-5, schwarz_thresh=1e-10,
-            want_density=False, incremental=False, inc_thresh=1e-11, rebuild_every=8):
+            want_density=False, incremental=False, inc_thresh=1e-11, rebuild_every=8, fp32_early=False,
+            fp32_switch=1e-5, fp32_scale=0.0, fp32_below=0.0, guess=None):
         """RHF to convergence.  incremental=True: density-difference J/K builds with density-weighted
-        screening between full builds (the energy on exit is always from a full build)."""
+        screening between full builds (the energy on exit is always from a full build).  fp32_early=True:
+        until the DIIS error drops below fp32_switch, quartets whose density-weighted bound is below
+        fp32_scale x (DIIS error) are FP32; fp32_below: quartets with a smaller bound stay FP32 afterwards
+        (the build that confirms convergence is all-FP64).  guess: initial total density (nbf x nbf)
+        instead of the core-Hamiltonian guess."""
         prm = ScfParams()
         lib().qcg_scf_default_params(ctypes.byref(prm))
         prm.max_iter, prm.de_tol, prm.fd_tol, prm.schwarz_thresh = max_iter, de_tol, fd_tol, schwarz_thresh
         prm.incremental, prm.inc_thresh, prm.rebuild_every = int(incremental), float(inc_thresh), int(rebuild_every)
+        prm.fp32_early, prm.fp32_switch, prm.fp32_below = int(fp32_early), float(fp32_switch), float(fp32_below)
+        prm.fp32_scale = float(fp32_scale)
+        if guess is not None:
+            guess = _f64(guess)
+            if guess.shape != (self.nbf, self.nbf):
+                raise QcgError(QCG_ERR_ARG, f"guess density must be {self.nbf}x{self.nbf}")
+            prm.D_guess = _p(guess)
         res = ScfResult()
         Z = _f64(mol.Z)
         R = _f64(mol.R).reshape(-1)
@@ -244,7 +286,8 @@ class Engine:
         self._screen = schwarz_thresh
         out = {"energy": res.energy, "e_nuc": res.e_nuc, "iterations": res.iterations,
                "converged": bool(res.converged), "fd_error": res.fd_error, "wall_s": res.wall_s,
-               "fock_ms": res.fock_ms, "full_builds": res.full_builds, "incremental_builds": res.incremental_builds}
+               "fock_ms": res.fock_ms, "full_builds": res.full_builds, "incremental_builds": res.incremental_builds,
+               "fp32_builds": res.fp32_builds}
         if D is not None:
             out["D"] = D
         return out

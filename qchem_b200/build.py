@@ -2,7 +2,8 @@
 
   python -m qchem_b200.build [--force] [-j N]
 
-Steps: generate the per-class MD code (csrc/gen_md.py), compile the 21 class objects plus the
+Steps: generate the per-class MD code (csrc/gen_md.py), compile the 2 x 21 class objects (FP64 and
+FP32) plus the
 runtime in parallel with nvcc (-gencode arch=compute_100a,code=sm_100a -lineinfo), link a shared
 library into qchem_b200/_lib/.  Objects are cached in qchem_b200/_build/ keyed by a hash of their
 inputs, so unchanged classes are not recompiled.
@@ -26,6 +27,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"] + ARCH
 NCLASS = 21
+HOST_OMP = ["-Xcompiler", "-fopenmp", "-Xcompiler", "-march=x86-64-v3"]   # the SCF's host linear algebra (eigensolver, products) is threaded
 
 
 def _read(p):
@@ -48,16 +50,18 @@ def _jobs():
     core = _headers(["md_core.cuh", "qcg_internal.h"])
     jobs = []
     src = os.path.join(CSRC, "eri_class.cu")
-    for k in range(NCLASS):
-        defs = [f"-DQCG_CLASS={k}"]
-        key = _hash([_read(src), _read(os.path.join(GEN, f"md_class_{k}.cuh"))] + core
-                    + _headers(["eri_kernels.cuh"]) + FLAGS + defs)
-        jobs.append((src, defs, os.path.join(BUILD, f"eri_class_{k}_{key}.o")))
+    for prec in (64, 32):
+        for k in range(NCLASS):
+            defs = [f"-DQCG_CLASS={k}", f"-DQCG_PREC={prec}"]
+            key = _hash([_read(src), _read(os.path.join(GEN, f"md_class_{k}.cuh"))] + core
+                        + _headers(["eri_kernels.cuh"]) + FLAGS + defs)
+            jobs.append((src, defs, os.path.join(BUILD, f"eri_class_{k}_f{prec}_{key}.o")))
     extra = {"runtime.cu": _headers(["boys_table.h"]) + [_read(os.path.join(INCLUDE, "qchem_b200.h"))]}
     for name in ("registry.cu", "fock_kernels.cu", "runtime.cu"):
         s = os.path.join(CSRC, name)
-        key = _hash([_read(s)] + core + extra.get(name, []) + FLAGS)
-        jobs.append((s, [], os.path.join(BUILD, f"{name[:-3]}_{key}.o")))
+        defs = HOST_OMP if name == "runtime.cu" else []
+        key = _hash([_read(s)] + core + extra.get(name, []) + FLAGS + defs)
+        jobs.append((s, defs, os.path.join(BUILD, f"{name[:-3]}_{key}.o")))
     return jobs
 
 
@@ -92,7 +96,7 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
                 os.remove(obj)
     # biggest classes first so that the slowest compiles start early
     todo.sort(key=lambda j: -os.path.getsize(os.path.join(GEN, f"md_class_{j[1][0].split('=')[1]}.cuh"))
-              if j[1] else 0)
+              if j[1] and j[1][0].startswith("-DQCG_CLASS") else 0)
     n = jobs or max(1, os.cpu_count() or 1)
     built = []
     with cf.ThreadPoolExecutor(max_workers=n) as ex:
@@ -105,7 +109,7 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
     stamp = LIB + ".key"
     if force or not os.path.exists(LIB) or not os.path.exists(stamp) or open(stamp).read() != key:
         tmp = LIB + ".tmp"
-        cmd = [NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objs
+        cmd = [NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objs + ["-lgomp"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n" + r.stderr[-4000:])

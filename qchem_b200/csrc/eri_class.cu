@@ -1,9 +1,16 @@
-// eri_class.cu -- instantiates the kernels of ONE quartet class; compiled once per class with
-// -DQCG_CLASS=k (k = X(X+1)/2 + Y for pair classes X >= Y) so that the 21 classes build in parallel.
+// eri_class.cu -- instantiates the kernels of ONE quartet class in ONE arithmetic type; compiled with
+// -DQCG_CLASS=k (k = X(X+1)/2 + Y for pair classes X >= Y) and -DQCG_PREC=64 or 32, so that the 21 classes
+// of both forms build in parallel.  The FP64 objects define launch_eri_batch_k, launch_jk_k and
+// launch_schwarz_k; the FP32 objects launch_eri_batch32_k and launch_jk32_k.
+#include <type_traits>
+
 #include "eri_kernels.cuh"
 
 #ifndef QCG_CLASS
 #error "compile with -DQCG_CLASS=<0..20>"
+#endif
+#ifndef QCG_PREC
+#define QCG_PREC 64
 #endif
 
 #define QCG_STR2(x) #x
@@ -11,6 +18,13 @@
 #define QCG_CAT2(a, b) a##b
 #define QCG_CAT(a, b) QCG_CAT2(a, b)
 #include QCG_STR(gen/QCG_CAT(md_class_, QCG_CLASS).cuh)
+#if QCG_PREC == 64
+#define QCG_NAME(base) QCG_CAT(QCG_CAT(base, _), QCG_CLASS)
+#elif QCG_PREC == 32
+#define QCG_NAME(base) QCG_CAT(QCG_CAT(base, 32_), QCG_CLASS)
+#else
+#error "QCG_PREC must be 64 or 32"
+#endif
 
 namespace qcg {
 
@@ -23,6 +37,7 @@ constexpr int cls_X()
 }
 constexpr int kX = cls_X();
 constexpr int kY = QCG_CLASS - kX * (kX + 1) / 2;
+using Real = std::conditional_t<QCG_PREC == 64, double, float>;
 
 struct Cls
 {
@@ -30,25 +45,27 @@ struct Cls
     static constexpr bool kRShared = gen::QCG_CAT(kRShared, QCG_CLASS);
     static constexpr bool kChunked = gen::QCG_CAT(kChunked, QCG_CLASS);
     static constexpr int kRSize = gen::QCG_CAT(kRSize, QCG_CLASS);
-    template <class Sink, bool LOCKSTEP = false>
+    template <class RT, class Sink, bool LOCKSTEP = false>
     static __device__ __forceinline__ void quartet(const PrimPairData& ab, const PrimPairData& cd,
-                                                   const double* __restrict__ bt, double* __restrict__ rs, int stride,
+                                                   const double* __restrict__ bt, RT* __restrict__ rs, int stride,
                                                    Sink& sink)
     {
-        gen::QCG_CAT(prim_quartet_, QCG_CLASS)<Sink, LOCKSTEP>(ab, cd, bt, rs, stride, sink);
+        gen::QCG_CAT(prim_quartet_, QCG_CLASS)<RT, Sink, LOCKSTEP>(ab, cd, bt, rs, stride, sink);
     }
 };
 
 // classes whose R table lives in shared memory run 64-thread blocks (per-thread R slice); the others 128
 constexpr int kThreads = Cls::kRShared ? 64 : 128;
-constexpr size_t kSmem = Cls::kRShared ? (size_t)kThreads * Cls::kRSize * sizeof(double) : 0;
+constexpr size_t kSmem = Cls::kRShared ? (size_t)kThreads * Cls::kRSize * sizeof(Real) : 0;
+// the Schwarz diagonals are always FP64
+constexpr size_t kSmem64 = Cls::kRShared ? (size_t)kThreads * Cls::kRSize * sizeof(double) : 0;
 
 template <class KernelPtr>
-void prepare(KernelPtr k)
+void prepare(KernelPtr k, size_t smem = kSmem)
 {
     static bool done = false;
-    if (!done && kSmem > 48 * 1024)
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem);
+    if (!done && smem > 48 * 1024)
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     done = true;
 }
 
@@ -62,19 +79,20 @@ long long grid_for(long long work, int nsm)
 
 // chunked classes: 128-thread blocks in lock step (one chunk of code in flight per block)
 constexpr int kLockThreads = 128;
-constexpr size_t kLockSmem = (size_t)kLockThreads * Cls::kRSize * sizeof(double);
+constexpr size_t kLockSmem = (size_t)kLockThreads * Cls::kRSize * sizeof(Real);
 
-// lock step measured faster for every chunked class except (dd|dd), whose 169 KB per 128-thread block
-// leaves no room for a second block (ERI microbenchmark, 10^6 quartets per class)
-constexpr bool kUseLockstep = Cls::kChunked && QCG_CLASS != 20;
+// lock step measured faster for every chunked class except FP64 (dd|dd), whose 169 KB per 128-thread
+// block leaves no room for a second block (ERI microbenchmark, 10^6 quartets per class); the FP32 form
+// needs half of that
+constexpr bool kUseLockstep = Cls::kChunked && (QCG_CLASS != 20 || QCG_PREC == 32);
 
-void QCG_CAT(launch_eri_batch_, QCG_CLASS)(const BasisDev& bs, const int4* q, const int* order, long long nq,
-                                           double* out, const double* boys, cudaStream_t st, int nsm)
+void QCG_NAME(launch_eri_batch)(const BasisDev& bs, const int4* q, const int* order, long long nq, Real* out,
+                                const double* boys, cudaStream_t st, int nsm)
 {
     if (nq <= 0) return;
     if constexpr (kUseLockstep)
     {
-        auto k = eri_batch_lockstep_kernel<Cls, kLockThreads>;
+        auto k = eri_batch_lockstep_kernel<Cls, kLockThreads, Real>;
         static bool done = false;
         if (!done && kLockSmem > 48 * 1024)
             cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLockSmem);
@@ -86,18 +104,18 @@ void QCG_CAT(launch_eri_batch_, QCG_CLASS)(const BasisDev& bs, const int4* q, co
     }
     else
     {
-        auto k = eri_batch_kernel<Cls, kThreads>;
+        auto k = eri_batch_kernel<Cls, kThreads, Real>;
         prepare(k);
         k<<<(unsigned)grid_for(nq, nsm), kThreads, kSmem, st>>>(bs, q, order, nq, out, boys);
     }
 }
 
-void QCG_CAT(launch_jk_, QCG_CLASS)(const JKWorkDev& w, const PairListDev& bra, const PairListDev& ket,
-                                    const PrimPairsDev& P, const int* f0, const double* D, double* J, double* K, int n,
-                                    const double* boys, cudaStream_t st, int nsm)
+void QCG_NAME(launch_jk)(const JKWorkDev& w, const PairListDev& bra, const PairListDev& ket, const PrimPairsDev& P,
+                         const int* f0, const double* D, double* J, double* K, int n, const double* boys,
+                         cudaStream_t st, int nsm)
 {
     if (w.total <= 0) return;
-    auto k = jk_kernel<Cls, kThreads>;
+    auto k = jk_kernel<Cls, kThreads, Real>;
     prepare(k);
     // quartets per lane run: enough threads for the whole GPU first, longer runs only for large builds
     long long run = w.total / ((long long)nsm * 1024);
@@ -106,6 +124,7 @@ void QCG_CAT(launch_jk_, QCG_CLASS)(const JKWorkDev& w, const PairListDev& bra, 
     k<<<(unsigned)grid_for(work, nsm), kThreads, kSmem, st>>>(w, bra, ket, P, f0, D, J, K, n, boys, (int)run);
 }
 
+#if QCG_PREC == 64
 // Schwarz diagonals exist only for the diagonal classes (X == Y)
 void QCG_CAT(launch_schwarz_, QCG_CLASS)(const PairListDev& pl, const PrimPairsDev& P, double* Q, const double* boys,
                                          cudaStream_t st)
@@ -114,9 +133,10 @@ void QCG_CAT(launch_schwarz_, QCG_CLASS)(const PairListDev& pl, const PrimPairsD
     {
         if (pl.n <= 0) return;
         auto k = schwarz_kernel<Cls, kThreads>;
-        prepare(k);
-        k<<<(pl.n + kThreads - 1) / kThreads, kThreads, kSmem, st>>>(pl, P, Q, boys);
+        prepare(k, kSmem64);
+        k<<<(pl.n + kThreads - 1) / kThreads, kThreads, kSmem64, st>>>(pl, P, Q, boys);
     }
 }
+#endif
 
 }   // namespace qcg

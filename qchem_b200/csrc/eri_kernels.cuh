@@ -13,15 +13,15 @@ namespace qcg {
 // ------------------------------------------------------------------------------------------------
 // accumulates every primitive quartet into the (zeroed) output block with fire-and-forget L2 reductions:
 // the thread never reads the block back, so no loads are hoisted into registers around the ERI code
-template <int LB, int LC, int LD>
+template <class RT, int LB, int LC, int LD>
 struct StoreSink
 {
     static constexpr bool kByValue = true;
-    double* o;
+    RT* o;
     static constexpr int NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
     __device__ __forceinline__ void ket_begin(int, int) {}
     __device__ __forceinline__ void ket_end(int, int) {}
-    __device__ __forceinline__ void operator()(int ia, int ib, int ic, int id, double v)
+    __device__ __forceinline__ void operator()(int ia, int ib, int ic, int id, RT v)
     {
         atomicAdd(o + ((ia * NB + ib) * NC + ic) * ND + id, v);
     }
@@ -35,16 +35,16 @@ __device__ __forceinline__ PrimPairData shell_prim_pair(const BasisDev& bs, int 
 }
 
 // the same with a per-thread switch: lanes that only keep a block in step write nothing
-template <int LB, int LC, int LD>
+template <class RT, int LB, int LC, int LD>
 struct MaskedStoreSink
 {
     static constexpr bool kByValue = true;
-    double* o;
+    RT* o;
     bool active;
     static constexpr int NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
     __device__ __forceinline__ void ket_begin(int, int) {}
     __device__ __forceinline__ void ket_end(int, int) {}
-    __device__ __forceinline__ void operator()(int ia, int ib, int ic, int id, double v)
+    __device__ __forceinline__ void operator()(int ia, int ib, int ic, int id, RT v)
     {
         if (active) atomicAdd(o + ((ia * NB + ib) * NC + ic) * ND + id, v);
     }
@@ -53,23 +53,31 @@ struct MaskedStoreSink
 // dynamic shared memory holding the per-thread R tables of classes with L >= 6 or chunked code
 extern __shared__ double qcg_smem[];
 
+// per-thread R slice in dynamic shared memory, in the arithmetic type of the kernel
+template <class RT>
+__device__ __forceinline__ RT* r_slice()
+{
+    return reinterpret_cast<RT*>(qcg_smem) + threadIdx.x;
+}
+
 // Quartets are visited through `order` (a permutation grouping equal contraction patterns, so that the
-// lanes of a warp run the same primitive loops); each writes its own output block.
-template <class Cls, int THREADS>
+// lanes of a warp run the same primitive loops); each writes its own output block.  RT is the arithmetic
+// and output type (double, or float for the FP32 form).
+template <class Cls, int THREADS, class RT>
 __global__ void __launch_bounds__(THREADS) eri_batch_kernel(BasisDev bs, const int4* __restrict__ quartets,
                                                             const int* __restrict__ order, long long nq,
-                                                            double* __restrict__ out,
+                                                            RT* __restrict__ out,
                                                             const double* __restrict__ boys_table)
 {
     constexpr long long BLK = (long long)ncart(Cls::LA) * ncart(Cls::LB) * ncart(Cls::LC) * ncart(Cls::LD);
-    double* rs = qcg_smem + threadIdx.x;
+    RT* rs = r_slice<RT>();
     for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < nq; g += (long long)gridDim.x * blockDim.x)
     {
         const long long q = order ? order[g] : g;
         const int4 s = quartets[q];
-        double* o = out + q * BLK;
-        for (int k = 0; k < (int)BLK; ++k) o[k] = 0.0;
-        StoreSink<Cls::LB, Cls::LC, Cls::LD> sink{o};
+        RT* o = out + q * BLK;
+        for (int k = 0; k < (int)BLK; ++k) o[k] = RT(0);
+        StoreSink<RT, Cls::LB, Cls::LC, Cls::LD> sink{o};
         const int ni = bs.nprim[s.x], nj = bs.nprim[s.y], nk = bs.nprim[s.z], nl = bs.nprim[s.w];
         const int nket = nk * nl, ntot = ni * nj * nket;
         for (int x = 0; x < ntot; ++x)
@@ -77,7 +85,7 @@ __global__ void __launch_bounds__(THREADS) eri_batch_kernel(BasisDev bs, const i
             const int ij = x / nket, kl = x - ij * nket;
             const PrimPairData ab = shell_prim_pair(bs, s.x, ij / nj, s.y, ij % nj);
             const PrimPairData cd = shell_prim_pair(bs, s.z, kl / nl, s.w, kl % nl);
-            Cls::quartet(ab, cd, boys_table, rs, THREADS, sink);
+            Cls::template quartet<RT>(ab, cd, boys_table, rs, THREADS, sink);
         }
     }
 }
@@ -86,15 +94,15 @@ __global__ void __launch_bounds__(THREADS) eri_batch_kernel(BasisDev bs, const i
 // quartets in rounds of THREADS, every thread runs the block's largest primitive count (surplus
 // iterations are masked), so all threads reach every barrier inside Cls::quartet<..., true> and the
 // block's warps walk the chunk code together.
-template <class Cls, int THREADS>
+template <class Cls, int THREADS, class RT>
 __global__ void __launch_bounds__(THREADS) eri_batch_lockstep_kernel(BasisDev bs, const int4* __restrict__ quartets,
                                                                      const int* __restrict__ order, long long nq,
-                                                                     double* __restrict__ out,
+                                                                     RT* __restrict__ out,
                                                                      const double* __restrict__ boys_table)
 {
     constexpr long long BLK = (long long)ncart(Cls::LA) * ncart(Cls::LB) * ncart(Cls::LC) * ncart(Cls::LD);
     __shared__ int s_nmax;
-    double* rs = qcg_smem + threadIdx.x;
+    RT* rs = r_slice<RT>();
     for (long long base = (long long)blockIdx.x * THREADS; base < nq; base += (long long)gridDim.x * THREADS)
     {
         const long long g = base + threadIdx.x;
@@ -102,9 +110,9 @@ __global__ void __launch_bounds__(THREADS) eri_batch_lockstep_kernel(BasisDev bs
         const long long gq = valid ? g : base;   // idle lanes shadow the round's first quartet
         const long long q = order ? order[gq] : gq;
         const int4 s = quartets[q];
-        double* o = out + q * BLK;
+        RT* o = out + q * BLK;
         if (valid)
-            for (int k = 0; k < (int)BLK; ++k) o[k] = 0.0;
+            for (int k = 0; k < (int)BLK; ++k) o[k] = RT(0);
         const int ni = bs.nprim[s.x], nj = bs.nprim[s.y], nk = bs.nprim[s.z], nl = bs.nprim[s.w];
         const int nket = nk * nl, ntot = ni * nj * nket;
         if (threadIdx.x == 0) s_nmax = 0;
@@ -113,7 +121,7 @@ __global__ void __launch_bounds__(THREADS) eri_batch_lockstep_kernel(BasisDev bs
         __syncthreads();
         const int nmax = s_nmax;
         __syncthreads();
-        MaskedStoreSink<Cls::LB, Cls::LC, Cls::LD> sink{o, false};
+        MaskedStoreSink<RT, Cls::LB, Cls::LC, Cls::LD> sink{o, false};
         for (int x = 0; x < nmax; ++x)
         {
             const int xx = x < ntot ? x : 0;
@@ -121,8 +129,8 @@ __global__ void __launch_bounds__(THREADS) eri_batch_lockstep_kernel(BasisDev bs
             const int ij = xx / nket, kl = xx - ij * nket;
             const PrimPairData ab = shell_prim_pair(bs, s.x, ij / nj, s.y, ij % nj);
             const PrimPairData cd = shell_prim_pair(bs, s.z, kl / nl, s.w, kl % nl);
-            Cls::template quartet<MaskedStoreSink<Cls::LB, Cls::LC, Cls::LD>, true>(ab, cd, boys_table, rs, THREADS,
-                                                                                   sink);
+            Cls::template quartet<RT, MaskedStoreSink<RT, Cls::LB, Cls::LC, Cls::LD>, true>(ab, cd, boys_table, rs,
+                                                                                           THREADS, sink);
         }
     }
 }
@@ -162,7 +170,7 @@ __global__ void __launch_bounds__(THREADS) schwarz_kernel(PairListDev pl, PrimPa
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= pl.n) return;
-    double* rs = qcg_smem + threadIdx.x;
+    double* rs = r_slice<double>();
     DiagSink<Cls::LA, Cls::LB> sink;
 #pragma unroll
     for (int k = 0; k < DiagSink<Cls::LA, Cls::LB>::NAB; ++k) sink.acc[k] = 0.0;
@@ -173,7 +181,7 @@ __global__ void __launch_bounds__(THREADS) schwarz_kernel(PairListDev pl, PrimPa
         for (int y = 0; y < n; ++y)
         {
             const PrimPairData cd = load_pp(P, o + y);
-            Cls::quartet(ab, cd, boys_table, rs, THREADS, sink);
+            Cls::template quartet<double>(ab, cd, boys_table, rs, THREADS, sink);
         }
     }
     double m = 0.0;
@@ -191,7 +199,7 @@ __global__ void __launch_bounds__(THREADS) schwarz_kernel(PairListDev pl, PrimPa
 // and J = J' + J'^T, K = K' + K'^T afterwards.  Partial sums are kept in registers along the
 // component loops; what leaves the thread goes to the L2-resident J'/K' with red.global.add.f64.
 // ------------------------------------------------------------------------------------------------
-template <int LA, int LB, int LC, int LD>
+template <class RT, int LA, int LB, int LC, int LD>
 struct JKSink
 {
     static constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD), NAB = NA * NB;
@@ -237,9 +245,9 @@ struct JKSink
             kbd[k] = 0.0;
         }
     }
-    __device__ __forceinline__ void operator()(int ia, int ib, int, int, double v)
+    __device__ __forceinline__ void operator()(int ia, int ib, int, int, RT v)
     {
-        const double w = s * v;
+        const double w = s * (double)v;   // FP64 accumulation in either arithmetic type
         jab[ia * NB + ib] += w * dls;
         jcd += w * __ldg(D + (size_t)(fa + ia) * n + fb + ib);
         kac[ia] += w * dbs[ib];
@@ -281,13 +289,17 @@ struct JKSink
 // lane usually share the bra pair: the bra pair is found by one binary search per run and then advanced,
 // and the bra-side J' sums stay in registers until the bra pair changes.  RUN is chosen by the launcher
 // from the class's quartet count (1 for small molecules, where parallelism matters more).
-template <class Cls, int THREADS>
+// RT is the arithmetic type of the ERI evaluation; a launch takes the quartets whose bound (Q_ab Q_cd, times
+// the density maximum when density screening is on) lies in [w.lo, w.hi), so that an FP64 and an FP32
+// launch split one build between them.
+template <class Cls, int THREADS, class RT>
 __global__ void __launch_bounds__(THREADS) jk_kernel(JKWorkDev w, PairListDev bra, PairListDev ket, PrimPairsDev P,
                                                      const int* __restrict__ shell_f0, const double* __restrict__ D,
                                                      double* __restrict__ J, double* __restrict__ K, int n,
                                                      const double* __restrict__ boys_table, int RUN)
 {
-    double* rs = qcg_smem + threadIdx.x;
+    RT* rs = r_slice<RT>();
+    const bool banded = w.lo > 0.0 || w.hi < 1e300;
     const int lane = threadIdx.x & 31;
     const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     const long long nwarp = ((long long)gridDim.x * blockDim.x) >> 5;
@@ -305,7 +317,7 @@ __global__ void __launch_bounds__(THREADS) jk_kernel(JKWorkDev w, PairListDev br
         }
         int i = lo;
         long long next = w.offs[i + 1];
-        JKSink<Cls::LA, Cls::LB, Cls::LC, Cls::LD> sink;
+        JKSink<RT, Cls::LA, Cls::LB, Cls::LC, Cls::LD> sink;
         sink.D = D; sink.J = J; sink.K = K; sink.n = n;
         int sa = bra.sa[i], sb = bra.sb[i];
         sink.set_bra(shell_f0[sa], shell_f0[sb]);
@@ -332,7 +344,13 @@ __global__ void __launch_bounds__(THREADS) jk_kernel(JKWorkDev w, PairListDev br
                 double m = fmax(M[sa * ns + sb], M[sc * ns + sd]);
                 m = fmax(m, fmax(M[sa * ns + sc], M[sa * ns + sd]));
                 m = fmax(m, fmax(M[sb * ns + sc], M[sb * ns + sd]));
-                if (bra.Q[i] * ket.Q[j] * m < w.dthr) continue;
+                const double bnd = bra.Q[i] * ket.Q[j] * m;
+                if (bnd < w.dthr || (banded && (bnd < w.lo || bnd >= w.hi))) continue;
+            }
+            else if (banded)
+            {
+                const double bnd = bra.Q[i] * ket.Q[j];
+                if (bnd < w.lo || bnd >= w.hi) continue;
             }
             sink.fc = shell_f0[sc];
             sink.fd = shell_f0[sd];
@@ -344,7 +362,7 @@ __global__ void __launch_bounds__(THREADS) jk_kernel(JKWorkDev w, PairListDev br
                 for (int y = 0; y < nj; ++y)
                 {
                     const PrimPairData cd = load_pp(P, oj + y);
-                    Cls::quartet(ab, cd, boys_table, rs, THREADS, sink);
+                    Cls::template quartet<RT>(ab, cd, boys_table, rs, THREADS, sink);
                 }
             }
         }

@@ -303,29 +303,35 @@ void launch_one_electron(const BasisDev& bs, const int* f0, int n, int natom, co
 }   // namespace qcg
 
 // ------------------------------------------------------------------------------------------------
-// FP64 FMA throughput probe: 8 independent dependency chains per thread, ITER fused multiply-adds
-// each, full grid.  Used to measure the roofline denominator of the ERI kernels on the running GPU.
+// FMA throughput probe (FP64 or FP32): 8 independent dependency chains per thread, ITER fused
+// multiply-adds each, full grid.  Measures the roofline denominators of the ERI kernels on the running GPU.
 // ------------------------------------------------------------------------------------------------
 namespace qcg {
-__global__ void dfma_peak_kernel(double* out, int iters, double a, double b)
+template <class T>
+__global__ void fma_peak_kernel(T* out, int iters, T a, T b)
 {
-    double x0 = threadIdx.x * 1e-9, x1 = x0 + 1e-9, x2 = x0 + 2e-9, x3 = x0 + 3e-9;
-    double x4 = x0 + 4e-9, x5 = x0 + 5e-9, x6 = x0 + 6e-9, x7 = x0 + 7e-9;
+    T x0 = threadIdx.x * T(1e-9), x1 = x0 + T(1e-9), x2 = x0 + T(2e-9), x3 = x0 + T(3e-9);
+    T x4 = x0 + T(4e-9), x5 = x0 + T(5e-9), x6 = x0 + T(6e-9), x7 = x0 + T(7e-9);
     for (int i = 0; i < iters; ++i)
     {
 #pragma unroll
         for (int k = 0; k < 16; ++k)
         {
-            x0 = fma(x0, a, b); x1 = fma(x1, a, b); x2 = fma(x2, a, b); x3 = fma(x3, a, b);
-            x4 = fma(x4, a, b); x5 = fma(x5, a, b); x6 = fma(x6, a, b); x7 = fma(x7, a, b);
+            x0 = qfma(x0, a, b); x1 = qfma(x1, a, b); x2 = qfma(x2, a, b); x3 = qfma(x3, a, b);
+            x4 = qfma(x4, a, b); x5 = qfma(x5, a, b); x6 = qfma(x6, a, b); x7 = qfma(x7, a, b);
         }
     }
-    const double s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
-    if (s == 1234.5678) out[0] = s;   // keeps the chains alive; never true for these inputs
+    const T s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+    if (s == T(1234.5678)) out[0] = s;   // keeps the chains alive; never true for these inputs
 }
 
 void launch_dfma_peak(double* out, int blocks, int threads, int iters, cudaStream_t st)
 {
-    dfma_peak_kernel<<<blocks, threads, 0, st>>>(out, iters, 0.999999, 1e-7);
+    fma_peak_kernel<double><<<blocks, threads, 0, st>>>(out, iters, 0.999999, 1e-7);
+}
+
+void launch_ffma_peak(float* out, int blocks, int threads, int iters, cudaStream_t st)
+{
+    fma_peak_kernel<float><<<blocks, threads, 0, st>>>(out, iters, 0.999999f, 1e-7f);
 }
 }   // namespace qcg

@@ -7,6 +7,8 @@ For class (LA LB | LC LD) the generated device function evaluates ONE primitive 
   R value read once per (c,d); then for every bra component (a,b) the factored sum
   sum_t Ex_t sum_u Ey_u sum_v Ez_v X_{tuv} and the sink call.
 All indices are literals, so nvcc keeps the tables in registers without any constexpr folding work.
+The code is a template on the arithmetic type RT (double, or float for the FP32 form); the primitive-pair
+data, the Boys argument and the prefactor lambda are formed in FP64 and rounded to RT once.
 
 Recursions follow qchem: R (Internal/MnD/Imp/RNLM.C:19-68), E (PG_Cart_MnD/Internal/Imp/Hermite2.C:95-139),
 Boys (Internal/Boys/Imp/AuxillaryFJ.C:13-48), prefactor (PG_Cart_MnD/Imp/GaussianRF.C:446-483).
@@ -67,7 +69,7 @@ def lit(x):
 
 def gen_E(name, LA, LB, PA, PB, a12):
     """1-D E table of one direction as scalars name_i_j_t, in the build order of Hermite2.C."""
-    out = [f"const double {name}_0_0_0 = 1.0;"]
+    out = [f"const RT {name}_0_0_0 = RT(1);"]
 
     def g(i, j, t):
         return f"{name}_{i}_{j}_{t}"
@@ -79,16 +81,16 @@ def gen_E(name, LA, LB, PA, PB, a12):
         if t <= i0 + j0:
             terms.append(f"{g(i0, j0, t)} * {P}")
         if t + 1 <= i0 + j0:
-            terms.append(f"{g(i0, j0, t + 1)} * {t + 1}.0")
+            terms.append(f"{g(i0, j0, t + 1)} * RT({t + 1})")
         return " + ".join(terms)
 
     for i in range(1, LA + 1):
         for t in range(0, i + 1):
-            out.append(f"const double {name}_{i}_0_{t} = {expr(i - 1, 0, t, PA)};")
+            out.append(f"const RT {name}_{i}_0_{t} = {expr(i - 1, 0, t, PA)};")
     for i in range(0, LA + 1):
         for j in range(1, LB + 1):
             for t in range(0, i + j + 1):
-                out.append(f"const double {name}_{i}_{j}_{t} = {expr(i, j - 1, t, PB)};")
+                out.append(f"const RT {name}_{i}_{j}_{t} = {expr(i, j - 1, t, PB)};")
     return out
 
 
@@ -98,12 +100,12 @@ CHUNK_OUTPUTS = 72         # ... of at most this many outputs (keeps each chunk'
 
 def e_tables(LA, LB, LC, LD):
     out = []
-    for dname, la, lb, PA, PB, a12 in (("ebx", LA, LB, "ab.PAx", "ab.PBx", "a12b"),
-                                       ("eby", LA, LB, "ab.PAy", "ab.PBy", "a12b"),
-                                       ("ebz", LA, LB, "ab.PAz", "ab.PBz", "a12b"),
-                                       ("ekx", LC, LD, "cd.PAx", "cd.PBx", "a12k"),
-                                       ("eky", LC, LD, "cd.PAy", "cd.PBy", "a12k"),
-                                       ("ekz", LC, LD, "cd.PAz", "cd.PBz", "a12k")):
+    for dname, la, lb, PA, PB, a12 in (("ebx", LA, LB, "bPAx", "bPBx", "a12b"),
+                                       ("eby", LA, LB, "bPAy", "bPBy", "a12b"),
+                                       ("ebz", LA, LB, "bPAz", "bPBz", "a12b"),
+                                       ("ekx", LC, LD, "kPAx", "kPBx", "a12k"),
+                                       ("eky", LC, LD, "kPAy", "kPBy", "a12k"),
+                                       ("ekz", LC, LD, "kPAz", "kPBz", "a12k")):
         out.extend(gen_E(dname, la, lb, PA, PB, a12))
     return out
 
@@ -121,18 +123,19 @@ def r_prologue(L, rsm, w):
     HL = nherm(L)
     w("    const double p = ab.p, q = cd.p, pq = p + q;")
     w("    const double alpha = p * q / pq;")
-    w("    const double X = ab.Px - cd.Px, Y = ab.Py - cd.Py, Z = ab.Pz - cd.Pz;")
-    w(f"    double F[{L + 1}];")
-    w(f"    boys<{L}>(alpha * (X * X + Y * Y + Z * Z), bt, F);")
-    w("    const double m2a = -2.0 * alpha;")
-    w(f"    double pwn[{L + 1}];")
-    w("    pwn[0] = 1.0;")
+    w("    const double Xd = ab.Px - cd.Px, Yd = ab.Py - cd.Py, Zd = ab.Pz - cd.Pz;")
+    w(f"    RT F[{L + 1}];")
+    w(f"    boys<{L}>(alpha * (Xd * Xd + Yd * Yd + Zd * Zd), bt, F);")
+    w("    const RT X = RT(Xd), Y = RT(Yd), Z = RT(Zd);")
+    w("    const RT m2a = RT(-2.0 * alpha);")
+    w(f"    RT pwn[{L + 1}];")
+    w("    pwn[0] = RT(1);")
     for n in range(1, L + 1):
         w(f"    pwn[{n}] = pwn[{n - 1}] * m2a;")
     if rsm:
         w("#define RR(i) rs[(i) * rstride]")
     else:
-        w(f"    double Rr[{HL}];")
+        w(f"    RT Rr[{HL}];")
         w("#define RR(i) Rr[i]")
     w(f"    RR(0) = pwn[{L}] * F[{L}];")
     for n in range(L - 1, -1, -1):
@@ -143,19 +146,19 @@ def r_prologue(L, rsm, w):
                     if t > 0:
                         e = f"X * RR({hidx(L, t - 1, u, v)})"
                         if t > 1:
-                            e += f" + {t - 1}.0 * RR({hidx(L, t - 2, u, v)})"
+                            e += f" + RT({t - 1}) * RR({hidx(L, t - 2, u, v)})"
                     elif u > 0:
                         e = f"Y * RR({hidx(L, 0, u - 1, v)})"
                         if u > 1:
-                            e += f" + {u - 1}.0 * RR({hidx(L, 0, u - 2, v)})"
+                            e += f" + RT({u - 1}) * RR({hidx(L, 0, u - 2, v)})"
                     else:
                         e = f"Z * RR({hidx(L, 0, 0, v - 1)})"
                         if v > 1:
-                            e += f" + {v - 1}.0 * RR({hidx(L, 0, 0, v - 2)})"
+                            e += f" + RT({v - 1}) * RR({hidx(L, 0, 0, v - 2)})"
                     w(f"    RR({hidx(L, t, u, v)}) = {e};")
         w(f"    RR(0) = pwn[{n}] * F[{n}];")
-    w("    const double lambda = 34.986836655249725693 / (p * q * sqrt(pq)) * ab.K * cd.K;")
-    w("    const double a12b = 0.5 / ab.p, a12k = 0.5 / cd.p;")
+    w("    const RT lambda = RT(34.986836655249725693 / (p * q * sqrt(pq)) * ab.K * cd.K);")
+    w("    const RT a12b = RT(0.5 / ab.p), a12k = RT(0.5 / cd.p);")
 
 
 def ket_blocks(LA, LB, LC, LD, cds, w):
@@ -172,32 +175,32 @@ def ket_blocks(LA, LB, LC, LD, cds, w):
                 for vp in range(c[2] + d[2] + 1)]
         for (tp, up, vp) in supp:
             sgn = "-" if (tp + up + vp) & 1 else ""
-            w(f"    const double s{tp}{up}{vp} = {sgn}ekx_{c[0]}_{d[0]}_{tp} * eky_{c[1]}_{d[1]}_{up} * "
+            w(f"    const RT s{tp}{up}{vp} = {sgn}ekx_{c[0]}_{d[0]}_{tp} * eky_{c[1]}_{d[1]}_{up} * "
               f"ekz_{c[2]}_{d[2]}_{vp};")
-        w("    double " + ", ".join(f"x{i} = 0.0" for i in range(NX)) + ";")
+        w("    RT " + ", ".join(f"x{i} = RT(0)" for i in range(NX)) + ";")
         contrib = {}
         for h in HAB:
             for hp in supp:
                 H = hidx(L, h[0] + hp[0], h[1] + hp[1], h[2] + hp[2])
                 contrib.setdefault(H, []).append((hidx(LAB, *h), hp))
         for H in sorted(contrib):
-            body = " ".join(f"x{xi} = fma(s{hp[0]}{hp[1]}{hp[2]}, r, x{xi});" for (xi, hp) in contrib[H])
-            w(f"    {{ const double r = RR({H}); {body} }}")
-        w(f"    const double lam_cd = lambda * {lit(comp_norm(c) * comp_norm(d))};")
+            body = " ".join(f"x{xi} = qfma(s{hp[0]}{hp[1]}{hp[2]}, r, x{xi});" for (xi, hp) in contrib[H])
+            w(f"    {{ const RT r = RR({H}); {body} }}")
+        w(f"    const RT lam_cd = lambda * RT({lit(comp_norm(c) * comp_norm(d))});")
         for ia, a in enumerate(A):
             for ib, b in enumerate(B):
                 w("    {")
-                w("      double sx = 0.0;")
+                w("      RT sx = RT(0);")
                 for t in range(a[0] + b[0] + 1):
-                    w("      { double sy = 0.0;")
+                    w("      { RT sy = RT(0);")
                     for u in range(a[1] + b[1] + 1):
                         vs = list(range(a[2] + b[2] + 1))
                         zs = f"ebz_{a[2]}_{b[2]}_0 * x{hidx(LAB, t, u, 0)}"
                         for v in vs[1:]:
-                            zs = f"fma(ebz_{a[2]}_{b[2]}_{v}, x{hidx(LAB, t, u, v)}, {zs})"
-                        w(f"        sy = fma(eby_{a[1]}_{b[1]}_{u}, {zs}, sy);")
-                    w(f"        sx = fma(ebx_{a[0]}_{b[0]}_{t}, sy, sx); }}")
-                w(f"      sink({ia}, {ib}, {ic}, {id_}, sx * (lam_cd * {lit(comp_norm(a) * comp_norm(b))}));")
+                            zs = f"qfma(ebz_{a[2]}_{b[2]}_{v}, x{hidx(LAB, t, u, v)}, {zs})"
+                        w(f"        sy = qfma(eby_{a[1]}_{b[1]}_{u}, {zs}, sy);")
+                    w(f"        sx = qfma(ebx_{a[0]}_{b[0]}_{t}, sy, sx); }}")
+                w(f"      sink({ia}, {ib}, {ic}, {id_}, sx * (lam_cd * RT({lit(comp_norm(a) * comp_norm(b))})));")
                 w("    }")
         w(f"    sink.ket_end({ic}, {id_});")
         w("    }")
@@ -228,18 +231,14 @@ def gen_class(LA, LB, LC, LD, idx):
             fn = f"prim_quartet_{idx}_chunk{ci}"
             chunk_names.append(fn)
             # each chunk rebuilds the 1-D E tables from the pair scalars (cheaper than reloading them)
-            w("template <class Sink>")
-            w(f"__device__ __noinline__ void {fn}(const double* __restrict__ rs, const int rstride,")
-            w("    const double a12b, const double bPAx, const double bPAy, const double bPAz, const double bPBx,")
-            w("    const double bPBy, const double bPBz, const double a12k, const double kPAx, const double kPAy,")
-            w("    const double kPAz, const double kPBx, const double kPBy, const double kPBz, const double lambda,")
+            w("template <class RT, class Sink>")
+            w(f"__device__ __noinline__ void {fn}(const RT* __restrict__ rs, const int rstride,")
+            w("    const RT a12b, const RT bPAx, const RT bPAy, const RT bPAz, const RT bPBx,")
+            w("    const RT bPBy, const RT bPBz, const RT a12k, const RT kPAx, const RT kPAy,")
+            w("    const RT kPAz, const RT kPBx, const RT kPBy, const RT kPBz, const RT lambda,")
             w("    typename SinkArg<Sink>::type sink)")
             w("{")
             for s_ in e_tables(LA, LB, LC, LD):
-                s_ = (s_.replace("ab.PAx", "bPAx").replace("ab.PAy", "bPAy").replace("ab.PAz", "bPAz")
-                      .replace("ab.PBx", "bPBx").replace("ab.PBy", "bPBy").replace("ab.PBz", "bPBz")
-                      .replace("cd.PAx", "kPAx").replace("cd.PAy", "kPAy").replace("cd.PAz", "kPAz")
-                      .replace("cd.PBx", "kPBx").replace("cd.PBy", "kPBy").replace("cd.PBz", "kPBz"))
                 w("    " + s_)
             w("#define RR(i) rs[(i) * rstride]")
             ket_blocks(LA, LB, LC, LD, cds, w)
@@ -248,17 +247,21 @@ def gen_class(LA, LB, LC, LD, idx):
     # LOCKSTEP: the caller guarantees that every thread of the block executes this call (block-uniform
     # control flow); the barriers then keep the block's warps on the same chunk, so that the instruction
     # working set is one chunk rather than the whole class
-    w("template <class Sink, bool LOCKSTEP = false>")
+    w("template <class RT, class Sink, bool LOCKSTEP = false>")
     w(f"__device__ __forceinline__ void prim_quartet_{idx}(const PrimPairData& ab, const PrimPairData& cd,")
-    w("    const double* __restrict__ bt, double* __restrict__ rs, const int rstride, Sink& sink)")
+    w("    const double* __restrict__ bt, RT* __restrict__ rs, const int rstride, Sink& sink)")
     w("{")
     w("    (void)rs; (void)rstride;")
     r_prologue(L, rsm, w)
+    w("    const RT bPAx = RT(ab.PAx), bPAy = RT(ab.PAy), bPAz = RT(ab.PAz);")
+    w("    const RT bPBx = RT(ab.PBx), bPBy = RT(ab.PBy), bPBz = RT(ab.PBz);")
+    w("    const RT kPAx = RT(cd.PAx), kPAy = RT(cd.PAy), kPAz = RT(cd.PAz);")
+    w("    const RT kPBx = RT(cd.PBx), kPBy = RT(cd.PBy), kPBz = RT(cd.PBz);")
     if chunked:
         for fn in chunk_names:
             w("    if constexpr (LOCKSTEP) __syncthreads();")
-            w(f"    {fn}<Sink>(rs, rstride, a12b, ab.PAx, ab.PAy, ab.PAz, ab.PBx, ab.PBy, ab.PBz, a12k, cd.PAx, cd.PAy, "
-              f"cd.PAz, cd.PBx, cd.PBy, cd.PBz, lambda, sink);")
+            w(f"    {fn}<RT, Sink>(rs, rstride, a12b, bPAx, bPAy, bPAz, bPBx, bPBy, bPBz, a12k, kPAx, kPAy, "
+              f"kPAz, kPBx, kPBy, kPBz, lambda, sink);")
     else:
         for s_ in e_tables(LA, LB, LC, LD):
             w("    " + s_)

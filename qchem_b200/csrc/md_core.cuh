@@ -1,4 +1,4 @@
-// md_core.cuh -- McMurchie-Davidson building blocks for sm_100a, FP64.
+// md_core.cuh -- McMurchie-Davidson building blocks for sm_100a (FP64, with an FP32 form).
 //
 // Per primitive quartet the work is (qchem: src/BasisSet/Molecule/Evaluators/PG_Cart_MnD/Imp/GaussianRF.C:446-483)
 //   1. Boys F_0..F_L(T), T = alpha |PQ|^2, alpha = pq/(p+q)   (Internal/Boys/Imp/AuxillaryFJ.C:13-48)
@@ -124,6 +124,44 @@ __device__ __forceinline__ void boys(double T, const double* __restrict__ table,
         for (int j = 0; j < JMAX; ++j) F[j + 1] = ((2 * j + 1) * F[j] - et) * inv2T;
     }
 }
+
+// FP32 form of the Boys function.  FP64 is kept where the table and the downward recursion live (T < 12);
+// above, the asymptotic branches are evaluated in FP32.
+template <int JMAX>
+__device__ __forceinline__ void boys(double T, const double* __restrict__ table, float (&F)[JMAX + 1])
+{
+    if (T < 12.0)
+    {
+        double Fd[JMAX + 1];
+        boys<JMAX>(T, table, Fd);
+#pragma unroll
+        for (int j = 0; j <= JMAX; ++j) F[j] = (float)Fd[j];
+    }
+    else
+    {
+        const float Tf = (float)T, et = expf(-Tf), iT = 1.0f / Tf;
+        float F0;
+        if (Tf < 30.0f)
+        {
+            float g;
+            if (Tf < 15.0f) g = 0.4999489092f - 0.2473631686f * iT + 0.321180909f * iT * iT - 0.3811559346f * iT * iT * iT;
+            else if (Tf < 18.0f) g = 0.4998436875f - 0.24249438f * iT + 0.24642845f * iT * iT;
+            else if (Tf < 24.0f) g = 0.499093162f - 0.2152832f * iT;
+            else g = 0.49f;
+            F0 = 0.5f * sqrtf(3.14159265358979f * iT) - et * g * iT;
+        }
+        else
+            F0 = 0.5f * sqrtf(3.14159265358979f * iT);
+        F[0] = F0;
+        const float inv2T = 0.5f * iT;
+#pragma unroll
+        for (int j = 0; j < JMAX; ++j) F[j + 1] = ((float)(2 * j + 1) * F[j] - et) * inv2T;
+    }
+}
+
+// fused multiply-add in the generated code's arithmetic type
+__device__ __forceinline__ double qfma(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ float qfma(float a, float b, float c) { return fmaf(a, b, c); }
 
 // Primitive-pair data: exponent sum, centre, P-A, P-B, and the prefactor K (contraction coefficients,
 // radial normalisations and exp(-ab/p |AB|^2) folded together).

@@ -52,24 +52,33 @@ struct JKWorkDev
     const double* dmax;
     int nshell;
     double dthr;
+    // precision band: this launch evaluates the quartets whose bound lies in [lo, hi) (0 and >= 1e300:
+    // every quartet)
+    double lo, hi;
 };
 
 void launch_block_max(const double* D, const int* shell_f0, const int* shell_L, int nshell, int n, double* dmax,
                       cudaStream_t st, int nsm);
 
-// launchers, one object file per quartet class (eri_class.cu compiled with -DQCG_CLASS=k)
+// launchers, two object files per quartet class (eri_class.cu compiled with -DQCG_CLASS=k and
+// -DQCG_PREC=64 or 32)
 using EriBatchLauncher = void (*)(const BasisDev&, const int4*, const int*, long long, double*, const double*,
                                   cudaStream_t, int);
 using JKLauncher = void (*)(const JKWorkDev&, const PairListDev&, const PairListDev&, const PrimPairsDev&, const int*,
                             const double*, double*, double*, int, const double*, cudaStream_t, int);
 using SchwarzLauncher = void (*)(const PairListDev&, const PrimPairsDev&, double*, const double*, cudaStream_t);
 
+using EriBatch32Launcher = void (*)(const BasisDev&, const int4*, const int*, long long, float*, const double*,
+                                    cudaStream_t, int);
+
 extern const EriBatchLauncher kEriBatchLaunchers[kNumQuartetClasses];
+extern const EriBatch32Launcher kEriBatch32Launchers[kNumQuartetClasses];
 
 // counting sort of a quartet batch by contraction pattern -> order (a permutation of 0..nq-1)
 void launch_pattern_sort(const BasisDev& bs, const int4* quartets, long long nq, unsigned char* key, int* hist,
                          int* cursor, int* order, cudaStream_t st, int nsm);
-extern const JKLauncher kJKLaunchers[kNumQuartetClasses];
+extern const JKLauncher kJKLaunchers[kNumQuartetClasses];     // FP64 evaluation
+extern const JKLauncher kJK32Launchers[kNumQuartetClasses];   // FP32 evaluation, FP64 accumulation
 extern const SchwarzLauncher kSchwarzLaunchers[kNumPairClasses];
 
 }   // namespace qcg

@@ -1,4 +1,4 @@
-// registry.cu -- tables of the per-class launchers compiled in the 21 eri_class objects.
+// registry.cu -- tables of the per-class launchers compiled in the 42 eri_class objects (21 classes x FP64/FP32).
 #include "qcg_internal.h"
 
 namespace qcg {
@@ -8,7 +8,11 @@ namespace qcg {
                               cudaStream_t, int);                                                                   \
     void launch_jk_##k(const JKWorkDev&, const PairListDev&, const PairListDev&, const PrimPairsDev&, const int*,    \
                        const double*, double*, double*, int, const double*, cudaStream_t, int);                      \
-    void launch_schwarz_##k(const PairListDev&, const PrimPairsDev&, double*, const double*, cudaStream_t);
+    void launch_schwarz_##k(const PairListDev&, const PrimPairsDev&, double*, const double*, cudaStream_t);      \
+    void launch_eri_batch32_##k(const BasisDev&, const int4*, const int*, long long, float*, const double*,        \
+                                cudaStream_t, int);                                                                 \
+    void launch_jk32_##k(const JKWorkDev&, const PairListDev&, const PairListDev&, const PrimPairsDev&, const int*,  \
+                         const double*, double*, double*, int, const double*, cudaStream_t, int);
 QCG_DECL(0) QCG_DECL(1) QCG_DECL(2) QCG_DECL(3) QCG_DECL(4) QCG_DECL(5) QCG_DECL(6) QCG_DECL(7) QCG_DECL(8)
 QCG_DECL(9) QCG_DECL(10) QCG_DECL(11) QCG_DECL(12) QCG_DECL(13) QCG_DECL(14) QCG_DECL(15) QCG_DECL(16)
 QCG_DECL(17) QCG_DECL(18) QCG_DECL(19) QCG_DECL(20)
@@ -24,6 +28,16 @@ const JKLauncher kJKLaunchers[kNumQuartetClasses] = {
     launch_jk_0,  launch_jk_1,  launch_jk_2,  launch_jk_3,  launch_jk_4,  launch_jk_5,  launch_jk_6,
     launch_jk_7,  launch_jk_8,  launch_jk_9,  launch_jk_10, launch_jk_11, launch_jk_12, launch_jk_13,
     launch_jk_14, launch_jk_15, launch_jk_16, launch_jk_17, launch_jk_18, launch_jk_19, launch_jk_20};
+const EriBatch32Launcher kEriBatch32Launchers[kNumQuartetClasses] = {
+    launch_eri_batch32_0,  launch_eri_batch32_1,  launch_eri_batch32_2,  launch_eri_batch32_3,  launch_eri_batch32_4,
+    launch_eri_batch32_5,  launch_eri_batch32_6,  launch_eri_batch32_7,  launch_eri_batch32_8,  launch_eri_batch32_9,
+    launch_eri_batch32_10, launch_eri_batch32_11, launch_eri_batch32_12, launch_eri_batch32_13, launch_eri_batch32_14,
+    launch_eri_batch32_15, launch_eri_batch32_16, launch_eri_batch32_17, launch_eri_batch32_18, launch_eri_batch32_19,
+    launch_eri_batch32_20};
+const JKLauncher kJK32Launchers[kNumQuartetClasses] = {
+    launch_jk32_0,  launch_jk32_1,  launch_jk32_2,  launch_jk32_3,  launch_jk32_4,  launch_jk32_5,  launch_jk32_6,
+    launch_jk32_7,  launch_jk32_8,  launch_jk32_9,  launch_jk32_10, launch_jk32_11, launch_jk32_12, launch_jk32_13,
+    launch_jk32_14, launch_jk32_15, launch_jk32_16, launch_jk32_17, launch_jk32_18, launch_jk32_19, launch_jk32_20};
 // diagonal classes X == Y have quartet index X(X+1)/2 + X
 const SchwarzLauncher kSchwarzLaunchers[kNumPairClasses] = {launch_schwarz_0, launch_schwarz_2,  launch_schwarz_5,
                                                             launch_schwarz_9, launch_schwarz_14, launch_schwarz_20};

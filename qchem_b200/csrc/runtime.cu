@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <array>
 #include <chrono>
+#include <type_traits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -27,6 +28,7 @@ void launch_symmetrize(const double* Jp, const double* Kp, double* J, double* K,
 void launch_one_electron(const BasisDev& bs, const int* f0, int n, int natom, const double* Z, const double* R,
                          double* S, double* T, double* V, const double* boys, cudaStream_t st, int nsm);
 void launch_dfma_peak(double* out, int blocks, int threads, int iters, cudaStream_t st);
+void launch_ffma_peak(float* out, int blocks, int threads, int iters, cudaStream_t st);
 }   // namespace qcg
 
 using namespace qcg;
@@ -114,6 +116,8 @@ struct qcg_handle
     PairListDev pl_dev[kNumPairClasses]{};
     PrimPairsDev pp_dev{};
     JKWorkDev work[kNumQuartetClasses]{};
+    double fp32_below = 0;   // qcg_set_fp32_bound: quartets with a smaller bound are evaluated in FP32
+    double* d_dmaxD = nullptr;   // per shell-pair max |D| of a full build's density (mixed precision)
     long long work_quartets = 0, work_prim_quartets = 0;
     double work_flops = 0;
     std::vector<double> Qfull;
@@ -227,13 +231,17 @@ double prim_norm(double a, int L)
 //   1. Householder reduction to tridiagonal T = Q^T A Q, one reflector per column,
 //   2. implicit symmetric QR steps with a Wilkinson shift on T (bulge chasing with Givens rotations),
 //      rotations accumulated into V = Q G_1^T G_2^T ...
+// The accumulated matrix is kept transposed (Qt[k][r] = Q[r][k]) so that both the reflectors and the
+// rotations of a sweep update contiguous rows: a sweep is applied to blocks of 32 columns of Qt at a time,
+// each block walking the whole rotation chain with its running row in registers.
 // ------------------------------------------------------------------------------------------------
 void syev(int n, const double* Ain, double* w, double* V)
 {
-    std::vector<double> T(Ain, Ain + (size_t)n * n), Q((size_t)n * n, 0.0), v(n), pv(n), wv(n);
+    std::vector<double> T(Ain, Ain + (size_t)n * n), Qt((size_t)n * n, 0.0), v(n), pv(n), wv(n), sr(n);
     auto t = [&](int i, int j) -> double& { return T[(size_t)i * n + j]; };
-    auto q = [&](int i, int j) -> double& { return Q[(size_t)i * n + j]; };
-    for (int i = 0; i < n; ++i) q(i, i) = 1.0;
+    auto qt = [&](int k, int r) -> double* { return Qt.data() + (size_t)k * n + r; };
+    for (int i = 0; i < n; ++i) *qt(i, i) = 1.0;
+    const bool par = n >= 192;
     for (int k = 0; k + 2 < n; ++k)
     {
         // reflector H = I - beta v v^T mapping x = T[k+1:, k] onto alpha e_1
@@ -249,29 +257,45 @@ void syev(int n, const double* Ain, double* w, double* V)
         if (vv == 0.0) continue;
         const double beta = 2.0 / vv;
         // trailing block update: A <- A - v w^T - w v^T with p = beta A v, w = p - (beta p.v / 2) v
-        double pdv = 0.0;
+#pragma omp parallel for schedule(static) if (par && n - k > 96)
         for (int i = k + 1; i < n; ++i)
         {
+            const double* ti = &t(i, 0);
             double s = 0.0;
-            for (int j = k + 1; j < n; ++j) s += t(i, j) * v[j];
+            for (int j = k + 1; j < n; ++j) s += ti[j] * v[j];
             pv[i] = beta * s;
-            pdv += pv[i] * v[i];
         }
+        double pdv = 0.0;
+        for (int i = k + 1; i < n; ++i) pdv += pv[i] * v[i];
         for (int i = k + 1; i < n; ++i) wv[i] = pv[i] - 0.5 * beta * pdv * v[i];
+#pragma omp parallel for schedule(static) if (par && n - k > 96)
         for (int i = k + 1; i < n; ++i)
-            for (int j = k + 1; j < n; ++j) t(i, j) -= v[i] * wv[j] + wv[i] * v[j];
+        {
+            double* ti = &t(i, 0);
+            const double vi = v[i], wi = wv[i];
+            for (int j = k + 1; j < n; ++j) ti[j] -= vi * wv[j] + wi * v[j];
+        }
         t(k + 1, k) = t(k, k + 1) = alpha;
         for (int i = k + 2; i < n; ++i) t(i, k) = t(k, i) = 0.0;
-        // Q <- Q H
-        for (int r = 0; r < n; ++r)
+        // Q <- Q H, i.e. Qt <- H Qt: s_r = sum_i v_i Qt[i][r], Qt[j][r] -= beta v_j s_r
+        std::fill(sr.begin(), sr.end(), 0.0);
+        for (int i = k + 1; i < n; ++i)
         {
-            double s = 0.0;
-            for (int j = k + 1; j < n; ++j) s += q(r, j) * v[j];
-            s *= beta;
-            for (int j = k + 1; j < n; ++j) q(r, j) -= s * v[j];
+            const double vi = v[i];
+            const double* qi = qt(i, 0);
+            for (int r = 0; r < n; ++r) sr[r] += vi * qi[r];
+        }
+#pragma omp parallel for schedule(static) if (par)
+        for (int j = k + 1; j < n; ++j)
+        {
+            double* qj = qt(j, 0);
+            const double f = beta * v[j];
+            for (int r = 0; r < n; ++r) qj[r] -= f * sr[r];
         }
     }
-    // rotation G on (k,k+1): T <- G T G^T, Q <- Q G^T, G = [[c, s], [-s, c]]
+    // rotation G on (k,k+1): T <- G T G^T, G = [[c, s], [-s, c]]; the matching Qt <- G Qt updates of one
+    // sweep are recorded and applied afterwards
+    std::vector<double> rc(n), rs(n);
     auto rotate = [&](int k, double c, double s, int lo, int hi) {
         for (int j = lo; j <= hi; ++j)
         {
@@ -285,11 +309,33 @@ void syev(int n, const double* Ain, double* w, double* V)
             t(i, k) = c * a + s * b;
             t(i, k + 1) = -s * a + c * b;
         }
-        for (int r = 0; r < n; ++r)
+        rc[k] = c;
+        rs[k] = s;
+    };
+    constexpr int RB = 32;
+    const int nblk = (n + RB - 1) / RB;
+    auto apply_sweep = [&](int l, int m) {
+#pragma omp parallel for schedule(static) if (par && m - l > 32)
+        for (int blk = 0; blk < nblk; ++blk)
         {
-            const double a = q(r, k), b = q(r, k + 1);
-            q(r, k) = c * a + s * b;
-            q(r, k + 1) = -s * a + c * b;
+            const int r0 = blk * RB, nr = std::min(RB, n - r0);
+            double a[RB];
+            const double* ql = qt(l, r0);
+            for (int r = 0; r < nr; ++r) a[r] = ql[r];
+            for (int k = l; k < m; ++k)
+            {
+                double* qk = qt(k, r0);
+                const double* qk1 = qt(k + 1, r0);
+                const double c = rc[k], s = rs[k];
+                for (int r = 0; r < nr; ++r)
+                {
+                    const double b = qk1[r];
+                    qk[r] = c * a[r] + s * b;
+                    a[r] = -s * a[r] + c * b;
+                }
+            }
+            double* qm = qt(m, r0);
+            for (int r = 0; r < nr; ++r) qm[r] = a[r];
         }
     };
     const double eps = 1e-15;
@@ -313,7 +359,7 @@ void syev(int n, const double* Ain, double* w, double* V)
         double x = t(l, l) - mu, z = t(l + 1, l);
         for (int k = l; k < m; ++k)
         {
-            const double r = std::hypot(x, z);
+            const double r = std::sqrt(x * x + z * z);
             const double c = r == 0.0 ? 1.0 : x / r, s = r == 0.0 ? 0.0 : z / r;
             rotate(k, c, s, std::max(l, k - 1), std::min(m, k + 2));
             if (k + 1 < m)
@@ -322,6 +368,7 @@ void syev(int n, const double* Ain, double* w, double* V)
                 z = t(k + 2, k);
             }
         }
+        apply_sweep(l, m);
     }
     std::vector<int> idx(n);
     std::iota(idx.begin(), idx.end(), 0);
@@ -329,7 +376,8 @@ void syev(int n, const double* Ain, double* w, double* V)
     for (int j = 0; j < n; ++j)
     {
         w[j] = t(idx[j], idx[j]);
-        for (int r = 0; r < n; ++r) V[(size_t)r * n + j] = q(r, idx[j]);
+        const double* qj = qt(idx[j], 0);
+        for (int r = 0; r < n; ++r) V[(size_t)r * n + j] = qj[r];
     }
 }
 
@@ -346,23 +394,27 @@ void gemm(int n, const double* A, bool ta, const double* B, bool tb, double* C)
             for (int j = 0; j < n; ++j) At[(size_t)i * n + j] = A[(size_t)j * n + i];
         a = At.data();
     }
-    if (!tb)
+    if (tb)
     {
         Bt.resize((size_t)n * n);
         for (int i = 0; i < n; ++i)
             for (int j = 0; j < n; ++j) Bt[(size_t)i * n + j] = B[(size_t)j * n + i];
         b = Bt.data();
     }
-    // C_ij = sum_k a_ik bT_jk
+    // row i of C = sum_k a_ik (row k of b): contiguous rows, vectorisable without reassociation
+#pragma omp parallel for schedule(static) if (n > 96)
     for (int i = 0; i < n; ++i)
-        for (int j = 0; j < n; ++j)
+    {
+        double* ci = C + (size_t)i * n;
+        const double* ai = a + (size_t)i * n;
+        for (int j = 0; j < n; ++j) ci[j] = 0.0;
+        for (int k = 0; k < n; ++k)
         {
-            const double* ai = a + (size_t)i * n;
-            const double* bj = b + (size_t)j * n;
-            double s = 0.0;
-            for (int k = 0; k < n; ++k) s += ai[k] * bj[k];
-            C[(size_t)i * n + j] = s;
+            const double aik = ai[k];
+            const double* bk = b + (size_t)k * n;
+            for (int j = 0; j < n; ++j) ci[j] += aik * bk[j];
         }
+    }
 }
 
 std::vector<double> solve_dense(int n, std::vector<double> A, std::vector<double> b)
@@ -567,6 +619,8 @@ void build_screening(qcg_handle* h, double thresh)
             h->work[k].total = offs.back();
             h->work[k].offs = h->upload(offs);
             h->work[k].same_class = (X == Y);
+            h->work[k].lo = 0.0;
+            h->work[k].hi = HUGE_VAL;
             h->work_quartets += offs.back();
             h->work_prim_quartets += pq;
             h->work_flops += (double)pq * class_flops(kPairLA[X], kPairLB[X], kPairLA[Y], kPairLB[Y]);
@@ -576,13 +630,23 @@ void build_screening(qcg_handle* h, double thresh)
     h->screened = true;
 }
 
+// fp32_below: quartets whose density-weighted bound Q_ab Q_cd max|D| (max over the six D blocks the
+// quartet digests) is below it are evaluated in FP32 (FP64 accumulation); 0 = all FP64, HUGE_VAL = all
+// FP32.  The weighting is what makes FP32 safe: the FP32 error of a quartet's contribution to J and K is
+// about 3e-7 of its bound.  dmax (the density maxima of dD) is computed here when the caller has none.
 void jk_device(qcg_handle* h, const double* dD, double* dJ, double* dK, int flags, qcg_stats* stats,
-               const double* dmax = nullptr, double dthr = 0.0)
+               const double* dmax = nullptr, double dthr = 0.0, double fp32_below = 0.0)
 {
     require(h->screened, "qcg_schwarz must be called before qcg_fock_jk", QCG_ERR_STATE);
     ensure_jk_buffers(h);
     const int n = h->nbf;
     const size_t nn = (size_t)n * n;
+    if (fp32_below > 0 && fp32_below < HUGE_VAL && !dmax)
+    {
+        if (!h->d_dmaxD) h->d_dmaxD = h->alloc<double>((size_t)h->nshell * h->nshell);
+        launch_block_max(dD, h->d_f0, h->bs.L, h->nshell, n, h->d_dmaxD, h->stream, h->nsm);
+        dmax = h->d_dmaxD;
+    }
     if (!h->ev0)
     {
         CK(cudaEventCreate(&h->ev0));
@@ -626,9 +690,22 @@ void jk_device(qcg_handle* h, const double* dD, double* dJ, double* dK, int flag
         wk.dmax = dmax;
         wk.nshell = h->nshell;
         wk.dthr = dthr;
-        kJKLaunchers[k](wk, h->pl_dev[X], h->pl_dev[Y], h->pp_dev, h->d_f0, dD, h->d_Jp, h->d_Kp, n, h->d_boys,
-                        h->side[slot], h->nsm);
-        slot = (slot + 1) % qcg_handle::kSide;
+        if (fp32_below < HUGE_VAL)
+        {
+            wk.lo = fp32_below;
+            wk.hi = HUGE_VAL;
+            kJKLaunchers[k](wk, h->pl_dev[X], h->pl_dev[Y], h->pp_dev, h->d_f0, dD, h->d_Jp, h->d_Kp, n, h->d_boys,
+                            h->side[slot], h->nsm);
+            slot = (slot + 1) % qcg_handle::kSide;
+        }
+        if (fp32_below > 0)
+        {
+            wk.lo = 0.0;
+            wk.hi = fp32_below;
+            kJK32Launchers[k](wk, h->pl_dev[X], h->pl_dev[Y], h->pp_dev, h->d_f0, dD, h->d_Jp, h->d_Kp, n, h->d_boys,
+                              h->side[slot], h->nsm);
+            slot = (slot + 1) % qcg_handle::kSide;
+        }
     }
     CK(cudaGetLastError());
     for (int s = 0; s < qcg_handle::kSide; ++s)
@@ -803,8 +880,21 @@ int qcg_norms(const qcg_handle* h, double* ns)
     return QCG_OK;
 }
 
-int qcg_eri_batch_device(qcg_handle* h, int la, int lb, int lc, int ld, long long nq, const int* d_quartets,
-                         double* d_out)
+extern "C++" {
+namespace {
+template <class T>
+void eri_batch_launch(qcg_handle* h, int k, const int* dq, long long m, T* dout)
+{
+    const int* order = batch_order(h, dq, m);
+    if constexpr (std::is_same_v<T, double>)
+        kEriBatchLaunchers[k](h->bs, (const int4*)dq, order, m, dout, h->d_boys, h->stream, h->nsm);
+    else
+        kEriBatch32Launchers[k](h->bs, (const int4*)dq, order, m, dout, h->d_boys, h->stream, h->nsm);
+    CK(cudaGetLastError());
+}
+
+template <class T>
+int eri_batch_device(qcg_handle* h, int la, int lb, int lc, int ld, long long nq, const int* d_quartets, T* d_out)
 {
     if (!h) return QCG_ERR_ARG;
     return guarded(h, [&] {
@@ -813,13 +903,12 @@ int qcg_eri_batch_device(qcg_handle* h, int la, int lb, int lc, int ld, long lon
         require(nq >= 0, "negative quartet count");
         if (nq == 0) return;
         require(d_quartets && d_out, "null argument");
-        const int* order = batch_order(h, d_quartets, nq);
-        kEriBatchLaunchers[k](h->bs, (const int4*)d_quartets, order, nq, d_out, h->d_boys, h->stream, h->nsm);
-        CK(cudaGetLastError());
+        eri_batch_launch(h, k, d_quartets, nq, d_out);
     });
 }
 
-int qcg_eri_batch(qcg_handle* h, int la, int lb, int lc, int ld, long long nq, const int* quartets, double* out)
+template <class T>
+int eri_batch_host(qcg_handle* h, int la, int lb, int lc, int ld, long long nq, const int* quartets, T* out)
 {
     if (!h) return QCG_ERR_ARG;
     return guarded(h, [&] {
@@ -837,20 +926,18 @@ int qcg_eri_batch(qcg_handle* h, int la, int lb, int lc, int ld, long long nq, c
                 require(h->L[s] == Ls[x], "shell angular momentum does not match the class");
             }
         const long long blk = (long long)ncart(la) * ncart(lb) * ncart(lc) * ncart(ld);
-        // bounded device footprint: chunks of at most 2^27 output doubles (1 GiB)
-        const long long chunk = std::max<long long>(1, std::min<long long>(nq, (1LL << 27) / blk));
+        // bounded device footprint: chunks of at most 1 GiB of output
+        const long long chunk = std::max<long long>(1, std::min<long long>(nq, (1LL << 30) / sizeof(T) / blk));
         int* dq = h->alloc<int>(4 * chunk);
-        double* dout = h->alloc<double>(chunk * blk);
+        T* dout = h->alloc<T>(chunk * blk);
         try
         {
             for (long long q0 = 0; q0 < nq; q0 += chunk)
             {
                 const long long m = std::min(chunk, nq - q0);
                 CK(cudaMemcpyAsync(dq, quartets + 4 * q0, 4 * m * sizeof(int), cudaMemcpyHostToDevice, h->stream));
-                const int* order = batch_order(h, dq, m);
-                kEriBatchLaunchers[k](h->bs, (const int4*)dq, order, m, dout, h->d_boys, h->stream, h->nsm);
-                CK(cudaGetLastError());
-                CK(cudaMemcpyAsync(out + q0 * blk, dout, m * blk * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+                eri_batch_launch(h, k, dq, m, dout);
+                CK(cudaMemcpyAsync(out + q0 * blk, dout, m * blk * sizeof(T), cudaMemcpyDeviceToHost, h->stream));
             }
             CK(cudaStreamSynchronize(h->stream));
         }
@@ -863,6 +950,30 @@ int qcg_eri_batch(qcg_handle* h, int la, int lb, int lc, int ld, long long nq, c
         h->release(dq);
         h->release(dout);
     });
+}
+}   // namespace
+}   // extern "C++"
+
+int qcg_eri_batch_device(qcg_handle* h, int la, int lb, int lc, int ld, long long nq, const int* d_quartets,
+                         double* d_out)
+{
+    return eri_batch_device(h, la, lb, lc, ld, nq, d_quartets, d_out);
+}
+
+int qcg_eri_batch_device_f32(qcg_handle* h, int la, int lb, int lc, int ld, long long nq, const int* d_quartets,
+                             float* d_out)
+{
+    return eri_batch_device(h, la, lb, lc, ld, nq, d_quartets, d_out);
+}
+
+int qcg_eri_batch(qcg_handle* h, int la, int lb, int lc, int ld, long long nq, const int* quartets, double* out)
+{
+    return eri_batch_host(h, la, lb, lc, ld, nq, quartets, out);
+}
+
+int qcg_eri_batch_f32(qcg_handle* h, int la, int lb, int lc, int ld, long long nq, const int* quartets, float* out)
+{
+    return eri_batch_host(h, la, lb, lc, ld, nq, quartets, out);
 }
 
 int qcg_schwarz(qcg_handle* h, double thresh, double* Q)
@@ -897,7 +1008,16 @@ int qcg_fock_jk_device(qcg_handle* h, const double* d_D, double* d_J, double* d_
     if (!h) return QCG_ERR_ARG;
     return guarded(h, [&] {
         require(d_D && d_J && d_K, "null argument");
-        jk_device(h, d_D, d_J, d_K, flags, stats);
+        jk_device(h, d_D, d_J, d_K, flags, stats, nullptr, 0.0, (flags & QCG_JK_FP32) ? HUGE_VAL : h->fp32_below);
+    });
+}
+
+int qcg_set_fp32_bound(qcg_handle* h, double bound)
+{
+    if (!h) return QCG_ERR_ARG;
+    return guarded(h, [&] {
+        require(bound >= 0 && !std::isnan(bound), "bound must be non-negative");
+        h->fp32_below = bound;
     });
 }
 
@@ -923,7 +1043,8 @@ int qcg_fock_jk(qcg_handle* h, const double* D, double* J, double* K, int flags,
         require(h->screened, "qcg_schwarz must be called before qcg_fock_jk", QCG_ERR_STATE);
         ensure_jk_buffers(h);
         CK(cudaMemcpyAsync(h->d_D, D, nn * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-        jk_device(h, h->d_D, h->d_J, h->d_K, flags | QCG_JK_SKIP_VALIDATION, stats);
+        jk_device(h, h->d_D, h->d_J, h->d_K, flags | QCG_JK_SKIP_VALIDATION, stats, nullptr, 0.0,
+                  (flags & QCG_JK_FP32) ? HUGE_VAL : h->fp32_below);
         CK(cudaMemcpyAsync(J, h->d_J, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
         CK(cudaMemcpyAsync(K, h->d_K, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
         int flag = 0;
@@ -971,6 +1092,11 @@ void qcg_scf_default_params(qcg_scf_params* p)
     p->incremental = 0;
     p->inc_thresh = 1e-11;
     p->rebuild_every = 8;
+    p->fp32_early = 0;
+    p->fp32_switch = 1e-5;
+    p->fp32_scale = 0.0;
+    p->fp32_below = 0.0;
+    p->D_guess = nullptr;
 }
 
 // Closed-shell SCF (SCFIterator.C:283-362 loop; DIIS gating/pruning per SCFAcceleratorDIIS.C:35-238)
@@ -1043,33 +1169,68 @@ int qcg_rhf(qcg_handle* h, int natom, const double* Z, const double* R, int nele
                     D[(size_t)i * n + j] = D[(size_t)j * n + i] = a;
                 }
         };
-        ortho(H, Fp);
-        diag_fill(Fp);   // core guess
+        if (prm.D_guess)
+        {
+            // caller's initial density (e.g. a learned guess): D as given, symmetrised; its orthonormal-basis
+            // image D' = X^T S D S X (X^T S X = 1) enters the first DIIS error
+            for (int i = 0; i < n; ++i)
+                for (int j = 0; j < n; ++j)
+                {
+                    const double x = 0.5 * (prm.D_guess[(size_t)i * n + j] + prm.D_guess[(size_t)j * n + i]);
+                    require(std::isfinite(x), "non-finite initial density", QCG_ERR_NONFINITE);
+                    D[(size_t)i * n + j] = x;
+                }
+            gemm(n, S.data(), false, X.data(), false, tmp.data());       // S X
+            gemm(n, D.data(), false, tmp.data(), false, Up.data());      // D S X
+            gemm(n, tmp.data(), true, Up.data(), false, Dp.data());      // X^T S D S X
+        }
+        else
+        {
+            ortho(H, Fp);
+            diag_fill(Fp);   // core guess
+        }
         std::deque<std::vector<double>> Es, Fps;
         std::vector<double> J(nn), K(nn), F(nn), Err(nn), a(nn), b(nn);
         std::vector<double> Dprev, Jprev, Kprev, dD(nn);
         double E = 0, Eold = 0, En = 0, fock_ms = 0;
         const bool inc = prm.incremental != 0;
-        int since_full = 0, nfull = 0, ninc = 0;
+        int since_full = 0, nfull = 0, ninc = 0, n32 = 0;
         bool force_full = true;
+        // precision schedule: until the DIIS error first falls below fp32_switch, quartets whose density-
+        // weighted bound is below fp32_scale * (previous DIIS error) are FP32; then FP64 (quartets below
+        // fp32_below still FP32).  The build that confirms convergence is always all-FP64.  A quartet's FP32
+        // error is about 3e-7 of its bound and up to ~nbf^2 quartets add into one Fock element, with the
+        // same sign in the worst case (early densities of diffuse bases have entries of 1e4 and more that
+        // cancel in the sums), so the default scale keeps nbf^2 * 3e-7 * bound at 1e-4 of the DIIS error.
+        // (At 1e-2 the early, oscillating iterations of the even-tempered water dimer were perturbed into a
+        // two-cycle that never converged; at 1e-3 and below every tested SCF kept its FP64 trajectory.)
+        bool fp32_phase = prm.fp32_early != 0, exact_next = false;
+        const double fp32_scale = prm.fp32_scale > 0 ? prm.fp32_scale : 1e-4 / (3e-7 * (double)n * n);
+        double En_prev = 1.0;
+        // QCG_SCF_TRACE=1: one line per iteration on stderr (energy, change, DIIS error, build kind)
+        const char* tr = std::getenv("QCG_SCF_TRACE");
+        const bool trace = tr && tr[0] == '1';
         double* d_dmax = nullptr;
         if (inc) d_dmax = h->alloc<double>((size_t)h->nshell * h->nshell);
         int it;
         for (it = 1; it <= prm.max_iter; ++it)
         {
             qcg_stats st{};
-            const bool full = !inc || force_full || since_full >= prm.rebuild_every;
+            const bool full = !inc || force_full || since_full >= prm.rebuild_every || exact_next;
+            const double band = exact_next ? 0.0 : (fp32_phase ? fp32_scale * En_prev : prm.fp32_below);
+            exact_next = false;
+            if (band > 0) ++n32;
             if (full)
             {
                 CK(cudaMemcpyAsync(h->d_D, D.data(), nn * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-                jk_device(h, h->d_D, h->d_J, h->d_K, QCG_JK_SKIP_VALIDATION, &st);
+                jk_device(h, h->d_D, h->d_J, h->d_K, QCG_JK_SKIP_VALIDATION, &st, nullptr, 0.0, band);
             }
             else
             {
                 for (size_t k = 0; k < nn; ++k) dD[k] = D[k] - Dprev[k];
                 CK(cudaMemcpyAsync(h->d_D, dD.data(), nn * sizeof(double), cudaMemcpyHostToDevice, h->stream));
                 launch_block_max(h->d_D, h->d_f0, h->bs.L, h->nshell, n, d_dmax, h->stream, h->nsm);
-                jk_device(h, h->d_D, h->d_J, h->d_K, QCG_JK_SKIP_VALIDATION, &st, d_dmax, prm.inc_thresh);
+                jk_device(h, h->d_D, h->d_J, h->d_K, QCG_JK_SKIP_VALIDATION, &st, d_dmax, prm.inc_thresh, band);
             }
             CK(cudaMemcpyAsync(J.data(), h->d_J, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
             CK(cudaMemcpyAsync(K.data(), h->d_K, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
@@ -1108,13 +1269,27 @@ int qcg_rhf(qcg_handle* h, int natom, const double* Z, const double* R, int nele
             En = std::sqrt(En);
             if (it > 1 && std::fabs(E - Eold) < prm.de_tol && En < prm.fd_tol)
             {
-                if (!full)
-                    force_full = true;   // confirm on a full build before stopping
+                if (!full || band != 0.0)
+                {
+                    // confirm on a full all-FP64 build before stopping
+                    force_full = true;
+                    exact_next = true;
+                    fp32_phase = false;
+                }
                 else
                 {
                     converged = true;
                     break;
                 }
+            }
+            if (trace)
+                std::fprintf(stderr, "qcg_rhf it %3d  E %.12f  dE %+.3e  [F,D] %.3e  %s  fp32 below %.2e\n", it, E,
+                             E - Eold, En, full ? "full" : "incr", band);
+            En_prev = En;
+            if (fp32_phase && it > 1 && En < prm.fp32_switch)
+            {
+                fp32_phase = false;   // FP64 from here on, starting from a full rebuild
+                force_full = true;
             }
             Eold = E;
             std::vector<double> Fuse = Fp;
@@ -1181,6 +1356,7 @@ int qcg_rhf(qcg_handle* h, int natom, const double* Z, const double* R, int nele
         result->fock_ms = fock_ms;
         result->full_builds = nfull;
         result->incremental_builds = ninc;
+        result->fp32_builds = n32;
         if (d_dmax) h->release(d_dmax);
         result->wall_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         if (D_out) std::copy(D.begin(), D.end(), D_out);
@@ -1250,24 +1426,28 @@ extern "C" int qcg_fock_jk_device_noalloc(qcg_handle* h, const double* d_D, doub
     });
 }
 
-// FP64 FMA peak of the current device: TFLOP/s of a pure-DFMA kernel over `reps` timed launches.
-int qcg_measure_fp64_peak(int reps, double* tflops, double* ms_per_launch)
+extern "C++" {
+namespace {
+// FMA peak of the current device: TFLOP/s of a pure-FMA kernel over `reps` timed launches
+template <class T, class Launch>
+int measure_fma_peak(int reps, double* tflops, double* ms_per_launch, Launch launch)
 {
     if (!tflops || reps <= 0) return QCG_ERR_ARG;
+    T* out = nullptr;
+    cudaEvent_t a = nullptr, b = nullptr;
+    int rc = QCG_OK;
     try
     {
         int dev = 0, nsm = 0;
         CK(cudaGetDevice(&dev));
         CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-        double* out = nullptr;
-        CK(cudaMalloc(&out, sizeof(double)));
-        cudaEvent_t a, b;
+        CK(cudaMalloc(&out, sizeof(T)));
         CK(cudaEventCreate(&a));
         CK(cudaEventCreate(&b));
         const int blocks = nsm * 8, threads = 256, iters = 2048;
-        launch_dfma_peak(out, blocks, threads, iters, nullptr);   // warm-up
+        launch(out, blocks, threads, iters, nullptr);   // warm-up
         CK(cudaEventRecord(a, nullptr));
-        for (int r = 0; r < reps; ++r) launch_dfma_peak(out, blocks, threads, iters, nullptr);
+        for (int r = 0; r < reps; ++r) launch(out, blocks, threads, iters, nullptr);
         CK(cudaEventRecord(b, nullptr));
         CK(cudaEventSynchronize(b));
         float ms = 0;
@@ -1275,15 +1455,27 @@ int qcg_measure_fp64_peak(int reps, double* tflops, double* ms_per_launch)
         const double flops = 2.0 * 8 * 16 * (double)iters * threads * blocks * reps;
         *tflops = flops / (ms * 1e-3) / 1e12;
         if (ms_per_launch) *ms_per_launch = ms / reps;
-        cudaEventDestroy(a);
-        cudaEventDestroy(b);
-        cudaFree(out);
-        return QCG_OK;
     }
     catch (const Error& e)
     {
-        return e.code;
+        rc = e.code;
     }
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    if (out) cudaFree(out);
+    return rc;
+}
+}   // namespace
+}   // extern "C++"
+
+int qcg_measure_fp64_peak(int reps, double* tflops, double* ms_per_launch)
+{
+    return measure_fma_peak<double>(reps, tflops, ms_per_launch, launch_dfma_peak);
+}
+
+int qcg_measure_fp32_peak(int reps, double* tflops, double* ms_per_launch)
+{
+    return measure_fma_peak<float>(reps, tflops, ms_per_launch, launch_ffma_peak);
 }
 
 // test hook: the host eigensolver used by the SCF (not part of the public header)
