@@ -162,6 +162,30 @@ void qcg_scf_default_params(qcg_scf_params* p);
 int qcg_rhf(qcg_handle* h, int natom, const double* Z, const double* R, int nelec, const qcg_scf_params* params,
             qcg_scf_result* result, double* D_out);
 
+/* ---- learned initial guess ------------------------------------------------------------------ */
+/* A multilayer perceptron (SiLU hidden layers, linear output) whose forward and backward passes and Adam
+ * updates run on the GPU: matrix-product operands rounded to BF16, FP32 accumulation, FP32 master
+ * weights.  It maps per-atom-pair geometry features to density-matrix blocks; the predicted density is
+ * handed to qcg_rhf through qcg_scf_params.D_guess.  No reference counterpart: the reference always
+ * starts from the core Hamiltonian (src/SCFIterator/Imp/Seed.C:70-80).  Row-major float32 device arrays;
+ * parameters are laid out layer by layer as W (out x in) then b (out). */
+typedef struct qcg_mlp qcg_mlp;
+int qcg_mlp_create(int nlayers, const int* widths /* nlayers+1 */, unsigned long long seed, qcg_mlp** out);
+void qcg_mlp_destroy(qcg_mlp* m);
+const char* qcg_mlp_last_error(const qcg_mlp* m);
+int qcg_mlp_set_stream(qcg_mlp* m, void* cuda_stream);
+int qcg_mlp_nparams(const qcg_mlp* m, long long* n);
+int qcg_mlp_params(qcg_mlp* m, float* host_params);            /* copy out (nparams floats) */
+int qcg_mlp_set_params(qcg_mlp* m, const float* host_params);  /* copy in; resets the Adam moments */
+/* y (rows x widths[L]) = network(x (rows x widths[0])) */
+int qcg_mlp_forward(qcg_mlp* m, int rows, const float* d_x, float* d_y);
+/* masked mean-squared error sum(mask (y - t)^2) / sum(mask) (mask entries 0 or 1) and its gradient with
+ * respect to every parameter (kept for qcg_mlp_adam; also copied to grad_host when given) */
+int qcg_mlp_loss_grad(qcg_mlp* m, int rows, const float* d_x, const float* d_target, const float* d_mask, float* loss,
+                      float* grad_host);
+/* one Adam step with decoupled weight decay on the last gradient */
+int qcg_mlp_adam(qcg_mlp* m, float lr, float beta1, float beta2, float eps, float weight_decay);
+
 /* ---- measurement ----------------------------------------------------------------------------- */
 /* FP64 fused-multiply-add throughput of the current device (TFLOP/s) from a pure-DFMA kernel timed over
  * `reps` launches: the roofline denominator of the ERI kernels.  No reference counterpart. */

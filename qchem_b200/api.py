@@ -37,7 +37,9 @@ EXPORTS = ["qcg_basis_create", "qcg_destroy", "qcg_last_error", "qcg_set_stream"
            "qcg_nshell", "qcg_norms", "qcg_eri_batch", "qcg_eri_batch_device", "qcg_schwarz", "qcg_fock_jk",
            "qcg_fock_jk_device", "qcg_one_electron", "qcg_scf_default_params", "qcg_rhf", "qcg_measure_fp64_peak",
            "qcg_fock_jk_device_noalloc", "qcg_eri_batch_f32", "qcg_eri_batch_device_f32", "qcg_set_fp32_bound",
-           "qcg_measure_fp32_peak"]
+           "qcg_measure_fp32_peak", "qcg_mlp_create", "qcg_mlp_destroy", "qcg_mlp_last_error", "qcg_mlp_set_stream",
+           "qcg_mlp_nparams", "qcg_mlp_params", "qcg_mlp_set_params", "qcg_mlp_forward", "qcg_mlp_loss_grad",
+           "qcg_mlp_adam"]
 
 
 class QcgError(RuntimeError):
@@ -106,6 +108,19 @@ def lib():
     L.qcg_internal_syev.argtypes = [i32, P(f64), P(f64), P(f64)]
     L.qcg_measure_fp64_peak.argtypes = [i32, P(f64), P(f64)]
     L.qcg_measure_fp32_peak.argtypes = [i32, P(f64), P(f64)]
+    f32 = ctypes.c_float
+    L.qcg_mlp_create.argtypes = [i32, P(i32), ctypes.c_ulonglong, P(vp)]
+    L.qcg_mlp_destroy.argtypes = [vp]
+    L.qcg_mlp_destroy.restype = None
+    L.qcg_mlp_last_error.argtypes = [vp]
+    L.qcg_mlp_last_error.restype = ctypes.c_char_p
+    L.qcg_mlp_set_stream.argtypes = [vp, vp]
+    L.qcg_mlp_nparams.argtypes = [vp, P(i64)]
+    L.qcg_mlp_params.argtypes = [vp, P(f32)]
+    L.qcg_mlp_set_params.argtypes = [vp, P(f32)]
+    L.qcg_mlp_forward.argtypes = [vp, i32, vp, vp]
+    L.qcg_mlp_loss_grad.argtypes = [vp, i32, vp, vp, vp, P(f32), P(f32)]
+    L.qcg_mlp_adam.argtypes = [vp, f32, f32, f32, f32, f32]
     _lib = L
     return L
 
@@ -291,6 +306,67 @@ class Engine:
         if D is not None:
             out["D"] = D
         return out
+
+
+class Mlp:
+    """The learned-guess network on the current CUDA device (include/qchem_b200.h, qcg_mlp_*): BF16-operand,
+    FP32-accumulated forward/backward kernels and Adam.  Activations, targets and masks are passed as device
+    pointers (row-major float32)."""
+
+    def __init__(self, widths: Sequence[int], seed: int = 0):
+        self.widths = [int(w) for w in widths]
+        w = np.array(self.widths, dtype=np.int32)
+        h = ctypes.c_void_p()
+        rc = lib().qcg_mlp_create(len(w) - 1, _p(w, ctypes.c_int), ctypes.c_ulonglong(seed), ctypes.byref(h))
+        if rc != QCG_OK:
+            raise QcgError(rc, "qcg_mlp_create failed")
+        self._h = h
+        n = ctypes.c_longlong()
+        lib().qcg_mlp_nparams(self._h, ctypes.byref(n))
+        self.nparams = n.value
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().qcg_mlp_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != QCG_OK:
+            raise QcgError(rc, lib().qcg_mlp_last_error(self._h).decode())
+
+    def set_stream(self, stream_ptr: int):
+        self._check(lib().qcg_mlp_set_stream(self._h, ctypes.c_void_p(int(stream_ptr))))
+
+    def params(self) -> np.ndarray:
+        p = np.zeros(self.nparams, dtype=np.float32)
+        self._check(lib().qcg_mlp_params(self._h, _p(p, ctypes.c_float)))
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        if p.size != self.nparams:
+            raise QcgError(QCG_ERR_ARG, f"expected {self.nparams} parameters")
+        self._check(lib().qcg_mlp_set_params(self._h, _p(p, ctypes.c_float)))
+
+    def forward(self, rows: int, d_x: int, d_y: int):
+        self._check(lib().qcg_mlp_forward(self._h, int(rows), ctypes.c_void_p(d_x), ctypes.c_void_p(d_y)))
+
+    def loss_grad(self, rows: int, d_x: int, d_t: int, d_mask: int, want_grad: bool = False):
+        loss = ctypes.c_float()
+        g = np.zeros(self.nparams, dtype=np.float32) if want_grad else None
+        self._check(lib().qcg_mlp_loss_grad(self._h, int(rows), ctypes.c_void_p(d_x), ctypes.c_void_p(d_t),
+                                            ctypes.c_void_p(d_mask), ctypes.byref(loss),
+                                            _p(g, ctypes.c_float) if g is not None else None))
+        return (loss.value, g) if want_grad else loss.value
+
+    def adam(self, lr=1e-3, beta1=0.9, beta2=0.999, eps=1e-8, weight_decay=0.0):
+        self._check(lib().qcg_mlp_adam(self._h, lr, beta1, beta2, eps, weight_decay))
 
 
 class OrbitalHFIBS:

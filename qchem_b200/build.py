@@ -56,8 +56,9 @@ def _jobs():
             key = _hash([_read(src), _read(os.path.join(GEN, f"md_class_{k}.cuh"))] + core
                         + _headers(["eri_kernels.cuh"]) + FLAGS + defs)
             jobs.append((src, defs, os.path.join(BUILD, f"eri_class_{k}_f{prec}_{key}.o")))
-    extra = {"runtime.cu": _headers(["boys_table.h"]) + [_read(os.path.join(INCLUDE, "qchem_b200.h"))]}
-    for name in ("registry.cu", "fock_kernels.cu", "runtime.cu"):
+    extra = {"runtime.cu": _headers(["boys_table.h"]) + [_read(os.path.join(INCLUDE, "qchem_b200.h"))],
+             "mlp.cu": [_read(os.path.join(INCLUDE, "qchem_b200.h"))]}
+    for name in ("registry.cu", "fock_kernels.cu", "runtime.cu", "mlp.cu"):
         s = os.path.join(CSRC, name)
         defs = HOST_OMP if name == "runtime.cu" else []
         key = _hash([_read(s)] + core + extra.get(name, []) + FLAGS + defs)

@@ -7,13 +7,15 @@
 #include <algorithm>
 #include <array>
 #include <chrono>
-#include <type_traits>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <numeric>
 #include <string>
+#include <type_traits>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/qchem_b200.h"
@@ -137,21 +139,75 @@ struct qcg_handle
     cudaStream_t side[kSide] = {};
     cudaEvent_t fork = nullptr, join[kSide] = {};
 
-    template <class T>
-    T* alloc(size_t count)
+    // Small buffers (pair lists, work offsets, basis arrays: a few hundred per handle) are carved out of
+    // 8 MiB slabs, so that setting up and destroying a handle costs a handful of cudaMalloc/cudaFree
+    // calls instead of hundreds; releasing a slab piece is a no-op until the handle goes.  Larger buffers
+    // have their own allocation.
+    static constexpr size_t kSlab = 8u << 20, kSmallMax = 1u << 20;
+    std::vector<DevBuf> slabs;
+    size_t slab_used = kSlab;
+    // pinned staging for uploads of host vectors (asynchronous copies; reused after a stream sync)
+    static constexpr size_t kStage = 4u << 20;
+    char* stage = nullptr;
+    size_t stage_used = 0;
+
+    // slab pieces in use (pointer -> bytes) and released pieces kept for reuse by size
+    std::unordered_map<void*, size_t> small_live;
+    std::unordered_multimap<size_t, void*> small_free;
+
+    void* raw_alloc(size_t bytes)
     {
-        const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
-        if (mem_limit > 0 && mem_used + (long long)bytes > mem_limit)
-            throw Error{QCG_ERR_ALLOC, "device memory limit of " + std::to_string(mem_limit) + " bytes exceeded"};
         void* p = nullptr;
         cudaError_t e = cudaMalloc(&p, bytes);
         if (e != cudaSuccess) throw Error{QCG_ERR_ALLOC, std::string("cudaMalloc: ") + cudaGetErrorString(e)};
-        allocs.push_back({p, bytes});
+        return p;
+    }
+    // mem_used counts the bytes handed out (the limit applies to those, not to slab capacity)
+    template <class T>
+    T* alloc(size_t count)
+    {
+        const size_t bytes = (std::max<size_t>(count, 1) * sizeof(T) + 255) & ~(size_t)255;
+        if (mem_limit > 0 && mem_used + (long long)bytes > mem_limit)
+            throw Error{QCG_ERR_ALLOC, "device memory limit of " + std::to_string(mem_limit) + " bytes exceeded"};
+        void* p = nullptr;
+        if (bytes <= kSmallMax)
+        {
+            auto it = small_free.find(bytes);
+            if (it != small_free.end())
+            {
+                p = it->second;
+                small_free.erase(it);
+            }
+            else
+            {
+                if (slab_used + bytes > kSlab)
+                {
+                    slabs.push_back({raw_alloc(kSlab), kSlab});
+                    slab_used = 0;
+                }
+                p = (char*)slabs.back().p + slab_used;
+                slab_used += bytes;
+            }
+            small_live[p] = bytes;
+        }
+        else
+        {
+            p = raw_alloc(bytes);
+            allocs.push_back({p, bytes});
+        }
         mem_used += bytes;
         return (T*)p;
     }
     void release(void* p)
     {
+        auto it = small_live.find(p);
+        if (it != small_live.end())
+        {
+            mem_used -= it->second;
+            small_free.emplace(it->second, p);
+            small_live.erase(it);
+            return;
+        }
         for (size_t i = 0; i < allocs.size(); ++i)
             if (allocs[i].p == p)
             {
@@ -165,12 +221,34 @@ struct qcg_handle
     T* upload(const std::vector<T>& v)
     {
         T* d = alloc<T>(v.size());
-        if (!v.empty()) CK(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, stream));
+        const size_t bytes = v.size() * sizeof(T);
+        if (bytes == 0) return d;
+        if (bytes > kStage)
+        {
+            CK(cudaMemcpyAsync(d, v.data(), bytes, cudaMemcpyHostToDevice, stream));
+            return d;
+        }
+        if (!stage)
+        {
+            CK(cudaMallocHost(&stage, kStage));
+            stage_used = 0;
+        }
+        if (stage_used + bytes > kStage)
+        {
+            CK(cudaStreamSynchronize(stream));   // earlier copies out of the staging buffer are done
+            stage_used = 0;
+        }
+        std::memcpy(stage + stage_used, v.data(), bytes);
+        CK(cudaMemcpyAsync(d, stage + stage_used, bytes, cudaMemcpyHostToDevice, stream));
+        stage_used = (stage_used + bytes + 255) & ~(size_t)255;
         return d;
     }
     ~qcg_handle()
     {
+        if (stream) cudaStreamSynchronize(stream);
         for (auto& a : allocs) cudaFree(a.p);
+        for (auto& a : slabs) cudaFree(a.p);
+        if (stage) cudaFreeHost(stage);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (ev2) cudaEventDestroy(ev2);
@@ -814,9 +892,7 @@ int qcg_basis_create(const int* shell_L, const int* shell_nprim, const double* e
                 h->ns.push_back(nrad * comp_norm(Ls, k));
         }
         CK(cudaGetDevice(&h->device));
-        cudaDeviceProp prop;
-        CK(cudaGetDeviceProperties(&prop, h->device));
-        h->nsm = prop.multiProcessorCount;
+        CK(cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, h->device));
         CK(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
         h->stream = h->own_stream;
         h->d_boys = h->alloc<double>(121 * 23);
@@ -848,6 +924,8 @@ const char* qcg_last_error(const qcg_handle* h) { return h ? h->last_error.c_str
 int qcg_set_stream(qcg_handle* h, void* s)
 {
     if (!h) return QCG_ERR_ARG;
+    // work queued on the previous stream (uploads out of the staging buffer among it) completes first
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) return QCG_ERR_CUDA;
     h->stream = (cudaStream_t)s;   // NULL is the CUDA default (legacy) stream
     return QCG_OK;
 }
