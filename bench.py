@@ -174,11 +174,13 @@ def main():
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--ref-sample", type=int, default=2000)
     ap.add_argument("--cpu-sample", type=int, default=1000)
-    ap.add_argument("--workload", default="eri", choices=["eri", "fock_config3", "rhf_config1", "rhf_learned"],
+    ap.add_argument("--workload", default="eri", choices=["eri", "fock_config3", "rhf_config1", "rhf_learned", "rhf_batch"],
                     help="eri: the headline ERI microbenchmark; fock_config3: one direct J/K build of the "
                          "32-water cluster per step; rhf_config1: one water RHF to convergence per step; "
                          "rhf_learned: train the learned guess on plain-SCF densities of water conformers and "
-                         "time held-out RHFs from it against the core guess")
+                         "time held-out RHFs from it against the core guess; rhf_batch: the batched RHF of "
+                         "random H/C/N/O molecules, all SCFs advanced together")
+    ap.add_argument("--nmol", type=int, default=256, help="rhf_batch: molecules in the batch")
     ap.add_argument("--train", type=int, default=1000, help="rhf_learned: training conformers")
     ap.add_argument("--held-out", type=int, default=100, help="rhf_learned: held-out conformers")
     args = ap.parse_args()
@@ -450,6 +452,8 @@ def run_secondary(args):
                         "d2h_bytes_per_step": 16 * n * n}}
     elif args.workload == "rhf_learned":
         line = run_learned(args, api, B, W, peak_tf)
+    elif args.workload == "rhf_batch":
+        line = run_batch(args, api, B, W)
     else:
         def solve(mol, sh, steps, warmup, **kw):
             for _ in range(warmup):
@@ -493,6 +497,44 @@ def run_secondary(args):
                                                  "speedup_vs_plain": w8 / w8c}},
                 "e2e": {"value": wall, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def run_batch(args, api, B, W):
+    """Batched RHF: args.nmol random closed-shell H/C/N/O molecules (2-24 atoms, heavy-atom random-walk
+    chains with H caps), one handle, one J/K build over all molecules per iteration.  A step is the whole
+    batch to convergence; beside it, the same molecules one handle at a time (first 16, extrapolated)."""
+    mols = W.random_molecules(args.nmol)
+    shells = [B.even_tempered(m) for m in mols]
+    be = api.BatchEngine(shells[:min(4, len(mols))])
+    be.rhf(mols[:min(4, len(mols))], max_iter=3)   # warm-up (module load, first launches)
+    del be
+    clocks = ClockSampler(0)
+    clocks.start()
+    t0 = time.perf_counter()
+    res = api.BatchEngine(shells).rhf(mols)
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    nsub = min(16, len(mols))
+    t0 = time.perf_counter()
+    single = [api.Engine(s).rhf(m) for m, s in zip(mols[:nsub], shells[:nsub])]
+    wall_single = (time.perf_counter() - t0) * len(mols) / nsub
+    dE = [abs(r["energy"] - q["energy"]) for r, q in zip(res[:nsub], single) if r["converged"] and q["converged"]]
+    nbf = [B.nbf(s) for s in shells]
+    conv = sum(r["converged"] for r in res)
+    return {"metric": "batched RHF: molecules to convergence per second (random H/C/N/O, 2-24 atoms, "
+                      "even-tempered basis, dE < 1e-10)",
+            "value": len(mols) / wall, "unit": "molecules/s", "n_gpus": 1, "steps": 1, "warmup": 1,
+            "ms_per_step": 1e3 * wall, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "rhf_batch_random_molecules", "molecules": len(mols), "nbf_mean": float(np.mean(nbf)),
+                       "nbf_max": int(max(nbf)), "converged": int(conv),
+                       "iterations_max": int(max(r["iterations"] for r in res)),
+                       "jk_builds": res[0]["builds"], "fock_ms_total": res[0]["fock_ms"]},
+            "one_handle_per_molecule_s_extrapolated": wall_single, "speedup_vs_one_handle_per_molecule":
+                wall_single / wall,
+            "max_abs_dE_vs_single_eh": max(dE) if dE else None, "compared": len(dE), "clocks": clk,
+            "e2e": {"value": len(mols) / wall, "unit": "molecules/s", "h2d_bytes_per_step": None,
+                    "d2h_bytes_per_step": None}}
 
 
 def run_learned(args, api, B, W, peak_tf):

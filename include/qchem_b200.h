@@ -101,6 +101,15 @@ typedef struct qcg_scf_result {
  * renormalises every Cartesian component to unit self-overlap); centres: 3 doubles per shell (bohr). */
 int qcg_basis_create(const int* shell_L, const int* shell_nprim, const double* exps, const double* coefs,
                      const double* centres, int nshell, qcg_handle** out);
+/* Several molecules in one handle (batched SCF): shells grouped by molecule in molecule order,
+ * shell_mol[i] in [0, nmol).  Shell pairs and quartets never mix molecules.  Every matrix argument of the
+ * J/K calls is then PACKED: molecule m's n_m x n_m block (row-major, the molecule's own function order)
+ * follows molecule m-1's.  qcg_basis_create is the nmol = 1 case.  No reference counterpart: the
+ * reference runs one molecule per Calculation. */
+int qcg_basis_create_batch(const int* shell_L, const int* shell_nprim, const double* exps, const double* coefs,
+                           const double* centres, int nshell, const int* shell_mol, int nmol, qcg_handle** out);
+int qcg_nmol(const qcg_handle* h, int* nmol);
+int qcg_mol_nbf(const qcg_handle* h, int* nbf_per_molecule);   /* nmol entries */
 void qcg_destroy(qcg_handle* h);
 const char* qcg_last_error(const qcg_handle* h);
 /* stream for all later work of this handle; NULL is the CUDA default (legacy) stream.  A new handle
@@ -154,6 +163,10 @@ int qcg_fock_jk_device_noalloc(qcg_handle* h, const double* d_D, double* d_J, do
 
 /* overlap, kinetic (1/2 <grad|grad>) and nuclear attraction, natom nuclei of charge Z at R (3 per atom) */
 int qcg_one_electron(qcg_handle* h, int natom, const double* Z, const double* R, double* S, double* T, double* V);
+/* the same for a batch handle: molecule m has mol_natom[m] nuclei (Z, R concatenated in molecule order);
+ * S, T, V packed */
+int qcg_one_electron_batch(qcg_handle* h, const int* mol_natom, const double* Z, const double* R, double* S,
+                           double* T, double* V);
 
 /* ---- RHF ------------------------------------------------------------------------------------- */
 void qcg_scf_default_params(qcg_scf_params* p);
@@ -161,6 +174,11 @@ void qcg_scf_default_params(qcg_scf_params* p);
  * GPU every iteration.  D_out (optional, nbf*nbf) receives the final density. */
 int qcg_rhf(qcg_handle* h, int natom, const double* Z, const double* R, int nelec, const qcg_scf_params* params,
             qcg_scf_result* result, double* D_out);
+/* All molecules of a batch handle to convergence together: each iteration is one J/K build over every
+ * molecule, then per-molecule host steps in parallel.  results: nmol entries (wall_s and fock_ms are the
+ * batch's); D_out optional, packed.  incremental / fp32 / D_guess parameters are ignored. */
+int qcg_rhf_batch(qcg_handle* h, const int* mol_natom, const double* Z, const double* R, const int* nelec,
+                  const qcg_scf_params* params, qcg_scf_result* results, double* D_out);
 
 /* ---- learned initial guess ------------------------------------------------------------------ */
 /* A multilayer perceptron (SiLU hidden layers, linear output) whose forward and backward passes and Adam

@@ -39,7 +39,8 @@ EXPORTS = ["qcg_basis_create", "qcg_destroy", "qcg_last_error", "qcg_set_stream"
            "qcg_fock_jk_device_noalloc", "qcg_eri_batch_f32", "qcg_eri_batch_device_f32", "qcg_set_fp32_bound",
            "qcg_measure_fp32_peak", "qcg_mlp_create", "qcg_mlp_destroy", "qcg_mlp_last_error", "qcg_mlp_set_stream",
            "qcg_mlp_nparams", "qcg_mlp_params", "qcg_mlp_set_params", "qcg_mlp_forward", "qcg_mlp_loss_grad",
-           "qcg_mlp_adam"]
+           "qcg_mlp_adam", "qcg_basis_create_batch", "qcg_nmol", "qcg_mol_nbf", "qcg_one_electron_batch",
+           "qcg_rhf_batch"]
 
 
 class QcgError(RuntimeError):
@@ -84,6 +85,11 @@ def lib():
     vp, i32, i64, f64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong, ctypes.c_double
     P = ctypes.POINTER
     L.qcg_basis_create.argtypes = [P(i32), P(i32), P(f64), P(f64), P(f64), i32, P(vp)]
+    L.qcg_basis_create_batch.argtypes = [P(i32), P(i32), P(f64), P(f64), P(f64), i32, P(i32), i32, P(vp)]
+    L.qcg_nmol.argtypes = [vp, P(i32)]
+    L.qcg_mol_nbf.argtypes = [vp, P(i32)]
+    L.qcg_one_electron_batch.argtypes = [vp, P(i32), P(f64), P(f64), P(f64), P(f64), P(f64)]
+    L.qcg_rhf_batch.argtypes = [vp, P(i32), P(f64), P(f64), P(i32), P(ScfParams), P(ScfResult), P(f64)]
     L.qcg_destroy.argtypes = [vp]
     L.qcg_destroy.restype = None
     L.qcg_last_error.argtypes = [vp]
@@ -305,6 +311,78 @@ class Engine:
                "fp32_builds": res.fp32_builds}
         if D is not None:
             out["D"] = D
+        return out
+
+
+class BatchEngine(Engine):
+    """Several molecules in one handle (qcg_basis_create_batch): one J/K build covers all of them, and
+    rhf() advances all their SCFs together.  Matrices cross the C ABI packed (molecule blocks one after
+    the other); this class packs and unpacks lists of per-molecule arrays."""
+
+    def __init__(self, shell_lists: Sequence[Sequence[_basis.Shell]]):
+        self.shell_lists = [list(x) for x in shell_lists]
+        self.shells = [s for x in self.shell_lists for s in x]
+        L, npr, cen, ex, co = _basis.flatten(self.shells)
+        mol = np.concatenate([np.full(len(x), m, dtype=np.int32) for m, x in enumerate(self.shell_lists)])
+        h = ctypes.c_void_p()
+        rc = lib().qcg_basis_create_batch(_p(L, ctypes.c_int), _p(npr, ctypes.c_int), _p(ex), _p(co), _p(cen),
+                                          len(self.shells), _p(mol, ctypes.c_int), len(self.shell_lists),
+                                          ctypes.byref(h))
+        self._h = h
+        if rc != QCG_OK:
+            msg = lib().qcg_last_error(h).decode() if h.value else "qcg_basis_create_batch failed"
+            self.close()
+            raise QcgError(rc, msg)
+        self.nmol = len(self.shell_lists)
+        nb = np.zeros(self.nmol, dtype=np.int32)
+        self._check(lib().qcg_mol_nbf(self._h, _p(nb, ctypes.c_int)))
+        self.mol_nbf = [int(x) for x in nb]
+        self.nbf = int(nb.sum())
+        self.packed_off = np.concatenate([[0], np.cumsum([n * n for n in self.mol_nbf])])
+        self._screen = None
+
+    def pack(self, mats):
+        return np.concatenate([_f64(m).reshape(-1) for m in mats])
+
+    def unpack(self, flat):
+        return [flat[self.packed_off[m]:self.packed_off[m + 1]].reshape(n, n) for m, n in enumerate(self.mol_nbf)]
+
+    def fock_jk(self, Ds, validate: bool = True, fp32: bool = False):
+        if self._screen is None:
+            self.schwarz()
+        D = self.pack(Ds)
+        J, K = np.zeros_like(D), np.zeros_like(D)
+        st = Stats()
+        flags = (0 if validate else QCG_JK_SKIP_VALIDATION) | (QCG_JK_FP32 if fp32 else 0)
+        self._check(lib().qcg_fock_jk(self._h, _p(D), _p(J), _p(K), flags, ctypes.byref(st)))
+        return self.unpack(J), self.unpack(K), st
+
+    def schwarz(self, thresh: float = 1e-10):
+        self._check(lib().qcg_schwarz(self._h, float(thresh), None))
+        self._screen = thresh
+
+    def rhf(self, mols: Sequence[_basis.Molecule], max_iter=100, de_tol=1e-10, fd_tol=1e-5, schwarz_thresh=1e-10,
+            want_density=False):
+        prm = ScfParams()
+        lib().qcg_scf_default_params(ctypes.byref(prm))
+        prm.max_iter, prm.de_tol, prm.fd_tol, prm.schwarz_thresh = max_iter, de_tol, fd_tol, schwarz_thresh
+        nat = np.array([len(m.Z) for m in mols], dtype=np.int32)
+        Z = _f64(np.concatenate([np.asarray(m.Z, dtype=float) for m in mols]))
+        R = _f64(np.concatenate([np.asarray(m.R, dtype=float).reshape(-1) for m in mols]))
+        ne = np.array([m.nelec for m in mols], dtype=np.int32)
+        res = (ScfResult * len(mols))()
+        D = np.zeros(int(self.packed_off[-1])) if want_density else None
+        rc = lib().qcg_rhf_batch(self._h, _p(nat, ctypes.c_int), _p(Z), _p(R), _p(ne, ctypes.c_int),
+                                 ctypes.byref(prm), res, _p(D) if D is not None else None)
+        if rc not in (QCG_OK, QCG_ERR_NOCONV):
+            self._check(rc)
+        self._screen = schwarz_thresh
+        out = [{"energy": r.energy, "e_nuc": r.e_nuc, "iterations": r.iterations, "converged": bool(r.converged),
+                "fd_error": r.fd_error, "wall_s": r.wall_s, "fock_ms": r.fock_ms, "builds": r.full_builds}
+               for r in res]
+        if D is not None:
+            for o, d in zip(out, self.unpack(D)):
+                o["D"] = d
         return out
 
 

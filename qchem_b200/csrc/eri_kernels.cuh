@@ -319,7 +319,20 @@ __global__ void __launch_bounds__(THREADS) jk_kernel(JKWorkDev w, PairListDev br
         long long next = w.offs[i + 1];
         JKSink<RT, Cls::LA, Cls::LB, Cls::LC, Cls::LD> sink;
         sink.D = D; sink.J = J; sink.K = K; sink.n = n;
+        // several molecules: the bra pair's molecule selects the packed blocks and their dimension
+        auto bind = [&](int ii) {
+            if (bra.mol)
+            {
+                const int m = bra.mol[ii];
+                const long long o = w.mols.off[m];
+                sink.D = D + o;
+                sink.J = J + o;
+                sink.K = K + o;
+                sink.n = w.mols.n[m];
+            }
+        };
         int sa = bra.sa[i], sb = bra.sb[i];
+        bind(i);
         sink.set_bra(shell_f0[sa], shell_f0[sb]);
         for (int r = 0; r < RUN && g < w.total; ++r, g += 32)
         {
@@ -333,9 +346,10 @@ __global__ void __launch_bounds__(THREADS) jk_kernel(JKWorkDev w, PairListDev br
                 } while (g >= next);
                 sa = bra.sa[i];
                 sb = bra.sb[i];
+                bind(i);
                 sink.set_bra(shell_f0[sa], shell_f0[sb]);
             }
-            const int j = (int)(g - w.offs[i]);
+            const int j = (w.kbase ? w.kbase[i] : 0) + (int)(g - w.offs[i]);
             const int sc = ket.sa[j], sd = ket.sb[j];
             if (w.dmax)
             {

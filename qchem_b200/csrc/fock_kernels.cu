@@ -7,32 +7,60 @@
 
 namespace qcg {
 
-// any non-finite entry -> flag bit 1; |D_ij - D_ji| > tol*(1+|D_ij|) -> flag bit 2
-__global__ void validate_density_kernel(const double* __restrict__ D, int n, double tol, int* flag)
+// element k of a (packed) matrix: its row i, column j and the index of its transpose partner
+struct ElemIdx
 {
-    const long long total = (long long)n * n;
+    int i, j;
+    long long t;
+};
+__device__ __forceinline__ ElemIdx elem_index(long long k, int n, const MolLayoutDev& ml)
+{
+    long long base = 0;
+    int nm = n;
+    if (ml.nmol > 1)
+    {
+        int lo = 0, hi = ml.nmol;   // off[lo] <= k < off[hi]
+        while (hi - lo > 1)
+        {
+            const int mid = (lo + hi) >> 1;
+            if (ml.off[mid] <= k) lo = mid;
+            else hi = mid;
+        }
+        base = ml.off[lo];
+        nm = ml.n[lo];
+    }
+    const long long r = k - base;
+    ElemIdx e;
+    e.i = (int)(r / nm);
+    e.j = (int)(r % nm);
+    e.t = base + (long long)e.j * nm + e.i;
+    return e;
+}
+
+// any non-finite entry -> flag bit 1; |D_ij - D_ji| > tol*(1+|D_ij|) -> flag bit 2 (per molecule block)
+__global__ void validate_density_kernel(const double* __restrict__ D, long long total, int n, MolLayoutDev ml,
+                                        double tol, int* flag)
+{
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total; k += (long long)gridDim.x * blockDim.x)
     {
-        const int i = (int)(k / n), j = (int)(k % n);
+        const ElemIdx e = elem_index(k, n, ml);
         const double a = D[k];
         if (!isfinite(a)) atomicOr(flag, 1);
-        else if (j > i)
+        else if (e.j > e.i)
         {
-            const double b = D[(long long)j * n + i];
+            const double b = D[e.t];
             if (fabs(a - b) > tol * (1.0 + fabs(a))) atomicOr(flag, 2);
         }
     }
 }
 
-// J = J' + J'^T, K = K' + K'^T; flags non-finite results
+// J = J' + J'^T, K = K' + K'^T (per molecule block); flags non-finite results
 __global__ void symmetrize_kernel(const double* __restrict__ Jp, const double* __restrict__ Kp, double* __restrict__ J,
-                                  double* __restrict__ K, int n, int* flag)
+                                  double* __restrict__ K, long long total, int n, MolLayoutDev ml, int* flag)
 {
-    const long long total = (long long)n * n;
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total; k += (long long)gridDim.x * blockDim.x)
     {
-        const int i = (int)(k / n), j = (int)(k % n);
-        const long long t = (long long)j * n + i;
+        const long long t = elem_index(k, n, ml).t;
         const double jv = Jp[k] + Jp[t], kv = Kp[k] + Kp[t];
         J[k] = jv;
         K[k] = kv;
@@ -121,14 +149,15 @@ void launch_block_max(const double* D, const int* shell_f0, const int* shell_L, 
     block_max_kernel<<<nsm * 4, 256, 0, st>>>(D, shell_f0, shell_L, nshell, n, dmax);
 }
 
-void launch_validate(const double* D, int n, double tol, int* flag, cudaStream_t st, int nsm)
+void launch_validate(const double* D, long long total, int n, const MolLayoutDev& ml, double tol, int* flag,
+                     cudaStream_t st, int nsm)
 {
-    validate_density_kernel<<<nsm * 4, 256, 0, st>>>(D, n, tol, flag);
+    validate_density_kernel<<<nsm * 4, 256, 0, st>>>(D, total, n, ml, tol, flag);
 }
-void launch_symmetrize(const double* Jp, const double* Kp, double* J, double* K, int n, int* flag, cudaStream_t st,
-                       int nsm)
+void launch_symmetrize(const double* Jp, const double* Kp, double* J, double* K, long long total, int n,
+                       const MolLayoutDev& ml, int* flag, cudaStream_t st, int nsm)
 {
-    symmetrize_kernel<<<nsm * 4, 256, 0, st>>>(Jp, Kp, J, K, n, flag);
+    symmetrize_kernel<<<nsm * 4, 256, 0, st>>>(Jp, Kp, J, K, total, n, ml, flag);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -182,17 +211,41 @@ __device__ inline double e0(const double (&E)[4][4][kEM + 1], int i, int j)
 }
 }   // namespace
 
+// Several molecules (pairs != null): the listed shell pairs (a >= b, same molecule) only, each molecule's
+// nuclei [atom0[m], atom0[m] + natoms[m]) only, results into its packed block.
 __global__ void one_electron_kernel(BasisDev bs, const int* __restrict__ shell_f0, int n, int natom,
                                     const double* __restrict__ Z, const double* __restrict__ RC,
                                     double* __restrict__ S, double* __restrict__ T, double* __restrict__ V,
-                                    const double* __restrict__ boys_table)
+                                    const double* __restrict__ boys_table, const int2* __restrict__ pairs,
+                                    long long npair_list, const int* __restrict__ shell_mol, MolLayoutDev ml,
+                                    const int* __restrict__ atom0, const int* __restrict__ natoms)
 {
-    const long long npairs = (long long)bs.nshell * bs.nshell;
+    const long long npairs = pairs ? npair_list : (long long)bs.nshell * bs.nshell;
     for (long long pr = blockIdx.x * (long long)blockDim.x + threadIdx.x; pr < npairs;
          pr += (long long)gridDim.x * blockDim.x)
     {
-        const int sa = (int)(pr / bs.nshell), sb = (int)(pr % bs.nshell);
+        int sa, sb;
+        if (pairs)
+        {
+            sa = pairs[pr].x;
+            sb = pairs[pr].y;
+        }
+        else
+        {
+            sa = (int)(pr / bs.nshell);
+            sb = (int)(pr % bs.nshell);
+        }
         if (sb > sa) continue;
+        long long base = 0;
+        int ld = n, c0 = 0, c1 = natom;
+        if (pairs)
+        {
+            const int m = shell_mol[sa];
+            base = ml.off[m];
+            ld = ml.n[m];
+            c0 = atom0[m];
+            c1 = c0 + natoms[m];
+        }
         const int la = bs.L[sa], lb = bs.L[sb];
         const int na = ncart(la), nb = ncart(lb);
         double s[36], t[36], v[36];
@@ -218,7 +271,7 @@ __global__ void one_electron_kernel(BasisDev bs, const int* __restrict__ shell_f
                 for (int x = 0; x < 5; ++x)
                     for (int y = 0; y < 5; ++y)
                         for (int z = 0; z < 5; ++z) Rs[x][y][z] = 0.0;
-                for (int c = 0; c < natom; ++c)
+                for (int c = c0; c < c1; ++c)
                 {
                     const double X = d.Px - RC[3 * c], Y = d.Py - RC[3 * c + 1], Zc = d.Pz - RC[3 * c + 2];
                     double F[5];
@@ -286,7 +339,8 @@ __global__ void one_electron_kernel(BasisDev bs, const int* __restrict__ shell_f
                 comp_of(lb, kb, pbx, pby, pbz);
                 const double nn = inv_sqrt_dfact(pax) * inv_sqrt_dfact(pay) * inv_sqrt_dfact(paz) * inv_sqrt_dfact(pbx)
                                 * inv_sqrt_dfact(pby) * inv_sqrt_dfact(pbz);
-                const long long i1 = (long long)(fa + ka) * n + fb + kb, i2 = (long long)(fb + kb) * n + fa + ka;
+                const long long i1 = base + (long long)(fa + ka) * ld + fb + kb,
+                                i2 = base + (long long)(fb + kb) * ld + fa + ka;
                 S[i1] = S[i2] = s[ka * nb + kb] * nn;
                 T[i1] = T[i2] = t[ka * nb + kb] * nn;
                 V[i1] = V[i2] = v[ka * nb + kb] * nn;
@@ -295,9 +349,12 @@ __global__ void one_electron_kernel(BasisDev bs, const int* __restrict__ shell_f
 }
 
 void launch_one_electron(const BasisDev& bs, const int* f0, int n, int natom, const double* Z, const double* R,
-                         double* S, double* T, double* V, const double* boys, cudaStream_t st, int nsm)
+                         double* S, double* T, double* V, const double* boys, cudaStream_t st, int nsm,
+                         const int2* pairs, long long npair_list, const int* shell_mol, const MolLayoutDev& ml,
+                         const int* atom0, const int* natoms)
 {
-    one_electron_kernel<<<nsm * 2, 64, 0, st>>>(bs, f0, n, natom, Z, R, S, T, V, boys);
+    one_electron_kernel<<<nsm * 2, 64, 0, st>>>(bs, f0, n, natom, Z, R, S, T, V, boys, pairs, npair_list, shell_mol,
+                                                ml, atom0, natoms);
 }
 
 }   // namespace qcg

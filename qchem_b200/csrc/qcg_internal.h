@@ -30,7 +30,8 @@ struct PrimPairsDev
     const double *p, *Px, *Py, *Pz, *PAx, *PAy, *PAz, *PBx, *PBy, *PBz, *K;
 };
 
-// shell pairs of one pair class, sorted by Schwarz bound descending
+// shell pairs of one pair class, sorted by Schwarz bound descending (by molecule, then Schwarz bound
+// descending, in a handle that holds several molecules)
 struct PairListDev
 {
     int n;
@@ -38,7 +39,17 @@ struct PairListDev
     const int* sb;
     const int* ppo;
     const int* npp;
-    const double* Q;   // Schwarz bound of each pair (same order)
+    const double* Q;     // Schwarz bound of each pair (same order)
+    const int* mol;      // molecule of each pair (null for a single molecule)
+};
+
+// Several molecules in one handle: matrices are packed, molecule m's n_m x n_m block (row-major, local
+// function indices) starting at element off[m]; nmol == 1 is the plain dense nbf x nbf layout.
+struct MolLayoutDev
+{
+    int nmol;
+    const long long* off;   // nmol + 1 entries, off[nmol] = elements of a packed matrix
+    const int* n;           // functions of each molecule
 };
 
 // flattened canonical quartets of one quartet class: bra pair i owns quartets offs[i] .. offs[i+1)
@@ -55,6 +66,10 @@ struct JKWorkDev
     // precision band: this launch evaluates the quartets whose bound lies in [lo, hi) (0 and >= 1e300:
     // every quartet)
     double lo, hi;
+    // several molecules: the kets of bra pair i start at kbase[i] (the bra's molecule's part of the ket
+    // class); D, J', K' of a quartet are the packed blocks of its molecule
+    const int* kbase;
+    MolLayoutDev mols;
 };
 
 void launch_block_max(const double* D, const int* shell_f0, const int* shell_L, int nshell, int n, double* dmax,

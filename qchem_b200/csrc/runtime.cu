@@ -24,11 +24,15 @@
 #include "boys_table.h"
 
 namespace qcg {
-void launch_validate(const double* D, int n, double tol, int* flag, cudaStream_t st, int nsm);
-void launch_symmetrize(const double* Jp, const double* Kp, double* J, double* K, int n, int* flag, cudaStream_t st,
-                       int nsm);
+void launch_validate(const double* D, long long total, int n, const MolLayoutDev& ml, double tol, int* flag,
+                     cudaStream_t st, int nsm);
+void launch_symmetrize(const double* Jp, const double* Kp, double* J, double* K, long long total, int n,
+                       const MolLayoutDev& ml, int* flag, cudaStream_t st, int nsm);
 void launch_one_electron(const BasisDev& bs, const int* f0, int n, int natom, const double* Z, const double* R,
-                         double* S, double* T, double* V, const double* boys, cudaStream_t st, int nsm);
+                         double* S, double* T, double* V, const double* boys, cudaStream_t st, int nsm,
+                         const int2* pairs = nullptr, long long npair_list = 0, const int* shell_mol = nullptr,
+                         const MolLayoutDev& ml = MolLayoutDev{1, nullptr, nullptr}, const int* atom0 = nullptr,
+                         const int* natoms = nullptr);
 void launch_dfma_peak(double* out, int blocks, int threads, int iters, cudaStream_t st);
 void launch_ffma_peak(float* out, int blocks, int threads, int iters, cudaStream_t st);
 }   // namespace qcg
@@ -102,6 +106,16 @@ struct qcg_handle
 
     // basis (host)
     int nshell = 0, nbf = 0;
+    // several molecules in one handle (qcg_basis_create_batch): shells grouped by molecule, f0 local to the
+    // molecule, every matrix packed as the molecules' n_m x n_m blocks one after the other
+    int nmol = 1;
+    std::vector<int> shell_mol, mol_shell0, mol_nbf;
+    std::vector<long long> mol_off;
+    long long packed = 0;   // elements of one matrix
+    int* d_shell_mol = nullptr;
+    long long* d_mol_off = nullptr;
+    int* d_mol_n = nullptr;
+    MolLayoutDev mols() const { return MolLayoutDev{nmol, d_mol_off, d_mol_n}; }
     std::vector<int> L, nprim, prim0, f0;
     std::vector<double> cen, alpha, coef, ns;
 
@@ -113,7 +127,8 @@ struct qcg_handle
     // pair lists and screening
     bool screened = false;
     double thresh = 0;
-    std::vector<int> pl_sa[kNumPairClasses], pl_sb[kNumPairClasses], pl_ppo[kNumPairClasses], pl_npp[kNumPairClasses];
+    std::vector<int> pl_sa[kNumPairClasses], pl_sb[kNumPairClasses], pl_ppo[kNumPairClasses], pl_npp[kNumPairClasses],
+        pl_mol[kNumPairClasses];
     std::vector<double> pl_Q[kNumPairClasses];
     PairListDev pl_dev[kNumPairClasses]{};
     PrimPairsDev pp_dev{};
@@ -525,10 +540,197 @@ std::vector<double> solve_dense(int n, std::vector<double> A, std::vector<double
     return x;
 }
 
+// ------------------------------------------------------------------------------------------------
+// Host state of one closed-shell SCF (SCFIterator.C:283-362, SCFAcceleratorDIIS.C:35-238): canonical
+// orthogonaliser X = U s^{-1/2}, density, Fock matrix in the orthonormal basis and the DIIS subspace.
+// ------------------------------------------------------------------------------------------------
+struct ScfCore
+{
+    int n = 0, nocc = 0;
+    double fdmax = 0, Enn = 0;
+    std::vector<double> S, H, X, D, Dp, F, Fp, Err, tmp, Up, w, a, b;
+    std::deque<std::vector<double>> Es, Fps;
+    double E = 0, Eold = 0, En = 0;
+
+    void init(int n_, int nocc_, std::vector<double> S_, std::vector<double> H_, double fdmax_, double Enn_,
+              const double* guess)
+    {
+        n = n_;
+        nocc = nocc_;
+        fdmax = fdmax_;
+        Enn = Enn_;
+        const size_t nn = (size_t)n * n;
+        S = std::move(S_);
+        H = std::move(H_);
+        X.assign(nn, 0.0);
+        std::vector<double> sw(n), U(nn);
+        syev(n, S.data(), sw.data(), U.data());
+        require(sw[0] > 0, "overlap matrix is not positive definite");
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j) X[(size_t)i * n + j] = U[(size_t)i * n + j] / std::sqrt(sw[j]);
+        tmp.assign(nn, 0.0);
+        Fp.assign(nn, 0.0);
+        Dp.assign(nn, 0.0);
+        D.assign(nn, 0.0);
+        Up.assign(nn, 0.0);
+        w.assign(n, 0.0);
+        F.assign(nn, 0.0);
+        Err.assign(nn, 0.0);
+        a.assign(nn, 0.0);
+        b.assign(nn, 0.0);
+        if (guess)
+        {
+            // caller's initial density (e.g. a learned guess): D as given, symmetrised; its orthonormal-basis
+            // image D' = X^T S D S X (X^T S X = 1) enters the first DIIS error
+            for (int i = 0; i < n; ++i)
+                for (int j = 0; j < n; ++j)
+                {
+                    const double x = 0.5 * (guess[(size_t)i * n + j] + guess[(size_t)j * n + i]);
+                    require(std::isfinite(x), "non-finite initial density", QCG_ERR_NONFINITE);
+                    D[(size_t)i * n + j] = x;
+                }
+            gemm(n, S.data(), false, X.data(), false, tmp.data());       // S X
+            gemm(n, D.data(), false, tmp.data(), false, Up.data());      // D S X
+            gemm(n, tmp.data(), true, Up.data(), false, Dp.data());      // X^T S D S X
+        }
+        else
+        {
+            ortho(H, Fp);
+            diag_fill(Fp);   // core guess (Seed.C:70-80)
+        }
+    }
+    void ortho(const std::vector<double>& M, std::vector<double>& out)
+    {
+        gemm(n, M.data(), false, X.data(), false, tmp.data());
+        gemm(n, X.data(), true, tmp.data(), false, out.data());
+    }
+    // aufbau density of an orthonormal-basis Fock matrix, back in the AO basis (exactly symmetric)
+    void diag_fill(const std::vector<double>& Fo)
+    {
+        syev(n, Fo.data(), w.data(), Up.data());
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j)
+            {
+                double s = 0;
+                for (int k = 0; k < nocc; ++k) s += Up[(size_t)i * n + k] * Up[(size_t)j * n + k];
+                Dp[(size_t)i * n + j] = 2 * s;
+            }
+        gemm(n, X.data(), false, Dp.data(), false, tmp.data());
+        gemm(n, tmp.data(), false, X.data(), true, D.data());
+        for (int i = 0; i < n; ++i)
+            for (int j = i + 1; j < n; ++j)
+            {
+                const double v = 0.5 * (D[(size_t)i * n + j] + D[(size_t)j * n + i]);
+                D[(size_t)i * n + j] = D[(size_t)j * n + i] = v;
+            }
+    }
+    // F = H + J - K/2, the energy of the current density and the DIIS error ||F'D' - D'F'||
+    void fock(const double* J, const double* K)
+    {
+        const size_t nn = (size_t)n * n;
+        double e = 0;
+        for (size_t k = 0; k < nn; ++k)
+        {
+            F[k] = H[k] + J[k] - 0.5 * K[k];
+            e += D[k] * (H[k] + F[k]);
+        }
+        E = 0.5 * e + Enn;
+        if (!std::isfinite(E)) throw Error{QCG_ERR_NONFINITE, "non-finite SCF energy"};
+        ortho(F, Fp);
+        gemm(n, Fp.data(), false, Dp.data(), false, a.data());
+        gemm(n, Dp.data(), false, Fp.data(), false, b.data());
+        En = 0;
+        for (size_t k = 0; k < nn; ++k)
+        {
+            Err[k] = a[k] - b[k];
+            En += Err[k] * Err[k];
+        }
+        En = std::sqrt(En);
+    }
+    // Pulay extrapolation over the last nproj (Err, F') pairs -- entered only while En <= fdmax, pruned from
+    // the oldest while the bordered matrix has a singular value below svtol -- then the new density
+    void step(const qcg_scf_params& prm)
+    {
+        const size_t nn = (size_t)n * n;
+        std::vector<double> Fuse = Fp;
+        if (En != 0.0 && En <= fdmax)
+        {
+            Es.push_back(Err);
+            Fps.push_back(Fp);
+            if ((int)Es.size() > prm.diis_nproj)
+            {
+                Es.pop_front();
+                Fps.pop_front();
+            }
+            auto bordered = [&]() {
+                const int m = (int)Es.size();
+                std::vector<double> B((m + 1) * (m + 1), 0.0);
+                for (int i = 0; i < m; ++i)
+                {
+                    B[i * (m + 1) + m] = B[m * (m + 1) + i] = 1.0;
+                    for (int j = i; j < m; ++j)
+                    {
+                        double s = 0;
+                        for (size_t k = 0; k < nn; ++k) s += Es[i][k] * Es[j][k];
+                        B[i * (m + 1) + j] = B[j * (m + 1) + i] = s;
+                    }
+                }
+                return B;
+            };
+            auto minsv = [&](const std::vector<double>& B) {
+                const int m1 = (int)std::lround(std::sqrt((double)B.size()));
+                std::vector<double> ev(m1), vv(B.size());
+                syev(m1, B.data(), ev.data(), vv.data());
+                double mn = 1e300;
+                for (double x : ev) mn = std::min(mn, std::fabs(x));
+                return mn;
+            };
+            if (Es.size() >= 2)
+            {
+                auto B = bordered();
+                while (Es.size() >= 2 && minsv(B) < prm.diis_svtol)
+                {
+                    Es.pop_front();
+                    Fps.pop_front();
+                    B = bordered();
+                }
+                const int m = (int)Es.size();
+                if (m >= 2)
+                {
+                    std::vector<double> rhs(m + 1, 0.0);
+                    rhs[m] = 1.0;
+                    auto c = solve_dense(m + 1, B, rhs);
+                    std::fill(Fuse.begin(), Fuse.end(), 0.0);
+                    for (int i = 0; i < m; ++i)
+                        for (size_t k = 0; k < nn; ++k) Fuse[k] += c[i] * Fps[i][k];
+                }
+            }
+        }
+        diag_fill(Fuse);
+    }
+};
+
+// nuclear repulsion and total nuclear charge of natom nuclei
+void nuclei(int natom, const double* Z, const double* R, double& Ztot, double& Enn)
+{
+    Ztot = 0;
+    Enn = 0;
+    for (int i = 0; i < natom; ++i)
+    {
+        Ztot += Z[i];
+        for (int j = 0; j < i; ++j)
+        {
+            double d2 = 0;
+            for (int x = 0; x < 3; ++x) d2 += (R[3 * i + x] - R[3 * j + x]) * (R[3 * i + x] - R[3 * j + x]);
+            Enn += Z[i] * Z[j] / std::sqrt(d2);
+        }
+    }
+}
+
 void ensure_jk_buffers(qcg_handle* h)
 {
     if (h->d_Jp) return;
-    const size_t nn = (size_t)h->nbf * h->nbf;
+    const size_t nn = (size_t)h->packed;
     h->d_D = h->alloc<double>(nn);
     h->d_Jp = h->alloc<double>(nn);
     h->d_Kp = h->alloc<double>(nn);
@@ -545,7 +747,7 @@ void build_screening(qcg_handle* h, double thresh)
     // shell pairs per class, (a,b) with L_a > L_b, or L_a == L_b and a >= b
     std::vector<int> sa[kNumPairClasses], sb[kNumPairClasses];
     for (int a = 0; a < h->nshell; ++a)
-        for (int b = 0; b <= a; ++b)
+        for (int b = h->mol_shell0[h->shell_mol[a]]; b <= a; ++b)   // pairs within one molecule
         {
             int x = a, y = b;
             if (h->L[y] > h->L[x]) std::swap(x, y);
@@ -620,7 +822,7 @@ void build_screening(qcg_handle* h, double thresh)
         int* dppo = h->upload(ppo[c]);
         int* dnpp = h->upload(npp[c]);
         double* dQ = h->alloc<double>(n);
-        PairListDev pl{n, dsa, dsb, dppo, dnpp, nullptr};
+        PairListDev pl{n, dsa, dsb, dppo, dnpp, nullptr, nullptr};
         kSchwarzLaunchers[c](pl, P0, dQ, h->d_boys, h->stream);
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(Qc[c].data(), dQ, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
@@ -630,30 +832,41 @@ void build_screening(qcg_handle* h, double thresh)
     for (void* p : tmp) h->release(p);
     for (const double* p : {P0.p, P0.Px, P0.Py, P0.Pz, P0.PAx, P0.PAy, P0.PAz, P0.PBx, P0.PBy, P0.PBz, P0.K})
         h->release((void*)p);
-    // full Q matrix for callers
-    h->Qfull.assign((size_t)h->nshell * h->nshell, 0.0);
     for (int c = 0; c < kNumPairClasses; ++c)
         for (size_t k = 0; k < sa[c].size(); ++k)
-        {
             if (!std::isfinite(Qc[c][k])) throw Error{QCG_ERR_NONFINITE, "non-finite Schwarz bound"};
-            h->Qfull[(size_t)sa[c][k] * h->nshell + sb[c][k]] = Qc[c][k];
-            h->Qfull[(size_t)sb[c][k] * h->nshell + sa[c][k]] = Qc[c][k];
-        }
-    // sort each class by Q descending, rebuild primitive pairs in that order
+    // full Q matrix for callers (single molecule)
+    h->Qfull.clear();
+    if (h->nmol == 1)
+    {
+        h->Qfull.assign((size_t)h->nshell * h->nshell, 0.0);
+        for (int c = 0; c < kNumPairClasses; ++c)
+            for (size_t k = 0; k < sa[c].size(); ++k)
+            {
+                h->Qfull[(size_t)sa[c][k] * h->nshell + sb[c][k]] = Qc[c][k];
+                h->Qfull[(size_t)sb[c][k] * h->nshell + sa[c][k]] = Qc[c][k];
+            }
+    }
+    // sort each class by molecule, then Q descending; rebuild primitive pairs in that order
     for (int c = 0; c < kNumPairClasses; ++c)
     {
         const size_t n = sa[c].size();
         std::vector<size_t> ord(n);
         std::iota(ord.begin(), ord.end(), 0);
-        std::stable_sort(ord.begin(), ord.end(), [&](size_t x, size_t y) { return Qc[c][x] > Qc[c][y]; });
+        std::stable_sort(ord.begin(), ord.end(), [&](size_t x, size_t y) {
+            const int mx = h->shell_mol[sa[c][x]], my = h->shell_mol[sa[c][y]];
+            return mx != my ? mx < my : Qc[c][x] > Qc[c][y];
+        });
         h->pl_sa[c].resize(n);
         h->pl_sb[c].resize(n);
         h->pl_Q[c].resize(n);
+        h->pl_mol[c].resize(n);
         for (size_t k = 0; k < n; ++k)
         {
             h->pl_sa[c][k] = sa[c][ord[k]];
             h->pl_sb[c][k] = sb[c][ord[k]];
             h->pl_Q[c][k] = Qc[c][ord[k]];
+            h->pl_mol[c][k] = h->shell_mol[sa[c][ord[k]]];
         }
     }
     build_pp(h->pl_sa, h->pl_sb, pp, h->pl_ppo, h->pl_npp);
@@ -662,7 +875,16 @@ void build_screening(qcg_handle* h, double thresh)
     {
         const int n = (int)h->pl_sa[c].size();
         h->pl_dev[c] = PairListDev{n, h->upload(h->pl_sa[c]), h->upload(h->pl_sb[c]), h->upload(h->pl_ppo[c]),
-                                   h->upload(h->pl_npp[c]), h->upload(h->pl_Q[c])};
+                                   h->upload(h->pl_npp[c]), h->upload(h->pl_Q[c]),
+                                   h->nmol > 1 ? h->upload(h->pl_mol[c]) : nullptr};
+    }
+    // each molecule's range [seg[c][m], seg[c][m+1]) in the sorted pair list of class c
+    std::vector<std::vector<int>> seg(kNumPairClasses, std::vector<int>(h->nmol + 1, 0));
+    for (int c = 0; c < kNumPairClasses; ++c)
+    {
+        std::vector<int> cnt(h->nmol, 0);
+        for (int m : h->pl_mol[c]) ++cnt[m];
+        for (int m = 0; m < h->nmol; ++m) seg[c][m + 1] = seg[c][m] + cnt[m];
     }
     // work lists: bra pair i of class X against the prefix of class Y with Q_i Q_j >= thresh
     h->work_quartets = 0;
@@ -675,27 +897,34 @@ void build_screening(qcg_handle* h, double thresh)
             const auto& qx = h->pl_Q[X];
             const auto& qy = h->pl_Q[Y];
             std::vector<long long> offs(qx.size() + 1, 0);
+            std::vector<int> kbase(qx.size(), 0);
             // prefix sums of ket primitive-pair counts for the primitive-quartet tally
             std::vector<long long> nppy(qy.size() + 1, 0);
             for (size_t j = 0; j < qy.size(); ++j) nppy[j + 1] = nppy[j] + h->pl_npp[Y][j];
             long long pq = 0;
             for (size_t i = 0; i < qx.size(); ++i)
             {
+                // kets: the bra's molecule's part of class Y, Q descending
+                const int m = h->pl_mol[X][i];
+                const int jb = seg[Y][m], je = seg[Y][m + 1];
                 long long cnt = 0;
                 if (qx[i] > 0)
                 {
                     const double need = thresh / qx[i];
-                    // qy descending: count of entries >= need
-                    cnt = std::upper_bound(qy.begin(), qy.end(), need, [](double v, double e) { return v > e; }) -
-                          qy.begin();
-                    // entries exactly equal to need pass too (upper_bound with > keeps ties in front)
+                    // count of entries >= need (upper_bound with > keeps ties in front)
+                    cnt = std::upper_bound(qy.begin() + jb, qy.begin() + je, need,
+                                           [](double v, double e) { return v > e; }) -
+                          (qy.begin() + jb);
                 }
-                if (X == Y) cnt = std::min<long long>(cnt, (long long)i + 1);
+                if (X == Y) cnt = std::min<long long>(cnt, (long long)i - jb + 1);
+                kbase[i] = jb;
                 offs[i + 1] = offs[i] + cnt;
-                pq += (long long)h->pl_npp[X][i] * nppy[cnt];
+                pq += (long long)h->pl_npp[X][i] * (nppy[jb + cnt] - nppy[jb]);
             }
             h->work[k].total = offs.back();
             h->work[k].offs = h->upload(offs);
+            h->work[k].kbase = h->nmol > 1 ? h->upload(kbase) : nullptr;
+            h->work[k].mols = h->mols();
             h->work[k].same_class = (X == Y);
             h->work[k].lo = 0.0;
             h->work[k].hi = HUGE_VAL;
@@ -718,7 +947,10 @@ void jk_device(qcg_handle* h, const double* dD, double* dJ, double* dK, int flag
     require(h->screened, "qcg_schwarz must be called before qcg_fock_jk", QCG_ERR_STATE);
     ensure_jk_buffers(h);
     const int n = h->nbf;
-    const size_t nn = (size_t)n * n;
+    const size_t nn = (size_t)h->packed;
+    // density screening and the density-weighted FP32 band index a shell x shell table: single molecule
+    require(h->nmol == 1 || (!dmax && (fp32_below <= 0 || fp32_below >= HUGE_VAL)),
+            "density-weighted screening and mixed precision need a single-molecule handle");
     if (fp32_below > 0 && fp32_below < HUGE_VAL && !dmax)
     {
         if (!h->d_dmaxD) h->d_dmaxD = h->alloc<double>((size_t)h->nshell * h->nshell);
@@ -734,7 +966,7 @@ void jk_device(qcg_handle* h, const double* dD, double* dJ, double* dK, int flag
     CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
     if (!(flags & QCG_JK_SKIP_VALIDATION))
     {
-        launch_validate(dD, n, 1e-10, h->d_flag, h->stream, h->nsm);
+        launch_validate(dD, (long long)nn, n, h->mols(), 1e-10, h->d_flag, h->stream, h->nsm);
         int flag = 0;
         CK(cudaMemcpyAsync(&flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
@@ -792,7 +1024,7 @@ void jk_device(qcg_handle* h, const double* dD, double* dJ, double* dK, int flag
         CK(cudaStreamWaitEvent(h->stream, h->join[s], 0));
     }
     CK(cudaEventRecord(h->ev2, h->stream));
-    launch_symmetrize(h->d_Jp, h->d_Kp, dJ, dK, n, h->d_flag, h->stream, h->nsm);
+    launch_symmetrize(h->d_Jp, h->d_Kp, dJ, dK, (long long)nn, n, h->mols(), h->d_flag, h->stream, h->nsm);
     CK(cudaGetLastError());
     if (stats)
     {
@@ -844,13 +1076,34 @@ extern "C" {
 int qcg_basis_create(const int* shell_L, const int* shell_nprim, const double* exps, const double* coefs,
                      const double* centres, int nshell, qcg_handle** out)
 {
+    return qcg_basis_create_batch(shell_L, shell_nprim, exps, coefs, centres, nshell, nullptr, 1, out);
+}
+
+int qcg_basis_create_batch(const int* shell_L, const int* shell_nprim, const double* exps, const double* coefs,
+                           const double* centres, int nshell, const int* shell_mol, int nmol, qcg_handle** out)
+{
     if (!out) return QCG_ERR_ARG;
     *out = nullptr;
     qcg_handle* h = new qcg_handle;
     int rc = guarded(h, [&] {
         require(shell_L && shell_nprim && exps && coefs && centres, "null argument");
         require(nshell > 0, "nshell must be positive");
+        require(nmol >= 1 && (nmol == 1 || shell_mol), "nmol must be positive (shell_mol is needed for several)");
         h->nshell = nshell;
+        h->nmol = nmol;
+        h->shell_mol.assign(nshell, 0);
+        if (shell_mol)
+            for (int s = 0; s < nshell; ++s)
+            {
+                require(shell_mol[s] >= 0 && shell_mol[s] < nmol, "shell molecule index out of range");
+                require(s == 0 || shell_mol[s] == shell_mol[s - 1] || shell_mol[s] == shell_mol[s - 1] + 1,
+                        "shells must be grouped by molecule in molecule order");
+                h->shell_mol[s] = shell_mol[s];
+            }
+        require(h->shell_mol[0] == 0 && h->shell_mol[nshell - 1] == nmol - 1, "every molecule needs shells");
+        h->mol_shell0.assign(nmol, 0);
+        h->mol_nbf.assign(nmol, 0);
+        for (int s = nshell - 1; s >= 0; --s) h->mol_shell0[h->shell_mol[s]] = s;
         int np = 0;
         for (int s = 0; s < nshell; ++s)
         {
@@ -860,7 +1113,9 @@ int qcg_basis_create(const int* shell_L, const int* shell_nprim, const double* e
             h->L.push_back(shell_L[s]);
             h->nprim.push_back(shell_nprim[s]);
             h->prim0.push_back(np);
-            h->f0.push_back(h->nbf);
+            // function offset local to the shell's molecule (global for a single molecule)
+            h->f0.push_back(h->mol_nbf[h->shell_mol[s]]);
+            h->mol_nbf[h->shell_mol[s]] += ncart(shell_L[s]);
             h->nbf += ncart(shell_L[s]);
             for (int i = 0; i < shell_nprim[s]; ++i)
             {
@@ -905,6 +1160,15 @@ int qcg_basis_create(const int* shell_L, const int* shell_nprim, const double* e
         h->bs.alpha = h->upload(h->alpha);
         h->bs.coef = h->upload(h->coef);
         h->d_f0 = h->upload(h->f0);
+        h->mol_off.assign(nmol + 1, 0);
+        for (int m = 0; m < nmol; ++m) h->mol_off[m + 1] = h->mol_off[m] + (long long)h->mol_nbf[m] * h->mol_nbf[m];
+        h->packed = h->mol_off[nmol];
+        if (nmol > 1)
+        {
+            h->d_shell_mol = h->upload(h->shell_mol);
+            h->d_mol_off = h->upload(h->mol_off);
+            h->d_mol_n = h->upload(h->mol_nbf);
+        }
         CK(cudaStreamSynchronize(h->stream));
     });
     if (rc != QCG_OK)
@@ -934,6 +1198,20 @@ int qcg_set_memory_limit(qcg_handle* h, long long bytes)
 {
     if (!h || bytes < 0) return QCG_ERR_ARG;
     h->mem_limit = bytes;
+    return QCG_OK;
+}
+
+int qcg_nmol(const qcg_handle* h, int* nmol)
+{
+    if (!h || !nmol) return QCG_ERR_ARG;
+    *nmol = h->nmol;
+    return QCG_OK;
+}
+
+int qcg_mol_nbf(const qcg_handle* h, int* nbf)
+{
+    if (!h || !nbf) return QCG_ERR_ARG;
+    std::copy(h->mol_nbf.begin(), h->mol_nbf.end(), nbf);
     return QCG_OK;
 }
 
@@ -1059,6 +1337,7 @@ int qcg_schwarz(qcg_handle* h, double thresh, double* Q)
     if (!h) return QCG_ERR_ARG;
     return guarded(h, [&] {
         require(std::isfinite(thresh) && thresh >= 0, "threshold must be finite and non-negative");
+        require(!Q || h->nmol == 1, "per-pair bounds are returned for single-molecule handles only");
         if (!h->screened || h->thresh != thresh)
         {
             // drop previous screening state (device buffers of pair lists and work lists)
@@ -1067,12 +1346,16 @@ int qcg_schwarz(qcg_handle* h, double thresh, double* Q)
                 for (int c = 0; c < kNumPairClasses; ++c)
                     for (const void* p : {(const void*)h->pl_dev[c].sa, (const void*)h->pl_dev[c].sb,
                                           (const void*)h->pl_dev[c].ppo, (const void*)h->pl_dev[c].npp,
-                                          (const void*)h->pl_dev[c].Q})
-                        h->release((void*)p);
+                                          (const void*)h->pl_dev[c].Q, (const void*)h->pl_dev[c].mol})
+                        if (p) h->release((void*)p);
                 const PrimPairsDev& P = h->pp_dev;
                 for (const double* p : {P.p, P.Px, P.Py, P.Pz, P.PAx, P.PAy, P.PAz, P.PBx, P.PBy, P.PBz, P.K})
                     h->release((void*)p);
-                for (int k = 0; k < kNumQuartetClasses; ++k) h->release((void*)h->work[k].offs);
+                for (int k = 0; k < kNumQuartetClasses; ++k)
+                {
+                    h->release((void*)h->work[k].offs);
+                    if (h->work[k].kbase) h->release((void*)h->work[k].kbase);
+                }
                 h->screened = false;
             }
             build_screening(h, thresh);
@@ -1104,19 +1387,23 @@ int qcg_fock_jk(qcg_handle* h, const double* D, double* J, double* K, int flags,
     if (!h) return QCG_ERR_ARG;
     return guarded(h, [&] {
         require(D && J && K, "null argument");
-        const int n = h->nbf;
-        const size_t nn = (size_t)n * n;
+        const size_t nn = (size_t)h->packed;
         if (!(flags & QCG_JK_SKIP_VALIDATION))
         {
             for (size_t k = 0; k < nn; ++k)
                 if (!std::isfinite(D[k])) throw Error{QCG_ERR_NONFINITE, "density matrix has NaN/Inf entries"};
-            for (int i = 0; i < n; ++i)
-                for (int j = i + 1; j < n; ++j)
-                {
-                    const double a = D[(size_t)i * n + j], b = D[(size_t)j * n + i];
-                    if (std::fabs(a - b) > 1e-10 * (1.0 + std::fabs(a)))
-                        throw Error{QCG_ERR_ASYMMETRIC, "density matrix is not symmetric"};
-                }
+            for (int m = 0; m < h->nmol; ++m)
+            {
+                const double* Dm = D + h->mol_off[m];
+                const int n = h->mol_nbf[m];
+                for (int i = 0; i < n; ++i)
+                    for (int j = i + 1; j < n; ++j)
+                    {
+                        const double a = Dm[(size_t)i * n + j], b = Dm[(size_t)j * n + i];
+                        if (std::fabs(a - b) > 1e-10 * (1.0 + std::fabs(a)))
+                            throw Error{QCG_ERR_ASYMMETRIC, "density matrix is not symmetric"};
+                    }
+            }
         }
         require(h->screened, "qcg_schwarz must be called before qcg_fock_jk", QCG_ERR_STATE);
         ensure_jk_buffers(h);
@@ -1137,6 +1424,7 @@ int qcg_one_electron(qcg_handle* h, int natom, const double* Z, const double* R,
     if (!h) return QCG_ERR_ARG;
     return guarded(h, [&] {
         require(natom >= 0 && (natom == 0 || (Z && R)) && S && T && V, "bad argument");
+        require(h->nmol == 1, "qcg_one_electron takes a single-molecule handle (qcg_one_electron_batch)");
         const int n = h->nbf;
         const size_t nn = (size_t)n * n;
         std::vector<double> z(Z, Z + natom), r(R, R + 3 * natom);
@@ -1153,6 +1441,55 @@ int qcg_one_electron(qcg_handle* h, int natom, const double* Z, const double* R,
         if (e == cudaSuccess) e = cudaMemcpyAsync(V, dV, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
         for (void* p : {(void*)dZ, (void*)dR, (void*)dS, (void*)dT, (void*)dV}) h->release(p);
+        if (e != cudaSuccess) throw Error{QCG_ERR_CUDA, std::string("one-electron integrals: ") + cudaGetErrorString(e)};
+    });
+}
+
+int qcg_one_electron_batch(qcg_handle* h, const int* mol_natom, const double* Z, const double* R, double* S,
+                           double* T, double* V)
+{
+    if (!h) return QCG_ERR_ARG;
+    return guarded(h, [&] {
+        require(mol_natom && Z && R && S && T && V, "null argument");
+        std::vector<int> atom0(h->nmol), nat(mol_natom, mol_natom + h->nmol);
+        int total = 0;
+        for (int m = 0; m < h->nmol; ++m)
+        {
+            require(nat[m] > 0, "every molecule needs at least one nucleus");
+            atom0[m] = total;
+            total += nat[m];
+        }
+        std::vector<double> z(Z, Z + total), r(R, R + 3 * total);
+        for (double x : r) require(std::isfinite(x), "non-finite nuclear position", QCG_ERR_NONFINITE);
+        // shell pairs (a >= b) within each molecule
+        std::vector<int2> pairs;
+        for (int a = 0; a < h->nshell; ++a)
+            for (int b = h->mol_shell0[h->shell_mol[a]]; b <= a; ++b) pairs.push_back(int2{a, b});
+        const size_t nn = (size_t)h->packed;
+        double* dZ = h->upload(z);
+        double* dR = h->upload(r);
+        int* dA0 = h->upload(atom0);
+        int* dNA = h->upload(nat);
+        int2* dP = h->upload(pairs);
+        int* dSM = h->nmol > 1 ? h->d_shell_mol : h->upload(std::vector<int>(h->nshell, 0));
+        std::vector<long long> off1 = {0, (long long)nn};
+        std::vector<int> n1 = {h->nbf};
+        long long* dOff = h->nmol > 1 ? h->d_mol_off : h->upload(off1);
+        int* dN = h->nmol > 1 ? h->d_mol_n : h->upload(n1);
+        double* dS = h->alloc<double>(nn);
+        double* dT = h->alloc<double>(nn);
+        double* dV = h->alloc<double>(nn);
+        launch_one_electron(h->bs, h->d_f0, h->nbf, total, dZ, dR, dS, dT, dV, h->d_boys, h->stream, h->nsm, dP,
+                            (long long)pairs.size(), dSM, MolLayoutDev{std::max(h->nmol, 2), dOff, dN}, dA0, dNA);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpyAsync(S, dS, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(T, dT, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(V, dV, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+        for (void* p : {(void*)dZ, (void*)dR, (void*)dA0, (void*)dNA, (void*)dP, (void*)dS, (void*)dT, (void*)dV})
+            h->release(p);
+        if (h->nmol == 1)
+            for (void* p : {(void*)dSM, (void*)dOff, (void*)dN}) h->release(p);
         if (e != cudaSuccess) throw Error{QCG_ERR_CUDA, std::string("one-electron integrals: ") + cudaGetErrorString(e)};
     });
 }
@@ -1189,22 +1526,14 @@ int qcg_rhf(qcg_handle* h, int natom, const double* Z, const double* R, int nele
         qcg_scf_default_params(&prm);
         if (params) prm = *params;
         require(result != nullptr, "null result");
+        require(h->nmol == 1, "qcg_rhf takes a single-molecule handle (qcg_rhf_batch for several)");
         require(natom > 0 && Z && R, "bad nuclei");
         require(nelec > 0 && nelec % 2 == 0, "closed-shell RHF needs a positive even electron count");
         const int n = h->nbf, nocc = nelec / 2;
         require(nocc <= n, "more occupied orbitals than basis functions");
         const size_t nn = (size_t)n * n;
         double Ztot = 0, Enn = 0;
-        for (int i = 0; i < natom; ++i)
-        {
-            Ztot += Z[i];
-            for (int j = 0; j < i; ++j)
-            {
-                double d2 = 0;
-                for (int x = 0; x < 3; ++x) d2 += (R[3 * i + x] - R[3 * j + x]) * (R[3 * i + x] - R[3 * j + x]);
-                Enn += Z[i] * Z[j] / std::sqrt(d2);
-            }
-        }
+        nuclei(natom, Z, R, Ztot, Enn);
         const double fdmax = prm.diis_fdmax > 0 ? prm.diis_fdmax : Ztot * Ztot * 0.1 / 32;
         std::vector<double> S(nn), T(nn), V(nn), H(nn);
         {
@@ -1217,60 +1546,12 @@ int qcg_rhf(qcg_handle* h, int natom, const double* Z, const double* R, int nele
             if (e != QCG_OK) throw Error{e, h->last_error};
         }
         ensure_jk_buffers(h);
-        // canonical orthogonalisation X = U s^{-1/2}
-        std::vector<double> sw(n), U(nn), X(nn);
-        syev(n, S.data(), sw.data(), U.data());
-        require(sw[0] > 0, "overlap matrix is not positive definite");
-        for (int i = 0; i < n; ++i)
-            for (int j = 0; j < n; ++j) X[(size_t)i * n + j] = U[(size_t)i * n + j] / std::sqrt(sw[j]);
-        std::vector<double> tmp(nn), Fp(nn), Dp(nn, 0.0), D(nn), Up(nn), w(n);
-        auto ortho = [&](const std::vector<double>& F, std::vector<double>& out) {
-            gemm(n, F.data(), false, X.data(), false, tmp.data());
-            gemm(n, X.data(), true, tmp.data(), false, out.data());
-        };
-        auto diag_fill = [&](const std::vector<double>& F) {
-            syev(n, F.data(), w.data(), Up.data());
-            for (int i = 0; i < n; ++i)
-                for (int j = 0; j < n; ++j)
-                {
-                    double s = 0;
-                    for (int k = 0; k < nocc; ++k) s += Up[(size_t)i * n + k] * Up[(size_t)j * n + k];
-                    Dp[(size_t)i * n + j] = 2 * s;
-                }
-            gemm(n, X.data(), false, Dp.data(), false, tmp.data());
-            gemm(n, tmp.data(), false, X.data(), true, D.data());
-            // exact symmetry for the validation in the J/K build
-            for (int i = 0; i < n; ++i)
-                for (int j = i + 1; j < n; ++j)
-                {
-                    const double a = 0.5 * (D[(size_t)i * n + j] + D[(size_t)j * n + i]);
-                    D[(size_t)i * n + j] = D[(size_t)j * n + i] = a;
-                }
-        };
-        if (prm.D_guess)
-        {
-            // caller's initial density (e.g. a learned guess): D as given, symmetrised; its orthonormal-basis
-            // image D' = X^T S D S X (X^T S X = 1) enters the first DIIS error
-            for (int i = 0; i < n; ++i)
-                for (int j = 0; j < n; ++j)
-                {
-                    const double x = 0.5 * (prm.D_guess[(size_t)i * n + j] + prm.D_guess[(size_t)j * n + i]);
-                    require(std::isfinite(x), "non-finite initial density", QCG_ERR_NONFINITE);
-                    D[(size_t)i * n + j] = x;
-                }
-            gemm(n, S.data(), false, X.data(), false, tmp.data());       // S X
-            gemm(n, D.data(), false, tmp.data(), false, Up.data());      // D S X
-            gemm(n, tmp.data(), true, Up.data(), false, Dp.data());      // X^T S D S X
-        }
-        else
-        {
-            ortho(H, Fp);
-            diag_fill(Fp);   // core guess
-        }
-        std::deque<std::vector<double>> Es, Fps;
-        std::vector<double> J(nn), K(nn), F(nn), Err(nn), a(nn), b(nn);
+        ScfCore sc;
+        sc.init(n, nocc, std::move(S), std::move(H), fdmax, Enn, prm.D_guess);
+        std::vector<double>& D = sc.D;
+        std::vector<double> J(nn), K(nn);
         std::vector<double> Dprev, Jprev, Kprev, dD(nn);
-        double E = 0, Eold = 0, En = 0, fock_ms = 0;
+        double fock_ms = 0;
         const bool inc = prm.incremental != 0;
         int since_full = 0, nfull = 0, ninc = 0, n32 = 0;
         bool force_full = true;
@@ -1327,25 +1608,8 @@ int qcg_rhf(qcg_handle* h, int natom, const double* Z, const double* R, int nele
                 ++ninc;
             }
             if (inc) { Dprev = D; Jprev = J; Kprev = K; }
-            double e = 0;
-            for (size_t k = 0; k < nn; ++k)
-            {
-                F[k] = H[k] + J[k] - 0.5 * K[k];
-                e += D[k] * (H[k] + F[k]);
-            }
-            E = 0.5 * e + Enn;
-            if (!std::isfinite(E)) throw Error{QCG_ERR_NONFINITE, "non-finite SCF energy"};
-            ortho(F, Fp);
-            gemm(n, Fp.data(), false, Dp.data(), false, a.data());
-            gemm(n, Dp.data(), false, Fp.data(), false, b.data());
-            En = 0;
-            for (size_t k = 0; k < nn; ++k)
-            {
-                Err[k] = a[k] - b[k];
-                En += Err[k] * Err[k];
-            }
-            En = std::sqrt(En);
-            if (it > 1 && std::fabs(E - Eold) < prm.de_tol && En < prm.fd_tol)
+            sc.fock(J.data(), K.data());
+            if (it > 1 && std::fabs(sc.E - sc.Eold) < prm.de_tol && sc.En < prm.fd_tol)
             {
                 if (!full || band != 0.0)
                 {
@@ -1361,76 +1625,22 @@ int qcg_rhf(qcg_handle* h, int natom, const double* Z, const double* R, int nele
                 }
             }
             if (trace)
-                std::fprintf(stderr, "qcg_rhf it %3d  E %.12f  dE %+.3e  [F,D] %.3e  %s  fp32 below %.2e\n", it, E,
-                             E - Eold, En, full ? "full" : "incr", band);
-            En_prev = En;
-            if (fp32_phase && it > 1 && En < prm.fp32_switch)
+                std::fprintf(stderr, "qcg_rhf it %3d  E %.12f  dE %+.3e  [F,D] %.3e  %s  fp32 below %.2e\n", it, sc.E,
+                             sc.E - sc.Eold, sc.En, full ? "full" : "incr", band);
+            En_prev = sc.En;
+            if (fp32_phase && it > 1 && sc.En < prm.fp32_switch)
             {
                 fp32_phase = false;   // FP64 from here on, starting from a full rebuild
                 force_full = true;
             }
-            Eold = E;
-            std::vector<double> Fuse = Fp;
-            if (En != 0.0 && En <= fdmax)
-            {
-                Es.push_back(Err);
-                Fps.push_back(Fp);
-                if ((int)Es.size() > prm.diis_nproj)
-                {
-                    Es.pop_front();
-                    Fps.pop_front();
-                }
-                auto bordered = [&]() {
-                    const int m = (int)Es.size();
-                    std::vector<double> B((m + 1) * (m + 1), 0.0);
-                    for (int i = 0; i < m; ++i)
-                    {
-                        B[i * (m + 1) + m] = B[m * (m + 1) + i] = 1.0;
-                        for (int j = i; j < m; ++j)
-                        {
-                            double s = 0;
-                            for (size_t k = 0; k < nn; ++k) s += Es[i][k] * Es[j][k];
-                            B[i * (m + 1) + j] = B[j * (m + 1) + i] = s;
-                        }
-                    }
-                    return B;
-                };
-                auto minsv = [&](const std::vector<double>& B) {
-                    const int m1 = (int)std::lround(std::sqrt((double)B.size()));
-                    std::vector<double> ev(m1), vv(B.size());
-                    syev(m1, B.data(), ev.data(), vv.data());
-                    double mn = 1e300;
-                    for (double x : ev) mn = std::min(mn, std::fabs(x));
-                    return mn;
-                };
-                if (Es.size() >= 2)
-                {
-                    auto B = bordered();
-                    while (Es.size() >= 2 && minsv(B) < prm.diis_svtol)
-                    {
-                        Es.pop_front();
-                        Fps.pop_front();
-                        B = bordered();
-                    }
-                    const int m = (int)Es.size();
-                    if (m >= 2)
-                    {
-                        std::vector<double> rhs(m + 1, 0.0);
-                        rhs[m] = 1.0;
-                        auto c = solve_dense(m + 1, B, rhs);
-                        std::fill(Fuse.begin(), Fuse.end(), 0.0);
-                        for (int i = 0; i < m; ++i)
-                            for (size_t k = 0; k < nn; ++k) Fuse[k] += c[i] * Fps[i][k];
-                    }
-                }
-            }
-            diag_fill(Fuse);
+            sc.Eold = sc.E;
+            sc.step(prm);
         }
-        result->energy = E;
+        result->energy = sc.E;
         result->e_nuc = Enn;
         result->iterations = std::min(it, prm.max_iter);
         result->converged = converged ? 1 : 0;
-        result->fd_error = En;
+        result->fd_error = sc.En;
         result->fock_ms = fock_ms;
         result->full_builds = nfull;
         result->incremental_builds = ninc;
@@ -1482,6 +1692,7 @@ extern "C" int qcg_fock_jk_device_noalloc(qcg_handle* h, const double* d_D, doub
                 "qcg_fock_jk_device_noalloc supports at most " + std::to_string(kNoAllocMaxNbf) +
                     " basis functions (this basis has " + std::to_string(h->nbf) + ")");
         require(h->screened, "qcg_schwarz must be called before qcg_fock_jk_device_noalloc", QCG_ERR_STATE);
+        require(h->nmol == 1, "qcg_fock_jk_device_noalloc takes a single-molecule handle");
         double* scratch = noalloc_scratch_for(h->device);
         const int n = h->nbf;
         const size_t nn = (size_t)n * n;
@@ -1499,7 +1710,8 @@ extern "C" int qcg_fock_jk_device_noalloc(qcg_handle* h, const double* d_D, doub
                             h->stream, h->nsm);
         }
         CK(cudaGetLastError());
-        launch_symmetrize(Jp, Kp, d_J, d_K, n, flag, h->stream, h->nsm);
+        launch_symmetrize(Jp, Kp, d_J, d_K, (long long)nn, n, MolLayoutDev{1, nullptr, nullptr}, flag, h->stream,
+                          h->nsm);
         CK(cudaGetLastError());
     });
 }
@@ -1554,6 +1766,130 @@ int qcg_measure_fp64_peak(int reps, double* tflops, double* ms_per_launch)
 int qcg_measure_fp32_peak(int reps, double* tflops, double* ms_per_launch)
 {
     return measure_fma_peak<float>(reps, tflops, ms_per_launch, launch_ffma_peak);
+}
+
+// Several closed-shell SCFs advanced together (one handle from qcg_basis_create_batch): every iteration is
+// ONE J/K build over all molecules (the class kernels take every molecule's quartets), then each molecule's
+// host step (Fock matrix, energy, DIIS, diagonalisation) runs in parallel over the molecules.  A molecule
+// stops updating once it meets the convergence test; the loop ends when all have.
+int qcg_rhf_batch(qcg_handle* h, const int* mol_natom, const double* Z, const double* R, const int* nelec,
+                  const qcg_scf_params* params, qcg_scf_result* results, double* D_out)
+{
+    if (!h) return QCG_ERR_ARG;
+    bool all_converged = false;
+    int rc = guarded(h, [&] {
+        auto t0 = std::chrono::steady_clock::now();
+        qcg_scf_params prm;
+        qcg_scf_default_params(&prm);
+        if (params) prm = *params;
+        require(mol_natom && Z && R && nelec && results, "null argument");
+        const int nmol = h->nmol;
+        std::vector<int> atom0(nmol + 1, 0);
+        for (int m = 0; m < nmol; ++m)
+        {
+            require(mol_natom[m] > 0, "every molecule needs at least one nucleus");
+            require(nelec[m] > 0 && nelec[m] % 2 == 0, "closed-shell RHF needs a positive even electron count");
+            require(nelec[m] / 2 <= h->mol_nbf[m], "more occupied orbitals than basis functions");
+            atom0[m + 1] = atom0[m] + mol_natom[m];
+        }
+        const size_t nn = (size_t)h->packed;
+        std::vector<double> S(nn), T(nn), V(nn);
+        {
+            int e = qcg_one_electron_batch(h, mol_natom, Z, R, S.data(), T.data(), V.data());
+            if (e != QCG_OK) throw Error{e, h->last_error};
+            e = qcg_schwarz(h, prm.schwarz_thresh, nullptr);
+            if (e != QCG_OK) throw Error{e, h->last_error};
+        }
+        ensure_jk_buffers(h);
+        std::vector<ScfCore> sc(nmol);
+        std::vector<std::string> err(nmol);
+        std::vector<double> Enn(nmol);
+        std::vector<int> done(nmol, 0), iters(nmol, 0);
+#pragma omp parallel for schedule(dynamic)
+        for (int m = 0; m < nmol; ++m)
+        {
+            try
+            {
+                const int n = h->mol_nbf[m];
+                const size_t o = h->mol_off[m], mm = (size_t)n * n;
+                double Ztot = 0;
+                nuclei(mol_natom[m], Z + atom0[m], R + 3 * atom0[m], Ztot, Enn[m]);
+                std::vector<double> Sm(S.begin() + o, S.begin() + o + mm), Hm(mm);
+                for (size_t k = 0; k < mm; ++k) Hm[k] = T[o + k] + V[o + k];
+                const double fdmax = prm.diis_fdmax > 0 ? prm.diis_fdmax : Ztot * Ztot * 0.1 / 32;
+                sc[m].init(n, nelec[m] / 2, std::move(Sm), std::move(Hm), fdmax, Enn[m], nullptr);
+            }
+            catch (const Error& e)
+            {
+                err[m] = e.msg;
+            }
+        }
+        for (int m = 0; m < nmol; ++m)
+            if (!err[m].empty()) throw Error{QCG_ERR_ARG, "molecule " + std::to_string(m) + ": " + err[m]};
+        std::vector<double> Dh(nn), J(nn), K(nn);
+        double fock_ms = 0;
+        int it, nconv = 0, nbuild = 0;
+        for (it = 1; it <= prm.max_iter && nconv < nmol; ++it)
+        {
+            ++nbuild;
+            for (int m = 0; m < nmol; ++m)
+                std::copy(sc[m].D.begin(), sc[m].D.end(), Dh.begin() + h->mol_off[m]);
+            qcg_stats st{};
+            CK(cudaMemcpyAsync(h->d_D, Dh.data(), nn * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+            jk_device(h, h->d_D, h->d_J, h->d_K, QCG_JK_SKIP_VALIDATION, &st);
+            CK(cudaMemcpyAsync(J.data(), h->d_J, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaMemcpyAsync(K.data(), h->d_K, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+            fock_ms += st.ms_total;
+#pragma omp parallel for schedule(dynamic)
+            for (int m = 0; m < nmol; ++m)
+            {
+                if (done[m]) continue;
+                try
+                {
+                    ScfCore& c = sc[m];
+                    c.fock(J.data() + h->mol_off[m], K.data() + h->mol_off[m]);
+                    iters[m] = it;
+                    if (it > 1 && std::fabs(c.E - c.Eold) < prm.de_tol && c.En < prm.fd_tol)
+                    {
+                        done[m] = 1;
+                        continue;
+                    }
+                    c.Eold = c.E;
+                    c.step(prm);
+                }
+                catch (const Error& e)
+                {
+                    err[m] = e.msg;
+                    done[m] = 1;
+                }
+            }
+            nconv = 0;
+            for (int m = 0; m < nmol; ++m)
+            {
+                if (!err[m].empty()) throw Error{QCG_ERR_NONFINITE, "molecule " + std::to_string(m) + ": " + err[m]};
+                nconv += done[m];
+            }
+        }
+        const double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        for (int m = 0; m < nmol; ++m)
+        {
+            qcg_scf_result& r = results[m];
+            r = qcg_scf_result{};
+            r.energy = sc[m].E;
+            r.e_nuc = Enn[m];
+            r.iterations = iters[m];
+            r.converged = done[m];
+            r.fd_error = sc[m].En;
+            r.wall_s = wall;
+            r.fock_ms = fock_ms;
+            r.full_builds = nbuild;
+            if (D_out) std::copy(sc[m].D.begin(), sc[m].D.end(), D_out + h->mol_off[m]);
+        }
+        all_converged = nconv == nmol;
+    });
+    if (rc == QCG_OK && !all_converged) return QCG_ERR_NOCONV;
+    return rc;
 }
 
 // test hook: the host eigensolver used by the SCF (not part of the public header)

@@ -140,9 +140,9 @@ def random_molecule(rng, n_atoms_max=24) -> Molecule:
             return Molecule(Z, np.array(R))
 
 
-def random_molecules(n=256, seed=SEED0 + 4000) -> List[Molecule]:
+def random_molecules(n=256, seed=SEED0 + 4000, max_atoms=24) -> List[Molecule]:
     rng = np.random.default_rng(seed)
-    return [random_molecule(rng) for _ in range(n)]
+    return [random_molecule(rng, max_atoms) for _ in range(n)]
 
 
 def basis_for(mol: Molecule) -> List[Shell]:

@@ -1,0 +1,56 @@
+"""Batched SCF (several molecules in one handle, one J/K build over all of them per iteration): every
+molecule's J, K and converged energy must equal those of its own single-molecule handle."""
+import numpy as np
+import pytest
+
+from qchem_b200 import api, basis as B, workloads as W
+
+pytestmark = pytest.mark.gpu
+
+FOCK_TOL = 1e-10
+E_TOL = 1e-8
+
+
+def _density(n, nocc, seed):
+    Q, _ = np.linalg.qr(np.random.default_rng(seed).normal(size=(n, nocc)))
+    return 2 * Q @ Q.T
+
+
+@pytest.fixture(scope="module")
+def mols():
+    ms = [W.water(), W.water_cluster(nx=2, ny=1, nz=1, seed=W.SEED0 + 3300)] + W.random_molecules(3, max_atoms=6)
+    return ms
+
+
+def test_batch_jk_equals_single_builds(mols):
+    shells = [B.even_tempered(m) for m in mols]
+    be = api.BatchEngine(shells)
+    assert be.nmol == len(mols) and be.mol_nbf == [B.nbf(s) for s in shells]
+    Ds = [_density(B.nbf(s), max(1, m.nelec // 2), 40 + k) for k, (m, s) in enumerate(zip(mols, shells))]
+    J, K, st = be.fock_jk(Ds)
+    total = 0
+    for k, (s, D) in enumerate(zip(shells, Ds)):
+        Js, Ks, sts = api.Engine(s).fock_jk(D)
+        assert np.abs(J[k] - Js).max() <= FOCK_TOL and np.abs(K[k] - Ks).max() <= FOCK_TOL, k
+        total += sts.quartets
+    assert st.quartets == total
+
+
+def test_batch_rhf_equals_single_rhf(mols):
+    shells = [B.even_tempered(m) for m in mols]
+    res = api.BatchEngine(shells).rhf(mols)
+    for m, s, r in zip(mols, shells, res):
+        ref = api.Engine(s).rhf(m)
+        assert r["converged"] == ref["converged"]
+        if ref["converged"]:
+            assert abs(r["energy"] - ref["energy"]) <= E_TOL
+            assert abs(r["iterations"] - ref["iterations"]) <= 1   # same trajectory up to summation order
+
+
+def test_batch_rejects_single_molecule_only_calls(mols):
+    be = api.BatchEngine([B.even_tempered(m) for m in mols[:2]])
+    with pytest.raises(api.QcgError):
+        be.one_electron(mols[0])
+    with pytest.raises(api.QcgError):
+        Engine_rhf = api.Engine.rhf
+        Engine_rhf(be, mols[0])
