@@ -149,6 +149,11 @@ int qcg_fock_jk_device(qcg_handle* h, const double* d_D, double* d_J, double* d_
  * evaluated in FP32 (accumulated in FP64), the rest in FP64.  0 (the default) keeps every quartet FP64.
  * No reference counterpart. */
 int qcg_set_fp32_bound(qcg_handle* h, double bound);
+/* 1: J/K builds repeated with the same arguments (device pointers, screening, precision) are captured as
+ * a CUDA graph on their second occurrence and replayed afterwards; 0 (default): launched kernel by kernel.
+ * Also switched on by the environment variable QCG_GRAPHS=1.  The handle's stream must not be the legacy
+ * default stream for capture to happen. */
+int qcg_set_graphs(qcg_handle* h, int enable);
 
 /* The J/K build of qcg_fock_jk_device for callers that must not allocate device memory once their setup
  * is done -- for example a host program whose device memory is owned by its own pool allocator, or one

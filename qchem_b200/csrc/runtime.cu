@@ -94,6 +94,21 @@ struct DevBuf
 
 }   // namespace
 
+// arguments that identify a J/K build for graph replay
+struct QcgGraphKey
+{
+    const void* D = nullptr;
+    const void* J = nullptr;
+    const void* K = nullptr;
+    const void* dmax = nullptr;
+    double dthr = -1, band = -1;
+    int gen = -1;
+    bool operator==(const QcgGraphKey& o) const
+    {
+        return D == o.D && J == o.J && K == o.K && dmax == o.dmax && dthr == o.dthr && band == o.band && gen == o.gen;
+    }
+};
+
 struct qcg_handle
 {
     int device = 0;
@@ -153,6 +168,17 @@ struct qcg_handle
     static constexpr int kSide = 6;
     cudaStream_t side[kSide] = {};
     cudaEvent_t fork = nullptr, join[kSide] = {};
+    // J/K builds replayed as CUDA graphs, keyed by their arguments and the screening generation
+    bool use_graphs = false;
+    int screen_gen = 0;
+    QcgGraphKey last_key{};
+    std::vector<std::pair<QcgGraphKey, cudaGraphExec_t>> graphs;
+    void drop_graphs()
+    {
+        for (auto& g : graphs) cudaGraphExecDestroy(g.second);
+        graphs.clear();
+        last_key = QcgGraphKey{};
+    }
 
     // Small buffers (pair lists, work offsets, basis arrays: a few hundred per handle) are carved out of
     // 8 MiB slabs, so that setting up and destroying a handle costs a handful of cudaMalloc/cudaFree
@@ -261,6 +287,7 @@ struct qcg_handle
     ~qcg_handle()
     {
         if (stream) cudaStreamSynchronize(stream);
+        drop_graphs();
         for (auto& a : allocs) cudaFree(a.p);
         for (auto& a : slabs) cudaFree(a.p);
         if (stage) cudaFreeHost(stage);
@@ -973,10 +1000,6 @@ void jk_device(qcg_handle* h, const double* dD, double* dJ, double* dK, int flag
         if (flag & 1) throw Error{QCG_ERR_NONFINITE, "density matrix has NaN/Inf entries"};
         if (flag & 2) throw Error{QCG_ERR_ASYMMETRIC, "density matrix is not symmetric"};
     }
-    CK(cudaEventRecord(h->ev0, h->stream));
-    CK(cudaMemsetAsync(h->d_Jp, 0, nn * sizeof(double), h->stream));
-    CK(cudaMemsetAsync(h->d_Kp, 0, nn * sizeof(double), h->stream));
-    CK(cudaEventRecord(h->ev1, h->stream));
     if (!h->fork)
     {
         CK(cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming));
@@ -986,46 +1009,99 @@ void jk_device(qcg_handle* h, const double* dD, double* dJ, double* dK, int flag
             CK(cudaEventCreateWithFlags(&h->join[s], cudaEventDisableTiming));
         }
     }
-    CK(cudaEventRecord(h->fork, h->stream));
-    for (int s = 0; s < qcg_handle::kSide; ++s) CK(cudaStreamWaitEvent(h->side[s], h->fork, 0));
-    // heaviest classes first so that the short ones fill the tail; classes spread over the side streams
-    int slot = 0;
-    for (int k = kNumQuartetClasses - 1; k >= 0; --k)
-    {
-        if (h->work[k].total <= 0) continue;
-        int X = 0;
-        while ((X + 1) * (X + 2) / 2 <= k) ++X;
-        const int Y = k - X * (X + 1) / 2;
-        JKWorkDev wk = h->work[k];
-        wk.dmax = dmax;
-        wk.nshell = h->nshell;
-        wk.dthr = dthr;
-        if (fp32_below < HUGE_VAL)
+    // the build: zero J'/K', class kernels over the side streams, symmetrisation (timing events only
+    // when the build is not a graph)
+    auto enqueue = [&](bool timed) {
+        CK(cudaMemsetAsync(h->d_Jp, 0, nn * sizeof(double), h->stream));
+        CK(cudaMemsetAsync(h->d_Kp, 0, nn * sizeof(double), h->stream));
+        if (timed) CK(cudaEventRecord(h->ev1, h->stream));
+        CK(cudaEventRecord(h->fork, h->stream));
+        for (int s = 0; s < qcg_handle::kSide; ++s) CK(cudaStreamWaitEvent(h->side[s], h->fork, 0));
+        // heaviest classes first so that the short ones fill the tail; classes spread over the side streams
+        int slot = 0;
+        for (int k = kNumQuartetClasses - 1; k >= 0; --k)
         {
-            wk.lo = fp32_below;
-            wk.hi = HUGE_VAL;
-            kJKLaunchers[k](wk, h->pl_dev[X], h->pl_dev[Y], h->pp_dev, h->d_f0, dD, h->d_Jp, h->d_Kp, n, h->d_boys,
-                            h->side[slot], h->nsm);
-            slot = (slot + 1) % qcg_handle::kSide;
+            if (h->work[k].total <= 0) continue;
+            int X = 0;
+            while ((X + 1) * (X + 2) / 2 <= k) ++X;
+            const int Y = k - X * (X + 1) / 2;
+            JKWorkDev wk = h->work[k];
+            wk.dmax = dmax;
+            wk.nshell = h->nshell;
+            wk.dthr = dthr;
+            if (fp32_below < HUGE_VAL)
+            {
+                wk.lo = fp32_below;
+                wk.hi = HUGE_VAL;
+                kJKLaunchers[k](wk, h->pl_dev[X], h->pl_dev[Y], h->pp_dev, h->d_f0, dD, h->d_Jp, h->d_Kp, n,
+                                h->d_boys, h->side[slot], h->nsm);
+                slot = (slot + 1) % qcg_handle::kSide;
+            }
+            if (fp32_below > 0)
+            {
+                wk.lo = 0.0;
+                wk.hi = fp32_below;
+                kJK32Launchers[k](wk, h->pl_dev[X], h->pl_dev[Y], h->pp_dev, h->d_f0, dD, h->d_Jp, h->d_Kp, n,
+                                  h->d_boys, h->side[slot], h->nsm);
+                slot = (slot + 1) % qcg_handle::kSide;
+            }
         }
-        if (fp32_below > 0)
+        CK(cudaGetLastError());
+        for (int s = 0; s < qcg_handle::kSide; ++s)
         {
-            wk.lo = 0.0;
-            wk.hi = fp32_below;
-            kJK32Launchers[k](wk, h->pl_dev[X], h->pl_dev[Y], h->pp_dev, h->d_f0, dD, h->d_Jp, h->d_Kp, n, h->d_boys,
-                              h->side[slot], h->nsm);
-            slot = (slot + 1) % qcg_handle::kSide;
+            CK(cudaEventRecord(h->join[s], h->side[s]));
+            CK(cudaStreamWaitEvent(h->stream, h->join[s], 0));
         }
-    }
-    CK(cudaGetLastError());
-    for (int s = 0; s < qcg_handle::kSide; ++s)
+        if (timed) CK(cudaEventRecord(h->ev2, h->stream));
+        launch_symmetrize(h->d_Jp, h->d_Kp, dJ, dK, (long long)nn, n, h->mols(), h->d_flag, h->stream, h->nsm);
+        CK(cudaGetLastError());
+    };
+    // With graphs enabled (qcg_set_graphs), a build whose arguments repeat (the SCF's builds into the
+    // handle's own buffers) is captured as a CUDA graph the second time it is seen and replayed from then on:
+    // one launch instead of ~25.  Off by default: the class kernels of even a 57-function build run ~0.5 ms,
+    // so replay saves little, and capture plus instantiation costs more than a 10-25 iteration SCF recovers.
+    const QcgGraphKey key{dD, dJ, dK, dmax, dthr, fp32_below, h->screen_gen};
+    cudaGraphExec_t exec = nullptr;
+    if ((flags & QCG_JK_SKIP_VALIDATION) && h->use_graphs && h->stream != nullptr)   // no capture on the legacy stream
     {
-        CK(cudaEventRecord(h->join[s], h->side[s]));
-        CK(cudaStreamWaitEvent(h->stream, h->join[s], 0));
+        for (auto& g : h->graphs)
+            if (g.first == key) exec = g.second;
+        if (!exec && h->last_key == key)
+        {
+            cudaGraph_t graph = nullptr;
+            CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+            try
+            {
+                enqueue(false);
+            }
+            catch (...)
+            {
+                cudaStreamEndCapture(h->stream, &graph);
+                if (graph) cudaGraphDestroy(graph);
+                throw;
+            }
+            CK(cudaStreamEndCapture(h->stream, &graph));
+            cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+            cudaGraphDestroy(graph);
+            if (e != cudaSuccess) throw Error{QCG_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e)};
+            if (h->graphs.size() >= 4)
+            {
+                cudaGraphExecDestroy(h->graphs.front().second);
+                h->graphs.erase(h->graphs.begin());
+            }
+            h->graphs.push_back({key, exec});
+        }
+        h->last_key = key;
     }
-    CK(cudaEventRecord(h->ev2, h->stream));
-    launch_symmetrize(h->d_Jp, h->d_Kp, dJ, dK, (long long)nn, n, h->mols(), h->d_flag, h->stream, h->nsm);
-    CK(cudaGetLastError());
+    CK(cudaEventRecord(h->ev0, h->stream));
+    if (exec)
+    {
+        CK(cudaGraphLaunch(exec, h->stream));
+        CK(cudaEventRecord(h->ev1, h->stream));   // no separate ERI interval inside a graph
+        CK(cudaEventRecord(h->ev2, h->stream));
+    }
+    else
+        enqueue(true);
     if (stats)
     {
         CK(cudaEventSynchronize(h->ev2));
@@ -1150,6 +1226,8 @@ int qcg_basis_create_batch(const int* shell_L, const int* shell_nprim, const dou
         CK(cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, h->device));
         CK(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
         h->stream = h->own_stream;
+        const char* ug = std::getenv("QCG_GRAPHS");   // 1: replay repeated J/K builds as CUDA graphs
+        h->use_graphs = ug && ug[0] == '1';
         h->d_boys = h->alloc<double>(121 * 23);
         CK(cudaMemcpyAsync(h->d_boys, kBoysTable, sizeof(kBoysTable), cudaMemcpyHostToDevice, h->stream));
         h->bs.nshell = nshell;
@@ -1358,6 +1436,8 @@ int qcg_schwarz(qcg_handle* h, double thresh, double* Q)
                 }
                 h->screened = false;
             }
+            h->drop_graphs();
+            ++h->screen_gen;
             build_screening(h, thresh);
         }
         if (Q) std::copy(h->Qfull.begin(), h->Qfull.end(), Q);
@@ -1371,6 +1451,14 @@ int qcg_fock_jk_device(qcg_handle* h, const double* d_D, double* d_J, double* d_
         require(d_D && d_J && d_K, "null argument");
         jk_device(h, d_D, d_J, d_K, flags, stats, nullptr, 0.0, (flags & QCG_JK_FP32) ? HUGE_VAL : h->fp32_below);
     });
+}
+
+int qcg_set_graphs(qcg_handle* h, int enable)
+{
+    if (!h) return QCG_ERR_ARG;
+    h->use_graphs = enable != 0;
+    if (!h->use_graphs) h->drop_graphs();
+    return QCG_OK;
 }
 
 int qcg_set_fp32_bound(qcg_handle* h, double bound)
