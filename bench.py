@@ -32,6 +32,7 @@ sys.path.insert(0, REPO)
 
 Q_PER_CLASS = 10_000_000
 CHUNK = 1_000_000
+E2E_CHUNK = 100_000      # quartets per host-buffer call in the e2e leg (1 GB of pinned output at (dd|dd))
 NPOOL = 32768
 METRIC = "ERI quartets/s (21 (s,p,d) classes, contraction 1-3, FP64 Cartesian)"
 UNIT = "quartets/s"
@@ -290,7 +291,7 @@ def main():
     # end to end through the host-buffer C ABI call (pinned host memory, copies inside the timed region)
     e2e = None
     if not args.no_e2e:
-        h_out = torch.empty(min(CHUNK, nq_cls) * max_blk, dtype=torch.float64).pin_memory()
+        h_out = torch.empty(min(E2E_CHUNK, nq_cls) * max_blk, dtype=torch.float64).pin_memory()
         eng_h = api.Engine(pool)
         lib = api.lib()
         import ctypes
@@ -298,8 +299,8 @@ def main():
         def e2e_step():
             h2d = d2h = 0
             for k, cls in enumerate(classes):
-                for c0 in range(0, nq_cls, CHUNK):
-                    m = min(CHUNK, nq_cls - c0)
+                for c0 in range(0, nq_cls, E2E_CHUNK):
+                    m = min(E2E_CHUNK, nq_cls - c0)
                     qptr = ctypes.cast(h_q[k].data_ptr() + 16 * c0, ctypes.POINTER(ctypes.c_int))
                     optr = ctypes.cast(h_out.data_ptr(), ctypes.POINTER(ctypes.c_double))
                     rc = lib.qcg_eri_batch(eng_h._h, *cls, m, qptr, optr)
@@ -403,53 +404,17 @@ def fp32_pass(torch, stream, eng, classes, d_q, prim_q, step, args):
 
 
 def run_secondary(args):
-    """Secondary workloads on one GPU: the config-3 Fock build or the config-1 RHF, each as a step."""
+    """Secondary workloads: the config-3 Fock build (any number of ranks), the RHF workloads (one GPU)."""
     import torch
     from qchem_b200 import api, basis as B, workloads as W
-    torch.cuda.set_device(0)
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     peak_tf, _ = api.measure_fp64_peak(20)
     if args.workload == "fock_config3":
-        mol = W.water_cluster()
-        sh = B.even_tempered(mol)
-        eng = api.Engine(sh)
-        eng.set_stream(stream.cuda_stream)
-        eng.schwarz(1e-10)
-        Dh = W.cluster_density(B.nbf(sh))
-        D = torch.tensor(Dh, device="cuda")
-        J, K = torch.empty_like(D), torch.empty_like(D)
-        for _ in range(args.warmup):
-            st = eng.fock_jk_device(D.data_ptr(), J.data_ptr(), K.data_ptr())
-        torch.cuda.synchronize()
-        clocks = ClockSampler(0)
-        clocks.start()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(args.steps):
-            st = eng.fock_jk_device(D.data_ptr(), J.data_ptr(), K.data_ptr())
-        e1.record(stream)
-        torch.cuda.synchronize()
-        clk = clocks.stop()
-        ms = e0.elapsed_time(e1) / args.steps
-        t0 = time.perf_counter()
-        for _ in range(args.steps):
-            eng.fock_jk(Dh)
-        e2e_s = (time.perf_counter() - t0) / args.steps
-        n = B.nbf(sh)
-        tf = st.flops / (ms * 1e-3) / 1e12
-        line = {"metric": "direct J/K Fock build, shell quartets/s (32-water cluster, N=1824)",
-                "value": st.quartets / (ms * 1e-3), "unit": "quartets/s", "n_gpus": 1, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": "fock_jk_water32_even_tempered", "nbf": n, "schwarz": 1e-10,
-                           "quartets": st.quartets, "prim_quartets": st.prim_quartets},
-                "gpu_launches": 24 * args.steps, "clocks": clk,
-                "roofline": {"bound": "fp64", "achieved": tf, "peak": peak_tf, "unit": "TFLOP/s", "frac": tf / peak_tf,
-                             "traffic": None, "kernel": "jk_kernel (all classes)",
-                             "peak_source": "measured here: library DFMA probe"},
-                "e2e": {"value": st.quartets / e2e_s, "unit": "quartets/s", "h2d_bytes_per_step": 8 * n * n,
-                        "d2h_bytes_per_step": 16 * n * n}}
+        line = run_fock3(args, torch, api, B, W, peak_tf, stream)
+        if line is None:
+            return
     elif args.workload == "rhf_learned":
         line = run_learned(args, api, B, W, peak_tf)
     elif args.workload == "rhf_batch":
@@ -497,6 +462,77 @@ def run_secondary(args):
                                                  "speedup_vs_plain": w8 / w8c}},
                 "e2e": {"value": wall, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def run_fock3(args, torch, api, B, W, peak_tf, stream):
+    """One direct J/K build of the 32-water cluster per step.  Under torchrun every rank evaluates its
+    1/world slice of the quartets (qcg_set_shard) and one NCCL all-reduce sums J and K (strong scaling);
+    the device time is the max over ranks.  e2e: the same from a pinned host density to pinned host J and
+    K."""
+    import datetime
+    import torch.distributed as dist
+    from qchem_b200.parallel import dist_env, max_over_ranks, sharded_fock_jk
+    rank, world, local = dist_env()
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    mol = W.water_cluster()
+    sh = B.even_tempered(mol)
+    eng = api.Engine(sh)
+    eng.set_stream(stream.cuda_stream)
+    eng.schwarz(1e-10)
+    n = B.nbf(sh)
+    Dh = torch.from_numpy(W.cluster_density(n)).pin_memory()
+    D = Dh.to(dev)
+    J, K = torch.empty_like(D), torch.empty_like(D)
+    Jh, Kh = torch.empty_like(Dh).pin_memory(), torch.empty_like(Dh).pin_memory()
+
+    def step():
+        return sharded_fock_jk(eng, D.data_ptr(), J.data_ptr(), K.data_ptr(), J, K, rank, world)
+
+    for _ in range(args.warmup):
+        st = step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        st = step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, dev)
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        D.copy_(Dh, non_blocking=True)
+        step()
+        Jh.copy_(J, non_blocking=True)
+        Kh.copy_(K, non_blocking=True)
+        torch.cuda.synchronize()
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / args.steps, dev)
+    tf = st.flops / (ms * 1e-3) / 1e12
+    line = {"metric": "direct J/K Fock build, shell quartets/s (32-water cluster, N=1824)",
+            "value": st.quartets / (ms * 1e-3), "unit": "quartets/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "fock_jk_water32_even_tempered", "nbf": n, "schwarz": 1e-10,
+                       "quartets": st.quartets, "prim_quartets": st.prim_quartets,
+                       "parallelism": f"quartet slices over {world} rank(s), NCCL all-reduce of J and K"},
+            "gpu_launches": 24 * args.steps, "clocks": clk,
+            "roofline": {"bound": "fp64", "achieved": tf, "peak": peak_tf * world, "unit": "TFLOP/s",
+                         "frac": tf / (peak_tf * world), "traffic": None, "kernel": "jk_kernel (all classes)",
+                         "peak_source": "measured here: library DFMA probe (x ranks)"},
+            "e2e": {"value": st.quartets / e2e_s, "unit": "quartets/s", "h2d_bytes_per_step": 8 * n * n,
+                    "d2h_bytes_per_step": 16 * n * n}}
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return line if rank == 0 else None
 
 
 def run_batch(args, api, B, W):

@@ -154,6 +154,12 @@ int qcg_set_fp32_bound(qcg_handle* h, double bound);
  * Also switched on by the environment variable QCG_GRAPHS=1.  The handle's stream must not be the legacy
  * default stream for capture to happen. */
 int qcg_set_graphs(qcg_handle* h, int enable);
+/* Several GPUs on one J/K build: with (rank, world) set, later qcg_fock_jk* calls evaluate only this rank's
+ * contiguous slice (1/world of the screened quartets of every class) and return the rank's PARTIAL J and K;
+ * the sum over ranks (one all-reduce) is the full J and K.  (0, 1), the default, is the whole build.  The
+ * qcg_stats figures still describe the whole build.  No reference counterpart (the reference is one
+ * process). */
+int qcg_set_shard(qcg_handle* h, int rank, int world);
 
 /* The J/K build of qcg_fock_jk_device for callers that must not allocate device memory once their setup
  * is done -- for example a host program whose device memory is owned by its own pool allocator, or one

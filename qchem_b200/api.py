@@ -40,7 +40,7 @@ EXPORTS = ["qcg_basis_create", "qcg_destroy", "qcg_last_error", "qcg_set_stream"
            "qcg_measure_fp32_peak", "qcg_mlp_create", "qcg_mlp_destroy", "qcg_mlp_last_error", "qcg_mlp_set_stream",
            "qcg_mlp_nparams", "qcg_mlp_params", "qcg_mlp_set_params", "qcg_mlp_forward", "qcg_mlp_loss_grad",
            "qcg_mlp_adam", "qcg_basis_create_batch", "qcg_nmol", "qcg_mol_nbf", "qcg_one_electron_batch",
-           "qcg_rhf_batch", "qcg_set_graphs"]
+           "qcg_rhf_batch", "qcg_set_graphs", "qcg_set_shard"]
 
 
 class QcgError(RuntimeError):
@@ -105,6 +105,7 @@ def lib():
     L.qcg_eri_batch_device_f32.argtypes = [vp, i32, i32, i32, i32, i64, vp, vp]
     L.qcg_set_fp32_bound.argtypes = [vp, f64]
     L.qcg_set_graphs.argtypes = [vp, i32]
+    L.qcg_set_shard.argtypes = [vp, i32, i32]
     L.qcg_schwarz.argtypes = [vp, f64, P(f64)]
     L.qcg_fock_jk.argtypes = [vp, P(f64), P(f64), P(f64), i32, P(Stats)]
     L.qcg_fock_jk_device.argtypes = [vp, vp, vp, vp, i32, P(Stats)]
@@ -235,6 +236,11 @@ class Engine:
         la, lb, lc, ld = cls
         f = lib().qcg_eri_batch_device_f32 if fp32 else lib().qcg_eri_batch_device
         self._check(f(self._h, la, lb, lc, ld, int(nq), ctypes.c_void_p(d_quartets_ptr), ctypes.c_void_p(d_out_ptr)))
+
+    def set_shard(self, rank: int, world: int):
+        """Later J/K builds evaluate this rank's 1/world slice of the quartets and return partial J and K
+        (summed over ranks they are the full build)."""
+        self._check(lib().qcg_set_shard(self._h, int(rank), int(world)))
 
     def set_graphs(self, enable: bool):
         """Replay repeated J/K builds as CUDA graphs (off by default)."""

@@ -114,13 +114,14 @@ void QCG_NAME(launch_jk)(const JKWorkDev& w, const PairListDev& bra, const PairL
                          const int* f0, const double* D, double* J, double* K, int n, const double* boys,
                          cudaStream_t st, int nsm)
 {
-    if (w.total <= 0) return;
+    const long long span = w.gend - w.gbeg;
+    if (span <= 0) return;
     auto k = jk_kernel<Cls, kThreads, Real>;
     prepare(k);
     // quartets per lane run: enough threads for the whole GPU first, longer runs only for large builds
-    long long run = w.total / ((long long)nsm * 1024);
+    long long run = span / ((long long)nsm * 1024);
     run = run < 1 ? 1 : (run > 8 ? 8 : run);
-    const long long work = (w.total + run - 1) / run;
+    const long long work = (span + run - 1) / run;
     k<<<(unsigned)grid_for(work, nsm), kThreads, kSmem, st>>>(w, bra, ket, P, f0, D, J, K, n, boys, (int)run);
 }
 

@@ -303,10 +303,10 @@ __global__ void __launch_bounds__(THREADS) jk_kernel(JKWorkDev w, PairListDev br
     const int lane = threadIdx.x & 31;
     const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     const long long nwarp = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long base = warp * 32 * RUN; base < w.total; base += nwarp * 32 * RUN)
+    for (long long base = w.gbeg + warp * 32 * RUN; base < w.gend; base += nwarp * 32 * RUN)
     {
         long long g = base + lane;
-        if (g >= w.total) continue;
+        if (g >= w.gend) continue;
         // bra pair i: offs[i] <= g < offs[i+1]
         int lo = 0, hi = bra.n;
         while (hi - lo > 1)
@@ -334,7 +334,7 @@ __global__ void __launch_bounds__(THREADS) jk_kernel(JKWorkDev w, PairListDev br
         int sa = bra.sa[i], sb = bra.sb[i];
         bind(i);
         sink.set_bra(shell_f0[sa], shell_f0[sb]);
-        for (int r = 0; r < RUN && g < w.total; ++r, g += 32)
+        for (int r = 0; r < RUN && g < w.gend; ++r, g += 32)
         {
             if (g >= next)
             {

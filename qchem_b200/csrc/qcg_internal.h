@@ -56,6 +56,9 @@ struct MolLayoutDev
 struct JKWorkDev
 {
     long long total;
+    // the slice [gbeg, gend) of the class's quartets this build evaluates (a rank's shard; 0 and total
+    // for the whole build)
+    long long gbeg, gend;
     const long long* offs;
     int same_class;
     // density screening of an incremental build: skip a quartet when

@@ -149,6 +149,7 @@ struct qcg_handle
     PrimPairsDev pp_dev{};
     JKWorkDev work[kNumQuartetClasses]{};
     double fp32_below = 0;   // qcg_set_fp32_bound: quartets with a smaller bound are evaluated in FP32
+    int shard_rank = 0, shard_world = 1;   // qcg_set_shard: this handle's slice of every J/K build
     double* d_dmaxD = nullptr;   // per shell-pair max |D| of a full build's density (mixed precision)
     long long work_quartets = 0, work_prim_quartets = 0;
     double work_flops = 0;
@@ -949,6 +950,8 @@ void build_screening(qcg_handle* h, double thresh)
                 pq += (long long)h->pl_npp[X][i] * (nppy[jb + cnt] - nppy[jb]);
             }
             h->work[k].total = offs.back();
+            h->work[k].gbeg = 0;
+            h->work[k].gend = offs.back();
             h->work[k].offs = h->upload(offs);
             h->work[k].kbase = h->nmol > 1 ? h->upload(kbase) : nullptr;
             h->work[k].mols = h->mols();
@@ -1026,6 +1029,10 @@ void jk_device(qcg_handle* h, const double* dD, double* dJ, double* dK, int flag
             while ((X + 1) * (X + 2) / 2 <= k) ++X;
             const int Y = k - X * (X + 1) / 2;
             JKWorkDev wk = h->work[k];
+            // this rank's contiguous slice of the class's quartets
+            wk.gbeg = wk.total * h->shard_rank / h->shard_world;
+            wk.gend = wk.total * (h->shard_rank + 1) / h->shard_world;
+            if (wk.gend <= wk.gbeg) continue;
             wk.dmax = dmax;
             wk.nshell = h->nshell;
             wk.dthr = dthr;
@@ -1450,6 +1457,17 @@ int qcg_fock_jk_device(qcg_handle* h, const double* d_D, double* d_J, double* d_
     return guarded(h, [&] {
         require(d_D && d_J && d_K, "null argument");
         jk_device(h, d_D, d_J, d_K, flags, stats, nullptr, 0.0, (flags & QCG_JK_FP32) ? HUGE_VAL : h->fp32_below);
+    });
+}
+
+int qcg_set_shard(qcg_handle* h, int rank, int world)
+{
+    if (!h) return QCG_ERR_ARG;
+    return guarded(h, [&] {
+        require(world >= 1 && rank >= 0 && rank < world, "need 0 <= rank < world");
+        h->shard_rank = rank;
+        h->shard_world = world;
+        h->drop_graphs();
     });
 }
 

@@ -3,7 +3,9 @@
 The ERI microbenchmark and the batched-molecule workload shard into independent units (quartets,
 molecules) with no data-path exchange: every rank evaluates its own units (weak scaling: a fixed amount
 per rank), and the only collective is the max-over-ranks of the timed region.  A direct J/K build of ONE
-molecule shards its quartet list and needs one sum-reduction of J and K; reduce_jk does that with NCCL.
+molecule shards its quartet list (the library's qcg_set_shard: each rank evaluates a contiguous 1/world
+slice of every class's screened quartets) and needs one sum-reduction of J and K; sharded_fock_jk does
+both, reduce_jk the NCCL all-reduce.
 """
 from __future__ import annotations
 
@@ -58,3 +60,17 @@ def reduce_jk(J, K):
         dist.all_reduce(J)
         dist.all_reduce(K)
     return J, K
+
+
+def sharded_fock_jk(engine, dD: int, dJ: int, dK: int, J, K, rank: int = None, world: int = None):
+    """One J/K build split over the ranks of the process group: this rank's slice into the device buffers
+    dJ/dK (the data pointers of the torch tensors J and K), then the sum over ranks in place.  rank/world
+    default to the process group's."""
+    import torch.distributed as dist
+    if rank is None or world is None:
+        on = dist.is_available() and dist.is_initialized()
+        rank, world = (dist.get_rank(), dist.get_world_size()) if on else (0, 1)
+    engine.set_shard(rank, world)
+    st = engine.fock_jk_device(dD, dJ, dK)
+    reduce_jk(J, K)
+    return st
