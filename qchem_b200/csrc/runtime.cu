@@ -160,6 +160,13 @@ struct qcg_handle
     unsigned char* d_key = nullptr;
     int *d_order = nullptr, *d_hist = nullptr, *d_cursor = nullptr;
 
+    // host-buffer ERI batches: two quartet/output buffer pairs (grow only) and a copy-out stream
+    void* hb_q[2] = {nullptr, nullptr};
+    void* hb_out[2] = {nullptr, nullptr};
+    size_t hb_qcap[2] = {0, 0}, hb_ocap[2] = {0, 0};
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t hb_done[2] = {nullptr, nullptr}, hb_free[2] = {nullptr, nullptr};
+
     // J/K buffers
     double *d_D = nullptr, *d_Jp = nullptr, *d_Kp = nullptr, *d_J = nullptr, *d_K = nullptr;
     int* d_flag = nullptr;
@@ -288,6 +295,7 @@ struct qcg_handle
     ~qcg_handle()
     {
         if (stream) cudaStreamSynchronize(stream);
+        if (copy_stream) cudaStreamSynchronize(copy_stream);
         drop_graphs();
         for (auto& a : allocs) cudaFree(a.p);
         for (auto& a : slabs) cudaFree(a.p);
@@ -296,6 +304,12 @@ struct qcg_handle
         if (ev1) cudaEventDestroy(ev1);
         if (ev2) cudaEventDestroy(ev2);
         if (fork) cudaEventDestroy(fork);
+        for (int k = 0; k < 2; ++k)
+        {
+            if (hb_done[k]) cudaEventDestroy(hb_done[k]);
+            if (hb_free[k]) cudaEventDestroy(hb_free[k]);
+        }
+        if (copy_stream) cudaStreamDestroy(copy_stream);
         for (int k = 0; k < kSide; ++k)
         {
             if (join[k]) cudaEventDestroy(join[k]);
@@ -1367,29 +1381,52 @@ int eri_batch_host(qcg_handle* h, int la, int lb, int lc, int ld, long long nq, 
                 require(h->L[s] == Ls[x], "shell angular momentum does not match the class");
             }
         const long long blk = (long long)ncart(la) * ncart(lb) * ncart(lc) * ncart(ld);
-        // bounded device footprint: chunks of at most 1 GiB of output
-        const long long chunk = std::max<long long>(1, std::min<long long>(nq, (1LL << 30) / sizeof(T) / blk));
-        int* dq = h->alloc<int>(4 * chunk);
-        T* dout = h->alloc<T>(chunk * blk);
-        try
+        // two device buffers of at most 512 MiB of output each, kept by the handle between calls: the
+        // copy of one chunk back to the host overlaps the evaluation of the next
+        const long long chunk =
+            std::max<long long>(1, std::min<long long>(nq, (1LL << 29) / (long long)sizeof(T) / blk));
+        const size_t qbytes = (size_t)4 * chunk * sizeof(int), obytes = (size_t)chunk * blk * sizeof(T);
+        if (!h->copy_stream)
         {
-            for (long long q0 = 0; q0 < nq; q0 += chunk)
+            CK(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+            for (int b = 0; b < 2; ++b)
             {
-                const long long m = std::min(chunk, nq - q0);
-                CK(cudaMemcpyAsync(dq, quartets + 4 * q0, 4 * m * sizeof(int), cudaMemcpyHostToDevice, h->stream));
-                eri_batch_launch(h, k, dq, m, dout);
-                CK(cudaMemcpyAsync(out + q0 * blk, dout, m * blk * sizeof(T), cudaMemcpyDeviceToHost, h->stream));
+                CK(cudaEventCreateWithFlags(&h->hb_done[b], cudaEventDisableTiming));
+                CK(cudaEventCreateWithFlags(&h->hb_free[b], cudaEventDisableTiming));
             }
-            CK(cudaStreamSynchronize(h->stream));
         }
-        catch (...)
+        for (int b = 0; b < 2; ++b)
         {
-            h->release(dq);
-            h->release(dout);
-            throw;
+            if (h->hb_qcap[b] < qbytes)
+            {
+                if (h->hb_q[b]) h->release(h->hb_q[b]);
+                h->hb_q[b] = h->alloc<char>(qbytes);
+                h->hb_qcap[b] = qbytes;
+            }
+            if (h->hb_ocap[b] < obytes)
+            {
+                if (h->hb_out[b]) h->release(h->hb_out[b]);
+                h->hb_out[b] = h->alloc<char>(obytes);
+                h->hb_ocap[b] = obytes;
+            }
+            CK(cudaEventRecord(h->hb_free[b], h->copy_stream));   // both buffers start free
         }
-        h->release(dq);
-        h->release(dout);
+        int b = 0;
+        for (long long q0 = 0; q0 < nq; q0 += chunk, b ^= 1)
+        {
+            const long long m = std::min(chunk, nq - q0);
+            int* dq = (int*)h->hb_q[b];
+            T* dout = (T*)h->hb_out[b];
+            CK(cudaStreamWaitEvent(h->stream, h->hb_free[b], 0));   // the buffer's previous copy-out is done
+            CK(cudaMemcpyAsync(dq, quartets + 4 * q0, 4 * m * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+            eri_batch_launch(h, k, dq, m, dout);
+            CK(cudaEventRecord(h->hb_done[b], h->stream));
+            CK(cudaStreamWaitEvent(h->copy_stream, h->hb_done[b], 0));
+            CK(cudaMemcpyAsync(out + q0 * blk, dout, m * blk * sizeof(T), cudaMemcpyDeviceToHost, h->copy_stream));
+            CK(cudaEventRecord(h->hb_free[b], h->copy_stream));
+        }
+        CK(cudaStreamSynchronize(h->copy_stream));
+        CK(cudaStreamSynchronize(h->stream));
     });
 }
 }   // namespace
