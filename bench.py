@@ -549,17 +549,20 @@ def run_batch(args, api, B, W):
     mols = W.random_molecules(args.nmol)
     shells = [B.even_tempered(m) for m in mols]
     be = api.BatchEngine(shells[:min(4, len(mols))])
-    be.rhf(mols[:min(4, len(mols))], max_iter=3)   # warm-up (module load, first launches)
+    be.rhf(mols[:min(4, len(mols))], max_iter=3, diis_fdmax=1e6)   # warm-up (module load, first launches)
     del be
     clocks = ClockSampler(0)
     clocks.start()
     t0 = time.perf_counter()
-    res = api.BatchEngine(shells).rhf(mols)
+    # DIIS from the first iteration (the reference's gate ||[F,D]|| <= Z^2 0.1/32 never opens for most of
+    # these molecules: plain Roothaan steps oscillate; with the gate open 18 of the first 32 converge
+    # instead of 3).  The same setting on both sides of the comparison.
+    res = api.BatchEngine(shells).rhf(mols, diis_fdmax=1e6)
     wall = time.perf_counter() - t0
     clk = clocks.stop()
     nsub = min(16, len(mols))
     t0 = time.perf_counter()
-    single = [api.Engine(s).rhf(m) for m, s in zip(mols[:nsub], shells[:nsub])]
+    single = [api.Engine(s).rhf(m, diis_fdmax=1e6) for m, s in zip(mols[:nsub], shells[:nsub])]
     wall_single = (time.perf_counter() - t0) * len(mols) / nsub
     dE = [abs(r["energy"] - q["energy"]) for r, q in zip(res[:nsub], single) if r["converged"] and q["converged"]]
     nbf = [B.nbf(s) for s in shells]
@@ -572,7 +575,8 @@ def run_batch(args, api, B, W):
             "config": {"workload": "rhf_batch_random_molecules", "molecules": len(mols), "nbf_mean": float(np.mean(nbf)),
                        "nbf_max": int(max(nbf)), "converged": int(conv),
                        "iterations_max": int(max(r["iterations"] for r in res)),
-                       "jk_builds": res[0]["builds"], "fock_ms_total": res[0]["fock_ms"]},
+                       "jk_builds": res[0]["builds"], "fock_ms_total": res[0]["fock_ms"],
+                       "diis": "from the first iteration (diis_fdmax = 1e6), nproj 4"},
             "one_handle_per_molecule_s_extrapolated": wall_single, "speedup_vs_one_handle_per_molecule":
                 wall_single / wall,
             "max_abs_dE_vs_single_eh": max(dE) if dE else None, "compared": len(dE), "clocks": clk,

@@ -289,7 +289,7 @@ class Engine:
 
     def rhf(self, mol: _basis.Molecule, max_iter=100, de_tol=1e-10, fd_tol=1e-5, schwarz_thresh=1e-10,
             want_density=False, incremental=False, inc_thresh=1e-11, rebuild_every=8, fp32_early=False,
-            fp32_switch=1e-5, fp32_scale=0.0, fp32_below=0.0, guess=None):
+            fp32_switch=1e-5, fp32_scale=0.0, fp32_below=0.0, guess=None, diis_nproj=4, diis_fdmax=0.0):
         """RHF to convergence.  incremental=True: density-difference J/K builds with density-weighted
         screening between full builds (the energy on exit is always from a full build).  fp32_early=True:
         until the DIIS error drops below fp32_switch, quartets whose density-weighted bound is below
@@ -302,6 +302,7 @@ class Engine:
         prm.incremental, prm.inc_thresh, prm.rebuild_every = int(incremental), float(inc_thresh), int(rebuild_every)
         prm.fp32_early, prm.fp32_switch, prm.fp32_below = int(fp32_early), float(fp32_switch), float(fp32_below)
         prm.fp32_scale = float(fp32_scale)
+        prm.diis_nproj, prm.diis_fdmax = int(diis_nproj), float(diis_fdmax)
         if guess is not None:
             guess = _f64(guess)
             if guess.shape != (self.nbf, self.nbf):
@@ -373,10 +374,11 @@ class BatchEngine(Engine):
         self._screen = thresh
 
     def rhf(self, mols: Sequence[_basis.Molecule], max_iter=100, de_tol=1e-10, fd_tol=1e-5, schwarz_thresh=1e-10,
-            want_density=False):
+            want_density=False, diis_nproj=4, diis_fdmax=0.0):
         prm = ScfParams()
         lib().qcg_scf_default_params(ctypes.byref(prm))
         prm.max_iter, prm.de_tol, prm.fd_tol, prm.schwarz_thresh = max_iter, de_tol, fd_tol, schwarz_thresh
+        prm.diis_nproj, prm.diis_fdmax = int(diis_nproj), float(diis_fdmax)
         nat = np.array([len(m.Z) for m in mols], dtype=np.int32)
         Z = _f64(np.concatenate([np.asarray(m.Z, dtype=float) for m in mols]))
         R = _f64(np.concatenate([np.asarray(m.R, dtype=float).reshape(-1) for m in mols]))
