@@ -229,5 +229,6 @@ def evaluate(model: Optional[LearnedGuess], mols: Sequence[_basis.Molecule], ref
         if e_ref is not None:
             dE.append(abs(r["energy"] - e_ref))
     return {"guess": guess, "iterations_mean": float(np.mean(its)), "iterations": [int(i) for i in its],
-            "wall_s_mean": float(np.mean(walls)), "wall_s": walls, "energies": energies, "converged": conv,
+            "wall_s_mean": float(np.mean(walls)), "wall_s_median": float(np.median(walls)), "wall_s": walls,
+            "energies": energies, "converged": conv,
             "max_abs_dE": float(np.max(dE)) if dE else None, "all_converged": bool(all(conv))}
