@@ -80,6 +80,7 @@ typedef struct qcg_scf_params {
                                  element (nbf^2 quartets of relative error 3e-7) at 1e-4 of the DIIS error */
     double fp32_below;        /* after the switch, quartets whose bound is below this stay FP32; default 0 */
     const double* D_guess;    /* optional initial total density, nbf*nbf (NULL: core-Hamiltonian guess) */
+    int autotune;             /* 1: qcg_autotune_jk on the first density before the first build; default 0 */
 } qcg_scf_params;
 
 typedef struct qcg_scf_result {
@@ -160,6 +161,12 @@ int qcg_set_graphs(qcg_handle* h, int enable);
  * qcg_stats figures still describe the whole build.  No reference counterpart (the reference is one
  * process). */
 int qcg_set_shard(qcg_handle* h, int rank, int world);
+/* Autotuner of the J/K launch shapes.  For every quartet class it times the class kernel on up to 2^20 of
+ * the handle's screened quartets (density d_D, `reps` timed launches per candidate) for each candidate
+ * (quartets per lane 1, 2, 4, 8, 16) x (blocks per SM 8, 16) and keeps the fastest for later builds of this
+ * handle, until the screening changes.  run_out / cap_out (optional, 21 ints each) receive the choices.
+ * No reference counterpart. */
+int qcg_autotune_jk(qcg_handle* h, const double* d_D, int reps, int* run_out, int* cap_out);
 
 /* The J/K build of qcg_fock_jk_device for callers that must not allocate device memory once their setup
  * is done -- for example a host program whose device memory is owned by its own pool allocator, or one

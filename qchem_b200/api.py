@@ -40,7 +40,7 @@ EXPORTS = ["qcg_basis_create", "qcg_destroy", "qcg_last_error", "qcg_set_stream"
            "qcg_measure_fp32_peak", "qcg_mlp_create", "qcg_mlp_destroy", "qcg_mlp_last_error", "qcg_mlp_set_stream",
            "qcg_mlp_nparams", "qcg_mlp_params", "qcg_mlp_set_params", "qcg_mlp_forward", "qcg_mlp_loss_grad",
            "qcg_mlp_adam", "qcg_basis_create_batch", "qcg_nmol", "qcg_mol_nbf", "qcg_one_electron_batch",
-           "qcg_rhf_batch", "qcg_set_graphs", "qcg_set_shard"]
+           "qcg_rhf_batch", "qcg_set_graphs", "qcg_set_shard", "qcg_autotune_jk"]
 
 
 class QcgError(RuntimeError):
@@ -60,7 +60,7 @@ class ScfParams(ctypes.Structure):
                 ("diis_svtol", ctypes.c_double), ("incremental", ctypes.c_int), ("inc_thresh", ctypes.c_double),
                 ("rebuild_every", ctypes.c_int), ("fp32_early", ctypes.c_int), ("fp32_switch", ctypes.c_double),
                 ("fp32_scale", ctypes.c_double), ("fp32_below", ctypes.c_double),
-                ("D_guess", ctypes.POINTER(ctypes.c_double))]
+                ("D_guess", ctypes.POINTER(ctypes.c_double)), ("autotune", ctypes.c_int)]
 
 
 class ScfResult(ctypes.Structure):
@@ -106,6 +106,7 @@ def lib():
     L.qcg_set_fp32_bound.argtypes = [vp, f64]
     L.qcg_set_graphs.argtypes = [vp, i32]
     L.qcg_set_shard.argtypes = [vp, i32, i32]
+    L.qcg_autotune_jk.argtypes = [vp, vp, i32, P(i32), P(i32)]
     L.qcg_schwarz.argtypes = [vp, f64, P(f64)]
     L.qcg_fock_jk.argtypes = [vp, P(f64), P(f64), P(f64), i32, P(Stats)]
     L.qcg_fock_jk_device.argtypes = [vp, vp, vp, vp, i32, P(Stats)]
@@ -242,6 +243,16 @@ class Engine:
         (summed over ranks they are the full build)."""
         self._check(lib().qcg_set_shard(self._h, int(rank), int(world)))
 
+    def autotune_jk(self, d_D: int, reps: int = 1):
+        """Tune the J/K launch shape of every class on the density at device pointer d_D; returns the chosen
+        (quartets per lane, blocks per SM) per class (0 for classes with no quartets)."""
+        if self._screen is None:
+            self.schwarz()
+        run, cap = np.zeros(21, dtype=np.int32), np.zeros(21, dtype=np.int32)
+        self._check(lib().qcg_autotune_jk(self._h, ctypes.c_void_p(d_D), int(reps), _p(run, ctypes.c_int),
+                                          _p(cap, ctypes.c_int)))
+        return list(zip(run.tolist(), cap.tolist()))
+
     def set_graphs(self, enable: bool):
         """Replay repeated J/K builds as CUDA graphs (off by default)."""
         self._check(lib().qcg_set_graphs(self._h, int(bool(enable))))
@@ -289,7 +300,8 @@ class Engine:
 
     def rhf(self, mol: _basis.Molecule, max_iter=100, de_tol=1e-10, fd_tol=1e-5, schwarz_thresh=1e-10,
             want_density=False, incremental=False, inc_thresh=1e-11, rebuild_every=8, fp32_early=False,
-            fp32_switch=1e-5, fp32_scale=0.0, fp32_below=0.0, guess=None, diis_nproj=4, diis_fdmax=0.0):
+            fp32_switch=1e-5, fp32_scale=0.0, fp32_below=0.0, guess=None, diis_nproj=4, diis_fdmax=0.0,
+            autotune=False):
         """RHF to convergence.  incremental=True: density-difference J/K builds with density-weighted
         screening between full builds (the energy on exit is always from a full build).  fp32_early=True:
         until the DIIS error drops below fp32_switch, quartets whose density-weighted bound is below
@@ -303,6 +315,7 @@ class Engine:
         prm.fp32_early, prm.fp32_switch, prm.fp32_below = int(fp32_early), float(fp32_switch), float(fp32_below)
         prm.fp32_scale = float(fp32_scale)
         prm.diis_nproj, prm.diis_fdmax = int(diis_nproj), float(diis_fdmax)
+        prm.autotune = int(bool(autotune))
         if guess is not None:
             guess = _f64(guess)
             if guess.shape != (self.nbf, self.nbf):
@@ -374,11 +387,12 @@ class BatchEngine(Engine):
         self._screen = thresh
 
     def rhf(self, mols: Sequence[_basis.Molecule], max_iter=100, de_tol=1e-10, fd_tol=1e-5, schwarz_thresh=1e-10,
-            want_density=False, diis_nproj=4, diis_fdmax=0.0):
+            want_density=False, diis_nproj=4, diis_fdmax=0.0, autotune=False):
         prm = ScfParams()
         lib().qcg_scf_default_params(ctypes.byref(prm))
         prm.max_iter, prm.de_tol, prm.fd_tol, prm.schwarz_thresh = max_iter, de_tol, fd_tol, schwarz_thresh
         prm.diis_nproj, prm.diis_fdmax = int(diis_nproj), float(diis_fdmax)
+        prm.autotune = int(bool(autotune))
         nat = np.array([len(m.Z) for m in mols], dtype=np.int32)
         Z = _f64(np.concatenate([np.asarray(m.Z, dtype=float) for m in mols]))
         R = _f64(np.concatenate([np.asarray(m.R, dtype=float).reshape(-1) for m in mols]))

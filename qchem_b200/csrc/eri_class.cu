@@ -119,10 +119,18 @@ void QCG_NAME(launch_jk)(const JKWorkDev& w, const PairListDev& bra, const PairL
     auto k = jk_kernel<Cls, kThreads, Real>;
     prepare(k);
     // quartets per lane run: enough threads for the whole GPU first, longer runs only for large builds
+    // (unless the autotuner chose the run and the grid cap)
     long long run = span / ((long long)nsm * 1024);
     run = run < 1 ? 1 : (run > 8 ? 8 : run);
+    if (w.run > 0) run = w.run;
     const long long work = (span + run - 1) / run;
-    k<<<(unsigned)grid_for(work, nsm), kThreads, kSmem, st>>>(w, bra, ket, P, f0, D, J, K, n, boys, (int)run);
+    long long blocks = grid_for(work, nsm);
+    if (w.cap > 0)
+    {
+        blocks = (work + kThreads - 1) / kThreads;
+        if (blocks > (long long)nsm * w.cap) blocks = (long long)nsm * w.cap;
+    }
+    k<<<(unsigned)blocks, kThreads, kSmem, st>>>(w, bra, ket, P, f0, D, J, K, n, boys, (int)run);
 }
 
 #if QCG_PREC == 64

@@ -73,6 +73,9 @@ struct JKWorkDev
     // class); D, J', K' of a quartet are the packed blocks of its molecule
     const int* kbase;
     MolLayoutDev mols;
+    // launch shape: quartets per lane and blocks-per-SM cap (0: the launcher's own choice; set by the
+    // autotuner, qcg_autotune_jk)
+    int run, cap;
 };
 
 void launch_block_max(const double* D, const int* shell_f0, const int* shell_L, int nshell, int n, double* dmax,

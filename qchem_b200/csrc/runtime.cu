@@ -150,6 +150,7 @@ struct qcg_handle
     JKWorkDev work[kNumQuartetClasses]{};
     double fp32_below = 0;   // qcg_set_fp32_bound: quartets with a smaller bound are evaluated in FP32
     int shard_rank = 0, shard_world = 1;   // qcg_set_shard: this handle's slice of every J/K build
+    int tuned_run[kNumQuartetClasses] = {}, tuned_cap[kNumQuartetClasses] = {};   // qcg_autotune_jk (0: default)
     double* d_dmaxD = nullptr;   // per shell-pair max |D| of a full build's density (mixed precision)
     long long work_quartets = 0, work_prim_quartets = 0;
     double work_flops = 0;
@@ -966,6 +967,8 @@ void build_screening(qcg_handle* h, double thresh)
             h->work[k].total = offs.back();
             h->work[k].gbeg = 0;
             h->work[k].gend = offs.back();
+            h->work[k].run = 0;
+            h->work[k].cap = 0;
             h->work[k].offs = h->upload(offs);
             h->work[k].kbase = h->nmol > 1 ? h->upload(kbase) : nullptr;
             h->work[k].mols = h->mols();
@@ -1043,6 +1046,8 @@ void jk_device(qcg_handle* h, const double* dD, double* dJ, double* dK, int flag
             while ((X + 1) * (X + 2) / 2 <= k) ++X;
             const int Y = k - X * (X + 1) / 2;
             JKWorkDev wk = h->work[k];
+            wk.run = h->tuned_run[k];
+            wk.cap = h->tuned_cap[k];
             // this rank's contiguous slice of the class's quartets
             wk.gbeg = wk.total * h->shard_rank / h->shard_world;
             wk.gend = wk.total * (h->shard_rank + 1) / h->shard_world;
@@ -1483,6 +1488,7 @@ int qcg_schwarz(qcg_handle* h, double thresh, double* Q)
             h->drop_graphs();
             ++h->screen_gen;
             build_screening(h, thresh);
+            for (int k = 0; k < kNumQuartetClasses; ++k) h->tuned_run[k] = h->tuned_cap[k] = 0;   // new lists
         }
         if (Q) std::copy(h->Qfull.begin(), h->Qfull.end(), Q);
     });
@@ -1494,6 +1500,72 @@ int qcg_fock_jk_device(qcg_handle* h, const double* d_D, double* d_J, double* d_
     return guarded(h, [&] {
         require(d_D && d_J && d_K, "null argument");
         jk_device(h, d_D, d_J, d_K, flags, stats, nullptr, 0.0, (flags & QCG_JK_FP32) ? HUGE_VAL : h->fp32_below);
+    });
+}
+
+// Autotuner of the J/K launch shapes: per class, time the class kernel on (a slice of at most 2^20 of)
+// its quartets with each candidate (quartets per lane x blocks-per-SM cap) and keep the fastest for later
+// builds.  The timed launches accumulate into the handle's J'/K' scratch, which every build zeroes.
+int qcg_autotune_jk(qcg_handle* h, const double* d_D, int reps, int* run_out, int* cap_out)
+{
+    if (!h) return QCG_ERR_ARG;
+    return guarded(h, [&] {
+        require(h->screened, "qcg_schwarz must be called before qcg_autotune_jk", QCG_ERR_STATE);
+        require(d_D && reps >= 1, "bad argument");
+        ensure_jk_buffers(h);
+        h->drop_graphs();
+        cudaEvent_t a = nullptr, b = nullptr;
+        CK(cudaEventCreate(&a));
+        CK(cudaEventCreate(&b));
+        const int runs[] = {1, 2, 4, 8, 16}, caps[] = {8, 16};
+        try
+        {
+            for (int k = 0; k < kNumQuartetClasses; ++k)
+            {
+                h->tuned_run[k] = h->tuned_cap[k] = 0;
+                if (h->work[k].total <= 0) continue;
+                int X = 0;
+                while ((X + 1) * (X + 2) / 2 <= k) ++X;
+                const int Y = k - X * (X + 1) / 2;
+                JKWorkDev wk = h->work[k];
+                wk.gbeg = 0;
+                wk.gend = std::min<long long>(wk.total, 1LL << 20);
+                float best = 1e30f;
+                for (int r : runs)
+                    for (int c : caps)
+                    {
+                        wk.run = r;
+                        wk.cap = c;
+                        kJKLaunchers[k](wk, h->pl_dev[X], h->pl_dev[Y], h->pp_dev, h->d_f0, d_D, h->d_Jp, h->d_Kp,
+                                        h->nbf, h->d_boys, h->stream, h->nsm);   // warm-up
+                        CK(cudaEventRecord(a, h->stream));
+                        for (int i = 0; i < reps; ++i)
+                            kJKLaunchers[k](wk, h->pl_dev[X], h->pl_dev[Y], h->pp_dev, h->d_f0, d_D, h->d_Jp, h->d_Kp,
+                                            h->nbf, h->d_boys, h->stream, h->nsm);
+                        CK(cudaEventRecord(b, h->stream));
+                        CK(cudaEventSynchronize(b));
+                        CK(cudaGetLastError());
+                        float ms = 0;
+                        CK(cudaEventElapsedTime(&ms, a, b));
+                        if (ms < best)
+                        {
+                            best = ms;
+                            h->tuned_run[k] = r;
+                            h->tuned_cap[k] = c;
+                        }
+                    }
+            }
+        }
+        catch (...)
+        {
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+            throw;
+        }
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        if (run_out) std::copy(h->tuned_run, h->tuned_run + kNumQuartetClasses, run_out);
+        if (cap_out) std::copy(h->tuned_cap, h->tuned_cap + kNumQuartetClasses, cap_out);
     });
 }
 
@@ -1655,6 +1727,7 @@ void qcg_scf_default_params(qcg_scf_params* p)
     p->fp32_scale = 0.0;
     p->fp32_below = 0.0;
     p->D_guess = nullptr;
+    p->autotune = 0;
 }
 
 // Closed-shell SCF (SCFIterator.C:283-362 loop; DIIS gating/pruning per SCFAcceleratorDIIS.C:35-238)
@@ -1725,6 +1798,11 @@ int qcg_rhf(qcg_handle* h, int natom, const double* Z, const double* R, int nele
             if (full)
             {
                 CK(cudaMemcpyAsync(h->d_D, D.data(), nn * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+                if (it == 1 && prm.autotune)
+                {
+                    const int e = qcg_autotune_jk(h, h->d_D, 1, nullptr, nullptr);
+                    if (e != QCG_OK) throw Error{e, h->last_error};
+                }
                 jk_device(h, h->d_D, h->d_J, h->d_K, QCG_JK_SKIP_VALIDATION, &st, nullptr, 0.0, band);
             }
             else
@@ -1979,6 +2057,11 @@ int qcg_rhf_batch(qcg_handle* h, const int* mol_natom, const double* Z, const do
                 std::copy(sc[m].D.begin(), sc[m].D.end(), Dh.begin() + h->mol_off[m]);
             qcg_stats st{};
             CK(cudaMemcpyAsync(h->d_D, Dh.data(), nn * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+            if (it == 1 && prm.autotune)
+            {
+                const int e = qcg_autotune_jk(h, h->d_D, 1, nullptr, nullptr);
+                if (e != QCG_OK) throw Error{e, h->last_error};
+            }
             jk_device(h, h->d_D, h->d_J, h->d_K, QCG_JK_SKIP_VALIDATION, &st);
             CK(cudaMemcpyAsync(J.data(), h->d_J, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
             CK(cudaMemcpyAsync(K.data(), h->d_K, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
