@@ -24,6 +24,7 @@ LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libqchem_b200.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+CUDA_LIB = os.path.join(os.path.dirname(os.path.dirname(NVCC)), "lib64")   # cuSOLVER / cuBLAS of the SCF step
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"] + ARCH
 NCLASS = 21
@@ -110,7 +111,8 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
     stamp = LIB + ".key"
     if force or not os.path.exists(LIB) or not os.path.exists(stamp) or open(stamp).read() != key:
         tmp = LIB + ".tmp"
-        cmd = [NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objs + ["-lgomp"]
+        cmd = [NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objs + [
+            "-lgomp", "-L", CUDA_LIB, "-lcusolver", "-lcublas", "-Xlinker", "-rpath=" + CUDA_LIB]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n" + r.stderr[-4000:])

@@ -12,11 +12,15 @@
 #include <cstdlib>
 #include <cstring>
 #include <deque>
+#include <memory>
 #include <numeric>
 #include <string>
 #include <type_traits>
 #include <unordered_map>
 #include <vector>
+
+#include <cublas_v2.h>
+#include <cusolverDn.h>
 
 #include "../../include/qchem_b200.h"
 #include "md_core.cuh"
@@ -584,6 +588,113 @@ std::vector<double> solve_dense(int n, std::vector<double> A, std::vector<double
 }
 
 // ------------------------------------------------------------------------------------------------
+// Dense FP64 linear algebra of the SCF step on the GPU for large bases (cuSOLVER syevd, cuBLAS dgemm), in
+// place of the host eigensolver and products above, whose O(n^3) cost at n ~ 2000 rivals the Fock build
+// itself (LASolverLapack.C:126-145 is the reference's eigensolver call).  Host arrays in and out (row-major);
+// device buffers and library handles are kept between calls.  Not thread-safe: one per SCF.
+// ------------------------------------------------------------------------------------------------
+struct GpuLinalg
+{
+    cudaStream_t st = nullptr;
+    cusolverDnHandle_t sol = nullptr;
+    cublasHandle_t blas = nullptr;
+    double *dA = nullptr, *dB = nullptr, *dC = nullptr, *dW = nullptr, *dWork = nullptr;
+    int* dInfo = nullptr;
+    int cap = 0, lwork = 0;
+
+    explicit GpuLinalg(cudaStream_t s) : st(s)
+    {
+        if (cusolverDnCreate(&sol) != CUSOLVER_STATUS_SUCCESS) throw Error{QCG_ERR_CUDA, "cusolverDnCreate failed"};
+        if (cublasCreate(&blas) != CUBLAS_STATUS_SUCCESS) throw Error{QCG_ERR_CUDA, "cublasCreate failed"};
+        cusolverDnSetStream(sol, st);
+        cublasSetStream(blas, st);
+    }
+    ~GpuLinalg()
+    {
+        if (st) cudaStreamSynchronize(st);
+        for (void* p : {(void*)dA, (void*)dB, (void*)dC, (void*)dW, (void*)dWork, (void*)dInfo}) cudaFree(p);
+        if (sol) cusolverDnDestroy(sol);
+        if (blas) cublasDestroy(blas);
+    }
+    void reserve(int n)
+    {
+        if (n <= cap) return;
+        for (double** p : {&dA, &dB, &dC, &dW}) { cudaFree(*p); *p = nullptr; }
+        const size_t nn = (size_t)n * n;
+        CK(cudaMalloc(&dA, nn * sizeof(double)));
+        CK(cudaMalloc(&dB, nn * sizeof(double)));
+        CK(cudaMalloc(&dC, nn * sizeof(double)));
+        CK(cudaMalloc(&dW, (size_t)n * sizeof(double)));
+        if (!dInfo) CK(cudaMalloc(&dInfo, sizeof(int)));
+        int lw = 0;
+        if (cusolverDnDsyevd_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, dA, n, dW, &lw) !=
+            CUSOLVER_STATUS_SUCCESS)
+            throw Error{QCG_ERR_CUDA, "cusolverDnDsyevd_bufferSize failed"};
+        cudaFree(dWork);
+        dWork = nullptr;
+        CK(cudaMalloc(&dWork, (size_t)std::max(lw, 1) * sizeof(double)));
+        lwork = lw;
+        cap = n;
+    }
+    // A = V diag(w) V^T, w ascending, V row-major with eigenvectors as columns (as syev above)
+    void syev(int n, const double* A, double* w, double* V)
+    {
+        reserve(n);
+        const size_t nn = (size_t)n * n;
+        CK(cudaMemcpyAsync(dA, A, nn * sizeof(double), cudaMemcpyHostToDevice, st));
+        if (cusolverDnDsyevd(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, dA, n, dW, dWork, lwork,
+                             dInfo) != CUSOLVER_STATUS_SUCCESS)
+            throw Error{QCG_ERR_CUDA, "cusolverDnDsyevd failed"};
+        // column-major result: eigenvector j is column j of dA; transpose to the row-major layout on the device
+        const double one = 1.0, zero = 0.0;
+        if (cublasDgeam(blas, CUBLAS_OP_T, CUBLAS_OP_N, n, n, &one, dA, n, &zero, dB, n, dB, n) != CUBLAS_STATUS_SUCCESS)
+            throw Error{QCG_ERR_CUDA, "cublasDgeam failed"};
+        int info = 0;
+        CK(cudaMemcpyAsync(w, dW, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(V, dB, nn * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(&info, dInfo, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (info != 0) throw Error{QCG_ERR_NOCONV, "cusolverDnDsyevd did not converge"};
+    }
+    // C = op(A) op(B), n x n row-major (a row-major array is its transpose column-major, so the product is
+    // computed as C^T = op(B)^T op(A)^T)
+    void gemm(int n, const double* A, bool ta, const double* B, bool tb, double* C)
+    {
+        reserve(n);
+        const size_t nn = (size_t)n * n;
+        CK(cudaMemcpyAsync(dA, A, nn * sizeof(double), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(dB, B, nn * sizeof(double), cudaMemcpyHostToDevice, st));
+        const double one = 1.0, zero = 0.0;
+        if (cublasDgemm(blas, tb ? CUBLAS_OP_T : CUBLAS_OP_N, ta ? CUBLAS_OP_T : CUBLAS_OP_N, n, n, n, &one, dB, n, dA,
+                        n, &zero, dC, n) != CUBLAS_STATUS_SUCCESS)
+            throw Error{QCG_ERR_CUDA, "cublasDgemm failed"};
+        CK(cudaMemcpyAsync(C, dC, nn * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+    }
+    // Dp = 2 U_occ U_occ^T from row-major U whose first nocc columns are the occupied orbitals
+    void occ_density(int n, int nocc, const double* U, double* Dp)
+    {
+        reserve(n);
+        const size_t nn = (size_t)n * n;
+        CK(cudaMemcpyAsync(dA, U, nn * sizeof(double), cudaMemcpyHostToDevice, st));
+        // column-major view M = U^T; its first nocc rows (ld n) are U_occ^T; Dp = 2 (U_occ^T)^T (U_occ^T)
+        const double two = 2.0, zero = 0.0;
+        if (cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, n, n, nocc, &two, dA, n, dA, n, &zero, dC, n) !=
+            CUBLAS_STATUS_SUCCESS)
+            throw Error{QCG_ERR_CUDA, "cublasDgemm failed"};
+        CK(cudaMemcpyAsync(Dp, dC, nn * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+    }
+};
+
+// bases with at least this many functions take the GPU path in qcg_rhf (QCG_GPU_LINALG_MIN overrides)
+int gpu_linalg_min()
+{
+    const char* e = std::getenv("QCG_GPU_LINALG_MIN");
+    return e ? std::atoi(e) : 256;
+}
+
+// ------------------------------------------------------------------------------------------------
 // Host state of one closed-shell SCF (SCFIterator.C:283-362, SCFAcceleratorDIIS.C:35-238): canonical
 // orthogonaliser X = U s^{-1/2}, density, Fock matrix in the orthonormal basis and the DIIS subspace.
 // ------------------------------------------------------------------------------------------------
@@ -594,6 +705,18 @@ struct ScfCore
     std::vector<double> S, H, X, D, Dp, F, Fp, Err, tmp, Up, w, a, b;
     std::deque<std::vector<double>> Es, Fps;
     double E = 0, Eold = 0, En = 0;
+    GpuLinalg* gl = nullptr;   // set: the O(n^3) steps run on the GPU
+
+    void xsyev(const double* A, double* wv, double* V)
+    {
+        if (gl) gl->syev(n, A, wv, V);
+        else syev(n, A, wv, V);
+    }
+    void xgemm(const double* A, bool ta, const double* B, bool tb, double* C)
+    {
+        if (gl) gl->gemm(n, A, ta, B, tb, C);
+        else gemm(n, A, ta, B, tb, C);
+    }
 
     void init(int n_, int nocc_, std::vector<double> S_, std::vector<double> H_, double fdmax_, double Enn_,
               const double* guess)
@@ -607,7 +730,7 @@ struct ScfCore
         H = std::move(H_);
         X.assign(nn, 0.0);
         std::vector<double> sw(n), U(nn);
-        syev(n, S.data(), sw.data(), U.data());
+        xsyev(S.data(), sw.data(), U.data());
         require(sw[0] > 0, "overlap matrix is not positive definite");
         for (int i = 0; i < n; ++i)
             for (int j = 0; j < n; ++j) X[(size_t)i * n + j] = U[(size_t)i * n + j] / std::sqrt(sw[j]);
@@ -632,9 +755,9 @@ struct ScfCore
                     require(std::isfinite(x), "non-finite initial density", QCG_ERR_NONFINITE);
                     D[(size_t)i * n + j] = x;
                 }
-            gemm(n, S.data(), false, X.data(), false, tmp.data());       // S X
-            gemm(n, D.data(), false, tmp.data(), false, Up.data());      // D S X
-            gemm(n, tmp.data(), true, Up.data(), false, Dp.data());      // X^T S D S X
+            xgemm(S.data(), false, X.data(), false, tmp.data());       // S X
+            xgemm(D.data(), false, tmp.data(), false, Up.data());      // D S X
+            xgemm(tmp.data(), true, Up.data(), false, Dp.data());      // X^T S D S X
         }
         else
         {
@@ -644,22 +767,25 @@ struct ScfCore
     }
     void ortho(const std::vector<double>& M, std::vector<double>& out)
     {
-        gemm(n, M.data(), false, X.data(), false, tmp.data());
-        gemm(n, X.data(), true, tmp.data(), false, out.data());
+        xgemm(M.data(), false, X.data(), false, tmp.data());
+        xgemm(X.data(), true, tmp.data(), false, out.data());
     }
     // aufbau density of an orthonormal-basis Fock matrix, back in the AO basis (exactly symmetric)
     void diag_fill(const std::vector<double>& Fo)
     {
-        syev(n, Fo.data(), w.data(), Up.data());
-        for (int i = 0; i < n; ++i)
-            for (int j = 0; j < n; ++j)
-            {
-                double s = 0;
-                for (int k = 0; k < nocc; ++k) s += Up[(size_t)i * n + k] * Up[(size_t)j * n + k];
-                Dp[(size_t)i * n + j] = 2 * s;
-            }
-        gemm(n, X.data(), false, Dp.data(), false, tmp.data());
-        gemm(n, tmp.data(), false, X.data(), true, D.data());
+        xsyev(Fo.data(), w.data(), Up.data());
+        if (gl)
+            gl->occ_density(n, nocc, Up.data(), Dp.data());
+        else
+            for (int i = 0; i < n; ++i)
+                for (int j = 0; j < n; ++j)
+                {
+                    double s = 0;
+                    for (int k = 0; k < nocc; ++k) s += Up[(size_t)i * n + k] * Up[(size_t)j * n + k];
+                    Dp[(size_t)i * n + j] = 2 * s;
+                }
+        xgemm(X.data(), false, Dp.data(), false, tmp.data());
+        xgemm(tmp.data(), false, X.data(), true, D.data());
         for (int i = 0; i < n; ++i)
             for (int j = i + 1; j < n; ++j)
             {
@@ -680,8 +806,8 @@ struct ScfCore
         E = 0.5 * e + Enn;
         if (!std::isfinite(E)) throw Error{QCG_ERR_NONFINITE, "non-finite SCF energy"};
         ortho(F, Fp);
-        gemm(n, Fp.data(), false, Dp.data(), false, a.data());
-        gemm(n, Dp.data(), false, Fp.data(), false, b.data());
+        xgemm(Fp.data(), false, Dp.data(), false, a.data());
+        xgemm(Dp.data(), false, Fp.data(), false, b.data());
         En = 0;
         for (size_t k = 0; k < nn; ++k)
         {
@@ -1763,6 +1889,12 @@ int qcg_rhf(qcg_handle* h, int natom, const double* Z, const double* R, int nele
         }
         ensure_jk_buffers(h);
         ScfCore sc;
+        std::unique_ptr<GpuLinalg> gl;
+        if (n >= gpu_linalg_min())
+        {
+            gl = std::make_unique<GpuLinalg>(h->stream);
+            sc.gl = gl.get();
+        }
         sc.init(n, nocc, std::move(S), std::move(H), fdmax, Enn, prm.D_guess);
         std::vector<double>& D = sc.D;
         std::vector<double> J(nn), K(nn);
