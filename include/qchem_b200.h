@@ -130,6 +130,11 @@ int qcg_eri_batch(qcg_handle* h, int la, int lb, int lc, int ld, long long nq, c
 /* same with device pointers (no validation of the shell L's; the stream is the handle's) */
 int qcg_eri_batch_device(qcg_handle* h, int la, int lb, int lc, int ld, long long nq, const int* d_quartets,
                          double* d_out);
+/* 3-centre Coulomb integrals (ab|c) of nt shell triples (3 int32 each; 2 >= la >= lb, lc <= 2):
+ * out[t][a][b][c], contracted and normalised like NR_Evaluator::RepulsionThreeC
+ * (src/BasisSet/Molecule/Evaluators/PG_Cart_MnD/Evaluator.C:1905-1908, primitive integral GaussianRF.C:415-444),
+ * the integrals of density-fitted Coulomb.  Fitting shells are ordinary shells of the handle.  Host buffers. */
+int qcg_eri3_batch(qcg_handle* h, int la, int lb, int lc, long long nt, const int* triples, double* out);
 /* FP32 forms of the two batch calls: the same integrals evaluated in FP32 arithmetic (pair data, Boys
  * argument, prefactor and Boys below T = 12 in FP64, rounded once) with float output.  No reference
  * counterpart (the reference is FP64 only). */

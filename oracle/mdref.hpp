@@ -497,4 +497,72 @@ inline void shell_quartet(const Basis& bs, int sa, int sb, int sc, int sd, doubl
                     out[o] *= bs.ns[A.f0 + a] * bs.ns[B.f0 + b] * bs.ns[C.f0 + c] * bs.ns[D.f0 + d];
 }
 
+// ---------------------------------------------------------------------------------------------------
+// 3-centre Coulomb (ab|c): the ab charge distribution against c's single-centre Hermite expansion, with
+// the overall sign (-1)^{L_c} and prefactor 2 pi^{5/2} / (p gamma sqrt(p + gamma)) E_ab
+// (GaussianRF.C:415-444); contracted and normalised like NR_Evaluator::RepulsionThreeC (Evaluator.C:1905-1908)
+// ---------------------------------------------------------------------------------------------------
+inline double prim_eri3(const PrimPair& ab, double gam, const Herm1D (&Hc)[3], const RTable& R,
+                        const std::array<int, 3>& pa, const std::array<int, 3>& pb, const std::array<int, 3>& pc)
+{
+    const double Pi52 = kPi * kPi * std::sqrt(kPi);
+    int Pab[3];
+    for (int x = 0; x < 3; ++x) Pab[x] = pa[x] + pb[x];
+    double s = 0.0;
+    for (int an = 0; an <= Pab[0]; ++an)
+        for (int al = 0; al <= Pab[1]; ++al)
+            for (int am = 0; am <= Pab[2]; ++am)
+            {
+                const double hab = ab.h2(an, al, am, pa, pb);
+                if (hab == 0.0) continue;
+                double Rs = 0.0;
+                for (int n = 0; n <= pc[0]; ++n)
+                    for (int l = 0; l <= pc[1]; ++l)
+                        for (int m = 0; m <= pc[2]; ++m)
+                        {
+                            const double h = Hc[0].get(n, pc[0], 0) * Hc[1].get(l, pc[1], 0) * Hc[2].get(m, pc[2], 0);
+                            if (h != 0.0) Rs += h * R(an + n, al + l, am + m);
+                        }
+                if (Rs != 0.0) s += hab * Rs;
+            }
+    double factor = 1.0 / (ab.p * gam * std::sqrt(ab.p + gam));
+    if ((pc[0] + pc[1] + pc[2]) & 1) factor = -factor;
+    return s * 2 * Pi52 * ab.Eij * factor;
+}
+
+// whole shell-triple block out[((ia*nb+ib)*nc+ic)]
+inline void shell_triple(const Basis& bs, int sa, int sb, int sc, double* out)
+{
+    const Shell& A = bs.shells[sa];
+    const Shell& B = bs.shells[sb];
+    const Shell& C = bs.shells[sc];
+    auto ca = components(A.L), cb = components(B.L), cc = components(C.L);
+    const int na = ca.size(), nb = cb.size(), nc = cc.size();
+    std::fill(out, out + na * nb * nc, 0.0);
+    for (size_t i = 0; i < A.alpha.size(); ++i)
+        for (size_t j = 0; j < B.alpha.size(); ++j)
+        {
+            PrimPair ab;
+            ab.build(A.alpha[i], A.A, A.L, B.alpha[j], B.A, B.L, 0);
+            for (size_t k = 0; k < C.alpha.size(); ++k)
+            {
+                const double gam = C.alpha[k];
+                Herm1D Hc[3];
+                for (int x = 0; x < 3; ++x) Hc[x].build(1.0 / (2 * gam), 0.0, 0.0, C.L, 0);   // one centre: P = C
+                RTable R;
+                std::array<double, 3> PQ{ab.P[0] - C.A[0], ab.P[1] - C.A[1], ab.P[2] - C.A[2]};
+                R.build(A.L + B.L + C.L, ab.p * gam / (ab.p + gam), PQ);
+                const double cf = A.coef[i] * B.coef[j] * C.coef[k];
+                int o = 0;
+                for (int a = 0; a < na; ++a)
+                    for (int b = 0; b < nb; ++b)
+                        for (int c = 0; c < nc; ++c, ++o) out[o] += cf * prim_eri3(ab, gam, Hc, R, ca[a], cb[b], cc[c]);
+            }
+        }
+    int o = 0;
+    for (int a = 0; a < na; ++a)
+        for (int b = 0; b < nb; ++b)
+            for (int c = 0; c < nc; ++c, ++o) out[o] *= bs.ns[A.f0 + a] * bs.ns[B.f0 + b] * bs.ns[C.f0 + c];
+}
+
 }   // namespace mdref

@@ -32,6 +32,7 @@ def lib():
         L.orc_fourc.restype = f64
         L.orc_shell_quartet.argtypes = [vp, i32, i32, i32, i32, P(f64)]
         L.orc_eri_batch.argtypes = [vp, i64, P(i32), i64, P(f64), i32]
+        L.orc_eri3_batch.argtypes = [vp, i64, P(i32), i64, P(f64), i32]
         L.orc_one_electron.argtypes = [vp, i32, P(f64), P(f64), P(f64), P(f64), P(f64)]
         L.orc_schwarz.argtypes = [vp, P(f64)]
         L.orc_jk_direct.argtypes = [vp, P(f64), P(f64), P(f64), f64, i32]
@@ -102,6 +103,15 @@ class OracleBasis:
         blk = s[q[0, 0]].nfunc * s[q[0, 1]].nfunc * s[q[0, 2]].nfunc * s[q[0, 3]].nfunc
         out = np.zeros((len(q), blk))
         lib().orc_eri_batch(self.h, len(q), _p(q, ctypes.c_int), blk, _p(out), int(nthreads))
+        return out
+
+    def eri3_batch(self, triples, nthreads=0):
+        """3-centre Coulomb blocks (ab|c), out[t][a][b][c], normalised like the reference's RepulsionThreeC."""
+        t = np.ascontiguousarray(triples, dtype=np.int32)
+        s = self.shells
+        blk = s[t[0, 0]].nfunc * s[t[0, 1]].nfunc * s[t[0, 2]].nfunc
+        out = np.zeros((len(t), blk))
+        lib().orc_eri3_batch(self.h, len(t), _p(t, ctypes.c_int), blk, _p(out), int(nthreads))
         return out
 
     def one_electron(self, mol):

@@ -387,6 +387,14 @@ void orc_eri_batch(void* h, long long nq, const int* q, long long block, double*
 #pragma omp parallel for schedule(dynamic, 64)
     for (long long i = 0; i < nq; ++i) shell_quartet(o->bs, q[4 * i], q[4 * i + 1], q[4 * i + 2], q[4 * i + 3], out + i * block);
 }
+// nt triples (3 shell indices each); out holds nt blocks of `block` doubles (3-centre Coulomb)
+void orc_eri3_batch(void* h, long long nt, const int* t, long long block, double* out, int nthreads)
+{
+    auto* o = (OBasis*)h;
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 64)
+    for (long long i = 0; i < nt; ++i) shell_triple(o->bs, t[3 * i], t[3 * i + 1], t[3 * i + 2], out + i * block);
+}
 void orc_one_electron(void* h, int natom, const double* Z, const double* R, double* S, double* T, double* V)
 {
     auto* o = (OBasis*)h;

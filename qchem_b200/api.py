@@ -40,7 +40,7 @@ EXPORTS = ["qcg_basis_create", "qcg_destroy", "qcg_last_error", "qcg_set_stream"
            "qcg_measure_fp32_peak", "qcg_mlp_create", "qcg_mlp_destroy", "qcg_mlp_last_error", "qcg_mlp_set_stream",
            "qcg_mlp_nparams", "qcg_mlp_params", "qcg_mlp_set_params", "qcg_mlp_forward", "qcg_mlp_loss_grad",
            "qcg_mlp_adam", "qcg_basis_create_batch", "qcg_nmol", "qcg_mol_nbf", "qcg_one_electron_batch",
-           "qcg_rhf_batch", "qcg_set_graphs", "qcg_set_shard", "qcg_autotune_jk"]
+           "qcg_rhf_batch", "qcg_set_graphs", "qcg_set_shard", "qcg_autotune_jk", "qcg_eri3_batch"]
 
 
 class QcgError(RuntimeError):
@@ -102,6 +102,7 @@ def lib():
     L.qcg_eri_batch.argtypes = [vp, i32, i32, i32, i32, i64, P(i32), P(f64)]
     L.qcg_eri_batch_device.argtypes = [vp, i32, i32, i32, i32, i64, vp, vp]
     L.qcg_eri_batch_f32.argtypes = [vp, i32, i32, i32, i32, i64, P(i32), P(ctypes.c_float)]
+    L.qcg_eri3_batch.argtypes = [vp, i32, i32, i32, i64, P(i32), P(f64)]
     L.qcg_eri_batch_device_f32.argtypes = [vp, i32, i32, i32, i32, i64, vp, vp]
     L.qcg_set_fp32_bound.argtypes = [vp, f64]
     L.qcg_set_graphs.argtypes = [vp, i32]
@@ -231,6 +232,15 @@ class Engine:
                                                 _p(out, ctypes.c_float)))
         else:
             self._check(lib().qcg_eri_batch(self._h, la, lb, lc, ld, len(q), _p(q, ctypes.c_int), _p(out)))
+        return out
+
+    def eri3_batch(self, cls3, triples) -> np.ndarray:
+        """3-centre Coulomb blocks (ab|c) of shell triples of class (la, lb, lc), la >= lb."""
+        t = np.ascontiguousarray(triples, dtype=np.int32)
+        la, lb, lc = cls3
+        nf = [(l + 1) * (l + 2) // 2 for l in cls3]
+        out = np.zeros((len(t), nf[0] * nf[1] * nf[2]))
+        self._check(lib().qcg_eri3_batch(self._h, la, lb, lc, len(t), _p(t, ctypes.c_int), _p(out)))
         return out
 
     def eri_batch_device(self, cls, d_quartets_ptr: int, nq: int, d_out_ptr: int, fp32: bool = False):

@@ -1383,12 +1383,19 @@ int qcg_basis_create_batch(const int* shell_L, const int* shell_nprim, const dou
         h->d_boys = h->alloc<double>(121 * 23);
         CK(cudaMemcpyAsync(h->d_boys, kBoysTable, sizeof(kBoysTable), cudaMemcpyHostToDevice, h->stream));
         h->bs.nshell = nshell;
-        h->bs.L = h->upload(h->L);
-        h->bs.nprim = h->upload(h->nprim);
-        h->bs.prim0 = h->upload(h->prim0);
-        h->bs.cen = h->upload(h->cen);
-        h->bs.alpha = h->upload(h->alpha);
-        h->bs.coef = h->upload(h->coef);
+        // the device arrays carry one more shell, index nshell, never part of the basis: the unnormalised
+        // s function of exponent 0 and coefficient 1, so that (ab|c) = (ab|c s0) (qcg_eri3_batch)
+        auto plus = [](std::vector<int> v, int x) { v.push_back(x); return v; };
+        auto plusd = [](std::vector<double> v, std::initializer_list<double> x) {
+            v.insert(v.end(), x);
+            return v;
+        };
+        h->bs.L = h->upload(plus(h->L, 0));
+        h->bs.nprim = h->upload(plus(h->nprim, 1));
+        h->bs.prim0 = h->upload(plus(h->prim0, np));
+        h->bs.cen = h->upload(plusd(h->cen, {0.0, 0.0, 0.0}));
+        h->bs.alpha = h->upload(plusd(h->alpha, {0.0}));
+        h->bs.coef = h->upload(plusd(h->coef, {1.0}));
         h->d_f0 = h->upload(h->f0);
         h->mol_off.assign(nmol + 1, 0);
         for (int m = 0; m < nmol; ++m) h->mol_off[m + 1] = h->mol_off[m] + (long long)h->mol_nbf[m] * h->mol_nbf[m];
@@ -1494,6 +1501,9 @@ int eri_batch_device(qcg_handle* h, int la, int lb, int lc, int ld, long long nq
 }
 
 template <class T>
+void eri_batch_run(qcg_handle* h, int la, int lb, int lc, int ld, long long nq, const int* quartets, T* out);
+
+template <class T>
 int eri_batch_host(qcg_handle* h, int la, int lb, int lc, int ld, long long nq, const int* quartets, T* out)
 {
     if (!h) return QCG_ERR_ARG;
@@ -1511,6 +1521,16 @@ int eri_batch_host(qcg_handle* h, int la, int lb, int lc, int ld, long long nq, 
                 require(s >= 0 && s < h->nshell, "shell index out of range");
                 require(h->L[s] == Ls[x], "shell angular momentum does not match the class");
             }
+        eri_batch_run(h, la, lb, lc, ld, nq, quartets, out);
+    });
+}
+
+// the device part of a host-buffer batch (quartets already checked; may name the unit shell nshell)
+template <class T>
+void eri_batch_run(qcg_handle* h, int la, int lb, int lc, int ld, long long nq, const int* quartets, T* out)
+{
+    {
+        const int k = class_index(la, lb, lc, ld);
         const long long blk = (long long)ncart(la) * ncart(lb) * ncart(lc) * ncart(ld);
         // two device buffers of at most 512 MiB of output each, kept by the handle between calls: the
         // copy of one chunk back to the host overlaps the evaluation of the next
@@ -1558,7 +1578,7 @@ int eri_batch_host(qcg_handle* h, int la, int lb, int lc, int ld, long long nq, 
         }
         CK(cudaStreamSynchronize(h->copy_stream));
         CK(cudaStreamSynchronize(h->stream));
-    });
+    }
 }
 }   // namespace
 }   // extern "C++"
@@ -1583,6 +1603,49 @@ int qcg_eri_batch(qcg_handle* h, int la, int lb, int lc, int ld, long long nq, c
 int qcg_eri_batch_f32(qcg_handle* h, int la, int lb, int lc, int ld, long long nq, const int* quartets, float* out)
 {
     return eri_batch_host(h, la, lb, lc, ld, nq, quartets, out);
+}
+
+// (ab|c) = (ab|c s0) with the handle's unit shell s0 (exponent 0, coefficient 1, index nshell): the 4-centre
+// class (la lb|lc s) when the bra pair class is not below (lc s), else (lc s|la lb) with the block transposed
+int qcg_eri3_batch(qcg_handle* h, int la, int lb, int lc, long long nt, const int* triples, double* out)
+{
+    if (!h) return QCG_ERR_ARG;
+    return guarded(h, [&] {
+        require(la >= 0 && la <= kMaxL && lb >= 0 && lb <= la && lc >= 0 && lc <= kMaxL,
+                "need 2 >= la >= lb >= 0 and 0 <= lc <= 2");
+        require(nt >= 0, "negative triple count");
+        if (nt == 0) return;
+        require(triples && out, "null argument");
+        const int Ls[3] = {la, lb, lc};
+        for (long long t = 0; t < nt; ++t)
+            for (int x = 0; x < 3; ++x)
+            {
+                const int sh = triples[3 * t + x];
+                require(sh >= 0 && sh < h->nshell, "shell index out of range");
+                require(h->L[sh] == Ls[x], "shell angular momentum does not match the class");
+            }
+        const int U = h->nshell;
+        const bool direct = pair_class(la, lb) >= pair_class(lc, 0);
+        std::vector<int> q(4 * (size_t)nt);
+        for (long long t = 0; t < nt; ++t)
+        {
+            const int a = triples[3 * t], b = triples[3 * t + 1], c = triples[3 * t + 2];
+            const int v[4] = {direct ? a : c, direct ? b : U, direct ? c : a, direct ? U : b};
+            std::copy(v, v + 4, q.begin() + 4 * t);
+        }
+        const int na = ncart(la), nb = ncart(lb), nc = ncart(lc);
+        const long long blk = (long long)na * nb * nc;
+        if (direct)
+        {
+            eri_batch_run(h, la, lb, lc, 0, nt, q.data(), out);
+            return;
+        }
+        std::vector<double> tmp((size_t)nt * blk);
+        eri_batch_run(h, lc, 0, la, lb, nt, q.data(), tmp.data());
+        for (long long t = 0; t < nt; ++t)
+            for (int c = 0; c < nc; ++c)
+                for (int ab = 0; ab < na * nb; ++ab) out[t * blk + ab * nc + c] = tmp[t * blk + c * na * nb + ab];
+    });
 }
 
 int qcg_schwarz(qcg_handle* h, double thresh, double* Q)

@@ -233,3 +233,32 @@ def test_config1_energy_rigid_motion(oracle_mod):
     mol2 = B.Molecule(mol.Z, R)
     e1 = oracle_mod.OracleBasis(B.even_tempered(mol2)).rhf(mol2)["energy"]
     assert abs(e0 - e1) < 1e-9
+
+
+def test_oracle_three_centre_closed_form_and_limit(oracle_mod):
+    """(ab|c) of the oracle: the closed form for three s functions, and the limit of the 4-centre
+    (ab|c s_eps) of a vanishing-exponent s function divided by its normalisation."""
+    import math
+    from qchem_b200 import basis as B
+    A, Bc, C = (0.0, 0.0, 0.0), (0.7, -0.4, 0.2), (1.5, 0.9, -1.1)
+    a, b, g = 0.9, 1.7, 0.6
+    sh = [B.Shell(0, A, [a], [1.0]), B.Shell(0, Bc, [b], [1.0]), B.Shell(0, C, [g], [1.0])]
+    ob = oracle_mod.OracleBasis(sh)
+    got = ob.eri3_batch(np.array([[0, 1, 2]]))[0, 0]
+    p = a + b
+    P = [(a * x + b * y) / p for x, y in zip(A, Bc)]
+    Eab = math.exp(-a * b / p * sum((x - y) ** 2 for x, y in zip(A, Bc)))
+    T = p * g / (p + g) * sum((x - y) ** 2 for x, y in zip(P, C))
+    F0 = 0.5 * math.sqrt(math.pi / T) * math.erf(math.sqrt(T))
+    norm = lambda al: (2 * al / math.pi) ** 0.75
+    ref = 2 * math.pi ** 2.5 / (p * g * math.sqrt(p + g)) * Eab * F0 * norm(a) * norm(b) * norm(g)
+    assert abs(got - ref) <= 1e-13 * abs(ref)
+    # higher angular momenta: (ab|c) = lim (ab|c s_eps) / N_eps
+    eps = 1e-9
+    for La, Lb, Lc in ((2, 1, 2), (1, 1, 1), (2, 2, 0), (0, 0, 2)):
+        sh = [B.Shell(La, A, [0.8, 2.1], [0.6, 0.4]), B.Shell(Lb, Bc, [1.3], [1.0]), B.Shell(Lc, C, [0.5], [1.0]),
+              B.Shell(0, (0.3, 0.1, -0.2), [eps], [1.0])]
+        ob = oracle_mod.OracleBasis(sh)
+        three = ob.eri3_batch(np.array([[0, 1, 2]]))[0]
+        four = ob.eri_batch(np.array([[0, 1, 2, 3]]))[0] / norm(eps)
+        assert np.abs(three - four).max() <= 1e-6 * np.abs(three).max(), (La, Lb, Lc)
