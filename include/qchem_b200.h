@@ -81,6 +81,8 @@ typedef struct qcg_scf_params {
     double fp32_below;        /* after the switch, quartets whose bound is below this stay FP32; default 0 */
     const double* D_guess;    /* optional initial total density, nbf*nbf (NULL: core-Hamiltonian guess) */
     int autotune;             /* 1: qcg_autotune_jk on the first density before the first build; default 0 */
+    int spherical;            /* 1: the SCF in real solid-harmonic functions (qcg_spherical_transform); D_guess
+                                 and D_out are then spherical; needs incremental = 0; default 0 */
 } qcg_scf_params;
 
 typedef struct qcg_scf_result {
@@ -183,6 +185,15 @@ int qcg_autotune_jk(qcg_handle* h, const double* d_D, int reps, int* run_out, in
  * keeps the last call's contents and is cleared at the start of each call), so calls that overlap on the
  * GPU race: issue them in order on one stream.  No validation of D.  Has no counterpart in the reference. */
 int qcg_fock_jk_device_noalloc(qcg_handle* h, const double* d_D, double* d_J, double* d_K);
+
+/* Real solid-harmonic (spherical) functions, the reference's PG_Spherical basis: per shell 2L+1 components
+ * ordered m = -L..L (p: y, z, x; d: xy, yz, z^2-(x^2+y^2)/2, xz, x^2-y^2), each normalised to unit
+ * self-overlap (src/BasisSet/Molecule/Evaluators/PG_Spherical_MnD/Evaluator.C:84-96, Imp/Evaluator.C:13-24).
+ * T (nbf x nbf_spherical, row-major) maps them onto the handle's Cartesian functions, chi_s = sum_t T_ts phi_t;
+ * J and K of a spherical density are T^T J[T D T^T] T and T^T K[...] T (host buffers, nbf_spherical^2). */
+int qcg_nbf_spherical(const qcg_handle* h, int* n);
+int qcg_spherical_transform(qcg_handle* h, double* T);
+int qcg_fock_jk_spherical(qcg_handle* h, const double* D, double* J, double* K, int flags, qcg_stats* stats);
 
 /* overlap, kinetic (1/2 <grad|grad>) and nuclear attraction, natom nuclei of charge Z at R (3 per atom) */
 int qcg_one_electron(qcg_handle* h, int natom, const double* Z, const double* R, double* S, double* T, double* V);

@@ -40,7 +40,8 @@ EXPORTS = ["qcg_basis_create", "qcg_destroy", "qcg_last_error", "qcg_set_stream"
            "qcg_measure_fp32_peak", "qcg_mlp_create", "qcg_mlp_destroy", "qcg_mlp_last_error", "qcg_mlp_set_stream",
            "qcg_mlp_nparams", "qcg_mlp_params", "qcg_mlp_set_params", "qcg_mlp_forward", "qcg_mlp_loss_grad",
            "qcg_mlp_adam", "qcg_basis_create_batch", "qcg_nmol", "qcg_mol_nbf", "qcg_one_electron_batch",
-           "qcg_rhf_batch", "qcg_set_graphs", "qcg_set_shard", "qcg_autotune_jk", "qcg_eri3_batch"]
+           "qcg_rhf_batch", "qcg_set_graphs", "qcg_set_shard", "qcg_autotune_jk", "qcg_eri3_batch",
+           "qcg_nbf_spherical", "qcg_spherical_transform", "qcg_fock_jk_spherical"]
 
 
 class QcgError(RuntimeError):
@@ -60,7 +61,7 @@ class ScfParams(ctypes.Structure):
                 ("diis_svtol", ctypes.c_double), ("incremental", ctypes.c_int), ("inc_thresh", ctypes.c_double),
                 ("rebuild_every", ctypes.c_int), ("fp32_early", ctypes.c_int), ("fp32_switch", ctypes.c_double),
                 ("fp32_scale", ctypes.c_double), ("fp32_below", ctypes.c_double),
-                ("D_guess", ctypes.POINTER(ctypes.c_double)), ("autotune", ctypes.c_int)]
+                ("D_guess", ctypes.POINTER(ctypes.c_double)), ("autotune", ctypes.c_int), ("spherical", ctypes.c_int)]
 
 
 class ScfResult(ctypes.Structure):
@@ -103,6 +104,9 @@ def lib():
     L.qcg_eri_batch_device.argtypes = [vp, i32, i32, i32, i32, i64, vp, vp]
     L.qcg_eri_batch_f32.argtypes = [vp, i32, i32, i32, i32, i64, P(i32), P(ctypes.c_float)]
     L.qcg_eri3_batch.argtypes = [vp, i32, i32, i32, i64, P(i32), P(f64)]
+    L.qcg_nbf_spherical.argtypes = [vp, P(i32)]
+    L.qcg_spherical_transform.argtypes = [vp, P(f64)]
+    L.qcg_fock_jk_spherical.argtypes = [vp, P(f64), P(f64), P(f64), i32, P(Stats)]
     L.qcg_eri_batch_device_f32.argtypes = [vp, i32, i32, i32, i32, i64, vp, vp]
     L.qcg_set_fp32_bound.argtypes = [vp, f64]
     L.qcg_set_graphs.argtypes = [vp, i32]
@@ -234,6 +238,32 @@ class Engine:
             self._check(lib().qcg_eri_batch(self._h, la, lb, lc, ld, len(q), _p(q, ctypes.c_int), _p(out)))
         return out
 
+    # -- spherical (real solid-harmonic) functions ----------------------------------------------
+    @property
+    def nbf_spherical(self) -> int:
+        n = ctypes.c_int()
+        self._check(lib().qcg_nbf_spherical(self._h, ctypes.byref(n)))
+        return n.value
+
+    def spherical_transform(self) -> np.ndarray:
+        """T (nbf x nbf_spherical): chi_s = sum_t T[t, s] phi_t, components ordered m = -l..l per shell."""
+        T = np.zeros((self.nbf, self.nbf_spherical))
+        self._check(lib().qcg_spherical_transform(self._h, _p(T)))
+        return T
+
+    def fock_jk_spherical(self, D, validate: bool = True):
+        if self._screen is None:
+            self.schwarz()
+        ns = self.nbf_spherical
+        D = _f64(D)
+        if D.shape != (ns, ns):
+            raise QcgError(QCG_ERR_ARG, f"spherical density must be {ns}x{ns}")
+        J, K = np.zeros_like(D), np.zeros_like(D)
+        st = Stats()
+        self._check(lib().qcg_fock_jk_spherical(self._h, _p(D), _p(J), _p(K), 0 if validate else QCG_JK_SKIP_VALIDATION,
+                                                ctypes.byref(st)))
+        return J, K, st
+
     def eri3_batch(self, cls3, triples) -> np.ndarray:
         """3-centre Coulomb blocks (ab|c) of shell triples of class (la, lb, lc), la >= lb."""
         t = np.ascontiguousarray(triples, dtype=np.int32)
@@ -311,7 +341,7 @@ class Engine:
     def rhf(self, mol: _basis.Molecule, max_iter=100, de_tol=1e-10, fd_tol=1e-5, schwarz_thresh=1e-10,
             want_density=False, incremental=False, inc_thresh=1e-11, rebuild_every=8, fp32_early=False,
             fp32_switch=1e-5, fp32_scale=0.0, fp32_below=0.0, guess=None, diis_nproj=4, diis_fdmax=0.0,
-            autotune=False):
+            autotune=False, spherical=False):
         """RHF to convergence.  incremental=True: density-difference J/K builds with density-weighted
         screening between full builds (the energy on exit is always from a full build).  fp32_early=True:
         until the DIIS error drops below fp32_switch, quartets whose density-weighted bound is below
@@ -326,15 +356,17 @@ class Engine:
         prm.fp32_scale = float(fp32_scale)
         prm.diis_nproj, prm.diis_fdmax = int(diis_nproj), float(diis_fdmax)
         prm.autotune = int(bool(autotune))
+        prm.spherical = int(bool(spherical))
+        nw = self.nbf_spherical if spherical else self.nbf
         if guess is not None:
             guess = _f64(guess)
-            if guess.shape != (self.nbf, self.nbf):
-                raise QcgError(QCG_ERR_ARG, f"guess density must be {self.nbf}x{self.nbf}")
+            if guess.shape != (nw, nw):
+                raise QcgError(QCG_ERR_ARG, f"guess density must be {nw}x{nw}")
             prm.D_guess = _p(guess)
         res = ScfResult()
         Z = _f64(mol.Z)
         R = _f64(mol.R).reshape(-1)
-        D = np.zeros((self.nbf, self.nbf)) if want_density else None
+        D = np.zeros((nw, nw)) if want_density else None
         rc = lib().qcg_rhf(self._h, len(Z), _p(Z), _p(R), int(mol.nelec), ctypes.byref(prm), ctypes.byref(res),
                            _p(D) if D is not None else None)
         if rc not in (QCG_OK, QCG_ERR_NOCONV):

@@ -154,6 +154,7 @@ struct qcg_handle
     JKWorkDev work[kNumQuartetClasses]{};
     double fp32_below = 0;   // qcg_set_fp32_bound: quartets with a smaller bound are evaluated in FP32
     int shard_rank = 0, shard_world = 1;   // qcg_set_shard: this handle's slice of every J/K build
+    std::shared_ptr<void> sph;             // the spherical map, built on first use
     int tuned_run[kNumQuartetClasses] = {}, tuned_cap[kNumQuartetClasses] = {};   // qcg_autotune_jk (0: default)
     double* d_dmaxD = nullptr;   // per shell-pair max |D| of a full build's density (mixed precision)
     long long work_quartets = 0, work_prim_quartets = 0;
@@ -693,6 +694,108 @@ int gpu_linalg_min()
     const char* e = std::getenv("QCG_GPU_LINALG_MIN");
     return e ? std::atoi(e) : 256;
 }
+
+// ------------------------------------------------------------------------------------------------
+// Real solid-harmonic (spherical) functions over the Cartesian engine.  A spherical component of a shell
+// is a fixed combination of the shell's raw Cartesian monomials, ordered m = -l..+l, normalised by its own
+// self-overlap (PG_Spherical_MnD/Imp/Evaluator.C:13-24); l = 1: y, z, x; l = 2: xy, yz, z^2-(x^2+y^2)/2,
+// xz, x^2-y^2 (the reference's SphericalShell table, src/Math/Angular.C).  With the Cartesian functions
+// normalised by ns, chi_s = sum_t T[t][s] phi_t, T[t][s] = N_s c_t / ns_t, and every spherical matrix is
+// T^T M T of the Cartesian one (J and K of D_sph are those of D_cart = T D_sph T^T).  T is block-diagonal
+// over shells, so each transform is a sweep over shell-pair blocks.
+// ------------------------------------------------------------------------------------------------
+struct SphericalMap
+{
+    int nc = 0, ns = 0;
+    std::vector<int> c0, s0, nca, nsa;          // per shell: first Cartesian / spherical function, counts
+    std::vector<std::vector<double>> blk;       // per shell: nca x nsa block of T, row-major
+
+    // Cartesian monomial coefficients of the spherical components of shell L (rows: spherical m = -l..l,
+    // columns: the shell's Cartesian components in PG order)
+    static std::vector<std::vector<double>> harmonics(int L)
+    {
+        if (L == 0) return {{1.0}};
+        if (L == 1) return {{0, 1, 0}, {0, 0, 1}, {1, 0, 0}};   // PG order x, y, z
+        // PG order for d: xx, xy, yy, xz, yz, zz
+        return {{0, 1, 0, 0, 0, 0}, {0, 0, 0, 0, 1, 0}, {-0.5, 0, -0.5, 0, 0, 1}, {0, 0, 0, 1, 0, 0}, {1, 0, -1, 0, 0, 0}};
+    }
+    void build(const qcg_handle* h, const std::vector<double>& Scart)
+    {
+        nc = h->nbf;
+        const int nsh = h->nshell;
+        c0.resize(nsh);
+        s0.resize(nsh);
+        nca.resize(nsh);
+        nsa.resize(nsh);
+        blk.assign(nsh, {});
+        ns = 0;
+        for (int a = 0; a < nsh; ++a)
+        {
+            const int L = h->L[a];
+            c0[a] = h->f0[a];
+            nca[a] = ncart(L);
+            nsa[a] = 2 * L + 1;
+            s0[a] = ns;
+            ns += nsa[a];
+            const auto Y = harmonics(L);
+            blk[a].assign((size_t)nca[a] * nsa[a], 0.0);
+            for (int m = 0; m < nsa[a]; ++m)
+            {
+                // raw self-overlap of sum_t Y[m][t] raw_t, raw_t = phi_t / ns_t
+                double raw = 0.0;
+                for (int t = 0; t < nca[a]; ++t)
+                    for (int u = 0; u < nca[a]; ++u)
+                        raw += Y[m][t] * Y[m][u] * Scart[(size_t)(c0[a] + t) * nc + c0[a] + u] /
+                               (h->ns[c0[a] + t] * h->ns[c0[a] + u]);
+                require(raw > 0, "spherical component with zero self-overlap");
+                const double N = 1.0 / std::sqrt(raw);
+                for (int t = 0; t < nca[a]; ++t) blk[a][(size_t)t * nsa[a] + m] = N * Y[m][t] / h->ns[c0[a] + t];
+            }
+        }
+    }
+    // D_cart = T D_sph T^T
+    void to_cart(const double* Ds, double* Dc) const
+    {
+        const int nsh = (int)c0.size();
+#pragma omp parallel for schedule(dynamic) if (nc > 256)
+        for (int a = 0; a < nsh; ++a)
+            for (int b = 0; b < nsh; ++b)
+                for (int t = 0; t < nca[a]; ++t)
+                    for (int u = 0; u < nca[b]; ++u)
+                    {
+                        double v = 0.0;
+                        for (int m = 0; m < nsa[a]; ++m)
+                        {
+                            const double ta = blk[a][(size_t)t * nsa[a] + m];
+                            if (ta == 0.0) continue;
+                            for (int k = 0; k < nsa[b]; ++k)
+                                v += ta * Ds[(size_t)(s0[a] + m) * ns + s0[b] + k] * blk[b][(size_t)u * nsa[b] + k];
+                        }
+                        Dc[(size_t)(c0[a] + t) * nc + c0[b] + u] = v;
+                    }
+    }
+    // M_sph = T^T M_cart T
+    void to_sph(const double* Mc, double* Ms) const
+    {
+        const int nsh = (int)c0.size();
+#pragma omp parallel for schedule(dynamic) if (nc > 256)
+        for (int a = 0; a < nsh; ++a)
+            for (int b = 0; b < nsh; ++b)
+                for (int m = 0; m < nsa[a]; ++m)
+                    for (int k = 0; k < nsa[b]; ++k)
+                    {
+                        double v = 0.0;
+                        for (int t = 0; t < nca[a]; ++t)
+                        {
+                            const double ta = blk[a][(size_t)t * nsa[a] + m];
+                            if (ta == 0.0) continue;
+                            for (int u = 0; u < nca[b]; ++u)
+                                v += ta * Mc[(size_t)(c0[a] + t) * nc + c0[b] + u] * blk[b][(size_t)u * nsa[b] + k];
+                        }
+                        Ms[(size_t)(s0[a] + m) * ns + s0[b] + k] = v;
+                    }
+    }
+};
 
 // ------------------------------------------------------------------------------------------------
 // Host state of one closed-shell SCF (SCFIterator.C:283-362, SCFAcceleratorDIIS.C:35-238): canonical
@@ -1849,6 +1952,66 @@ int qcg_one_electron(qcg_handle* h, int natom, const double* Z, const double* R,
     });
 }
 
+int qcg_nbf_spherical(const qcg_handle* h, int* n)
+{
+    if (!h || !n) return QCG_ERR_ARG;
+    int s = 0;
+    for (int L : h->L) s += 2 * L + 1;
+    *n = s;
+    return QCG_OK;
+}
+
+namespace {
+extern "C++" {
+// the handle's spherical map (needs the Cartesian overlap, from the one-electron kernel without nuclei)
+const SphericalMap& spherical_map(qcg_handle* h)
+{
+    if (!h->sph)
+    {
+        require(h->nmol == 1, "spherical functions need a single-molecule handle");
+        const size_t nn = (size_t)h->nbf * h->nbf;
+        std::vector<double> S(nn), T(nn), V(nn);
+        const int e = qcg_one_electron(h, 0, nullptr, nullptr, S.data(), T.data(), V.data());
+        if (e != QCG_OK) throw Error{e, h->last_error};
+        auto m = std::make_shared<SphericalMap>();
+        m->build(h, S);
+        h->sph = m;
+    }
+    return *std::static_pointer_cast<SphericalMap>(h->sph);
+}
+}
+}   // namespace
+
+int qcg_spherical_transform(qcg_handle* h, double* T)
+{
+    if (!h) return QCG_ERR_ARG;
+    return guarded(h, [&] {
+        require(T != nullptr, "null argument");
+        const SphericalMap& m = spherical_map(h);
+        std::fill(T, T + (size_t)m.nc * m.ns, 0.0);
+        for (size_t a = 0; a < m.c0.size(); ++a)
+            for (int t = 0; t < m.nca[a]; ++t)
+                for (int k = 0; k < m.nsa[a]; ++k)
+                    T[(size_t)(m.c0[a] + t) * m.ns + m.s0[a] + k] = m.blk[a][(size_t)t * m.nsa[a] + k];
+    });
+}
+
+int qcg_fock_jk_spherical(qcg_handle* h, const double* D, double* J, double* K, int flags, qcg_stats* stats)
+{
+    if (!h) return QCG_ERR_ARG;
+    return guarded(h, [&] {
+        require(D && J && K, "null argument");
+        const SphericalMap& m = spherical_map(h);
+        const size_t nc = (size_t)m.nc * m.nc;
+        std::vector<double> Dc(nc), Jc(nc), Kc(nc);
+        m.to_cart(D, Dc.data());
+        const int e = qcg_fock_jk(h, Dc.data(), Jc.data(), Kc.data(), flags, stats);
+        if (e != QCG_OK) throw Error{e, h->last_error};
+        m.to_sph(Jc.data(), J);
+        m.to_sph(Kc.data(), K);
+    });
+}
+
 int qcg_one_electron_batch(qcg_handle* h, const int* mol_natom, const double* Z, const double* R, double* S,
                            double* T, double* V)
 {
@@ -1917,6 +2080,7 @@ void qcg_scf_default_params(qcg_scf_params* p)
     p->fp32_below = 0.0;
     p->D_guess = nullptr;
     p->autotune = 0;
+    p->spherical = 0;
 }
 
 // Closed-shell SCF (SCFIterator.C:283-362 loop; DIIS gating/pruning per SCFAcceleratorDIIS.C:35-238)
@@ -1951,16 +2115,34 @@ int qcg_rhf(qcg_handle* h, int natom, const double* Z, const double* R, int nele
             if (e != QCG_OK) throw Error{e, h->last_error};
         }
         ensure_jk_buffers(h);
+        // spherical basis: the SCF runs on T^T S T, T^T H T; every build takes D_cart = T D T^T and returns
+        // T^T J T, T^T K T (the reference's PG_Spherical path: same Cartesian kernels, transformed)
+        std::unique_ptr<SphericalMap> sph;
+        int nw = n;
+        if (prm.spherical)
+        {
+            require(prm.incremental == 0, "the spherical SCF uses full builds (incremental = 0)");
+            sph = std::make_unique<SphericalMap>();
+            sph->build(h, S);
+            nw = sph->ns;
+            require(nocc <= nw, "more occupied orbitals than spherical basis functions");
+            std::vector<double> Ss((size_t)nw * nw), Hs((size_t)nw * nw);
+            sph->to_sph(S.data(), Ss.data());
+            sph->to_sph(H.data(), Hs.data());
+            S = std::move(Ss);
+            H = std::move(Hs);
+        }
         ScfCore sc;
         std::unique_ptr<GpuLinalg> gl;
-        if (n >= gpu_linalg_min())
+        if (nw >= gpu_linalg_min())
         {
             gl = std::make_unique<GpuLinalg>(h->stream);
             sc.gl = gl.get();
         }
-        sc.init(n, nocc, std::move(S), std::move(H), fdmax, Enn, prm.D_guess);
+        sc.init(nw, nocc, std::move(S), std::move(H), fdmax, Enn, prm.D_guess);
         std::vector<double>& D = sc.D;
         std::vector<double> J(nn), K(nn);
+        std::vector<double> Dc(sph ? nn : 0), Js(sph ? (size_t)nw * nw : 0), Ks(sph ? (size_t)nw * nw : 0);
         std::vector<double> Dprev, Jprev, Kprev, dD(nn);
         double fock_ms = 0;
         const bool inc = prm.incremental != 0;
@@ -1992,7 +2174,13 @@ int qcg_rhf(qcg_handle* h, int natom, const double* Z, const double* R, int nele
             if (band > 0) ++n32;
             if (full)
             {
-                CK(cudaMemcpyAsync(h->d_D, D.data(), nn * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+                const double* Dup = D.data();
+                if (sph)
+                {
+                    sph->to_cart(D.data(), Dc.data());
+                    Dup = Dc.data();
+                }
+                CK(cudaMemcpyAsync(h->d_D, Dup, nn * sizeof(double), cudaMemcpyHostToDevice, h->stream));
                 if (it == 1 && prm.autotune)
                 {
                     const int e = qcg_autotune_jk(h, h->d_D, 1, nullptr, nullptr);
@@ -2024,7 +2212,14 @@ int qcg_rhf(qcg_handle* h, int natom, const double* Z, const double* R, int nele
                 ++ninc;
             }
             if (inc) { Dprev = D; Jprev = J; Kprev = K; }
-            sc.fock(J.data(), K.data());
+            if (sph)
+            {
+                sph->to_sph(J.data(), Js.data());
+                sph->to_sph(K.data(), Ks.data());
+                sc.fock(Js.data(), Ks.data());
+            }
+            else
+                sc.fock(J.data(), K.data());
             if (it > 1 && std::fabs(sc.E - sc.Eold) < prm.de_tol && sc.En < prm.fd_tol)
             {
                 if (!full || band != 0.0)
