@@ -1606,6 +1606,34 @@ int eri_batch_device(qcg_handle* h, int la, int lb, int lc, int ld, long long nq
 template <class T>
 void eri_batch_run(qcg_handle* h, int la, int lb, int lc, int ld, long long nq, const int* quartets, T* out);
 
+// Checks rows of `width` shell indices (quartets or triples) against the handle: every index in range
+// and of angular momentum Ls[x] in column x.  The scan runs over the host cores and builds no message
+// per element; only the first bad row, if any, is examined again to raise the error.
+void check_shell_rows(const qcg_handle* h, const int* idx, long long nrow, int width, const int* Ls)
+{
+    const int ns = h->nshell;
+    const int* L = h->L.data();
+    long long bad = nrow;
+#pragma omp parallel for schedule(static) reduction(min : bad) if (nrow > 65536)
+    for (long long r = 0; r < nrow; ++r)
+    {
+        bool ok = true;
+        for (int x = 0; x < width; ++x)
+        {
+            const int s = idx[width * r + x];
+            ok = ok && (unsigned)s < (unsigned)ns && L[s] == Ls[x];
+        }
+        if (!ok && r < bad) bad = r;
+    }
+    if (bad == nrow) return;
+    for (int x = 0; x < width; ++x)
+    {
+        const int s = idx[width * bad + x];
+        require(s >= 0 && s < ns, "shell index out of range");
+        require(L[s] == Ls[x], "shell angular momentum does not match the class");
+    }
+}
+
 template <class T>
 int eri_batch_host(qcg_handle* h, int la, int lb, int lc, int ld, long long nq, const int* quartets, T* out)
 {
@@ -1617,13 +1645,7 @@ int eri_batch_host(qcg_handle* h, int la, int lb, int lc, int ld, long long nq, 
         if (nq == 0) return;
         require(quartets && out, "null argument");
         const int Ls[4] = {la, lb, lc, ld};
-        for (long long q = 0; q < nq; ++q)
-            for (int x = 0; x < 4; ++x)
-            {
-                const int s = quartets[4 * q + x];
-                require(s >= 0 && s < h->nshell, "shell index out of range");
-                require(h->L[s] == Ls[x], "shell angular momentum does not match the class");
-            }
+        check_shell_rows(h, quartets, nq, 4, Ls);
         eri_batch_run(h, la, lb, lc, ld, nq, quartets, out);
     });
 }
@@ -1720,13 +1742,7 @@ int qcg_eri3_batch(qcg_handle* h, int la, int lb, int lc, long long nt, const in
         if (nt == 0) return;
         require(triples && out, "null argument");
         const int Ls[3] = {la, lb, lc};
-        for (long long t = 0; t < nt; ++t)
-            for (int x = 0; x < 3; ++x)
-            {
-                const int sh = triples[3 * t + x];
-                require(sh >= 0 && sh < h->nshell, "shell index out of range");
-                require(h->L[sh] == Ls[x], "shell angular momentum does not match the class");
-            }
+        check_shell_rows(h, triples, nt, 3, Ls);
         const int U = h->nshell;
         const bool direct = pair_class(la, lb) >= pair_class(lc, 0);
         std::vector<int> q(4 * (size_t)nt);
