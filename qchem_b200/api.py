@@ -41,7 +41,7 @@ EXPORTS = ["qcg_basis_create", "qcg_destroy", "qcg_last_error", "qcg_set_stream"
            "qcg_mlp_nparams", "qcg_mlp_params", "qcg_mlp_set_params", "qcg_mlp_forward", "qcg_mlp_loss_grad",
            "qcg_mlp_adam", "qcg_basis_create_batch", "qcg_nmol", "qcg_mol_nbf", "qcg_one_electron_batch",
            "qcg_rhf_batch", "qcg_set_graphs", "qcg_set_shard", "qcg_autotune_jk", "qcg_eri3_batch",
-           "qcg_nbf_spherical", "qcg_spherical_transform", "qcg_fock_jk_spherical"]
+           "qcg_nbf_spherical", "qcg_spherical_transform", "qcg_fock_jk_spherical", "qcg_release_cache"]
 
 
 class QcgError(RuntimeError):
@@ -93,6 +93,8 @@ def lib():
     L.qcg_rhf_batch.argtypes = [vp, P(i32), P(f64), P(f64), P(i32), P(ScfParams), P(ScfResult), P(f64)]
     L.qcg_destroy.argtypes = [vp]
     L.qcg_destroy.restype = None
+    L.qcg_release_cache.argtypes = []
+    L.qcg_release_cache.restype = None
     L.qcg_last_error.argtypes = [vp]
     L.qcg_last_error.restype = ctypes.c_char_p
     L.qcg_set_stream.argtypes = [vp, vp]
@@ -156,6 +158,12 @@ def syev(A: np.ndarray):
     if rc != QCG_OK:
         raise QcgError(rc, "eigensolver failed")
     return w, V
+
+
+def release_cache() -> None:
+    """Free the idle device slabs, pinned staging buffers, streams and events that destroyed handles left
+    for reuse (qcg_release_cache)."""
+    lib().qcg_release_cache()
 
 
 def measure_fp64_peak(reps: int = 20):

@@ -13,6 +13,7 @@
 #include <cstring>
 #include <deque>
 #include <memory>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <type_traits>
@@ -94,6 +95,139 @@ struct DevBuf
 {
     void* p = nullptr;
     size_t bytes = 0;
+};
+
+// Idle resources of destroyed handles, kept for the next handle on the same device: device slabs, pinned
+// staging buffers, non-blocking streams and events.  Creating and destroying these costs milliseconds per
+// handle (cudaFree and cudaFreeHost synchronise the device), which is a third of a 57-function RHF; a
+// process that runs many small SCFs pays it once.  A handle hands its resources back only after
+// synchronising its streams, so nothing in the cache has work in flight.  qcg_release_cache frees the
+// cache; the cache object itself is never destroyed, so nothing is freed after the CUDA runtime is torn
+// down at exit.
+class ResourceCache
+{
+public:
+    static constexpr size_t kSlab = 8u << 20, kStage = 4u << 20;
+    static ResourceCache& get()
+    {
+        static ResourceCache* c = new ResourceCache;
+        return *c;
+    }
+    void* slab(int dev)
+    {
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            auto& v = per_[dev].slabs;
+            if (!v.empty())
+            {
+                void* p = v.back();
+                v.pop_back();
+                return p;
+            }
+        }
+        void* p = nullptr;
+        const cudaError_t e = cudaMalloc(&p, kSlab);
+        if (e != cudaSuccess) throw Error{QCG_ERR_ALLOC, std::string("cudaMalloc: ") + cudaGetErrorString(e)};
+        return p;
+    }
+    char* stage()
+    {
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            if (!stages_.empty())
+            {
+                char* p = stages_.back();
+                stages_.pop_back();
+                return p;
+            }
+        }
+        char* p = nullptr;
+        CK(cudaMallocHost(&p, kStage));
+        return p;
+    }
+    cudaStream_t stream(int dev)
+    {
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            auto& v = per_[dev].streams;
+            if (!v.empty())
+            {
+                cudaStream_t s = v.back();
+                v.pop_back();
+                return s;
+            }
+        }
+        cudaStream_t s = nullptr;
+        CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        return s;
+    }
+    // timing: an event that can time (cudaEventElapsedTime); otherwise created with cudaEventDisableTiming
+    cudaEvent_t event(int dev, bool timing)
+    {
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            auto& v = timing ? per_[dev].tevents : per_[dev].sevents;
+            if (!v.empty())
+            {
+                cudaEvent_t e = v.back();
+                v.pop_back();
+                return e;
+            }
+        }
+        cudaEvent_t e = nullptr;
+        CK(timing ? cudaEventCreate(&e) : cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        return e;
+    }
+    void give_slab(int dev, void* p)
+    {
+        std::lock_guard<std::mutex> g(mu_);
+        per_[dev].slabs.push_back(p);
+    }
+    void give_stage(char* p)
+    {
+        std::lock_guard<std::mutex> g(mu_);
+        stages_.push_back(p);
+    }
+    void give_stream(int dev, cudaStream_t s)
+    {
+        std::lock_guard<std::mutex> g(mu_);
+        per_[dev].streams.push_back(s);
+    }
+    void give_event(int dev, cudaEvent_t e, bool timing)
+    {
+        std::lock_guard<std::mutex> g(mu_);
+        (timing ? per_[dev].tevents : per_[dev].sevents).push_back(e);
+    }
+    // frees everything idle (resources of live handles are not in the cache)
+    void release_all()
+    {
+        std::lock_guard<std::mutex> g(mu_);
+        int cur = 0;
+        cudaGetDevice(&cur);
+        for (auto& kv : per_)
+        {
+            cudaSetDevice(kv.first);
+            for (void* p : kv.second.slabs) cudaFree(p);
+            for (cudaStream_t s : kv.second.streams) cudaStreamDestroy(s);
+            for (cudaEvent_t e : kv.second.tevents) cudaEventDestroy(e);
+            for (cudaEvent_t e : kv.second.sevents) cudaEventDestroy(e);
+        }
+        per_.clear();
+        cudaSetDevice(cur);
+        for (char* p : stages_) cudaFreeHost(p);
+        stages_.clear();
+    }
+
+private:
+    struct PerDevice
+    {
+        std::vector<void*> slabs;
+        std::vector<cudaStream_t> streams;
+        std::vector<cudaEvent_t> tevents, sevents;
+    };
+    std::mutex mu_;
+    std::unordered_map<int, PerDevice> per_;
+    std::vector<char*> stages_;
 };
 
 }   // namespace
@@ -198,11 +332,11 @@ struct qcg_handle
     // 8 MiB slabs, so that setting up and destroying a handle costs a handful of cudaMalloc/cudaFree
     // calls instead of hundreds; releasing a slab piece is a no-op until the handle goes.  Larger buffers
     // have their own allocation.
-    static constexpr size_t kSlab = 8u << 20, kSmallMax = 1u << 20;
+    static constexpr size_t kSlab = ResourceCache::kSlab, kSmallMax = 1u << 20;
     std::vector<DevBuf> slabs;
     size_t slab_used = kSlab;
     // pinned staging for uploads of host vectors (asynchronous copies; reused after a stream sync)
-    static constexpr size_t kStage = 4u << 20;
+    static constexpr size_t kStage = ResourceCache::kStage;
     char* stage = nullptr;
     size_t stage_used = 0;
 
@@ -237,7 +371,7 @@ struct qcg_handle
             {
                 if (slab_used + bytes > kSlab)
                 {
-                    slabs.push_back({raw_alloc(kSlab), kSlab});
+                    slabs.push_back({ResourceCache::get().slab(device), kSlab});
                     slab_used = 0;
                 }
                 p = (char*)slabs.back().p + slab_used;
@@ -285,7 +419,7 @@ struct qcg_handle
         }
         if (!stage)
         {
-            CK(cudaMallocHost(&stage, kStage));
+            stage = ResourceCache::get().stage();
             stage_used = 0;
         }
         if (stage_used + bytes > kStage)
@@ -298,30 +432,57 @@ struct qcg_handle
         stage_used = (stage_used + bytes + 255) & ~(size_t)255;
         return d;
     }
+    // streams and events come from the process-wide cache and go back to it, idle, when the handle goes
+    cudaStream_t new_stream() { return ResourceCache::get().stream(device); }
+    cudaEvent_t new_event(bool timing) { return ResourceCache::get().event(device, timing); }
     ~qcg_handle()
     {
         if (stream) cudaStreamSynchronize(stream);
         if (copy_stream) cudaStreamSynchronize(copy_stream);
+        for (int k = 0; k < kSide; ++k)
+            if (side[k]) cudaStreamSynchronize(side[k]);
+        if (own_stream) cudaStreamSynchronize(own_stream);
         drop_graphs();
         for (auto& a : allocs) cudaFree(a.p);
-        for (auto& a : slabs) cudaFree(a.p);
-        if (stage) cudaFreeHost(stage);
-        if (ev0) cudaEventDestroy(ev0);
-        if (ev1) cudaEventDestroy(ev1);
-        if (ev2) cudaEventDestroy(ev2);
-        if (fork) cudaEventDestroy(fork);
+        // a handle whose context failed gives nothing back: its resources may be unusable
+        const bool healthy = cudaGetLastError() == cudaSuccess;
+        auto& rc = ResourceCache::get();
+        auto give_event = [&](cudaEvent_t e, bool timing) {
+            if (!e) return;
+            if (healthy) rc.give_event(device, e, timing);
+            else cudaEventDestroy(e);
+        };
+        auto give_stream = [&](cudaStream_t s) {
+            if (!s) return;
+            if (healthy) rc.give_stream(device, s);
+            else cudaStreamDestroy(s);
+        };
+        for (auto& a : slabs)
+        {
+            if (healthy) rc.give_slab(device, a.p);
+            else cudaFree(a.p);
+        }
+        if (stage)
+        {
+            if (healthy) rc.give_stage(stage);
+            else cudaFreeHost(stage);
+        }
+        give_event(ev0, true);
+        give_event(ev1, true);
+        give_event(ev2, true);
+        give_event(fork, false);
         for (int k = 0; k < 2; ++k)
         {
-            if (hb_done[k]) cudaEventDestroy(hb_done[k]);
-            if (hb_free[k]) cudaEventDestroy(hb_free[k]);
+            give_event(hb_done[k], false);
+            give_event(hb_free[k], false);
         }
-        if (copy_stream) cudaStreamDestroy(copy_stream);
+        give_stream(copy_stream);
         for (int k = 0; k < kSide; ++k)
         {
-            if (join[k]) cudaEventDestroy(join[k]);
-            if (side[k]) cudaStreamDestroy(side[k]);
+            give_event(join[k], false);
+            give_stream(side[k]);
         }
-        if (own_stream) cudaStreamDestroy(own_stream);
+        give_stream(own_stream);
     }
 };
 
@@ -1235,9 +1396,9 @@ void jk_device(qcg_handle* h, const double* dD, double* dJ, double* dK, int flag
     }
     if (!h->ev0)
     {
-        CK(cudaEventCreate(&h->ev0));
-        CK(cudaEventCreate(&h->ev1));
-        CK(cudaEventCreate(&h->ev2));
+        h->ev0 = h->new_event(true);
+        h->ev1 = h->new_event(true);
+        h->ev2 = h->new_event(true);
     }
     CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
     if (!(flags & QCG_JK_SKIP_VALIDATION))
@@ -1251,11 +1412,11 @@ void jk_device(qcg_handle* h, const double* dD, double* dJ, double* dK, int flag
     }
     if (!h->fork)
     {
-        CK(cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming));
+        h->fork = h->new_event(false);
         for (int s = 0; s < qcg_handle::kSide; ++s)
         {
-            CK(cudaStreamCreateWithFlags(&h->side[s], cudaStreamNonBlocking));
-            CK(cudaEventCreateWithFlags(&h->join[s], cudaEventDisableTiming));
+            h->side[s] = h->new_stream();
+            h->join[s] = h->new_event(false);
         }
     }
     // the build: zero J'/K', class kernels over the side streams, symmetrisation (timing events only
@@ -1479,7 +1640,7 @@ int qcg_basis_create_batch(const int* shell_L, const int* shell_nprim, const dou
         }
         CK(cudaGetDevice(&h->device));
         CK(cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, h->device));
-        CK(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
+        h->own_stream = h->new_stream();
         h->stream = h->own_stream;
         const char* ug = std::getenv("QCG_GRAPHS");   // 1: replay repeated J/K builds as CUDA graphs
         h->use_graphs = ug && ug[0] == '1';
@@ -1522,6 +1683,8 @@ int qcg_basis_create_batch(const int* shell_L, const int* shell_nprim, const dou
 }
 
 void qcg_destroy(qcg_handle* h) { delete h; }
+
+void qcg_release_cache(void) { ResourceCache::get().release_all(); }
 
 const char* qcg_last_error(const qcg_handle* h) { return h ? h->last_error.c_str() : "null handle"; }
 
@@ -1664,11 +1827,11 @@ void eri_batch_run(qcg_handle* h, int la, int lb, int lc, int ld, long long nq, 
         const size_t qbytes = (size_t)4 * chunk * sizeof(int), obytes = (size_t)chunk * blk * sizeof(T);
         if (!h->copy_stream)
         {
-            CK(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+            h->copy_stream = h->new_stream();
             for (int b = 0; b < 2; ++b)
             {
-                CK(cudaEventCreateWithFlags(&h->hb_done[b], cudaEventDisableTiming));
-                CK(cudaEventCreateWithFlags(&h->hb_free[b], cudaEventDisableTiming));
+                h->hb_done[b] = h->new_event(false);
+                h->hb_free[b] = h->new_event(false);
             }
         }
         for (int b = 0; b < 2; ++b)
