@@ -122,6 +122,7 @@ def lib():
     L.qcg_scf_default_params.restype = None
     L.qcg_rhf.argtypes = [vp, i32, P(f64), P(f64), i32, P(ScfParams), P(ScfResult), P(f64)]
     L.qcg_internal_syev.argtypes = [i32, P(f64), P(f64), P(f64)]
+    L.qcg_internal_syev_lowest.argtypes = [i32, P(f64), i32, P(f64), P(f64)]
     L.qcg_measure_fp64_peak.argtypes = [i32, P(f64), P(f64)]
     L.qcg_measure_fp32_peak.argtypes = [i32, P(f64), P(f64)]
     f32 = ctypes.c_float
@@ -158,6 +159,18 @@ def syev(A: np.ndarray):
     if rc != QCG_OK:
         raise QcgError(rc, "eigensolver failed")
     return w, V
+
+
+def syev_lowest(A: np.ndarray, k: int):
+    """The SCF step's partial host eigensolver (exposed for tests): all eigenvalues and the eigenvectors of
+    the k lowest (the first k columns of V)."""
+    A = _f64(A)
+    n = A.shape[0]
+    w, V = np.zeros(n), np.zeros((n, n))
+    rc = lib().qcg_internal_syev_lowest(n, _p(A), int(k), _p(w), _p(V))
+    if rc != QCG_OK:
+        raise QcgError(rc, "eigensolver failed")
+    return w, V[:, :k]
 
 
 def release_cache() -> None:

@@ -683,6 +683,246 @@ void syev(int n, const double* Ain, double* w, double* V)
     }
 }
 
+// The lowest k eigenpairs of a symmetric n x n matrix: all n eigenvalues in w (ascending) and the
+// eigenvectors of the k lowest in the first k columns of V (row-major n x n; the other columns are left
+// as they are).  The SCF step needs only the occupied orbitals, so this skips the two O(n^3) parts of
+// syev that produce the rest: forming Q and accumulating the QR rotations into it.
+//   1. Householder reduction T = Q^T A Q, Q = H_0 H_1 ... H_{n-3}, keeping the reflectors (v_j, beta_j);
+//   2. all eigenvalues of T by the implicit QR sweeps of syev, without vectors (O(n^2));
+//   3. eigenvectors x of T for the k lowest eigenvalues by inverse iteration (tridiagonal LU with partial
+//      pivoting, three solves from a fixed start vector), re-orthogonalised by modified Gram-Schmidt
+//      inside clusters of eigenvalues closer than 1e-3 ||T||, with equal eigenvalues pulled apart by
+//      10 eps ||T|| (the scheme of LAPACK's stein);
+//   4. v = H_0 (H_1 (... (H_{n-3} x))).
+// Each vector's tridiagonal residual and the vectors' orthonormality are checked; if either is off by
+// more than 1e-10 relative, the full solver runs instead.
+void syev_lowest(int n, const double* Ain, int k, double* w, double* V)
+{
+    if (k >= n || n < 3)
+    {
+        syev(n, Ain, w, V);
+        return;
+    }
+    if (k <= 0)
+    {
+        std::vector<double> Vt((size_t)n * n);
+        syev(n, Ain, w, Vt.data());
+        return;
+    }
+    std::vector<double> T(Ain, Ain + (size_t)n * n), R((size_t)n * n, 0.0), beta(n, 0.0), v(n), pv(n), wv(n);
+    auto t = [&](int i, int j) -> double& { return T[(size_t)i * n + j]; };
+    const bool par = n >= 192;
+    for (int j = 0; j + 2 < n; ++j)
+    {
+        double xn = 0.0;
+        for (int i = j + 1; i < n; ++i) xn += t(i, j) * t(i, j);
+        xn = std::sqrt(xn);
+        if (xn == 0.0) continue;
+        const double alpha = t(j + 1, j) > 0 ? -xn : xn;
+        for (int i = j + 1; i < n; ++i) v[i] = t(i, j);
+        v[j + 1] -= alpha;
+        double vv = 0.0;
+        for (int i = j + 1; i < n; ++i) vv += v[i] * v[i];
+        if (vv == 0.0) continue;
+        const double b = 2.0 / vv;
+#pragma omp parallel for schedule(static) if (par && n - j > 96)
+        for (int i = j + 1; i < n; ++i)
+        {
+            const double* ti = &t(i, 0);
+            double s = 0.0;
+            for (int c = j + 1; c < n; ++c) s += ti[c] * v[c];
+            pv[i] = b * s;
+        }
+        double pdv = 0.0;
+        for (int i = j + 1; i < n; ++i) pdv += pv[i] * v[i];
+        for (int i = j + 1; i < n; ++i) wv[i] = pv[i] - 0.5 * b * pdv * v[i];
+#pragma omp parallel for schedule(static) if (par && n - j > 96)
+        for (int i = j + 1; i < n; ++i)
+        {
+            double* ti = &t(i, 0);
+            const double vi = v[i], wi = wv[i];
+            for (int c = j + 1; c < n; ++c) ti[c] -= vi * wv[c] + wi * v[c];
+        }
+        t(j + 1, j) = t(j, j + 1) = alpha;
+        for (int i = j + 2; i < n; ++i) t(i, j) = t(j, i) = 0.0;
+        for (int i = j + 1; i < n; ++i) R[(size_t)j * n + i] = v[i];
+        beta[j] = b;
+    }
+    std::vector<double> d(n), e(n, 0.0);
+    for (int i = 0; i < n; ++i) d[i] = t(i, i);
+    for (int i = 0; i + 1 < n; ++i) e[i] = t(i + 1, i);
+    double tnorm = 0.0;
+    for (int i = 0; i < n; ++i)
+        tnorm = std::max(tnorm, std::fabs(d[i]) + std::fabs(e[i]) + (i > 0 ? std::fabs(e[i - 1]) : 0.0));
+    // eigenvalues: the QR sweeps of syev on the band of T, no vectors
+    auto rotate = [&](int j, double c, double s, int lo, int hi) {
+        for (int q = lo; q <= hi; ++q)
+        {
+            const double a = t(j, q), b = t(j + 1, q);
+            t(j, q) = c * a + s * b;
+            t(j + 1, q) = -s * a + c * b;
+        }
+        for (int q = lo; q <= hi; ++q)
+        {
+            const double a = t(q, j), b = t(q, j + 1);
+            t(q, j) = c * a + s * b;
+            t(q, j + 1) = -s * a + c * b;
+        }
+    };
+    const double eps = 1e-15;
+    int m = n - 1, steps = 0;
+    while (m > 0)
+    {
+        if (std::fabs(t(m, m - 1)) <= eps * (std::fabs(t(m, m)) + std::fabs(t(m - 1, m - 1))))
+        {
+            t(m, m - 1) = t(m - 1, m) = 0.0;
+            --m;
+            continue;
+        }
+        int l = m - 1;
+        while (l > 0 && std::fabs(t(l, l - 1)) > eps * (std::fabs(t(l, l)) + std::fabs(t(l - 1, l - 1)))) --l;
+        if (++steps > 60 * n) throw Error{QCG_ERR_NOCONV, "eigensolver did not converge"};
+        const double a = t(m - 1, m - 1), b = t(m, m - 1), c2 = t(m, m);
+        const double delta = 0.5 * (a - c2);
+        const double mu = delta == 0.0 ? c2 - std::fabs(b)
+                                       : c2 - b * b / (delta + (delta > 0 ? 1.0 : -1.0) * std::hypot(delta, b));
+        double x = t(l, l) - mu, z = t(l + 1, l);
+        for (int j = l; j < m; ++j)
+        {
+            const double r = std::sqrt(x * x + z * z);
+            const double c = r == 0.0 ? 1.0 : x / r, s = r == 0.0 ? 0.0 : z / r;
+            rotate(j, c, s, std::max(l, j - 1), std::min(m, j + 2));
+            if (j + 1 < m)
+            {
+                x = t(j + 1, j);
+                z = t(j + 2, j);
+            }
+        }
+    }
+    for (int i = 0; i < n; ++i) w[i] = t(i, i);
+    std::sort(w, w + n);
+    // inverse iteration on the tridiagonal (d, e)
+    const double ulp = 2.220446049250313e-16;
+    const double sep = 10.0 * ulp * tnorm, ortol = 1e-3 * tnorm;
+    std::vector<double> X((size_t)k * n), u0(n), u1(n), u2(n), mult(n), y(n);
+    std::vector<char> swp(n);
+    double sigma_prev = 0.0;
+    int j0 = 0;
+    for (int j = 0; j < k; ++j)
+    {
+        double sigma = w[j];
+        if (j == 0 || w[j] - w[j - 1] > ortol) j0 = j;
+        else if (sigma - sigma_prev < sep) sigma = sigma_prev + sep;
+        sigma_prev = sigma;
+        // LU of T - sigma I with partial pivoting: row i of U holds u0 (diagonal), u1, u2 (two above)
+        double a = d[0] - sigma, b = e[0], c = 0.0;
+        for (int i = 0; i + 1 < n; ++i)
+        {
+            const double ra = e[i], rb = d[i + 1] - sigma, rc = i + 2 < n ? e[i + 1] : 0.0;
+            if (std::fabs(ra) > std::fabs(a))
+            {
+                swp[i] = 1;
+                u0[i] = ra; u1[i] = rb; u2[i] = rc;
+                const double f = a / ra;
+                mult[i] = f;
+                a = b - f * rb;
+                b = c - f * rc;
+            }
+            else
+            {
+                swp[i] = 0;
+                u0[i] = a; u1[i] = b; u2[i] = c;
+                const double f = a == 0.0 ? 0.0 : ra / a;
+                mult[i] = f;
+                a = rb - f * b;
+                b = rc - f * c;
+            }
+            c = 0.0;
+        }
+        u0[n - 1] = a;
+        for (int i = 0; i < n; ++i)
+            if (std::fabs(u0[i]) < ulp * tnorm) u0[i] = u0[i] < 0 ? -ulp * tnorm : ulp * tnorm;
+        double* xj = &X[(size_t)j * n];
+        // fixed start vector with no special structure
+        uint64_t st = 0x9E3779B97F4A7C15ULL * (uint64_t)(j + 1);
+        for (int i = 0; i < n; ++i)
+        {
+            st = st * 6364136223846793005ULL + 1442695040888963407ULL;
+            xj[i] = (double)(st >> 11) * (1.0 / 9007199254740992.0) - 0.5;
+        }
+        for (int it = 0; it < 3; ++it)
+        {
+            for (int i = 0; i < n; ++i) y[i] = xj[i];
+            for (int i = 0; i + 1 < n; ++i)
+            {
+                if (swp[i]) std::swap(y[i], y[i + 1]);
+                y[i + 1] -= mult[i] * y[i];
+            }
+            for (int i = n - 1; i >= 0; --i)
+            {
+                double s = y[i];
+                if (i + 1 < n) s -= u1[i] * y[i + 1];
+                if (i + 2 < n) s -= u2[i] * y[i + 2];
+                y[i] = s / u0[i];
+            }
+            for (int p = j0; p < j; ++p)
+            {
+                const double* xp = &X[(size_t)p * n];
+                double dot = 0.0;
+                for (int i = 0; i < n; ++i) dot += xp[i] * y[i];
+                for (int i = 0; i < n; ++i) y[i] -= dot * xp[i];
+            }
+            double nrm = 0.0;
+            for (int i = 0; i < n; ++i) nrm += y[i] * y[i];
+            nrm = std::sqrt(nrm);
+            if (!(nrm > 0.0) || !std::isfinite(nrm)) break;
+            for (int i = 0; i < n; ++i) xj[i] = y[i] / nrm;
+        }
+    }
+    // self-check: tridiagonal residuals and orthonormality
+    bool ok = true;
+    for (int j = 0; j < k && ok; ++j)
+    {
+        const double* xj = &X[(size_t)j * n];
+        double res = 0.0, nrm = 0.0;
+        for (int i = 0; i < n; ++i)
+        {
+            double r = (d[i] - w[j]) * xj[i];
+            if (i > 0) r += e[i - 1] * xj[i - 1];
+            if (i + 1 < n) r += e[i] * xj[i + 1];
+            res = std::max(res, std::fabs(r));
+            nrm += xj[i] * xj[i];
+        }
+        ok = std::isfinite(res) && res <= 1e-10 * std::max(tnorm, 1e-300) && std::fabs(nrm - 1.0) <= 1e-10;
+        for (int p = 0; p < j && ok; ++p)
+        {
+            double dot = 0.0;
+            for (int i = 0; i < n; ++i) dot += X[(size_t)p * n + i] * xj[i];
+            ok = std::fabs(dot) <= 1e-10;
+        }
+    }
+    if (!ok)
+    {
+        syev(n, Ain, w, V);
+        return;
+    }
+    // back-transformation v = H_0 (... (H_{n-3} x))
+    for (int j = 0; j < k; ++j)
+    {
+        double* xj = &X[(size_t)j * n];
+        for (int q = n - 3; q >= 0; --q)
+        {
+            if (beta[q] == 0.0) continue;
+            const double* rq = &R[(size_t)q * n];
+            double s = 0.0;
+            for (int i = q + 1; i < n; ++i) s += rq[i] * xj[i];
+            s *= beta[q];
+            for (int i = q + 1; i < n; ++i) xj[i] -= s * rq[i];
+        }
+        for (int i = 0; i < n; ++i) V[(size_t)i * n + j] = xj[i];
+    }
+}
+
 // C = op(A) op(B), n x n, row-major
 void gemm(int n, const double* A, bool ta, const double* B, bool tb, double* C)
 {
@@ -1037,7 +1277,9 @@ struct ScfCore
     // aufbau density of an orthonormal-basis Fock matrix, back in the AO basis (exactly symmetric)
     void diag_fill(const std::vector<double>& Fo)
     {
-        xsyev(Fo.data(), w.data(), Up.data());
+        // only the occupied eigenvectors enter the density
+        if (gl) gl->syev(n, Fo.data(), w.data(), Up.data());
+        else syev_lowest(n, Fo.data(), nocc, w.data(), Up.data());
         if (gl)
             gl->occ_density(n, nocc, Up.data(), Dp.data());
         else
@@ -2693,6 +2935,20 @@ int qcg_internal_syev(int n, const double* A, double* w, double* V)
     try
     {
         syev(n, A, w, V);
+        return QCG_OK;
+    }
+    catch (const Error& e)
+    {
+        return e.code;
+    }
+}
+
+// test hook: the SCF step's partial eigensolver (all eigenvalues, the k lowest eigenvectors)
+int qcg_internal_syev_lowest(int n, const double* A, int k, double* w, double* V)
+{
+    try
+    {
+        syev_lowest(n, A, k, w, V);
         return QCG_OK;
     }
     catch (const Error& e)

@@ -52,6 +52,44 @@ def test_syev_degenerate_and_diagonal():
     np.testing.assert_allclose(w, [0, 0, 0, 4], atol=1e-14)
 
 
+def _check_lowest(A, k):
+    w, V = api.syev_lowest(A, k)
+    wr, Vr = np.linalg.eigh(A)
+    scale = max(1.0, np.abs(wr).max())
+    np.testing.assert_allclose(w, wr, atol=1e-11 * scale)
+    assert V.shape == (A.shape[0], k)
+    np.testing.assert_allclose(V.T @ V, np.eye(k), atol=1e-11)
+    np.testing.assert_allclose(A @ V, V * w[:k], atol=1e-10 * scale)
+    # the occupied-subspace projector, which is what the SCF density uses, where the spectrum has a gap
+    if k < A.shape[0] and wr[k] - wr[k - 1] > 1e-6 * scale:
+        np.testing.assert_allclose(V @ V.T, Vr[:, :k] @ Vr[:, :k].T, atol=1e-10)
+
+
+def test_syev_lowest_matches_numpy():
+    rng = np.random.default_rng(7)
+    for n, k in ((3, 1), (5, 2), (57, 5), (120, 17), (225, 60), (57, 56), (57, 57)):
+        A = rng.normal(size=(n, n))
+        _check_lowest(A + A.T, k)
+
+
+def test_syev_lowest_degenerate_spectra():
+    rng = np.random.default_rng(8)
+    n = 40
+    Q, _ = np.linalg.qr(rng.normal(size=(n, n)))
+    # exactly repeated lowest eigenvalues (a 3-fold and a 2-fold level), then a gap
+    lam = np.concatenate([[-5.0] * 3, [-2.0] * 2, np.linspace(1, 30, n - 5)])
+    A = (Q * lam) @ Q.T
+    A = 0.5 * (A + A.T)
+    for k in (3, 5, 7):
+        _check_lowest(A, k)
+    # diagonal and block-diagonal inputs (the reduction is the identity), and the zero matrix
+    _check_lowest(np.diag([3.0, 1.0, 2.0, 1.0, 0.5]), 2)
+    _check_lowest(np.kron(np.eye(4), np.array([[2.0, 1.0], [1.0, 2.0]])), 4)
+    w, V = api.syev_lowest(np.zeros((6, 6)), 2)
+    np.testing.assert_allclose(w, 0.0)
+    np.testing.assert_allclose(V.T @ V, np.eye(2), atol=1e-12)
+
+
 def test_even_tempered_layout():
     mol = W.water()
     sh = B.even_tempered(mol)
