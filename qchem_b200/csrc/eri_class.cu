@@ -45,12 +45,21 @@ struct Cls
     static constexpr bool kRShared = gen::QCG_CAT(kRShared, QCG_CLASS);
     static constexpr bool kChunked = gen::QCG_CAT(kChunked, QCG_CLASS);
     static constexpr int kRSize = gen::QCG_CAT(kRSize, QCG_CLASS);
+    static constexpr int kNChunk = gen::QCG_CAT(kNChunk, QCG_CLASS);
     template <class RT, class Sink, bool LOCKSTEP = false>
     static __device__ __forceinline__ void quartet(const PrimPairData& ab, const PrimPairData& cd,
                                                    const double* __restrict__ bt, RT* __restrict__ rs, int stride,
                                                    Sink& sink)
     {
         gen::QCG_CAT(prim_quartet_, QCG_CLASS)<RT, Sink, LOCKSTEP>(ab, cd, bt, rs, stride, sink);
+    }
+    // ket-component chunk c of the quartet alone, after rebuilding Boys and R (chunked classes)
+    template <class RT, class Sink>
+    static __device__ __forceinline__ void quartet_chunk(int c, const PrimPairData& ab, const PrimPairData& cd,
+                                                         const double* __restrict__ bt, RT* __restrict__ rs,
+                                                         int stride, Sink& sink)
+    {
+        gen::QCG_CAT(prim_quartet_chunk_, QCG_CLASS)<RT, Sink>(c, ab, cd, bt, rs, stride, sink);
     }
 };
 
@@ -116,6 +125,23 @@ void QCG_NAME(launch_jk)(const JKWorkDev& w, const PairListDev& bra, const PairL
 {
     const long long span = w.gend - w.gbeg;
     if (span <= 0) return;
+    if constexpr (Cls::kChunked)
+    {
+        // at most one block of quartets per SM: a plain launch would leave most of the GPU idle while each
+        // lane runs a whole quartet's code, so the quartets' ket-component chunks go to separate warps
+        if (span <= (long long)nsm * kThreads)
+        {
+            auto ks = jk_split_kernel<Cls, kThreads, Real>;
+            static bool split_ready = false;
+            if (!split_ready && kSmem > 48 * 1024)
+                cudaFuncSetAttribute(ks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem);
+            split_ready = true;
+            const long long items = ((span + 31) & ~31LL) * Cls::kNChunk;
+            const long long blocks = (items + kThreads - 1) / kThreads;
+            ks<<<(unsigned)blocks, kThreads, kSmem, st>>>(w, bra, ket, P, f0, D, J, K, n, boys);
+            return;
+        }
+    }
     auto k = jk_kernel<Cls, kThreads, Real>;
     prepare(k);
     // quartets per lane run: enough threads for the whole GPU first, longer runs only for large builds

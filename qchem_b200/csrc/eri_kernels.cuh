@@ -212,6 +212,7 @@ struct JKSink
     double kac[NA], kbc[NB], kad[NA], kbd[NB];
     double dls, jcd;
     double dbs[NB], das[NA], dbl[NB], dal[NA];
+    int row_la = -1;   // ket row (c component) whose K'[., la] sums are still in registers
 
     // a new bra pair: J'[a b] partial sums start from zero
     __device__ __forceinline__ void set_bra(int fa_, int fb_)
@@ -228,6 +229,7 @@ struct JKSink
     __device__ __forceinline__ void ket_begin(int ic, int id)
     {
         const int la = fc + ic, si = fd + id;
+        row_la = la;
         dls = __ldg(D + (size_t)la * n + si);
         jcd = 0.0;
 #pragma unroll
@@ -269,7 +271,18 @@ struct JKSink
             for (int k = 0; k < NA; ++k) { atomicAdd(K + (size_t)(fa + k) * n + la, kac[k]); kac[k] = 0.0; }
 #pragma unroll
             for (int k = 0; k < NB; ++k) { atomicAdd(K + (size_t)(fb + k) * n + la, kbc[k]); kbc[k] = 0.0; }
+            row_la = -1;
         }
+    }
+    // a chunk of ket components that ends inside a ket row leaves that row's K'[., la] sums in registers
+    __device__ __forceinline__ void flush_k_row()
+    {
+        if (row_la < 0) return;
+#pragma unroll
+        for (int k = 0; k < NA; ++k) { atomicAdd(K + (size_t)(fa + k) * n + row_la, kac[k]); kac[k] = 0.0; }
+#pragma unroll
+        for (int k = 0; k < NB; ++k) { atomicAdd(K + (size_t)(fb + k) * n + row_la, kbc[k]); kbc[k] = 0.0; }
+        row_la = -1;
     }
     // the bra pair is done (or the lane's run ends): flush J'[a b]
     __device__ __forceinline__ void flush_bra()
@@ -285,6 +298,30 @@ struct JKSink
     }
 };
 
+// true when quartet (bra pair i, ket pair j) is skipped: its density-weighted bound is below the density
+// threshold, or its bound lies outside this launch's precision band [w.lo, w.hi)
+__device__ __forceinline__ bool jk_skip(const JKWorkDev& w, const PairListDev& bra, const PairListDev& ket, int i,
+                                        int j, int sa, int sb, int sc, int sd)
+{
+    const bool banded = w.lo > 0.0 || w.hi < 1e300;
+    if (w.dmax)
+    {
+        const double* M = w.dmax;
+        const int ns = w.nshell;
+        double m = fmax(M[sa * ns + sb], M[sc * ns + sd]);
+        m = fmax(m, fmax(M[sa * ns + sc], M[sa * ns + sd]));
+        m = fmax(m, fmax(M[sb * ns + sc], M[sb * ns + sd]));
+        const double bnd = bra.Q[i] * ket.Q[j] * m;
+        return bnd < w.dthr || (banded && (bnd < w.lo || bnd >= w.hi));
+    }
+    if (banded)
+    {
+        const double bnd = bra.Q[i] * ket.Q[j];
+        return bnd < w.lo || bnd >= w.hi;
+    }
+    return false;
+}
+
 // Each lane walks RUN quartets spaced one warp apart (g = base + lane + 32 k), so consecutive quartets of a
 // lane usually share the bra pair: the bra pair is found by one binary search per run and then advanced,
 // and the bra-side J' sums stay in registers until the bra pair changes.  RUN is chosen by the launcher
@@ -299,7 +336,6 @@ __global__ void __launch_bounds__(THREADS) jk_kernel(JKWorkDev w, PairListDev br
                                                      const double* __restrict__ boys_table, int RUN)
 {
     RT* rs = r_slice<RT>();
-    const bool banded = w.lo > 0.0 || w.hi < 1e300;
     const int lane = threadIdx.x & 31;
     const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     const long long nwarp = ((long long)gridDim.x * blockDim.x) >> 5;
@@ -351,21 +387,7 @@ __global__ void __launch_bounds__(THREADS) jk_kernel(JKWorkDev w, PairListDev br
             }
             const int j = (w.kbase ? w.kbase[i] : 0) + (int)(g - w.offs[i]);
             const int sc = ket.sa[j], sd = ket.sb[j];
-            if (w.dmax)
-            {
-                const double* M = w.dmax;
-                const int ns = w.nshell;
-                double m = fmax(M[sa * ns + sb], M[sc * ns + sd]);
-                m = fmax(m, fmax(M[sa * ns + sc], M[sa * ns + sd]));
-                m = fmax(m, fmax(M[sb * ns + sc], M[sb * ns + sd]));
-                const double bnd = bra.Q[i] * ket.Q[j] * m;
-                if (bnd < w.dthr || (banded && (bnd < w.lo || bnd >= w.hi))) continue;
-            }
-            else if (banded)
-            {
-                const double bnd = bra.Q[i] * ket.Q[j];
-                if (bnd < w.lo || bnd >= w.hi) continue;
-            }
+            if (jk_skip(w, bra, ket, i, j, sa, sb, sc, sd)) continue;
             sink.fc = shell_f0[sc];
             sink.fd = shell_f0[sd];
             sink.s = (sa == sb ? 0.5 : 1.0) * (sc == sd ? 0.5 : 1.0) * ((w.same_class && i == j) ? 0.5 : 1.0);
@@ -378,6 +400,70 @@ __global__ void __launch_bounds__(THREADS) jk_kernel(JKWorkDev w, PairListDev br
                     const PrimPairData cd = load_pp(P, oj + y);
                     Cls::template quartet<RT>(ab, cd, boys_table, rs, THREADS, sink);
                 }
+            }
+        }
+        sink.flush_bra();
+    }
+}
+
+// Launches of the chunked classes with too few quartets to fill the GPU: work item t = c * span32 + q
+// (span32 = the quartet count rounded up to a multiple of 32) runs ket-component chunk c of quartet
+// w.gbeg + q.  A warp's lanes share the chunk, and the chunks of one quartet run on different warps at the
+// same time, so the launch takes about one chunk's time instead of one whole quartet's.  Each item
+// rebuilds Boys and R and digests its chunk's outputs like jk_kernel (the digestion is linear).
+template <class Cls, int THREADS, class RT>
+__global__ void __launch_bounds__(THREADS) jk_split_kernel(JKWorkDev w, PairListDev bra, PairListDev ket,
+                                                           PrimPairsDev P, const int* __restrict__ shell_f0,
+                                                           const double* __restrict__ D, double* __restrict__ J,
+                                                           double* __restrict__ K, int n,
+                                                           const double* __restrict__ boys_table)
+{
+    RT* rs = r_slice<RT>();
+    const long long span = w.gend - w.gbeg, span32 = (span + 31) & ~31LL;
+    const long long nitem = span32 * Cls::kNChunk;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nitem;
+         t += (long long)gridDim.x * blockDim.x)
+    {
+        const int c = (int)(t / span32);
+        const long long q = t - c * span32;
+        if (q >= span) continue;
+        const long long g = w.gbeg + q;
+        int lo = 0, hi = bra.n;
+        while (hi - lo > 1)
+        {
+            const int mid = (lo + hi) >> 1;
+            if (w.offs[mid] <= g) lo = mid;
+            else hi = mid;
+        }
+        const int i = lo;
+        const int j = (w.kbase ? w.kbase[i] : 0) + (int)(g - w.offs[i]);
+        const int sa = bra.sa[i], sb = bra.sb[i], sc = ket.sa[j], sd = ket.sb[j];
+        if (jk_skip(w, bra, ket, i, j, sa, sb, sc, sd)) continue;
+        JKSink<RT, Cls::LA, Cls::LB, Cls::LC, Cls::LD> sink;
+        sink.D = D; sink.J = J; sink.K = K; sink.n = n;
+        if (bra.mol)
+        {
+            const int m = bra.mol[i];
+            const long long o = w.mols.off[m];
+            sink.D = D + o;
+            sink.J = J + o;
+            sink.K = K + o;
+            sink.n = w.mols.n[m];
+        }
+        sink.set_bra(shell_f0[sa], shell_f0[sb]);
+        sink.fc = shell_f0[sc];
+        sink.fd = shell_f0[sd];
+        sink.s = (sa == sb ? 0.5 : 1.0) * (sc == sd ? 0.5 : 1.0) * ((w.same_class && i == j) ? 0.5 : 1.0);
+        const int oi = bra.ppo[i], ni = bra.npp[i], oj = ket.ppo[j], nj = ket.npp[j];
+        for (int x = 0; x < ni; ++x)
+        {
+            const PrimPairData ab = load_pp(P, oi + x);
+            for (int y = 0; y < nj; ++y)
+            {
+                const PrimPairData cd = load_pp(P, oj + y);
+                Cls::template quartet_chunk<RT>(c, ab, cd, boys_table, rs, THREADS, sink);
+                // the next primitive quartet restarts the chunk, possibly inside a different ket row
+                sink.flush_k_row();
             }
         }
         sink.flush_bra();

@@ -226,6 +226,11 @@ def gen_class(LA, LB, LC, LD, idx):
     chunk_names = []
     if chunked:
         per = max(1, CHUNK_OUTPUTS // nab)
+        w(f"constexpr int kNChunk{idx} = {(len(all_cds) + per - 1) // per};")
+    else:
+        w(f"constexpr int kNChunk{idx} = 1;")
+    if chunked:
+        per = max(1, CHUNK_OUTPUTS // nab)
         chunks = [all_cds[i:i + per] for i in range(0, len(all_cds), per)]
         for ci, cds in enumerate(chunks):
             fn = f"prim_quartet_{idx}_chunk{ci}"
@@ -267,6 +272,31 @@ def gen_class(LA, LB, LC, LD, idx):
             w("    " + s_)
         ket_blocks(LA, LB, LC, LD, all_cds, w)
     w("#undef RR")
+    w("}")
+    # chunk c alone (after Boys and R): lets several warps share one quartet's ket components when a class
+    # has too few quartets to fill the GPU; an unchunked class has the single chunk 0
+    w("template <class RT, class Sink>")
+    w(f"__device__ __forceinline__ void prim_quartet_chunk_{idx}(const int c, const PrimPairData& ab,")
+    w("    const PrimPairData& cd, const double* __restrict__ bt, RT* __restrict__ rs, const int rstride,")
+    w("    Sink& sink)")
+    w("{")
+    if chunked:
+        r_prologue(L, True, w)
+        w("    const RT bPAx = RT(ab.PAx), bPAy = RT(ab.PAy), bPAz = RT(ab.PAz);")
+        w("    const RT bPBx = RT(ab.PBx), bPBy = RT(ab.PBy), bPBz = RT(ab.PBz);")
+        w("    const RT kPAx = RT(cd.PAx), kPAy = RT(cd.PAy), kPAz = RT(cd.PAz);")
+        w("    const RT kPBx = RT(cd.PBx), kPBy = RT(cd.PBy), kPBz = RT(cd.PBz);")
+        w("    switch (c)")
+        w("    {")
+        for ci, fn in enumerate(chunk_names):
+            w(f"    case {ci}: {fn}<RT, Sink>(rs, rstride, a12b, bPAx, bPAy, bPAz, bPBx, bPBy, bPBz, a12k, kPAx, "
+              f"kPAy, kPAz, kPBx, kPBy, kPBz, lambda, sink); break;")
+        w("    default: break;")
+        w("    }")
+        w("#undef RR")
+    else:
+        w("    (void)c;")
+        w(f"    prim_quartet_{idx}<RT, Sink>(ab, cd, bt, rs, rstride, sink);")
     w("}")
     return o
 
