@@ -162,15 +162,15 @@ def syev(A: np.ndarray):
 
 
 def syev_lowest(A: np.ndarray, k: int):
-    """The SCF step's partial host eigensolver (exposed for tests): all eigenvalues and the eigenvectors of
-    the k lowest (the first k columns of V)."""
+    """The SCF step's partial host eigensolver (exposed for tests): the k lowest eigenvalues (ascending) and
+    their eigenvectors (columns)."""
     A = _f64(A)
     n = A.shape[0]
     w, V = np.zeros(n), np.zeros((n, n))
     rc = lib().qcg_internal_syev_lowest(n, _p(A), int(k), _p(w), _p(V))
     if rc != QCG_OK:
         raise QcgError(rc, "eigensolver failed")
-    return w, V[:, :k]
+    return w[:k], V[:, :k]
 
 
 def release_cache() -> None:

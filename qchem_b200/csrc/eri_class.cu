@@ -162,11 +162,27 @@ void QCG_NAME(launch_jk)(const JKWorkDev& w, const PairListDev& bra, const PairL
 #if QCG_PREC == 64
 // Schwarz diagonals exist only for the diagonal classes (X == Y)
 void QCG_CAT(launch_schwarz_, QCG_CLASS)(const PairListDev& pl, const PrimPairsDev& P, double* Q, const double* boys,
-                                         cudaStream_t st)
+                                         cudaStream_t st, int nsm)
 {
     if constexpr (kX == kY)
     {
         if (pl.n <= 0) return;
+        if constexpr (Cls::kChunked)
+        {
+            // few pairs: their diagonal quartets' chunks on separate warps (see jk_split_kernel)
+            if ((long long)pl.n <= (long long)nsm * kThreads)
+            {
+                auto ks = schwarz_split_kernel<Cls, kThreads>;
+                static bool split_ready = false;
+                if (!split_ready && kSmem64 > 48 * 1024)
+                    cudaFuncSetAttribute(ks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem64);
+                split_ready = true;
+                cudaMemsetAsync(Q, 0, (size_t)pl.n * sizeof(double), st);
+                const long long items = (((long long)pl.n + 31) & ~31LL) * Cls::kNChunk;
+                ks<<<(unsigned)((items + kThreads - 1) / kThreads), kThreads, kSmem64, st>>>(pl, P, Q, boys);
+                return;
+            }
+        }
         auto k = schwarz_kernel<Cls, kThreads>;
         prepare(k, kSmem64);
         k<<<(pl.n + kThreads - 1) / kThreads, kThreads, kSmem64, st>>>(pl, P, Q, boys);

@@ -190,6 +190,44 @@ __global__ void __launch_bounds__(THREADS) schwarz_kernel(PairListDev pl, PrimPa
     Q[i] = sqrt(m);
 }
 
+// The same for the chunked classes when they have few pairs: work item t = c * n32 + i (n32 = the pair
+// count rounded up to a multiple of 32) evaluates ket-component chunk c of pair i's diagonal quartet, whose
+// diagonal elements are exactly the chunk's (c d) = (a b) components, and merges its maximum into Q[i]
+// (zeroed by the launcher) with an atomic maximum on the bit pattern, which orders non-negative doubles.
+template <class Cls, int THREADS>
+__global__ void __launch_bounds__(THREADS) schwarz_split_kernel(PairListDev pl, PrimPairsDev P,
+                                                                double* __restrict__ Q,
+                                                                const double* __restrict__ boys_table)
+{
+    const long long n32 = ((long long)pl.n + 31) & ~31LL;
+    const long long nitem = n32 * Cls::kNChunk;
+    double* rs = r_slice<double>();
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nitem;
+         t += (long long)gridDim.x * blockDim.x)
+    {
+        const int c = (int)(t / n32);
+        const long long i = t - c * n32;
+        if (i >= pl.n) continue;
+        DiagSink<Cls::LA, Cls::LB> sink;
+#pragma unroll
+        for (int k = 0; k < DiagSink<Cls::LA, Cls::LB>::NAB; ++k) sink.acc[k] = 0.0;
+        const int o = pl.ppo[i], n = pl.npp[i];
+        for (int x = 0; x < n; ++x)
+        {
+            const PrimPairData ab = load_pp(P, o + x);
+            for (int y = 0; y < n; ++y)
+            {
+                const PrimPairData cd = load_pp(P, o + y);
+                Cls::template quartet_chunk<double>(c, ab, cd, boys_table, rs, THREADS, sink);
+            }
+        }
+        double m = 0.0;
+#pragma unroll
+        for (int k = 0; k < DiagSink<Cls::LA, Cls::LB>::NAB; ++k) m = fmax(m, fabs(sink.acc[k]));
+        atomicMax(reinterpret_cast<unsigned long long*>(Q + i), (unsigned long long)__double_as_longlong(sqrt(m)));
+    }
+}
+
 // ------------------------------------------------------------------------------------------------
 // Fused ERI + J/K digestion.  For a canonical quartet with weight w = s * (mu nu|la si),
 // s = 1/2^{[a=b]+[c=d]+[ab=cd]}, the eight permutational images reduce to

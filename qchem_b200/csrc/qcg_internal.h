@@ -87,7 +87,7 @@ using EriBatchLauncher = void (*)(const BasisDev&, const int4*, const int*, long
                                   cudaStream_t, int);
 using JKLauncher = void (*)(const JKWorkDev&, const PairListDev&, const PairListDev&, const PrimPairsDev&, const int*,
                             const double*, double*, double*, int, const double*, cudaStream_t, int);
-using SchwarzLauncher = void (*)(const PairListDev&, const PrimPairsDev&, double*, const double*, cudaStream_t);
+using SchwarzLauncher = void (*)(const PairListDev&, const PrimPairsDev&, double*, const double*, cudaStream_t, int);
 
 using EriBatch32Launcher = void (*)(const BasisDev&, const int4*, const int*, long long, float*, const double*,
                                     cudaStream_t, int);

@@ -8,7 +8,7 @@ namespace qcg {
                               cudaStream_t, int);                                                                   \
     void launch_jk_##k(const JKWorkDev&, const PairListDev&, const PairListDev&, const PrimPairsDev&, const int*,    \
                        const double*, double*, double*, int, const double*, cudaStream_t, int);                      \
-    void launch_schwarz_##k(const PairListDev&, const PrimPairsDev&, double*, const double*, cudaStream_t);      \
+    void launch_schwarz_##k(const PairListDev&, const PrimPairsDev&, double*, const double*, cudaStream_t, int);      \
     void launch_eri_batch32_##k(const BasisDev&, const int4*, const int*, long long, float*, const double*,        \
                                 cudaStream_t, int);                                                                 \
     void launch_jk32_##k(const JKWorkDev&, const PairListDev&, const PairListDev&, const PrimPairsDev&, const int*,  \

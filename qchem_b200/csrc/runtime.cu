@@ -559,24 +559,36 @@ void syev(int n, const double* Ain, double* w, double* V)
         if (vv == 0.0) continue;
         const double beta = 2.0 / vv;
         // trailing block update: A <- A - v w^T - w v^T with p = beta A v, w = p - (beta p.v / 2) v
-#pragma omp parallel for schedule(static) if (par && n - k > 96)
-        for (int i = k + 1; i < n; ++i)
-        {
+        auto matvec_row = [&](int i) {
             const double* ti = &t(i, 0);
             double s = 0.0;
+#pragma omp simd reduction(+ : s)
             for (int j = k + 1; j < n; ++j) s += ti[j] * v[j];
             pv[i] = beta * s;
+        };
+        // small problems stay out of the OpenMP runtime (entering a region costs about as much as a row)
+        if (par && n - k > 96)
+        {
+#pragma omp parallel for schedule(static)
+            for (int i = k + 1; i < n; ++i) matvec_row(i);
         }
+        else
+            for (int i = k + 1; i < n; ++i) matvec_row(i);
         double pdv = 0.0;
         for (int i = k + 1; i < n; ++i) pdv += pv[i] * v[i];
         for (int i = k + 1; i < n; ++i) wv[i] = pv[i] - 0.5 * beta * pdv * v[i];
-#pragma omp parallel for schedule(static) if (par && n - k > 96)
-        for (int i = k + 1; i < n; ++i)
-        {
+        auto update_row = [&](int i) {
             double* ti = &t(i, 0);
             const double vi = v[i], wi = wv[i];
             for (int j = k + 1; j < n; ++j) ti[j] -= vi * wv[j] + wi * v[j];
+        };
+        if (par && n - k > 96)
+        {
+#pragma omp parallel for schedule(static)
+            for (int i = k + 1; i < n; ++i) update_row(i);
         }
+        else
+            for (int i = k + 1; i < n; ++i) update_row(i);
         t(k + 1, k) = t(k, k + 1) = alpha;
         for (int i = k + 2; i < n; ++i) t(i, k) = t(k, i) = 0.0;
         // Q <- Q H, i.e. Qt <- H Qt: s_r = sum_i v_i Qt[i][r], Qt[j][r] -= beta v_j s_r
@@ -587,13 +599,18 @@ void syev(int n, const double* Ain, double* w, double* V)
             const double* qi = qt(i, 0);
             for (int r = 0; r < n; ++r) sr[r] += vi * qi[r];
         }
-#pragma omp parallel for schedule(static) if (par)
-        for (int j = k + 1; j < n; ++j)
-        {
+        auto q_row = [&](int j) {
             double* qj = qt(j, 0);
             const double f = beta * v[j];
             for (int r = 0; r < n; ++r) qj[r] -= f * sr[r];
+        };
+        if (par)
+        {
+#pragma omp parallel for schedule(static)
+            for (int j = k + 1; j < n; ++j) q_row(j);
         }
+        else
+            for (int j = k + 1; j < n; ++j) q_row(j);
     }
     // rotation G on (k,k+1): T <- G T G^T, G = [[c, s], [-s, c]]; the matching Qt <- G Qt updates of one
     // sweep are recorded and applied afterwards
@@ -617,9 +634,7 @@ void syev(int n, const double* Ain, double* w, double* V)
     constexpr int RB = 32;
     const int nblk = (n + RB - 1) / RB;
     auto apply_sweep = [&](int l, int m) {
-#pragma omp parallel for schedule(static) if (par && m - l > 32)
-        for (int blk = 0; blk < nblk; ++blk)
-        {
+        auto block = [&](int blk) {
             const int r0 = blk * RB, nr = std::min(RB, n - r0);
             double a[RB];
             const double* ql = qt(l, r0);
@@ -638,7 +653,14 @@ void syev(int n, const double* Ain, double* w, double* V)
             }
             double* qm = qt(m, r0);
             for (int r = 0; r < nr; ++r) qm[r] = a[r];
+        };
+        if (par && m - l > 32)
+        {
+#pragma omp parallel for schedule(static)
+            for (int blk = 0; blk < nblk; ++blk) block(blk);
         }
+        else
+            for (int blk = 0; blk < nblk; ++blk) block(blk);
     };
     const double eps = 1e-15;
     int m = n - 1, steps = 0;
@@ -683,30 +705,30 @@ void syev(int n, const double* Ain, double* w, double* V)
     }
 }
 
-// The lowest k eigenpairs of a symmetric n x n matrix: all n eigenvalues in w (ascending) and the
-// eigenvectors of the k lowest in the first k columns of V (row-major n x n; the other columns are left
-// as they are).  The SCF step needs only the occupied orbitals, so this skips the two O(n^3) parts of
-// syev that produce the rest: forming Q and accumulating the QR rotations into it.
+// The lowest k eigenpairs of a symmetric n x n matrix: the k lowest eigenvalues in w[0..k) (ascending)
+// and their eigenvectors in the first k columns of V (row-major n x n; the other columns are left as they
+// are).  The SCF step needs only the occupied orbitals, so this skips the O(n^3) parts of syev that
+// produce the rest: forming Q and accumulating the QR rotations into it.
 //   1. Householder reduction T = Q^T A Q, Q = H_0 H_1 ... H_{n-3}, keeping the reflectors (v_j, beta_j);
-//   2. all eigenvalues of T by the implicit QR sweeps of syev, without vectors (O(n^2));
-//   3. eigenvectors x of T for the k lowest eigenvalues by inverse iteration (tridiagonal LU with partial
-//      pivoting, three solves from a fixed start vector), re-orthogonalised by modified Gram-Schmidt
-//      inside clusters of eigenvalues closer than 1e-3 ||T||, with equal eigenvalues pulled apart by
-//      10 eps ||T|| (the scheme of LAPACK's stein);
+//   2. the k lowest eigenvalues of T by bisection on Sturm counts (negative pivots of T - x I = L D L^T),
+//      refined to the Rayleigh quotients of the vectors of step 3;
+//   3. eigenvectors x of T by inverse iteration (tridiagonal LU with partial pivoting, three solves from a
+//      fixed start vector), re-orthogonalised by modified Gram-Schmidt inside clusters of eigenvalues
+//      closer than 1e-3 ||T||, with equal eigenvalues pulled apart by 10 eps ||T|| (the scheme of
+//      LAPACK's stein);
 //   4. v = H_0 (H_1 (... (H_{n-3} x))).
 // Each vector's tridiagonal residual and the vectors' orthonormality are checked; if either is off by
 // more than 1e-10 relative, the full solver runs instead.
 void syev_lowest(int n, const double* Ain, int k, double* w, double* V)
 {
-    if (k >= n || n < 3)
+    if (k >= n || n < 3 || k <= 0)
     {
-        syev(n, Ain, w, V);
-        return;
-    }
-    if (k <= 0)
-    {
-        std::vector<double> Vt((size_t)n * n);
-        syev(n, Ain, w, Vt.data());
+        std::vector<double> wa(n), Va((size_t)n * n);
+        syev(n, Ain, wa.data(), Va.data());
+        const int kk = std::min(std::max(k, 0), n);
+        for (int j = 0; j < kk; ++j) w[j] = wa[j];
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < kk; ++j) V[(size_t)i * n + j] = Va[(size_t)i * n + j];
         return;
     }
     std::vector<double> T(Ain, Ain + (size_t)n * n), R((size_t)n * n, 0.0), beta(n, 0.0), v(n), pv(n), wv(n);
@@ -725,24 +747,37 @@ void syev_lowest(int n, const double* Ain, int k, double* w, double* V)
         for (int i = j + 1; i < n; ++i) vv += v[i] * v[i];
         if (vv == 0.0) continue;
         const double b = 2.0 / vv;
-#pragma omp parallel for schedule(static) if (par && n - j > 96)
-        for (int i = j + 1; i < n; ++i)
-        {
+        auto matvec_row = [&](int i) {
             const double* ti = &t(i, 0);
             double s = 0.0;
+#pragma omp simd reduction(+ : s)
             for (int c = j + 1; c < n; ++c) s += ti[c] * v[c];
             pv[i] = b * s;
+        };
+        // small problems stay out of the OpenMP runtime: entering a parallel region, even one whose if
+        // clause is false, costs about as much as a row of this size
+        if (par && n - j > 96)
+        {
+#pragma omp parallel for schedule(static)
+            for (int i = j + 1; i < n; ++i) matvec_row(i);
         }
+        else
+            for (int i = j + 1; i < n; ++i) matvec_row(i);
         double pdv = 0.0;
         for (int i = j + 1; i < n; ++i) pdv += pv[i] * v[i];
         for (int i = j + 1; i < n; ++i) wv[i] = pv[i] - 0.5 * b * pdv * v[i];
-#pragma omp parallel for schedule(static) if (par && n - j > 96)
-        for (int i = j + 1; i < n; ++i)
-        {
+        auto update_row = [&](int i) {
             double* ti = &t(i, 0);
             const double vi = v[i], wi = wv[i];
             for (int c = j + 1; c < n; ++c) ti[c] -= vi * wv[c] + wi * v[c];
+        };
+        if (par && n - j > 96)
+        {
+#pragma omp parallel for schedule(static)
+            for (int i = j + 1; i < n; ++i) update_row(i);
         }
+        else
+            for (int i = j + 1; i < n; ++i) update_row(i);
         t(j + 1, j) = t(j, j + 1) = alpha;
         for (int i = j + 2; i < n; ++i) t(i, j) = t(j, i) = 0.0;
         for (int i = j + 1; i < n; ++i) R[(size_t)j * n + i] = v[i];
@@ -751,58 +786,76 @@ void syev_lowest(int n, const double* Ain, int k, double* w, double* V)
     std::vector<double> d(n), e(n, 0.0);
     for (int i = 0; i < n; ++i) d[i] = t(i, i);
     for (int i = 0; i + 1 < n; ++i) e[i] = t(i + 1, i);
-    double tnorm = 0.0;
+    double tnorm = 0.0, glo = HUGE_VAL, ghi = -HUGE_VAL, emax2 = 0.0;
     for (int i = 0; i < n; ++i)
-        tnorm = std::max(tnorm, std::fabs(d[i]) + std::fabs(e[i]) + (i > 0 ? std::fabs(e[i - 1]) : 0.0));
-    // eigenvalues: the QR sweeps of syev on the band of T, no vectors
-    auto rotate = [&](int j, double c, double s, int lo, int hi) {
-        for (int q = lo; q <= hi; ++q)
-        {
-            const double a = t(j, q), b = t(j + 1, q);
-            t(j, q) = c * a + s * b;
-            t(j + 1, q) = -s * a + c * b;
-        }
-        for (int q = lo; q <= hi; ++q)
-        {
-            const double a = t(q, j), b = t(q, j + 1);
-            t(q, j) = c * a + s * b;
-            t(q, j + 1) = -s * a + c * b;
-        }
-    };
-    const double eps = 1e-15;
-    int m = n - 1, steps = 0;
-    while (m > 0)
     {
-        if (std::fabs(t(m, m - 1)) <= eps * (std::fabs(t(m, m)) + std::fabs(t(m - 1, m - 1))))
+        const double r = std::fabs(e[i]) + (i > 0 ? std::fabs(e[i - 1]) : 0.0);
+        tnorm = std::max(tnorm, std::fabs(d[i]) + r);
+        glo = std::min(glo, d[i] - r);
+        ghi = std::max(ghi, d[i] + r);
+        emax2 = std::max(emax2, e[i] * e[i]);
+    }
+    const double ulp = 2.220446049250313e-16;
+    // the k lowest eigenvalues: bisection inside the Gershgorin interval on the count of eigenvalues below x
+    const double pivmin = std::max(1e-300, 4.0 * ulp * ulp * std::max(emax2, 1e-300));
+    auto count_below = [&](double x) {
+        int cnt = 0;
+        double q = d[0] - x;
+        if (std::fabs(q) < pivmin) q = -pivmin;
+        if (q < 0) ++cnt;
+        for (int i = 1; i < n; ++i)
         {
-            t(m, m - 1) = t(m - 1, m) = 0.0;
-            --m;
-            continue;
+            q = (d[i] - x) - e[i - 1] * e[i - 1] / q;
+            if (std::fabs(q) < pivmin) q = -pivmin;
+            if (q < 0) ++cnt;
         }
-        int l = m - 1;
-        while (l > 0 && std::fabs(t(l, l - 1)) > eps * (std::fabs(t(l, l)) + std::fabs(t(l - 1, l - 1)))) --l;
-        if (++steps > 60 * n) throw Error{QCG_ERR_NOCONV, "eigensolver did not converge"};
-        const double a = t(m - 1, m - 1), b = t(m, m - 1), c2 = t(m, m);
-        const double delta = 0.5 * (a - c2);
-        const double mu = delta == 0.0 ? c2 - std::fabs(b)
-                                       : c2 - b * b / (delta + (delta > 0 ? 1.0 : -1.0) * std::hypot(delta, b));
-        double x = t(l, l) - mu, z = t(l + 1, l);
-        for (int j = l; j < m; ++j)
+        return cnt;
+    };
+    const double pad = 2.0 * ulp * std::max(tnorm, 1e-300) + pivmin;
+    glo -= pad;
+    ghi += pad;
+    // all k intervals are bisected together: the Sturm recurrence is a chain of dependent divisions, and k
+    // interleaved chains keep the divider busy.  Intervals stop at 1e-12 ||T||; the final eigenvalues are
+    // the Rayleigh quotients of the inverse-iteration vectors below.
+    {
+        std::vector<double> ba(k, glo), bb(k, ghi), mid(k), q(k);
+        std::vector<int> cnt(k);
+        const double tol = 1e-12 * std::max(tnorm, 1e-300) + pivmin;
+        for (int it = 0; it < 200; ++it)
         {
-            const double r = std::sqrt(x * x + z * z);
-            const double c = r == 0.0 ? 1.0 : x / r, s = r == 0.0 ? 0.0 : z / r;
-            rotate(j, c, s, std::max(l, j - 1), std::min(m, j + 2));
-            if (j + 1 < m)
+            bool open = false;
+            for (int j = 0; j < k; ++j)
             {
-                x = t(j + 1, j);
-                z = t(j + 2, j);
+                mid[j] = 0.5 * (ba[j] + bb[j]);
+                open = open || (bb[j] - ba[j] > tol && mid[j] > ba[j] && mid[j] < bb[j]);
+            }
+            if (!open) break;
+            for (int j = 0; j < k; ++j)
+            {
+                q[j] = d[0] - mid[j];
+                if (std::fabs(q[j]) < pivmin) q[j] = -pivmin;
+                cnt[j] = q[j] < 0 ? 1 : 0;
+            }
+            for (int i = 1; i < n; ++i)
+            {
+                const double di = d[i], e2 = e[i - 1] * e[i - 1];
+                for (int j = 0; j < k; ++j)
+                {
+                    double qq = (di - mid[j]) - e2 / q[j];
+                    if (std::fabs(qq) < pivmin) qq = -pivmin;
+                    q[j] = qq;
+                    cnt[j] += qq < 0 ? 1 : 0;
+                }
+            }
+            for (int j = 0; j < k; ++j)
+            {
+                if (cnt[j] > j) bb[j] = mid[j];
+                else ba[j] = mid[j];
             }
         }
+        for (int j = 0; j < k; ++j) w[j] = 0.5 * (ba[j] + bb[j]);
     }
-    for (int i = 0; i < n; ++i) w[i] = t(i, i);
-    std::sort(w, w + n);
     // inverse iteration on the tridiagonal (d, e)
-    const double ulp = 2.220446049250313e-16;
     const double sep = 10.0 * ulp * tnorm, ortol = 1e-3 * tnorm;
     std::vector<double> X((size_t)k * n), u0(n), u1(n), u2(n), mult(n), y(n);
     std::vector<char> swp(n);
@@ -879,6 +932,20 @@ void syev_lowest(int n, const double* Ain, int k, double* w, double* V)
             for (int i = 0; i < n; ++i) xj[i] = y[i] / nrm;
         }
     }
+    // eigenvalues: Rayleigh quotients x^T T x of the (unit) vectors
+    for (int j = 0; j < k; ++j)
+    {
+        const double* xj = &X[(size_t)j * n];
+        double rq = 0.0;
+        for (int i = 0; i < n; ++i)
+        {
+            double tx = d[i] * xj[i];
+            if (i > 0) tx += e[i - 1] * xj[i - 1];
+            if (i + 1 < n) tx += e[i] * xj[i + 1];
+            rq += xj[i] * tx;
+        }
+        w[j] = rq;
+    }
     // self-check: tridiagonal residuals and orthonormality
     bool ok = true;
     for (int j = 0; j < k && ok; ++j)
@@ -903,7 +970,11 @@ void syev_lowest(int n, const double* Ain, int k, double* w, double* V)
     }
     if (!ok)
     {
-        syev(n, Ain, w, V);
+        std::vector<double> wa(n), Va((size_t)n * n);
+        syev(n, Ain, wa.data(), Va.data());
+        for (int j = 0; j < k; ++j) w[j] = wa[j];
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < k; ++j) V[(size_t)i * n + j] = Va[(size_t)i * n + j];
         return;
     }
     // back-transformation v = H_0 (... (H_{n-3} x))
@@ -915,12 +986,52 @@ void syev_lowest(int n, const double* Ain, int k, double* w, double* V)
             if (beta[q] == 0.0) continue;
             const double* rq = &R[(size_t)q * n];
             double s = 0.0;
+#pragma omp simd reduction(+ : s)
             for (int i = q + 1; i < n; ++i) s += rq[i] * xj[i];
             s *= beta[q];
             for (int i = q + 1; i < n; ++i) xj[i] -= s * rq[i];
         }
         for (int i = 0; i < n; ++i) V[(size_t)i * n + j] = xj[i];
     }
+}
+
+// X = L^{-T} for the Cholesky factor S = L L^T of a symmetric positive definite S (row-major n x n):
+// X is upper triangular with X^T S X = 1.  Returns false (X unspecified) if a pivot is not positive.
+bool cholesky_orthogonaliser(int n, const double* S, double* X)
+{
+    std::vector<double> L((size_t)n * n, 0.0);
+    for (int j = 0; j < n; ++j)
+    {
+        double dj = S[(size_t)j * n + j];
+        const double* lj = &L[(size_t)j * n];
+        for (int k = 0; k < j; ++k) dj -= lj[k] * lj[k];
+        if (!(dj > 0.0)) return false;
+        const double ljj = std::sqrt(dj);
+        L[(size_t)j * n + j] = ljj;
+        for (int i = j + 1; i < n; ++i)
+        {
+            const double* li = &L[(size_t)i * n];
+            double v = S[(size_t)i * n + j];
+            for (int k = 0; k < j; ++k) v -= li[k] * lj[k];
+            L[(size_t)i * n + j] = v / ljj;
+        }
+    }
+    // M = L^{-1} (lower triangular) by forward substitution, column by column; X = M^T
+    std::vector<double> M((size_t)n * n, 0.0);
+    for (int c = 0; c < n; ++c)
+    {
+        M[(size_t)c * n + c] = 1.0 / L[(size_t)c * n + c];
+        for (int i = c + 1; i < n; ++i)
+        {
+            const double* li = &L[(size_t)i * n];
+            double v = 0.0;
+            for (int k = c; k < i; ++k) v -= li[k] * M[(size_t)k * n + c];
+            M[(size_t)i * n + c] = v / li[i];
+        }
+    }
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) X[(size_t)i * n + j] = M[(size_t)j * n + i];
+    return true;
 }
 
 // C = op(A) op(B), n x n, row-major
@@ -944,9 +1055,7 @@ void gemm(int n, const double* A, bool ta, const double* B, bool tb, double* C)
         b = Bt.data();
     }
     // row i of C = sum_k a_ik (row k of b): contiguous rows, vectorisable without reassociation
-#pragma omp parallel for schedule(static) if (n > 96)
-    for (int i = 0; i < n; ++i)
-    {
+    auto row = [&](int i) {
         double* ci = C + (size_t)i * n;
         const double* ai = a + (size_t)i * n;
         for (int j = 0; j < n; ++j) ci[j] = 0.0;
@@ -956,7 +1065,14 @@ void gemm(int n, const double* A, bool ta, const double* B, bool tb, double* C)
             const double* bk = b + (size_t)k * n;
             for (int j = 0; j < n; ++j) ci[j] += aik * bk[j];
         }
+    };
+    if (n > 96)
+    {
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < n; ++i) row(i);
     }
+    else
+        for (int i = 0; i < n; ++i) row(i);
 }
 
 std::vector<double> solve_dense(int n, std::vector<double> A, std::vector<double> b)
@@ -1206,7 +1322,7 @@ struct ScfCore
 {
     int n = 0, nocc = 0;
     double fdmax = 0, Enn = 0;
-    std::vector<double> S, H, X, D, Dp, F, Fp, Err, tmp, Up, w, a, b;
+    std::vector<double> S, H, X, Xt, D, Dp, F, Fp, Err, tmp, Up, w, a, b, Cocc;
     std::deque<std::vector<double>> Es, Fps;
     double E = 0, Eold = 0, En = 0;
     GpuLinalg* gl = nullptr;   // set: the O(n^3) steps run on the GPU
@@ -1233,11 +1349,22 @@ struct ScfCore
         S = std::move(S_);
         H = std::move(H_);
         X.assign(nn, 0.0);
-        std::vector<double> sw(n), U(nn);
-        xsyev(S.data(), sw.data(), U.data());
-        require(sw[0] > 0, "overlap matrix is not positive definite");
+        // orthogonaliser X with X^T S X = 1.  On the host: X = L^{-T} from the Cholesky factor S = L L^T
+        // (n^3/3 against the eigendecomposition's ~6 n^3); every such X differs from the canonical U s^{-1/2}
+        // by an orthogonal rotation, which leaves the DIIS error norms, the aufbau density and the energy
+        // unchanged.  On the GPU, and if the factorisation meets a non-positive pivot: X = U s^{-1/2}.
+        if (gl || !cholesky_orthogonaliser(n, S.data(), X.data()))
+        {
+            std::vector<double> sw(n), U(nn);
+            xsyev(S.data(), sw.data(), U.data());
+            require(sw[0] > 0, "overlap matrix is not positive definite");
+            for (int i = 0; i < n; ++i)
+                for (int j = 0; j < n; ++j) X[(size_t)i * n + j] = U[(size_t)i * n + j] / std::sqrt(sw[j]);
+        }
+        Xt.assign(nn, 0.0);
         for (int i = 0; i < n; ++i)
-            for (int j = 0; j < n; ++j) X[(size_t)i * n + j] = U[(size_t)i * n + j] / std::sqrt(sw[j]);
+            for (int j = 0; j < n; ++j) Xt[(size_t)j * n + i] = X[(size_t)i * n + j];
+        Cocc.assign((size_t)n * std::max(nocc, 1), 0.0);
         tmp.assign(nn, 0.0);
         Fp.assign(nn, 0.0);
         Dp.assign(nn, 0.0);
@@ -1272,7 +1399,8 @@ struct ScfCore
     void ortho(const std::vector<double>& M, std::vector<double>& out)
     {
         xgemm(M.data(), false, X.data(), false, tmp.data());
-        xgemm(X.data(), true, tmp.data(), false, out.data());
+        if (gl) xgemm(X.data(), true, tmp.data(), false, out.data());
+        else gemm(n, Xt.data(), false, tmp.data(), false, out.data());   // X^T kept from set-up
     }
     // aufbau density of an orthonormal-basis Fock matrix, back in the AO basis (exactly symmetric)
     void diag_fill(const std::vector<double>& Fo)
@@ -1281,22 +1409,46 @@ struct ScfCore
         if (gl) gl->syev(n, Fo.data(), w.data(), Up.data());
         else syev_lowest(n, Fo.data(), nocc, w.data(), Up.data());
         if (gl)
+        {
             gl->occ_density(n, nocc, Up.data(), Dp.data());
-        else
+            xgemm(X.data(), false, Dp.data(), false, tmp.data());
+            xgemm(tmp.data(), false, X.data(), true, D.data());
             for (int i = 0; i < n; ++i)
-                for (int j = 0; j < n; ++j)
+                for (int j = i + 1; j < n; ++j)
                 {
-                    double s = 0;
-                    for (int k = 0; k < nocc; ++k) s += Up[(size_t)i * n + k] * Up[(size_t)j * n + k];
-                    Dp[(size_t)i * n + j] = 2 * s;
+                    const double v = 0.5 * (D[(size_t)i * n + j] + D[(size_t)j * n + i]);
+                    D[(size_t)i * n + j] = D[(size_t)j * n + i] = v;
                 }
-        xgemm(X.data(), false, Dp.data(), false, tmp.data());
-        xgemm(tmp.data(), false, X.data(), true, D.data());
+            return;
+        }
+        // host: D' = 2 U_occ U_occ^T and D = X D' X^T = 2 C C^T with C = X U_occ, O(n^2 nocc) each and
+        // symmetric by construction
         for (int i = 0; i < n; ++i)
-            for (int j = i + 1; j < n; ++j)
+            for (int j = 0; j <= i; ++j)
             {
-                const double v = 0.5 * (D[(size_t)i * n + j] + D[(size_t)j * n + i]);
-                D[(size_t)i * n + j] = D[(size_t)j * n + i] = v;
+                double s = 0;
+                for (int k = 0; k < nocc; ++k) s += Up[(size_t)i * n + k] * Up[(size_t)j * n + k];
+                Dp[(size_t)i * n + j] = Dp[(size_t)j * n + i] = 2 * s;
+            }
+        for (int i = 0; i < n; ++i)
+        {
+            double* ci = &Cocc[(size_t)i * nocc];
+            for (int k = 0; k < nocc; ++k) ci[k] = 0.0;
+            for (int j = 0; j < n; ++j)
+            {
+                const double xij = X[(size_t)i * n + j];
+                const double* uj = &Up[(size_t)j * n];
+                for (int k = 0; k < nocc; ++k) ci[k] += xij * uj[k];
+            }
+        }
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j <= i; ++j)
+            {
+                double s = 0;
+                const double* ci = &Cocc[(size_t)i * nocc];
+                const double* cj = &Cocc[(size_t)j * nocc];
+                for (int k = 0; k < nocc; ++k) s += ci[k] * cj[k];
+                D[(size_t)i * n + j] = D[(size_t)j * n + i] = 2 * s;
             }
     }
     // F = H + J - K/2, the energy of the current density and the DIIS error ||F'D' - D'F'||
@@ -1313,13 +1465,17 @@ struct ScfCore
         if (!std::isfinite(E)) throw Error{QCG_ERR_NONFINITE, "non-finite SCF energy"};
         ortho(F, Fp);
         xgemm(Fp.data(), false, Dp.data(), false, a.data());
-        xgemm(Dp.data(), false, Fp.data(), false, b.data());
-        En = 0;
-        for (size_t k = 0; k < nn; ++k)
+        if (gl)
         {
-            Err[k] = a[k] - b[k];
-            En += Err[k] * Err[k];
+            xgemm(Dp.data(), false, Fp.data(), false, b.data());
+            for (size_t k = 0; k < nn; ++k) Err[k] = a[k] - b[k];
         }
+        else
+            // F' and D' are symmetric, so D'F' = (F'D')^T
+            for (int i = 0; i < n; ++i)
+                for (int j = 0; j < n; ++j) Err[(size_t)i * n + j] = a[(size_t)i * n + j] - a[(size_t)j * n + i];
+        En = 0;
+        for (size_t k = 0; k < nn; ++k) En += Err[k] * Err[k];
         En = std::sqrt(En);
     }
     // Pulay extrapolation over the last nproj (Err, F') pairs -- entered only while En <= fdmax, pruned from
@@ -1399,6 +1555,18 @@ void nuclei(int natom, const double* Z, const double* R, double& Ztot, double& E
             for (int x = 0; x < 3; ++x) d2 += (R[3 * i + x] - R[3 * j + x]) * (R[3 * i + x] - R[3 * j + x]);
             Enn += Z[i] * Z[j] / std::sqrt(d2);
         }
+    }
+}
+
+// the handle's side streams and their fork/join events (class kernels of one build run side by side)
+void ensure_side_streams(qcg_handle* h)
+{
+    if (h->fork) return;
+    h->fork = h->new_event(false);
+    for (int s = 0; s < qcg_handle::kSide; ++s)
+    {
+        h->side[s] = h->new_stream();
+        h->join[s] = h->new_event(false);
     }
 }
 
@@ -1487,22 +1655,42 @@ void build_screening(qcg_handle* h, double thresh)
     PrimPairsDev P0 = upload_pp(pp);
     std::vector<double> Qc[kNumPairClasses];
     std::vector<void*> tmp;
+    // the six diagonal classes side by side: the uploads are on the handle's stream, the side streams
+    // start after them and the handle's stream waits for all of them before copying the bounds back (a copy
+    // into pageable memory returns only when it is done, so no copy is queued between the launches)
+    ensure_side_streams(h);
+    std::vector<std::array<int*, 4>> lists(kNumPairClasses);
+    std::vector<double*> dQs(kNumPairClasses, nullptr);
     for (int c = 0; c < kNumPairClasses; ++c)
     {
         const int n = (int)sa[c].size();
         Qc[c].assign(n, 0.0);
         if (n == 0) continue;
-        int* dsa = h->upload(sa[c]);
-        int* dsb = h->upload(sb[c]);
-        int* dppo = h->upload(ppo[c]);
-        int* dnpp = h->upload(npp[c]);
-        double* dQ = h->alloc<double>(n);
-        PairListDev pl{n, dsa, dsb, dppo, dnpp, nullptr, nullptr};
-        kSchwarzLaunchers[c](pl, P0, dQ, h->d_boys, h->stream);
-        CK(cudaGetLastError());
-        CK(cudaMemcpyAsync(Qc[c].data(), dQ, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-        tmp.insert(tmp.end(), {dsa, dsb, dppo, dnpp, dQ});
+        lists[c] = {h->upload(sa[c]), h->upload(sb[c]), h->upload(ppo[c]), h->upload(npp[c])};
+        dQs[c] = h->alloc<double>(n);
     }
+    // the side streams must also see the uploads just queued on the handle's stream
+    CK(cudaEventRecord(h->fork, h->stream));
+    for (int s = 0; s < qcg_handle::kSide; ++s) CK(cudaStreamWaitEvent(h->side[s], h->fork, 0));
+    for (int c = kNumPairClasses - 1; c >= 0; --c)
+    {
+        const int n = (int)sa[c].size();
+        if (n == 0) continue;
+        cudaStream_t st = h->side[c % qcg_handle::kSide];
+        PairListDev pl{n, lists[c][0], lists[c][1], lists[c][2], lists[c][3], nullptr, nullptr};
+        kSchwarzLaunchers[c](pl, P0, dQs[c], h->d_boys, st, h->nsm);
+        CK(cudaGetLastError());
+        tmp.insert(tmp.end(), {lists[c][0], lists[c][1], lists[c][2], lists[c][3], dQs[c]});
+    }
+    for (int s = 0; s < qcg_handle::kSide; ++s)
+    {
+        CK(cudaEventRecord(h->join[s], h->side[s]));
+        CK(cudaStreamWaitEvent(h->stream, h->join[s], 0));
+    }
+    for (int c = 0; c < kNumPairClasses; ++c)
+        if (!sa[c].empty())
+            CK(cudaMemcpyAsync(Qc[c].data(), dQs[c], sa[c].size() * sizeof(double), cudaMemcpyDeviceToHost,
+                               h->stream));
     CK(cudaStreamSynchronize(h->stream));
     for (void* p : tmp) h->release(p);
     for (const double* p : {P0.p, P0.Px, P0.Py, P0.Pz, P0.PAx, P0.PAy, P0.PAz, P0.PBx, P0.PBy, P0.PBz, P0.K})
@@ -1652,15 +1840,7 @@ void jk_device(qcg_handle* h, const double* dD, double* dJ, double* dK, int flag
         if (flag & 1) throw Error{QCG_ERR_NONFINITE, "density matrix has NaN/Inf entries"};
         if (flag & 2) throw Error{QCG_ERR_ASYMMETRIC, "density matrix is not symmetric"};
     }
-    if (!h->fork)
-    {
-        h->fork = h->new_event(false);
-        for (int s = 0; s < qcg_handle::kSide; ++s)
-        {
-            h->side[s] = h->new_stream();
-            h->join[s] = h->new_event(false);
-        }
-    }
+    ensure_side_streams(h);
     // the build: zero J'/K', class kernels over the side streams, symmetrisation (timing events only
     // when the build is not a graph)
     auto enqueue = [&](bool timed) {
@@ -2526,15 +2706,18 @@ int qcg_rhf(qcg_handle* h, int natom, const double* Z, const double* R, int nele
         nuclei(natom, Z, R, Ztot, Enn);
         const double fdmax = prm.diis_fdmax > 0 ? prm.diis_fdmax : Ztot * Ztot * 0.1 / 32;
         std::vector<double> S(nn), T(nn), V(nn), H(nn);
+        const auto s0 = std::chrono::steady_clock::now();
         {
             int e = qcg_one_electron(h, natom, Z, R, S.data(), T.data(), V.data());
             if (e != QCG_OK) throw Error{e, h->last_error};
         }
         for (size_t k = 0; k < nn; ++k) H[k] = T[k] + V[k];
+        const auto s1 = std::chrono::steady_clock::now();
         {
             int e = qcg_schwarz(h, prm.schwarz_thresh, nullptr);
             if (e != QCG_OK) throw Error{e, h->last_error};
         }
+        const auto s2 = std::chrono::steady_clock::now();
         ensure_jk_buffers(h);
         // spherical basis: the SCF runs on T^T S T, T^T H T; every build takes D_cart = T D T^T and returns
         // T^T J T, T^T K T (the reference's PG_Spherical path: same Cartesian kernels, transformed)
@@ -2561,6 +2744,7 @@ int qcg_rhf(qcg_handle* h, int natom, const double* Z, const double* R, int nele
             sc.gl = gl.get();
         }
         sc.init(nw, nocc, std::move(S), std::move(H), fdmax, Enn, prm.D_guess);
+        const auto s3 = std::chrono::steady_clock::now();
         std::vector<double>& D = sc.D;
         std::vector<double> J(nn), K(nn);
         std::vector<double> Dc(sph ? nn : 0), Js(sph ? (size_t)nw * nw : 0), Ks(sph ? (size_t)nw * nw : 0);
@@ -2580,14 +2764,23 @@ int qcg_rhf(qcg_handle* h, int natom, const double* Z, const double* R, int nele
         bool fp32_phase = prm.fp32_early != 0, exact_next = false;
         const double fp32_scale = prm.fp32_scale > 0 ? prm.fp32_scale : 1e-4 / (3e-7 * (double)n * n);
         double En_prev = 1.0;
-        // QCG_SCF_TRACE=1: one line per iteration on stderr (energy, change, DIIS error, build kind)
+        // QCG_SCF_TRACE=1: one line per iteration on stderr (energy, change, DIIS error, build kind);
+        // QCG_SCF_TRACE=2 adds the host wall time of the iteration's phases (enqueue of the upload and the
+        // build, wait for the build and the download, Fock/energy/DIIS error, DIIS step and diagonalisation)
         const char* tr = std::getenv("QCG_SCF_TRACE");
-        const bool trace = tr && tr[0] == '1';
+        const bool trace = tr && (tr[0] == '1' || tr[0] == '2');
+        const bool trace_times = tr && tr[0] == '2';
+        using clk = std::chrono::steady_clock;
+        auto us = [](clk::time_point a, clk::time_point b) {
+            return std::chrono::duration<double, std::micro>(b - a).count();
+        };
+        double t_enq = 0, t_wait = 0, t_fock = 0, t_step = 0;
         double* d_dmax = nullptr;
         if (inc) d_dmax = h->alloc<double>((size_t)h->nshell * h->nshell);
         int it;
         for (it = 1; it <= prm.max_iter; ++it)
         {
+            const auto c0 = clk::now();
             qcg_stats st{};
             const bool full = !inc || force_full || since_full >= prm.rebuild_every || exact_next;
             const double band = exact_next ? 0.0 : (fp32_phase ? fp32_scale * En_prev : prm.fp32_below);
@@ -2616,9 +2809,11 @@ int qcg_rhf(qcg_handle* h, int natom, const double* Z, const double* R, int nele
                 launch_block_max(h->d_D, h->d_f0, h->bs.L, h->nshell, n, d_dmax, h->stream, h->nsm);
                 jk_device(h, h->d_D, h->d_J, h->d_K, QCG_JK_SKIP_VALIDATION, &st, d_dmax, prm.inc_thresh, band);
             }
+            const auto c1 = clk::now();
             CK(cudaMemcpyAsync(J.data(), h->d_J, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
             CK(cudaMemcpyAsync(K.data(), h->d_K, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
             CK(cudaStreamSynchronize(h->stream));
+            const auto c2 = clk::now();
             fock_ms += st.ms_total;
             if (full)
             {
@@ -2641,6 +2836,10 @@ int qcg_rhf(qcg_handle* h, int natom, const double* Z, const double* R, int nele
             }
             else
                 sc.fock(J.data(), K.data());
+            const auto c3 = clk::now();
+            t_enq += us(c0, c1);
+            t_wait += us(c1, c2);
+            t_fock += us(c2, c3);
             if (it > 1 && std::fabs(sc.E - sc.Eold) < prm.de_tol && sc.En < prm.fd_tol)
             {
                 if (!full || band != 0.0)
@@ -2666,8 +2865,19 @@ int qcg_rhf(qcg_handle* h, int natom, const double* Z, const double* R, int nele
                 force_full = true;
             }
             sc.Eold = sc.E;
+            const auto c4 = clk::now();
             sc.step(prm);
+            t_step += us(c4, clk::now());
         }
+        if (trace_times)
+            std::fprintf(stderr, "qcg_rhf host times over %d iterations (us): enqueue %.0f, wait %.0f, fock %.0f, "
+                         "step %.0f; device J/K %.0f; set-up and rest %.0f\n", std::min(it, prm.max_iter), t_enq,
+                         t_wait, t_fock, t_step, 1e3 * fock_ms,
+                         std::chrono::duration<double, std::micro>(clk::now() - t0).count() - t_enq - t_wait -
+                             t_fock - t_step);
+        if (trace_times)
+            std::fprintf(stderr, "qcg_rhf set-up (us): one-electron %.0f, screening %.0f, orthogonaliser and guess %.0f\n",
+                         us(s0, s1), us(s1, s2), us(s2, s3));
         result->energy = sc.E;
         result->e_nuc = Enn;
         result->iterations = std::min(it, prm.max_iter);
@@ -2943,7 +3153,7 @@ int qcg_internal_syev(int n, const double* A, double* w, double* V)
     }
 }
 
-// test hook: the SCF step's partial eigensolver (all eigenvalues, the k lowest eigenvectors)
+// test hook: the SCF step's partial eigensolver (the k lowest eigenpairs)
 int qcg_internal_syev_lowest(int n, const double* A, int k, double* w, double* V)
 {
     try
