@@ -217,7 +217,8 @@ int qcg_rhf(qcg_handle* h, int natom, const double* Z, const double* R, int nele
             qcg_scf_result* result, double* D_out);
 /* All molecules of a batch handle to convergence together: each iteration is one J/K build over every
  * molecule, then per-molecule host steps in parallel.  results: nmol entries (wall_s and fock_ms are the
- * batch's); D_out optional, packed.  incremental / fp32 / D_guess parameters are ignored. */
+ * batch's); D_out optional, packed.  D_guess (optional) is packed too: one initial density per molecule.
+ * The incremental and fp32 parameters are ignored. */
 int qcg_rhf_batch(qcg_handle* h, const int* mol_natom, const double* Z, const double* R, const int* nelec,
                   const qcg_scf_params* params, qcg_scf_result* results, double* D_out);
 

@@ -450,12 +450,20 @@ class BatchEngine(Engine):
         self._screen = thresh
 
     def rhf(self, mols: Sequence[_basis.Molecule], max_iter=100, de_tol=1e-10, fd_tol=1e-5, schwarz_thresh=1e-10,
-            want_density=False, diis_nproj=4, diis_fdmax=0.0, autotune=False):
+            want_density=False, diis_nproj=4, diis_fdmax=0.0, autotune=False, guesses=None):
+        """guesses: optional list of per-molecule initial densities (None entries are not allowed; omit the
+        argument for the core guess everywhere)."""
         prm = ScfParams()
         lib().qcg_scf_default_params(ctypes.byref(prm))
         prm.max_iter, prm.de_tol, prm.fd_tol, prm.schwarz_thresh = max_iter, de_tol, fd_tol, schwarz_thresh
         prm.diis_nproj, prm.diis_fdmax = int(diis_nproj), float(diis_fdmax)
         prm.autotune = int(bool(autotune))
+        Dg = None
+        if guesses is not None:
+            if len(guesses) != len(mols):
+                raise QcgError(QCG_ERR_ARG, "one guess density per molecule")
+            Dg = self.pack(guesses)
+            prm.D_guess = _p(Dg)
         nat = np.array([len(m.Z) for m in mols], dtype=np.int32)
         Z = _f64(np.concatenate([np.asarray(m.Z, dtype=float) for m in mols]))
         R = _f64(np.concatenate([np.asarray(m.R, dtype=float).reshape(-1) for m in mols]))

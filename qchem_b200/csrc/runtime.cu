@@ -3059,7 +3059,9 @@ int qcg_rhf_batch(qcg_handle* h, const int* mol_natom, const double* Z, const do
                 std::vector<double> Sm(S.begin() + o, S.begin() + o + mm), Hm(mm);
                 for (size_t k = 0; k < mm; ++k) Hm[k] = T[o + k] + V[o + k];
                 const double fdmax = prm.diis_fdmax > 0 ? prm.diis_fdmax : Ztot * Ztot * 0.1 / 32;
-                sc[m].init(n, nelec[m] / 2, std::move(Sm), std::move(Hm), fdmax, Enn[m], nullptr);
+                // D_guess, when given, is packed like every batch matrix: molecule m's block at mol_off[m]
+                sc[m].init(n, nelec[m] / 2, std::move(Sm), std::move(Hm), fdmax, Enn[m],
+                           prm.D_guess ? prm.D_guess + o : nullptr);
             }
             catch (const Error& e)
             {

@@ -93,18 +93,20 @@ class PairLayout:
         return D
 
     def features(self, mol: _basis.Molecule, template: _basis.Molecule) -> np.ndarray:
+        """One row per atom pair: element one-hots of both atoms, [a == b], R_AB, exp(-R_AB/2), R_B - R_A,
+        the pair slot (one-hot) and the conformer's displacement from the template (all coordinates)."""
         R = np.asarray(mol.R, dtype=float)
         disp = (R - np.asarray(template.R, dtype=float)).ravel()
-        rows = []
-        for p, (a, b) in enumerate(self.pairs):
-            d = R[b] - R[a]
-            r = float(np.linalg.norm(d))
-            f = [float(self.Z[a] == e) for e in ELEMENTS] + [float(self.Z[b] == e) for e in ELEMENTS]
-            f += [float(a == b), r, float(np.exp(-0.5 * r))] + list(d)
-            slot = [0.0] * len(self.pairs)
-            slot[p] = 1.0
-            rows.append(f + slot + list(disp))
-        return np.array(rows, dtype=np.float64)
+        a = np.array([p[0] for p in self.pairs])
+        b = np.array([p[1] for p in self.pairs])
+        Z = np.asarray(self.Z)
+        el = np.asarray(ELEMENTS)
+        d = R[b] - R[a]
+        r = np.sqrt((d * d).sum(axis=1))
+        P = len(self.pairs)
+        return np.concatenate([(Z[a][:, None] == el[None, :]).astype(float), (Z[b][:, None] == el[None, :]).astype(float),
+                               (a == b).astype(float)[:, None], r[:, None], np.exp(-0.5 * r)[:, None], d, np.eye(P),
+                               np.broadcast_to(disp, (P, disp.size))], axis=1)
 
 
 class LearnedGuess:
@@ -176,12 +178,30 @@ class LearnedGuess:
     def predict_blocks(self, mols: Sequence[_basis.Molecule], device: str = "cuda") -> np.ndarray:
         import torch
         P = len(self.layout.pairs)
-        x = torch.from_numpy(self._xn(mols)).to(device)
-        y = torch.empty((x.shape[0], self.layout.nout), dtype=torch.float32, device=device)
-        self.net.set_stream(torch.cuda.current_stream(torch.device(device)).cuda_stream)
-        self.net.forward(x.shape[0], x.data_ptr(), y.data_ptr())
-        yn = y.cpu().numpy().astype(np.float64).reshape(len(mols), P, -1)
-        return (yn * self.y_sd + self.y_mu) * self.layout.mask()
+        xn = self._xn(mols)
+        rows = xn.shape[0]
+        # input/output buffers (pinned host and device) and the stream binding are kept between calls: a
+        # single-molecule prediction is a handful of small launches, so allocation and pageable copies
+        # would cost more than the network
+        key = (rows, str(device))
+        if getattr(self, "_io_key", None) != key:
+            dev = torch.device(device)
+            self._io = (torch.empty((rows, xn.shape[1]), dtype=torch.float32).pin_memory(),
+                        torch.empty((rows, xn.shape[1]), dtype=torch.float32, device=dev),
+                        torch.empty((rows, self.layout.nout), dtype=torch.float32, device=dev),
+                        torch.empty((rows, self.layout.nout), dtype=torch.float32).pin_memory(),
+                        torch.cuda.current_stream(dev))
+            self._io_key = key
+            self._mask = self.layout.mask()
+        hx, dx, dy, hy, stream = self._io
+        self.net.set_stream(stream.cuda_stream)
+        hx.numpy()[...] = xn
+        dx.copy_(hx, non_blocking=True)
+        self.net.forward(rows, dx.data_ptr(), dy.data_ptr())
+        hy.copy_(dy, non_blocking=True)
+        stream.synchronize()
+        yn = hy.numpy().astype(np.float64).reshape(len(mols), P, -1)
+        return (yn * self.y_sd + self.y_mu) * self._mask
 
     def predict(self, mol: _basis.Molecule, device: str = "cuda") -> np.ndarray:
         return self.layout.assemble(self.predict_blocks([mol], device)[0], self.nbf)
@@ -232,3 +252,23 @@ def evaluate(model: Optional[LearnedGuess], mols: Sequence[_basis.Molecule], ref
             "wall_s_mean": float(np.mean(walls)), "wall_s_median": float(np.median(walls)), "wall_s": walls,
             "energies": energies, "converged": conv,
             "max_abs_dE": float(np.max(dE)) if dE else None, "all_converged": bool(all(conv))}
+
+
+def evaluate_batched(model: LearnedGuess, mols: Sequence[_basis.Molecule], ref_energies: Sequence[float],
+                     **rhf_kw) -> dict:
+    """The learned guess with batching: every conformer's guess from one network pass, every SCF in one
+    batch handle (one J/K build per iteration over all molecules).  The wall time covers the guesses, the
+    handle set-up and the SCF; wall_s_per_molecule is that time divided by the number of molecules (a
+    throughput figure, not one molecule's latency)."""
+    t0 = time.perf_counter()
+    blocks = model.predict_blocks(mols)
+    guesses = [model.layout.assemble(b, model.nbf) for b in blocks]
+    be = api.BatchEngine([model.shells_of(m) for m in mols])
+    res = be.rhf(mols, guesses=guesses, **rhf_kw)
+    wall = time.perf_counter() - t0
+    dE = [abs(r["energy"] - e) for r, e in zip(res, ref_energies) if e is not None and r["converged"]]
+    its = [r["iterations"] for r in res]
+    return {"guess": "learned", "molecules": len(mols), "wall_s": wall, "wall_s_per_molecule": wall / len(mols),
+            "iterations_mean": float(np.mean(its)), "iterations_max": int(max(its)),
+            "all_converged": bool(all(r["converged"] for r in res)),
+            "max_abs_dE": float(np.max(dE)) if dE else None}

@@ -54,3 +54,19 @@ def test_batch_rejects_single_molecule_only_calls(mols):
     with pytest.raises(api.QcgError):
         Engine_rhf = api.Engine.rhf
         Engine_rhf(be, mols[0])
+
+
+def test_batch_rhf_from_per_molecule_guesses(mols):
+    """Packed initial densities (one per molecule): started from each molecule's own converged density,
+    every SCF of the batch stops within a few iterations at the energy of its single-molecule run, and a
+    guess list of the wrong length is refused."""
+    shells = [B.even_tempered(m) for m in mols]
+    refs = [api.Engine(s).rhf(m, want_density=True) for m, s in zip(mols, shells)]
+    keep = [k for k, r in enumerate(refs) if r["converged"]]
+    ms, ss = [mols[k] for k in keep], [shells[k] for k in keep]
+    res = api.BatchEngine(ss).rhf(ms, guesses=[refs[k]["D"] for k in keep])
+    for k, r in zip(keep, res):
+        assert r["converged"] and r["iterations"] <= 3, (k, r["iterations"])
+        assert abs(r["energy"] - refs[k]["energy"]) <= E_TOL
+    with pytest.raises(api.QcgError):
+        api.BatchEngine(ss).rhf(ms, guesses=[refs[keep[0]]["D"]] * (len(keep) + 1))
