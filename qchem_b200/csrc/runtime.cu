@@ -406,14 +406,32 @@ struct qcg_handle
                 return;
             }
     }
+    // Uploads between begin_uploads() and flush_uploads() are merged: a piece whose device address and
+    // staging offset both continue the previous piece (consecutive slab allocations do) extends one pending
+    // copy, so a run of small uploads costs one cudaMemcpyAsync.  Nothing queued on the stream may read an
+    // uploaded array before the flush.
+    bool defer_uploads = false;
+    char* pend_dev = nullptr;
+    char* pend_stage = nullptr;
+    size_t pend_span = 0;
+    void begin_uploads() { defer_uploads = true; }
+    void flush_uploads()
+    {
+        if (pend_span) CK(cudaMemcpyAsync(pend_dev, pend_stage, pend_span, cudaMemcpyHostToDevice, stream));
+        pend_span = 0;
+        defer_uploads = false;
+    }
     template <class T>
     T* upload(const std::vector<T>& v)
     {
         T* d = alloc<T>(v.size());
         const size_t bytes = v.size() * sizeof(T);
         if (bytes == 0) return d;
+        const size_t span = (bytes + 255) & ~(size_t)255;   // the allocation's extent (alloc rounds to 256)
         if (bytes > kStage)
         {
+            if (pend_span) CK(cudaMemcpyAsync(pend_dev, pend_stage, pend_span, cudaMemcpyHostToDevice, stream));
+            pend_span = 0;
             CK(cudaMemcpyAsync(d, v.data(), bytes, cudaMemcpyHostToDevice, stream));
             return d;
         }
@@ -422,14 +440,30 @@ struct qcg_handle
             stage = ResourceCache::get().stage();
             stage_used = 0;
         }
-        if (stage_used + bytes > kStage)
+        if (stage_used + span > kStage)
         {
+            if (pend_span) CK(cudaMemcpyAsync(pend_dev, pend_stage, pend_span, cudaMemcpyHostToDevice, stream));
+            pend_span = 0;
             CK(cudaStreamSynchronize(stream));   // earlier copies out of the staging buffer are done
             stage_used = 0;
         }
-        std::memcpy(stage + stage_used, v.data(), bytes);
-        CK(cudaMemcpyAsync(d, stage + stage_used, bytes, cudaMemcpyHostToDevice, stream));
-        stage_used = (stage_used + bytes + 255) & ~(size_t)255;
+        char* src = stage + stage_used;
+        std::memcpy(src, v.data(), bytes);
+        stage_used += span;
+        if (!defer_uploads)
+        {
+            CK(cudaMemcpyAsync(d, src, bytes, cudaMemcpyHostToDevice, stream));
+            return d;
+        }
+        if (pend_span && (char*)d == pend_dev + pend_span && src == pend_stage + pend_span)
+        {
+            pend_span += span;
+            return d;
+        }
+        if (pend_span) CK(cudaMemcpyAsync(pend_dev, pend_stage, pend_span, cudaMemcpyHostToDevice, stream));
+        pend_dev = (char*)d;
+        pend_stage = src;
+        pend_span = span;
         return d;
     }
     // streams and events come from the process-wide cache and go back to it, idle, when the handle goes
@@ -1587,6 +1621,17 @@ void ensure_jk_buffers(qcg_handle* h)
 // ------------------------------------------------------------------------------------------------
 void build_screening(qcg_handle* h, double thresh)
 {
+    // merged uploads never outlive this call: on an error the pending copy is dropped (the screening is
+    // then incomplete and h->screened stays false) and later uploads are issued one by one again
+    struct UploadModeReset
+    {
+        qcg_handle* h;
+        ~UploadModeReset()
+        {
+            h->pend_span = 0;
+            h->defer_uploads = false;
+        }
+    } upload_mode_reset{h};
     // shell pairs per class, (a,b) with L_a > L_b, or L_a == L_b and a >= b
     std::vector<int> sa[kNumPairClasses], sb[kNumPairClasses];
     for (int a = 0; a < h->nshell; ++a)
@@ -1652,6 +1697,7 @@ void build_screening(qcg_handle* h, double thresh)
     std::vector<PP> pp;
     std::vector<int> ppo[kNumPairClasses], npp[kNumPairClasses];
     build_pp(sa, sb, pp, ppo, npp);
+    h->begin_uploads();   // merged until the Schwarz launches
     PrimPairsDev P0 = upload_pp(pp);
     std::vector<double> Qc[kNumPairClasses];
     std::vector<void*> tmp;
@@ -1670,6 +1716,7 @@ void build_screening(qcg_handle* h, double thresh)
         dQs[c] = h->alloc<double>(n);
     }
     // the side streams must also see the uploads just queued on the handle's stream
+    h->flush_uploads();
     CK(cudaEventRecord(h->fork, h->stream));
     for (int s = 0; s < qcg_handle::kSide; ++s) CK(cudaStreamWaitEvent(h->side[s], h->fork, 0));
     for (int c = kNumPairClasses - 1; c >= 0; --c)
@@ -1733,6 +1780,7 @@ void build_screening(qcg_handle* h, double thresh)
         }
     }
     build_pp(h->pl_sa, h->pl_sb, pp, h->pl_ppo, h->pl_npp);
+    h->begin_uploads();   // merged until the end of the screening
     h->pp_dev = upload_pp(pp);
     for (int c = 0; c < kNumPairClasses; ++c)
     {
@@ -1799,6 +1847,7 @@ void build_screening(qcg_handle* h, double thresh)
             h->work_prim_quartets += pq;
             h->work_flops += (double)pq * class_flops(kPairLA[X], kPairLB[X], kPairLA[Y], kPairLB[Y]);
         }
+    h->flush_uploads();
     CK(cudaStreamSynchronize(h->stream));
     h->thresh = thresh;
     h->screened = true;
