@@ -178,6 +178,31 @@ public:
         CK(timing ? cudaEventCreate(&e) : cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         return e;
     }
+    // pinned host blocks of at least `bytes` (capacities are powers of two from 1 MiB; *cap receives it)
+    char* pinned(size_t bytes, size_t* cap)
+    {
+        size_t c = (size_t)1 << 20;
+        while (c < bytes) c <<= 1;
+        *cap = c;
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            auto it = pinned_.find(c);
+            if (it != pinned_.end())
+            {
+                char* p = it->second;
+                pinned_.erase(it);
+                return p;
+            }
+        }
+        char* p = nullptr;
+        CK(cudaMallocHost(&p, c));
+        return p;
+    }
+    void give_pinned(char* p, size_t cap)
+    {
+        std::lock_guard<std::mutex> g(mu_);
+        pinned_.emplace(cap, p);
+    }
     void give_slab(int dev, void* p)
     {
         std::lock_guard<std::mutex> g(mu_);
@@ -216,6 +241,8 @@ public:
         cudaSetDevice(cur);
         for (char* p : stages_) cudaFreeHost(p);
         stages_.clear();
+        for (auto& kv : pinned_) cudaFreeHost(kv.second);
+        pinned_.clear();
     }
 
 private:
@@ -228,6 +255,18 @@ private:
     std::mutex mu_;
     std::unordered_map<int, PerDevice> per_;
     std::vector<char*> stages_;
+    std::unordered_multimap<size_t, char*> pinned_;
+};
+
+// a pinned host array from the resource cache for the lifetime of one call
+struct PinnedArray
+{
+    double* p = nullptr;
+    size_t cap = 0;
+    explicit PinnedArray(size_t n) { p = (double*)ResourceCache::get().pinned(std::max<size_t>(n, 1) * sizeof(double), &cap); }
+    ~PinnedArray() { ResourceCache::get().give_pinned((char*)p, cap); }
+    PinnedArray(const PinnedArray&) = delete;
+    PinnedArray& operator=(const PinnedArray&) = delete;
 };
 
 }   // namespace
@@ -2796,8 +2835,10 @@ int qcg_rhf(qcg_handle* h, int natom, const double* Z, const double* R, int nele
         const auto s3 = std::chrono::steady_clock::now();
         std::vector<double>& D = sc.D;
         std::vector<double> J(nn), K(nn);
+        // the density goes up and J, K come back every iteration: through pinned (cached) host arrays
+        PinnedArray Dpin(nn), Jpin(nn), Kpin(nn);
         std::vector<double> Dc(sph ? nn : 0), Js(sph ? (size_t)nw * nw : 0), Ks(sph ? (size_t)nw * nw : 0);
-        std::vector<double> Dprev, Jprev, Kprev, dD(nn);
+        std::vector<double> Dprev, Jprev, Kprev;
         double fock_ms = 0;
         const bool inc = prm.incremental != 0;
         int since_full = 0, nfull = 0, ninc = 0, n32 = 0;
@@ -2843,7 +2884,8 @@ int qcg_rhf(qcg_handle* h, int natom, const double* Z, const double* R, int nele
                     sph->to_cart(D.data(), Dc.data());
                     Dup = Dc.data();
                 }
-                CK(cudaMemcpyAsync(h->d_D, Dup, nn * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+                std::copy(Dup, Dup + nn, Dpin.p);
+                CK(cudaMemcpyAsync(h->d_D, Dpin.p, nn * sizeof(double), cudaMemcpyHostToDevice, h->stream));
                 if (it == 1 && prm.autotune)
                 {
                     const int e = qcg_autotune_jk(h, h->d_D, 1, nullptr, nullptr);
@@ -2853,15 +2895,17 @@ int qcg_rhf(qcg_handle* h, int natom, const double* Z, const double* R, int nele
             }
             else
             {
-                for (size_t k = 0; k < nn; ++k) dD[k] = D[k] - Dprev[k];
-                CK(cudaMemcpyAsync(h->d_D, dD.data(), nn * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+                for (size_t k = 0; k < nn; ++k) Dpin.p[k] = D[k] - Dprev[k];
+                CK(cudaMemcpyAsync(h->d_D, Dpin.p, nn * sizeof(double), cudaMemcpyHostToDevice, h->stream));
                 launch_block_max(h->d_D, h->d_f0, h->bs.L, h->nshell, n, d_dmax, h->stream, h->nsm);
                 jk_device(h, h->d_D, h->d_J, h->d_K, QCG_JK_SKIP_VALIDATION, &st, d_dmax, prm.inc_thresh, band);
             }
             const auto c1 = clk::now();
-            CK(cudaMemcpyAsync(J.data(), h->d_J, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-            CK(cudaMemcpyAsync(K.data(), h->d_K, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaMemcpyAsync(Jpin.p, h->d_J, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaMemcpyAsync(Kpin.p, h->d_K, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
             CK(cudaStreamSynchronize(h->stream));
+            std::copy(Jpin.p, Jpin.p + nn, J.begin());
+            std::copy(Kpin.p, Kpin.p + nn, K.begin());
             const auto c2 = clk::now();
             fock_ms += st.ms_total;
             if (full)
@@ -3119,24 +3163,28 @@ int qcg_rhf_batch(qcg_handle* h, const int* mol_natom, const double* Z, const do
         }
         for (int m = 0; m < nmol; ++m)
             if (!err[m].empty()) throw Error{QCG_ERR_ARG, "molecule " + std::to_string(m) + ": " + err[m]};
-        std::vector<double> Dh(nn), J(nn), K(nn);
+        // the packed D, J and K cross PCIe every iteration: pinned (cached) host arrays; each molecule writes
+        // its next density into Dh in the parallel step
+        PinnedArray Dh(nn), Jp(nn), Kp(nn);
+        double* J = Jp.p;
+        double* K = Kp.p;
+#pragma omp parallel for schedule(static)
+        for (int m = 0; m < nmol; ++m) std::copy(sc[m].D.begin(), sc[m].D.end(), Dh.p + h->mol_off[m]);
         double fock_ms = 0;
         int it, nconv = 0, nbuild = 0;
         for (it = 1; it <= prm.max_iter && nconv < nmol; ++it)
         {
             ++nbuild;
-            for (int m = 0; m < nmol; ++m)
-                std::copy(sc[m].D.begin(), sc[m].D.end(), Dh.begin() + h->mol_off[m]);
             qcg_stats st{};
-            CK(cudaMemcpyAsync(h->d_D, Dh.data(), nn * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+            CK(cudaMemcpyAsync(h->d_D, Dh.p, nn * sizeof(double), cudaMemcpyHostToDevice, h->stream));
             if (it == 1 && prm.autotune)
             {
                 const int e = qcg_autotune_jk(h, h->d_D, 1, nullptr, nullptr);
                 if (e != QCG_OK) throw Error{e, h->last_error};
             }
             jk_device(h, h->d_D, h->d_J, h->d_K, QCG_JK_SKIP_VALIDATION, &st);
-            CK(cudaMemcpyAsync(J.data(), h->d_J, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-            CK(cudaMemcpyAsync(K.data(), h->d_K, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaMemcpyAsync(J, h->d_J, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaMemcpyAsync(K, h->d_K, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
             CK(cudaStreamSynchronize(h->stream));
             fock_ms += st.ms_total;
 #pragma omp parallel for schedule(dynamic)
@@ -3146,7 +3194,7 @@ int qcg_rhf_batch(qcg_handle* h, const int* mol_natom, const double* Z, const do
                 try
                 {
                     ScfCore& c = sc[m];
-                    c.fock(J.data() + h->mol_off[m], K.data() + h->mol_off[m]);
+                    c.fock(J + h->mol_off[m], K + h->mol_off[m]);
                     iters[m] = it;
                     if (it > 1 && std::fabs(c.E - c.Eold) < prm.de_tol && c.En < prm.fd_tol)
                     {
@@ -3155,6 +3203,7 @@ int qcg_rhf_batch(qcg_handle* h, const int* mol_natom, const double* Z, const do
                     }
                     c.Eold = c.E;
                     c.step(prm);
+                    std::copy(c.D.begin(), c.D.end(), Dh.p + h->mol_off[m]);
                 }
                 catch (const Error& e)
                 {
