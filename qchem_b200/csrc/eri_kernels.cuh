@@ -423,6 +423,7 @@ __global__ void __launch_bounds__(THREADS) jk_kernel(JKWorkDev w, PairListDev br
                 bind(i);
                 sink.set_bra(shell_f0[sa], shell_f0[sb]);
             }
+            if (w.mol_active && bra.mol && !w.mol_active[bra.mol[i]]) continue;
             const int j = (w.kbase ? w.kbase[i] : 0) + (int)(g - w.offs[i]);
             const int sc = ket.sa[j], sd = ket.sb[j];
             if (jk_skip(w, bra, ket, i, j, sa, sb, sc, sd)) continue;
@@ -474,6 +475,7 @@ __global__ void __launch_bounds__(THREADS) jk_split_kernel(JKWorkDev w, PairList
             else hi = mid;
         }
         const int i = lo;
+        if (w.mol_active && bra.mol && !w.mol_active[bra.mol[i]]) continue;
         const int j = (w.kbase ? w.kbase[i] : 0) + (int)(g - w.offs[i]);
         const int sa = bra.sa[i], sb = bra.sb[i], sc = ket.sa[j], sd = ket.sb[j];
         if (jk_skip(w, bra, ket, i, j, sa, sb, sc, sd)) continue;

@@ -76,6 +76,9 @@ struct JKWorkDev
     // launch shape: quartets per lane and blocks-per-SM cap (0: the launcher's own choice; set by the
     // autotuner, qcg_autotune_jk)
     int run, cap;
+    // several molecules: mol_active[m] == 0 skips molecule m's quartets (a batched SCF's converged
+    // molecules); null: every molecule
+    const int* mol_active;
 };
 
 void launch_block_max(const double* D, const int* shell_f0, const int* shell_L, int nshell, int n, double* dmax,

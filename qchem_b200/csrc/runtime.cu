@@ -307,6 +307,7 @@ struct qcg_handle
     int* d_shell_mol = nullptr;
     long long* d_mol_off = nullptr;
     int* d_mol_n = nullptr;
+    const int* d_mol_active = nullptr;   // set by the batched SCF while it runs: molecules still iterating
     MolLayoutDev mols() const { return MolLayoutDev{nmol, d_mol_off, d_mol_n}; }
     std::vector<int> L, nprim, prim0, f0;
     std::vector<double> cen, alpha, coef, ns;
@@ -1948,6 +1949,7 @@ void jk_device(qcg_handle* h, const double* dD, double* dJ, double* dK, int flag
             JKWorkDev wk = h->work[k];
             wk.run = h->tuned_run[k];
             wk.cap = h->tuned_cap[k];
+            wk.mol_active = h->d_mol_active;
             // this rank's contiguous slice of the class's quartets
             wk.gbeg = wk.total * h->shard_rank / h->shard_world;
             wk.gend = wk.total * (h->shard_rank + 1) / h->shard_world;
@@ -3168,6 +3170,24 @@ int qcg_rhf_batch(qcg_handle* h, const int* mol_natom, const double* Z, const do
         PinnedArray Dh(nn), Jp(nn), Kp(nn);
         double* J = Jp.p;
         double* K = Kp.p;
+        // converged molecules leave the J/K builds: a device flag per molecule, cleared as each converges
+        struct ActiveReset
+        {
+            qcg_handle* h;
+            int* d = nullptr;
+            ~ActiveReset()
+            {
+                h->d_mol_active = nullptr;
+                if (d) h->release(d);
+            }
+        } active{h};
+        std::vector<int> act(nmol, 1);
+        if (nmol > 1)
+        {
+            active.d = h->alloc<int>(nmol);
+            CK(cudaMemcpyAsync(active.d, act.data(), nmol * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+            h->d_mol_active = active.d;
+        }
 #pragma omp parallel for schedule(static)
         for (int m = 0; m < nmol; ++m) std::copy(sc[m].D.begin(), sc[m].D.end(), Dh.p + h->mol_off[m]);
         double fock_ms = 0;
@@ -3212,11 +3232,21 @@ int qcg_rhf_batch(qcg_handle* h, const int* mol_natom, const double* Z, const do
                 }
             }
             nconv = 0;
+            bool changed = false;
             for (int m = 0; m < nmol; ++m)
             {
                 if (!err[m].empty()) throw Error{QCG_ERR_NONFINITE, "molecule " + std::to_string(m) + ": " + err[m]};
                 nconv += done[m];
+                if (done[m] && act[m])
+                {
+                    act[m] = 0;
+                    changed = true;
+                }
             }
+            // the copy is ordered before the next build on the same stream; act is not touched again until
+            // the stream is synchronised after that build
+            if (changed && active.d)
+                CK(cudaMemcpyAsync(active.d, act.data(), nmol * sizeof(int), cudaMemcpyHostToDevice, h->stream));
         }
         const double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         for (int m = 0; m < nmol; ++m)
