@@ -123,6 +123,7 @@ def lib():
     L.qcg_rhf.argtypes = [vp, i32, P(f64), P(f64), i32, P(ScfParams), P(ScfResult), P(f64)]
     L.qcg_internal_syev.argtypes = [i32, P(f64), P(f64), P(f64)]
     L.qcg_internal_syev_lowest.argtypes = [i32, P(f64), i32, P(f64), P(f64)]
+    L.qcg_internal_orthogonaliser.argtypes = [i32, P(f64), P(f64)]
     L.qcg_measure_fp64_peak.argtypes = [i32, P(f64), P(f64)]
     L.qcg_measure_fp32_peak.argtypes = [i32, P(f64), P(f64)]
     f32 = ctypes.c_float
@@ -171,6 +172,15 @@ def syev_lowest(A: np.ndarray, k: int):
     if rc != QCG_OK:
         raise QcgError(rc, "eigensolver failed")
     return w[:k], V[:, :k]
+
+
+def orthogonaliser(S: np.ndarray):
+    """The host SCF's orthogonaliser X = L^{-T} (S = L L^T), exposed for tests; None if S is not positive
+    definite (the SCF then falls back to U s^{-1/2})."""
+    S = _f64(S)
+    n = S.shape[0]
+    X = np.zeros((n, n))
+    return X if lib().qcg_internal_orthogonaliser(n, _p(S), _p(X)) == 1 else None
 
 
 def release_cache() -> None:

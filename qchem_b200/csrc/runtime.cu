@@ -3283,6 +3283,12 @@ int qcg_internal_syev(int n, const double* A, double* w, double* V)
     }
 }
 
+// test hook: the host SCF's Cholesky orthogonaliser (1: X written; 0: S is not positive definite)
+int qcg_internal_orthogonaliser(int n, const double* S, double* X)
+{
+    return cholesky_orthogonaliser(n, S, X) ? 1 : 0;
+}
+
 // test hook: the SCF step's partial eigensolver (the k lowest eigenpairs)
 int qcg_internal_syev_lowest(int n, const double* A, int k, double* w, double* V)
 {

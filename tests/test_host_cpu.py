@@ -91,6 +91,25 @@ def test_syev_lowest_degenerate_spectra():
     np.testing.assert_allclose(V.T @ V, np.eye(2), atol=1e-12)
 
 
+def test_orthogonaliser_is_upper_triangular_and_orthonormalising():
+    rng = np.random.default_rng(9)
+    for n in (1, 5, 57, 120):
+        M = rng.normal(size=(n, n))
+        S = M @ M.T + n * np.eye(n)
+        X = api.orthogonaliser(S)
+        assert X is not None
+        np.testing.assert_allclose(X.T @ S @ X, np.eye(n), atol=1e-12 * n)
+        np.testing.assert_array_equal(np.tril(X, -1), 0.0)
+    # the overlap of the config-1 water basis (diffuse, condition number ~1e4 and above)
+    sh = B.even_tempered(W.water())
+    from oracle.oracle import OracleBasis
+    S = OracleBasis(sh).one_electron(W.water())[0]
+    X = api.orthogonaliser(S)
+    np.testing.assert_allclose(X.T @ S @ X, np.eye(len(S)), atol=1e-10)
+    # not positive definite: refused, so that the SCF falls back to the eigendecomposition
+    assert api.orthogonaliser(np.diag([1.0, -1.0, 2.0])) is None
+
+
 def test_even_tempered_layout():
     mol = W.water()
     sh = B.even_tempered(mol)
