@@ -316,3 +316,134 @@ def main(outdir):
 
 if __name__ == "__main__":
     main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(os.path.dirname(os.path.abspath(__file__)), "gen"))
+
+
+# ------------------------------------------------------------------------------------------------------
+# Horizontal-recurrence (HRR) form, generated on request only (main_hrr): the primitive quartets produce
+# [e0|f0] for e over the Cartesian components of L = LA..LA+LB on centre A and f over L = LC..LC+LD on
+# centre C (E^{e0} tables, one index per pair), accumulated over the primitives of a contracted quartet;
+# the contracted block is then carried to (ab|cd) by
+#     (x, y + 1_i) = (x + 1_i, y) + D_i (x, y),   D = C - D on the ket, A - B on the bra,
+# once per contracted quartet instead of once per primitive quartet.  The library's kernels do not use it
+# yet; tests/test_gen_md_host.py checks it against the oracle on the host.
+# ------------------------------------------------------------------------------------------------------
+def comps_range(L0, L1):
+    return [c for L in range(L0, L1 + 1) for c in comps(L)]
+
+
+def hrr_code(Lx, Ly, src, dst, D, w, prefix):
+    """Straight-line HRR for all (x, y), x in comps(Lx), y in comps(Ly), from src(k) = the value of
+    (comps_range(Lx, Lx + Ly)[k], 0); every intermediate (x, y) node is computed once."""
+    F = comps_range(Lx, Lx + Ly)
+    fidx = {c: k for k, c in enumerate(F)}
+    memo = {}
+
+    def node(x, y):
+        key = (x, y)
+        if key in memo:
+            return memo[key]
+        if sum(y) == 0:
+            memo[key] = src(fidx[x])
+            return memo[key]
+        i = next(a for a in range(3) if y[a] > 0)
+        y1 = tuple(y[a] - (a == i) for a in range(3))
+        x1 = tuple(x[a] + (a == i) for a in range(3))
+        hi, lo = node(x1, y1), node(x, y1)
+        name = f"{prefix}{len(memo)}"
+        w(f"    const RT {name} = qfma({D[i]}, {lo}, {hi});")
+        memo[key] = name
+        return name
+
+    for ix, x in enumerate(comps(Lx)):
+        for iy, y in enumerate(comps(Ly)):
+            w(dst(ix, iy, node(x, y), comp_norm(x) * comp_norm(y)))
+
+
+def gen_class_hrr(LA, LB, LC, LD, idx):
+    L = LA + LB + LC + LD
+    LAB, LCD = LA + LB, LC + LD
+    E, F = comps_range(LA, LAB), comps_range(LC, LCD)
+    HAB = herm_list(LAB)
+    NX = len(HAB)
+    rsm = L >= R_SMEM_MIN_L
+    o = []
+    w = o.append
+    w(f"// class {idx} in HRR form: [e0|f0] has {len(E)} x {len(F)} entries")
+    w(f"constexpr int kHrrE{idx} = {len(E)};")
+    w(f"constexpr int kHrrF{idx} = {len(F)};")
+    # primitive quartet -> sink(ie, if, value)
+    w("template <class RT, class Sink>")
+    w(f"__device__ __forceinline__ void prim_quartet_hrr_{idx}(const PrimPairData& ab, const PrimPairData& cd,")
+    w("    const double* __restrict__ bt, RT* __restrict__ rs, const int rstride, Sink& sink)")
+    w("{")
+    w("    (void)rs; (void)rstride;")
+    r_prologue(L, rsm, w)
+    w("    const RT bPAx = RT(ab.PAx), bPAy = RT(ab.PAy), bPAz = RT(ab.PAz);")
+    w("    const RT kPAx = RT(cd.PAx), kPAy = RT(cd.PAy), kPAz = RT(cd.PAz);")
+    for dname, Lmax, PA, a12 in (("ebx", LAB, "bPAx", "a12b"), ("eby", LAB, "bPAy", "a12b"),
+                                 ("ebz", LAB, "bPAz", "a12b"), ("ekx", LCD, "kPAx", "a12k"),
+                                 ("eky", LCD, "kPAy", "a12k"), ("ekz", LCD, "kPAz", "a12k")):
+        for s_ in gen_E(dname, Lmax, 0, PA, "0", a12):
+            w("    " + s_)
+    for jf, f in enumerate(F):
+        w(f"    {{ // f = {f}")
+        supp = [(tp, up, vp) for tp in range(f[0] + 1) for up in range(f[1] + 1) for vp in range(f[2] + 1)]
+        for (tp, up, vp) in supp:
+            sgn = "-" if (tp + up + vp) & 1 else ""
+            w(f"    const RT s{tp}{up}{vp} = {sgn}ekx_{f[0]}_0_{tp} * eky_{f[1]}_0_{up} * ekz_{f[2]}_0_{vp};")
+        w("    RT " + ", ".join(f"x{i} = RT(0)" for i in range(NX)) + ";")
+        contrib = {}
+        for h in HAB:
+            for hp in supp:
+                H = hidx(L, h[0] + hp[0], h[1] + hp[1], h[2] + hp[2])
+                contrib.setdefault(H, []).append((hidx(LAB, *h), hp))
+        for H in sorted(contrib):
+            body = " ".join(f"x{xi} = qfma(s{hp[0]}{hp[1]}{hp[2]}, r, x{xi});" for (xi, hp) in contrib[H])
+            w(f"    {{ const RT r = RR({H}); {body} }}")
+        for je, e in enumerate(E):
+            w("    {")
+            w("      RT sx = RT(0);")
+            for t in range(e[0] + 1):
+                w("      { RT sy = RT(0);")
+                for u in range(e[1] + 1):
+                    zs = f"ebz_{e[2]}_0_0 * x{hidx(LAB, t, u, 0)}"
+                    for v in range(1, e[2] + 1):
+                        zs = f"qfma(ebz_{e[2]}_0_{v}, x{hidx(LAB, t, u, v)}, {zs})"
+                    w(f"        sy = qfma(eby_{e[1]}_0_{u}, {zs}, sy);")
+                w(f"        sx = qfma(ebx_{e[0]}_0_{t}, sy, sx); }}")
+            w(f"      sink({je}, {jf}, sx * lambda);")
+            w("    }")
+        w("    }")
+    w("#undef RR")
+    w("}")
+    # ket HRR of one e row: p[f] -> y[c * ND + d], times the (c, d) component norms
+    nd = len(comps(LD))
+    w("template <class RT>")
+    w(f"__device__ __forceinline__ void hrr_ket_{idx}(const RT* __restrict__ p, RT* __restrict__ y, const RT CDx,")
+    w("    const RT CDy, const RT CDz)")
+    w("{")
+    hrr_code(LC, LD, lambda k: f"p[{k}]", lambda ix, iy, v, nrm: f"    y[{ix * nd + iy}] = {v} * RT({lit(nrm)});",
+             ("CDx", "CDy", "CDz"), w, "t")
+    w("}")
+    # bra HRR of one (c, d) column: y[e * ys] -> o[(a * NB + b) * os], times the (a, b) component norms
+    nb = len(comps(LB))
+    w("template <class RT>")
+    w(f"__device__ __forceinline__ void hrr_bra_{idx}(const RT* __restrict__ y, const int ys, RT* __restrict__ o,")
+    w("    const int os, const RT ABx, const RT ABy, const RT ABz)")
+    w("{")
+    hrr_code(LA, LB, lambda k: f"y[{k} * ys]",
+             lambda ix, iy, v, nrm: f"    o[{ix * nb + iy} * os] = {v} * RT({lit(nrm)});", ("ABx", "ABy", "ABz"), w,
+             "t")
+    w("}")
+    return o
+
+
+def main_hrr(outdir):
+    """Writes md_hrr_<k>.cuh (the HRR form of class k) for k = 0..20 into outdir."""
+    os.makedirs(outdir, exist_ok=True)
+    for k, (la, lb, lc, ld) in enumerate(classes()):
+        body = gen_class_hrr(la, lb, lc, ld, k)
+        text = ("// generated by gen_md.py (HRR form) -- do not edit\n#pragma once\n#include \"../md_core.cuh\"\n"
+                "namespace qcg {\nnamespace gen {\n" + "\n".join(body) + "\n}  // namespace gen\n}  // namespace qcg\n")
+        with open(os.path.join(outdir, f"md_hrr_{k}.cuh"), "w") as f:
+            f.write(text)

@@ -128,3 +128,76 @@ extern "C" int host_md_eri_f32(long long nq, const int* L, const int* np, const 
 {
     return host_eri<float>(nq, L, np, exps, coefs, cen, out);
 }
+
+#ifdef HM_HRR
+// The HRR form of the same class (gen_md.main_hrr writes gen_hrr/md_hrr_<k>.cuh): [e0|f0] accumulated over
+// the primitive quartets, then the ket recurrence per e row and the bra recurrence per (c d) column.
+#include HM_STR(gen_hrr/HM_CAT(md_hrr_, QCG_CLASS).cuh)
+
+namespace {
+template <class RT>
+struct HrrSink
+{
+    RT* p;
+    int nf;
+    void operator()(int ie, int jf, RT v) { p[ie * nf + jf] += v; }
+};
+}   // namespace
+
+template <class RT>
+int host_eri_hrr(long long nq, const int* L, const int* np, const double* exps, const double* coefs,
+                 const double* cen, RT* out)
+{
+    constexpr int NE = HM_CAT(qcg::gen::kHrrE, QCG_CLASS), NF = HM_CAT(qcg::gen::kHrrF, QCG_CLASS);
+    std::vector<RT> rs(qcg::nherm(16)), P((size_t)NE * NF);
+    for (long long q = 0; q < nq; ++q)
+    {
+        int l[4], n[4];
+        std::vector<double> w[4];
+        for (int s = 0; s < 4; ++s)
+        {
+            const long long r = 4 * q + s;
+            l[s] = L[r];
+            n[s] = np[r];
+            if (n[s] < 1 || n[s] > 8) return 1;
+            w[s] = shell_coefs(l[s], n[s], exps + 8 * r, coefs + 8 * r);
+        }
+        const int na = qcg::ncart(l[0]), nb = qcg::ncart(l[1]), ncd = qcg::ncart(l[2]) * qcg::ncart(l[3]);
+        std::vector<RT> Y((size_t)NE * ncd);
+        std::fill(P.begin(), P.end(), RT(0));
+        HrrSink<RT> sink{P.data(), NF};
+        const double* c0 = cen + 12 * q;
+        for (int i = 0; i < n[0]; ++i)
+            for (int j = 0; j < n[1]; ++j)
+            {
+                const qcg::PrimPairData pab = qcg::make_prim_pair(
+                    exps[8 * (4 * q) + i], c0[0], c0[1], c0[2], w[0][i], exps[8 * (4 * q + 1) + j], c0[3], c0[4],
+                    c0[5], w[1][j]);
+                for (int k = 0; k < n[2]; ++k)
+                    for (int m = 0; m < n[3]; ++m)
+                    {
+                        const qcg::PrimPairData pcd = qcg::make_prim_pair(
+                            exps[8 * (4 * q + 2) + k], c0[6], c0[7], c0[8], w[2][k], exps[8 * (4 * q + 3) + m],
+                            c0[9], c0[10], c0[11], w[3][m]);
+                        HM_CAT(qcg::gen::prim_quartet_hrr_, QCG_CLASS)<RT, HrrSink<RT>>(pab, pcd, kBoysTable,
+                                                                                       rs.data(), 1, sink);
+                    }
+            }
+        const RT CDx = RT(c0[6] - c0[9]), CDy = RT(c0[7] - c0[10]), CDz = RT(c0[8] - c0[11]);
+        const RT ABx = RT(c0[0] - c0[3]), ABy = RT(c0[1] - c0[4]), ABz = RT(c0[2] - c0[5]);
+        for (int e = 0; e < NE; ++e)
+            HM_CAT(qcg::gen::hrr_ket_, QCG_CLASS)<RT>(P.data() + (size_t)e * NF, Y.data() + (size_t)e * ncd, CDx, CDy,
+                                                     CDz);
+        RT* o = out + q * (long long)na * nb * ncd;
+        for (int cd = 0; cd < ncd; ++cd)
+            HM_CAT(qcg::gen::hrr_bra_, QCG_CLASS)<RT>(Y.data() + cd, ncd, o + cd, ncd, ABx, ABy, ABz);
+    }
+    return 0;
+}
+
+extern "C" int host_md_eri_hrr(long long nq, const int* L, const int* np, const double* exps, const double* coefs,
+                               const double* cen, double* out)
+{
+    return host_eri_hrr<double>(nq, L, np, exps, coefs, cen, out);
+}
+#endif

@@ -2,7 +2,8 @@
 kernels run) are compiled for the host with tests/host_md/host_md.cpp and checked against the CPU oracle
 at the GPU parity bar, 1e-12 absolute, for every (s,p,d) class on contracted random shells.  This pins the
 code generator, the Boys function, the R recursion and the Hermite transforms on the CPU; the GPU tests
-pin the kernels that run them."""
+pin the kernels that run them.  The generator's horizontal-recurrence form (gen_md.main_hrr, not yet used
+by the kernels) is held to the same bar."""
 import concurrent.futures as cf
 import ctypes
 import os
@@ -33,18 +34,20 @@ def host_classes(tmp_path_factory):
     finally:
         sys.path.pop(0)
     gen_md.main(os.path.join(tmp, "gen"))
+    gen_md.main_hrr(os.path.join(tmp, "gen_hrr"))
     for name in ("md_core.cuh", "boys_table.h"):
         shutil.copy(os.path.join(CSRC, name), tmp)
     src = os.path.join(HERE, "host_md", "host_md.cpp")
 
     def compile_class(k):
         out = os.path.join(tmp, f"host_md_{k}.so")
-        r = subprocess.run(["g++", "-std=c++17", "-O1", "-fPIC", "-shared", f"-DQCG_CLASS={k}", "-I", tmp, src, "-o",
-                            out], capture_output=True, text=True)
+        r = subprocess.run(["g++", "-std=c++17", "-O1", "-fPIC", "-shared", f"-DQCG_CLASS={k}", "-DHM_HRR", "-I", tmp,
+                            src, "-o", out], capture_output=True, text=True)
         assert r.returncode == 0, r.stderr[-3000:]
         lib = ctypes.CDLL(out)
         lib.host_md_eri.restype = ctypes.c_int
         lib.host_md_eri_f32.restype = ctypes.c_int
+        lib.host_md_eri_hrr.restype = ctypes.c_int
         assert lib.host_md_class() == k
         return k, lib
 
@@ -111,3 +114,23 @@ def test_generated_class_fp32_form(k, host_classes, oracle_mod):
     ref = oracle_mod.OracleBasis(pool).eri_batch(q).reshape(-1)
     rel = np.abs(out.astype(np.float64) - ref).max() / np.abs(ref).max()
     assert 0 < rel <= 2e-5, (cls, rel)
+
+
+@pytest.mark.parametrize("k", range(21))
+def test_generated_class_hrr_form(k, host_classes, oracle_mod):
+    """[e0|f0] accumulated over the primitives, then the ket and bra horizontal recurrences: the same
+    integrals as the direct form, to 1e-12 absolute and relative to the largest integral."""
+    cls = W.quartet_classes()[k]
+    pool = W.shell_pool(16, seed=W.SEED0 + 2100, box=3.0)
+    q = W.eri_class_batch(cls, NQ, 16, seed=W.SEED0 + 2100 + k)
+    L, npr, ex, co, cen = _pack(pool, q)
+    blk = int(np.prod([(l + 1) * (l + 2) // 2 for l in cls]))
+    out = np.zeros(NQ * blk)
+    p = lambda a, t: a.ctypes.data_as(ctypes.POINTER(t))
+    rc = host_classes[k].host_md_eri_hrr(ctypes.c_longlong(NQ), p(L, ctypes.c_int), p(npr, ctypes.c_int),
+                                         p(ex, ctypes.c_double), p(co, ctypes.c_double), p(cen, ctypes.c_double),
+                                         p(out, ctypes.c_double))
+    assert rc == 0
+    ref = oracle_mod.OracleBasis(pool).eri_batch(q).reshape(-1)
+    err = np.abs(out - ref).max()
+    assert err <= ERI_ABS and err <= 1e-12 * np.abs(ref).max(), (cls, err, np.abs(ref).max())
