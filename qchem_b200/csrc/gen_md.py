@@ -333,9 +333,12 @@ def comps_range(L0, L1):
 
 def hrr_code(Lx, Ly, src, dst, D, w, prefix):
     """Straight-line HRR for all (x, y), x in comps(Lx), y in comps(Ly), from src(k) = the value of
-    (comps_range(Lx, Lx + Ly)[k], 0); every intermediate (x, y) node is computed once."""
+    (comps_range(Lx, Lx + Ly)[k], 0); every intermediate (x, y) node is computed once.  All sources are
+    loaded before the first result is stored, so the results may overwrite the sources (in place)."""
     F = comps_range(Lx, Lx + Ly)
     fidx = {c: k for k, c in enumerate(F)}
+    for k in range(len(F)):
+        w(f"    const RT {prefix}s{k} = {src(k)};")
     memo = {}
 
     def node(x, y):
@@ -343,7 +346,7 @@ def hrr_code(Lx, Ly, src, dst, D, w, prefix):
         if key in memo:
             return memo[key]
         if sum(y) == 0:
-            memo[key] = src(fidx[x])
+            memo[key] = f"{prefix}s{fidx[x]}"
             return memo[key]
         i = next(a for a in range(3) if y[a] > 0)
         y1 = tuple(y[a] - (a == i) for a in range(3))
@@ -416,19 +419,20 @@ def gen_class_hrr(LA, LB, LC, LD, idx):
         w("    }")
     w("#undef RR")
     w("}")
-    # ket HRR of one e row: p[f] -> y[c * ND + d], times the (c, d) component norms
+    # ket HRR of one e row: p[f] -> y[c * ND + d], times the (c, d) component norms (y may be p)
     nd = len(comps(LD))
     w("template <class RT>")
-    w(f"__device__ __forceinline__ void hrr_ket_{idx}(const RT* __restrict__ p, RT* __restrict__ y, const RT CDx,")
+    w(f"__device__ __forceinline__ void hrr_ket_{idx}(const RT* p, RT* y, const RT CDx,")
     w("    const RT CDy, const RT CDz)")
     w("{")
     hrr_code(LC, LD, lambda k: f"p[{k}]", lambda ix, iy, v, nrm: f"    y[{ix * nd + iy}] = {v} * RT({lit(nrm)});",
              ("CDx", "CDy", "CDz"), w, "t")
     w("}")
     # bra HRR of one (c, d) column: y[e * ys] -> o[(a * NB + b) * os], times the (a, b) component norms
+    # (o may be y, with os == ys)
     nb = len(comps(LB))
     w("template <class RT>")
-    w(f"__device__ __forceinline__ void hrr_bra_{idx}(const RT* __restrict__ y, const int ys, RT* __restrict__ o,")
+    w(f"__device__ __forceinline__ void hrr_bra_{idx}(const RT* y, const int ys, RT* o,")
     w("    const int os, const RT ABx, const RT ABy, const RT ABz)")
     w("{")
     hrr_code(LA, LB, lambda k: f"y[{k} * ys]",

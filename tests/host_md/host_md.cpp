@@ -200,4 +200,61 @@ extern "C" int host_md_eri_hrr(long long nq, const int* L, const int* np, const 
 {
     return host_eri_hrr<double>(nq, L, np, exps, coefs, cen, out);
 }
+
+// The data flow planned for the GPU kernel, inside each quartet's own output block (n_a n_b rows of
+// n_c n_d): [e0|f0] accumulated at o[e * ncd + f], the ket recurrence in place per e row, then the bra
+// recurrence in place per (c d) column.
+extern "C" int host_md_eri_hrr_inplace(long long nq, const int* L, const int* np, const double* exps,
+                                       const double* coefs, const double* cen, double* out)
+{
+    constexpr int NE = HM_CAT(qcg::gen::kHrrE, QCG_CLASS), NF = HM_CAT(qcg::gen::kHrrF, QCG_CLASS);
+    std::vector<double> rs(qcg::nherm(16));
+    for (long long q = 0; q < nq; ++q)
+    {
+        int l[4], n[4];
+        std::vector<double> w[4];
+        for (int s = 0; s < 4; ++s)
+        {
+            const long long r = 4 * q + s;
+            l[s] = L[r];
+            n[s] = np[r];
+            if (n[s] < 1 || n[s] > 8) return 1;
+            w[s] = shell_coefs(l[s], n[s], exps + 8 * r, coefs + 8 * r);
+        }
+        const int na = qcg::ncart(l[0]), nb = qcg::ncart(l[1]), ncd = qcg::ncart(l[2]) * qcg::ncart(l[3]);
+        if (NE > na * nb || NF > ncd) return 2;
+        double* o = out + q * (long long)na * nb * ncd;
+        for (int k = 0; k < na * nb * ncd; ++k) o[k] = 0.0;
+        struct RowSink
+        {
+            double* o;
+            int ncd;
+            void operator()(int ie, int jf, double v) { o[ie * ncd + jf] += v; }
+        } sink{o, ncd};
+        const double* c0 = cen + 12 * q;
+        for (int i = 0; i < n[0]; ++i)
+            for (int j = 0; j < n[1]; ++j)
+            {
+                const qcg::PrimPairData pab = qcg::make_prim_pair(
+                    exps[8 * (4 * q) + i], c0[0], c0[1], c0[2], w[0][i], exps[8 * (4 * q + 1) + j], c0[3], c0[4],
+                    c0[5], w[1][j]);
+                for (int k = 0; k < n[2]; ++k)
+                    for (int m = 0; m < n[3]; ++m)
+                    {
+                        const qcg::PrimPairData pcd = qcg::make_prim_pair(
+                            exps[8 * (4 * q + 2) + k], c0[6], c0[7], c0[8], w[2][k], exps[8 * (4 * q + 3) + m],
+                            c0[9], c0[10], c0[11], w[3][m]);
+                        HM_CAT(qcg::gen::prim_quartet_hrr_, QCG_CLASS)<double, RowSink>(pab, pcd, kBoysTable,
+                                                                                       rs.data(), 1, sink);
+                    }
+            }
+        for (int e = 0; e < NE; ++e)
+            HM_CAT(qcg::gen::hrr_ket_, QCG_CLASS)<double>(o + (size_t)e * ncd, o + (size_t)e * ncd, c0[6] - c0[9],
+                                                         c0[7] - c0[10], c0[8] - c0[11]);
+        for (int cd = 0; cd < ncd; ++cd)
+            HM_CAT(qcg::gen::hrr_bra_, QCG_CLASS)<double>(o + cd, ncd, o + cd, ncd, c0[0] - c0[3], c0[1] - c0[4],
+                                                         c0[2] - c0[5]);
+    }
+    return 0;
+}
 #endif

@@ -48,6 +48,7 @@ def host_classes(tmp_path_factory):
         lib.host_md_eri.restype = ctypes.c_int
         lib.host_md_eri_f32.restype = ctypes.c_int
         lib.host_md_eri_hrr.restype = ctypes.c_int
+        lib.host_md_eri_hrr_inplace.restype = ctypes.c_int
         assert lib.host_md_class() == k
         return k, lib
 
@@ -127,10 +128,12 @@ def test_generated_class_hrr_form(k, host_classes, oracle_mod):
     blk = int(np.prod([(l + 1) * (l + 2) // 2 for l in cls]))
     out = np.zeros(NQ * blk)
     p = lambda a, t: a.ctypes.data_as(ctypes.POINTER(t))
-    rc = host_classes[k].host_md_eri_hrr(ctypes.c_longlong(NQ), p(L, ctypes.c_int), p(npr, ctypes.c_int),
-                                         p(ex, ctypes.c_double), p(co, ctypes.c_double), p(cen, ctypes.c_double),
-                                         p(out, ctypes.c_double))
-    assert rc == 0
     ref = oracle_mod.OracleBasis(pool).eri_batch(q).reshape(-1)
-    err = np.abs(out - ref).max()
-    assert err <= ERI_ABS and err <= 1e-12 * np.abs(ref).max(), (cls, err, np.abs(ref).max())
+    # separate buffers, and in place in each quartet's output block (the planned kernel data flow)
+    for fn in (host_classes[k].host_md_eri_hrr, host_classes[k].host_md_eri_hrr_inplace):
+        out[:] = np.nan
+        rc = fn(ctypes.c_longlong(NQ), p(L, ctypes.c_int), p(npr, ctypes.c_int), p(ex, ctypes.c_double),
+                p(co, ctypes.c_double), p(cen, ctypes.c_double), p(out, ctypes.c_double))
+        assert rc == 0
+        err = np.abs(out - ref).max()
+        assert err <= ERI_ABS and err <= 1e-12 * np.abs(ref).max(), (cls, fn.__name__, err, np.abs(ref).max())
