@@ -1,0 +1,94 @@
+// host_jk.cpp -- test harness: the library's J/K digestion sink (JKSink in qchem_b200/csrc/eri_kernels.cuh)
+// driven by the generated code of ONE quartet class on the host, for one shell quartet at a time.  It
+// digests either the whole quartet (as jk_kernel does) or chunk by chunk, each chunk with its own sink and
+// a row flush after every primitive quartet (as jk_split_kernel does).  Build with the CUDA stand-in first
+// on the include path:
+//   g++ -std=c++17 -O1 -fPIC -shared -DQCG_CLASS=<k> -I tests/host_md/shim -I <csrc> host_jk.cpp -o ...
+#include <cmath>
+#include <vector>
+
+#include <cuda_runtime.h>   // the stand-in from tests/host_md/shim, before any library header
+#include "eri_kernels.cuh"
+#include "boys_table.h"
+
+HostDim3 blockIdx, threadIdx, blockDim, gridDim;
+namespace qcg {
+double qcg_smem[1];   // the kernels' shared R window (unused: the harness passes its own R slice)
+}
+
+#define HJ_STR2(x) #x
+#define HJ_STR(x) HJ_STR2(x)
+#define HJ_CAT2(a, b) a##b
+#define HJ_CAT(a, b) HJ_CAT2(a, b)
+#include HJ_STR(gen/HJ_CAT(md_class_, QCG_CLASS).cuh)
+
+namespace {
+constexpr int kPairLAh[6] = {0, 1, 1, 2, 2, 2}, kPairLBh[6] = {0, 0, 1, 0, 1, 2};
+constexpr int cls_X()
+{
+    int X = 0;
+    while ((X + 1) * (X + 2) / 2 <= QCG_CLASS) ++X;
+    return X;
+}
+constexpr int kX = cls_X(), kY = QCG_CLASS - kX * (kX + 1) / 2;
+constexpr int LA = kPairLAh[kX], LB = kPairLBh[kX], LC = kPairLAh[kY], LD = kPairLBh[kY];
+using Sink = qcg::JKSink<double, LA, LB, LC, LD>;
+}   // namespace
+
+extern "C" int host_jk_nchunk() { return HJ_CAT(qcg::gen::kNChunk, QCG_CLASS); }
+
+// One quartet of primitive pairs: npa x npc primitive pairs given as PrimPairData rows (11 doubles each:
+// p, P, PA, PB, K), function offsets fa fb fc fd into the n x n matrices, symmetry weight s.  Adds the
+// quartet's contributions to J' and K' (row-major n x n).  split = 0: the whole quartet through one sink;
+// split = 1: every ket-component chunk through its own sink, with a row flush after each primitive quartet.
+extern "C" int host_jk_quartet(int npa, const double* pa, int npc, const double* pc, int fa, int fb, int fc, int fd,
+                               double s, const double* D, double* J, double* K, int n, int split)
+{
+    auto load = [](const double* r) {
+        qcg::PrimPairData d;
+        d.p = r[0];
+        d.Px = r[1]; d.Py = r[2]; d.Pz = r[3];
+        d.PAx = r[4]; d.PAy = r[5]; d.PAz = r[6];
+        d.PBx = r[7]; d.PBy = r[8]; d.PBz = r[9];
+        d.K = r[10];
+        return d;
+    };
+    std::vector<double> rs(qcg::nherm(16));
+    const int nchunk = split ? HJ_CAT(qcg::gen::kNChunk, QCG_CLASS) : 1;
+    for (int c = 0; c < nchunk; ++c)
+    {
+        Sink sink;
+        sink.D = D;
+        sink.J = J;
+        sink.K = K;
+        sink.n = n;
+        sink.set_bra(fa, fb);
+        sink.fc = fc;
+        sink.fd = fd;
+        sink.s = s;
+        for (int x = 0; x < npa; ++x)
+            for (int y = 0; y < npc; ++y)
+            {
+                const qcg::PrimPairData ab = load(pa + 11 * x), cd = load(pc + 11 * y);
+                if (split)
+                {
+                    HJ_CAT(qcg::gen::prim_quartet_chunk_, QCG_CLASS)<double, Sink>(c, ab, cd, kBoysTable, rs.data(),
+                                                                                  1, sink);
+                    sink.flush_k_row();
+                }
+                else
+                    HJ_CAT(qcg::gen::prim_quartet_, QCG_CLASS)<double, Sink>(ab, cd, kBoysTable, rs.data(), 1, sink);
+            }
+        sink.flush_bra();
+    }
+    return 0;
+}
+
+// the primitive-pair row of two primitives, as the library forms it (make_prim_pair)
+extern "C" void host_prim_pair(double a, const double* A, double ca, double b, const double* B, double cb,
+                               double* row)
+{
+    const qcg::PrimPairData d = qcg::make_prim_pair(a, A[0], A[1], A[2], ca, b, B[0], B[1], B[2], cb);
+    const double v[11] = {d.p, d.Px, d.Py, d.Pz, d.PAx, d.PAy, d.PAz, d.PBx, d.PBy, d.PBz, d.K};
+    for (int k = 0; k < 11; ++k) row[k] = v[k];
+}

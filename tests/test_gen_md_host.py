@@ -3,7 +3,9 @@ kernels run) are compiled for the host with tests/host_md/host_md.cpp and checke
 at the GPU parity bar, 1e-12 absolute, for every (s,p,d) class on contracted random shells.  This pins the
 code generator, the Boys function, the R recursion and the Hermite transforms on the CPU; the GPU tests
 pin the kernels that run them.  The generator's horizontal-recurrence form (gen_md.main_hrr, not yet used
-by the kernels) is held to the same bar."""
+by the kernels) is held to the same bar, and the library's J/K digestion sink (eri_kernels.cuh, compiled
+with the CUDA stand-in in tests/host_md/shim) is checked against its digestion formulas, as one quartet and
+chunk by chunk as the few-quartet J/K kernel runs it."""
 import concurrent.futures as cf
 import ctypes
 import os
@@ -137,3 +139,110 @@ def test_generated_class_hrr_form(k, host_classes, oracle_mod):
         assert rc == 0
         err = np.abs(out - ref).max()
         assert err <= ERI_ABS and err <= 1e-12 * np.abs(ref).max(), (cls, fn.__name__, err, np.abs(ref).max())
+
+
+@pytest.fixture(scope="session")
+def host_jk(tmp_path_factory):
+    """{class index: ctypes library} of tests/host_md/host_jk.cpp (the J/K digestion sink on the host)."""
+    if shutil.which("g++") is None:
+        pytest.skip("g++ is not available")
+    tmp = str(tmp_path_factory.mktemp("host_jk"))
+    sys.path.insert(0, CSRC)
+    try:
+        import gen_md
+    finally:
+        sys.path.pop(0)
+    gen_md.main(os.path.join(tmp, "gen"))
+    for name in ("md_core.cuh", "boys_table.h", "eri_kernels.cuh", "qcg_internal.h"):
+        shutil.copy(os.path.join(CSRC, name), tmp)
+    src = os.path.join(HERE, "host_md", "host_jk.cpp")
+    shim = os.path.join(HERE, "host_md", "shim")
+
+    def compile_class(k):
+        out = os.path.join(tmp, f"host_jk_{k}.so")
+        r = subprocess.run(["g++", "-std=c++17", "-O1", "-fPIC", "-shared", f"-DQCG_CLASS={k}", "-I", shim, "-I", tmp,
+                            src, "-o", out], capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr[-3000:]
+        lib = ctypes.CDLL(out)
+        lib.host_jk_quartet.restype = ctypes.c_int
+        lib.host_jk_nchunk.restype = ctypes.c_int
+        return k, lib
+
+    with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
+        return dict(ex.map(compile_class, range(len(W.quartet_classes()))))
+
+
+def _norm_coefs(sh):
+    """The library's contraction preprocessing: (L,0,0) primitive norms folded in, unit radial self-overlap."""
+    a = np.asarray(sh.exps, dtype=float)
+    L = sh.L
+    dfact = float(np.prod(np.arange(2 * L - 1, 0, -2))) if L > 0 else 1.0
+    w = np.asarray(sh.coefs, dtype=float) * np.sqrt((4 * a) ** L / ((np.pi / (2 * a)) ** 1.5 * dfact))
+    p = a[:, None] + a[None, :]
+    ss = (w[:, None] * w[None, :] * (np.pi / p) ** 1.5 / (2 * p) ** L).sum()
+    return w / np.sqrt(ss)
+
+
+@pytest.mark.parametrize("k", range(21))
+def test_jk_sink_digests_like_its_formulas(k, host_classes, host_jk):
+    """For one shell quartet of each class: J' and K' from the library's digestion sink, both as one
+    quartet (jk_kernel) and chunk by chunk with a row flush after every primitive quartet
+    (jk_split_kernel), against the digestion formulas applied to the quartet's ERI block."""
+    cls = W.quartet_classes()[k]
+    pool = W.shell_pool(16, seed=W.SEED0 + 2200, box=3.0)
+    q = W.eri_class_batch(cls, 40, 16, seed=W.SEED0 + 2200 + k)
+    quartet = next(x for x in q if len(set(int(s) for s in x)) == 4)   # four distinct shells
+    shells = [pool[int(s)] for s in quartet]
+    nf = [(s.L + 1) * (s.L + 2) // 2 for s in shells]
+    f0 = np.concatenate([[0], np.cumsum(nf)[:-1]]).astype(int)
+    n = int(sum(nf))
+    # the quartet's ERI block from the generated code (checked against the oracle above)
+    L, npr, ex, co, cen = _pack(pool, np.asarray([quartet]))
+    eri = np.zeros(int(np.prod(nf)))
+    p = lambda a, t: a.ctypes.data_as(ctypes.POINTER(t))
+    assert host_classes[k].host_md_eri(ctypes.c_longlong(1), p(L, ctypes.c_int), p(npr, ctypes.c_int),
+                                       p(ex, ctypes.c_double), p(co, ctypes.c_double), p(cen, ctypes.c_double),
+                                       p(eri, ctypes.c_double)) == 0
+    eri = eri.reshape(nf)
+    rng = np.random.default_rng(k)
+    D = rng.normal(size=(n, n))
+    D = D + D.T
+    s = 0.75   # a symmetry weight as the kernels pass it
+    # the sink's formulas: w = s (mu nu|la si); J'[mu nu] += 2 w D[la si], J'[la si] += 2 w D[mu nu],
+    # K'[mu la] += w D[nu si], K'[nu la] += w D[mu si], K'[mu si] += w D[nu la], K'[nu si] += w D[mu la]
+    Jr, Kr = np.zeros((n, n)), np.zeros((n, n))
+    for a in range(nf[0]):
+        for b in range(nf[1]):
+            for c in range(nf[2]):
+                for d in range(nf[3]):
+                    mu, nu, la, si = f0[0] + a, f0[1] + b, f0[2] + c, f0[3] + d
+                    wv = s * eri[a, b, c, d]
+                    Jr[mu, nu] += 2 * wv * D[la, si]
+                    Jr[la, si] += 2 * wv * D[mu, nu]
+                    Kr[mu, la] += wv * D[nu, si]
+                    Kr[nu, la] += wv * D[mu, si]
+                    Kr[mu, si] += wv * D[nu, la]
+                    Kr[nu, si] += wv * D[mu, la]
+    # primitive pairs as the library forms them
+    def pairs(s1, s2):
+        w1, w2 = _norm_coefs(s1), _norm_coefs(s2)
+        rows = []
+        for i, a in enumerate(s1.exps):
+            for j, b in enumerate(s2.exps):
+                row = np.zeros(11)
+                host_jk[k].host_prim_pair(ctypes.c_double(a), p(np.asarray(s1.centre, dtype=float), ctypes.c_double),
+                                          ctypes.c_double(w1[i]), ctypes.c_double(b),
+                                          p(np.asarray(s2.centre, dtype=float), ctypes.c_double),
+                                          ctypes.c_double(w2[j]), p(row, ctypes.c_double))
+                rows.append(row)
+        return np.ascontiguousarray(np.array(rows))
+    pab, pcd = pairs(shells[0], shells[1]), pairs(shells[2], shells[3])
+    scale = max(np.abs(Jr).max(), np.abs(Kr).max())
+    for split in (0, 1):
+        J, K = np.zeros((n, n)), np.zeros((n, n))
+        assert host_jk[k].host_jk_quartet(len(pab), p(pab, ctypes.c_double), len(pcd), p(pcd, ctypes.c_double),
+                                          int(f0[0]), int(f0[1]), int(f0[2]), int(f0[3]), ctypes.c_double(s),
+                                          p(D, ctypes.c_double), p(J, ctypes.c_double), p(K, ctypes.c_double), n,
+                                          split) == 0
+        assert np.abs(J - Jr).max() <= 1e-12 * scale and np.abs(K - Kr).max() <= 1e-12 * scale, (cls, split)
+    assert host_jk[k].host_jk_nchunk() >= 1
