@@ -13,7 +13,8 @@
 
 HostDim3 blockIdx, threadIdx, blockDim, gridDim;
 namespace qcg {
-double qcg_smem[1];   // the kernels' shared R window (unused: the harness passes its own R slice)
+// the kernels' shared-memory window: per-thread R slices of up to 165 entries at a stride of the block size
+double qcg_smem[128 * 165];
 }
 
 #define HJ_STR2(x) #x
@@ -91,4 +92,67 @@ extern "C" void host_prim_pair(double a, const double* A, double ca, double b, c
     const qcg::PrimPairData d = qcg::make_prim_pair(a, A[0], A[1], A[2], ca, b, B[0], B[1], B[2], cb);
     const double v[11] = {d.p, d.Px, d.Py, d.Pz, d.PAx, d.PAy, d.PAz, d.PBx, d.PBy, d.PBz, d.K};
     for (int k = 0; k < 11; ++k) row[k] = v[k];
+}
+
+namespace {
+// the class wrapper the kernels expect (as qchem_b200/csrc/eri_class.cu defines it)
+struct Cls
+{
+    static constexpr int LA = ::LA, LB = ::LB, LC = ::LC, LD = ::LD;
+    static constexpr bool kRShared = HJ_CAT(qcg::gen::kRShared, QCG_CLASS);
+    static constexpr bool kChunked = HJ_CAT(qcg::gen::kChunked, QCG_CLASS);
+    static constexpr int kRSize = HJ_CAT(qcg::gen::kRSize, QCG_CLASS);
+    static constexpr int kNChunk = HJ_CAT(qcg::gen::kNChunk, QCG_CLASS);
+    template <class RT, class S, bool LOCKSTEP = false>
+    static void quartet(const qcg::PrimPairData& ab, const qcg::PrimPairData& cd, const double* bt, RT* rs,
+                        int stride, S& sink)
+    {
+        HJ_CAT(qcg::gen::prim_quartet_, QCG_CLASS)<RT, S, LOCKSTEP>(ab, cd, bt, rs, stride, sink);
+    }
+    template <class RT, class S>
+    static void quartet_chunk(int c, const qcg::PrimPairData& ab, const qcg::PrimPairData& cd, const double* bt,
+                              RT* rs, int stride, S& sink)
+    {
+        HJ_CAT(qcg::gen::prim_quartet_chunk_, QCG_CLASS)<RT, S>(c, ab, cd, bt, rs, stride, sink);
+    }
+};
+constexpr int kThreads = Cls::kRShared ? 64 : 128;   // the library's block size for the class
+}   // namespace
+
+// The library's J/K kernels over a hand-made work list, every (block, thread) of the grid run in turn:
+// split = 0 runs jk_kernel with `run` quartets per lane, split = 1 runs jk_split_kernel.  Pair lists are
+// (sa, sb, ppo, npp, Q) per pair; P holds the primitive pairs as 11 arrays of np entries (p, P, PA, PB, K);
+// offs[i] .. offs[i+1] are bra pair i's quartets (kets from 0).  No density screening, no precision band.
+extern "C" int host_jk_kernel(int split, int run, int grid, int nbra, const int* bsa, const int* bsb,
+                              const int* bppo, const int* bnpp, const double* bQ, int nket, const int* ksa,
+                              const int* ksb, const int* kppo, const int* knpp, const double* kQ, const double* P,
+                              int np, const long long* offs, int same_class, const int* f0, const double* D, double* J,
+                              double* K, int n)
+{
+    if (kThreads * Cls::kRSize > 128 * 165) return 1;
+    qcg::PairListDev bra{nbra, bsa, bsb, bppo, bnpp, bQ, nullptr}, ket{nket, ksa, ksb, kppo, knpp, kQ, nullptr};
+    qcg::PrimPairsDev pp{P, P + np, P + 2 * np, P + 3 * np, P + 4 * np, P + 5 * np, P + 6 * np, P + 7 * np,
+                         P + 8 * np, P + 9 * np, P + 10 * np};
+    qcg::JKWorkDev w{};
+    w.total = offs[nbra];
+    w.gbeg = 0;
+    w.gend = w.total;
+    w.offs = offs;
+    w.same_class = same_class;
+    w.lo = 0.0;
+    w.hi = HUGE_VAL;
+    w.mols = qcg::MolLayoutDev{1, nullptr, nullptr};
+    blockDim.x = kThreads;
+    gridDim.x = grid;
+    for (int b = 0; b < grid; ++b)
+        for (int t = 0; t < kThreads; ++t)
+        {
+            blockIdx.x = b;
+            threadIdx.x = t;
+            if (split)
+                qcg::jk_split_kernel<Cls, kThreads, double>(w, bra, ket, pp, f0, D, J, K, n, kBoysTable);
+            else
+                qcg::jk_kernel<Cls, kThreads, double>(w, bra, ket, pp, f0, D, J, K, n, kBoysTable, run);
+        }
+    return 0;
 }

@@ -166,6 +166,7 @@ def host_jk(tmp_path_factory):
         lib = ctypes.CDLL(out)
         lib.host_jk_quartet.restype = ctypes.c_int
         lib.host_jk_nchunk.restype = ctypes.c_int
+        lib.host_jk_kernel.restype = ctypes.c_int
         return k, lib
 
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
@@ -246,3 +247,92 @@ def test_jk_sink_digests_like_its_formulas(k, host_classes, host_jk):
                                           split) == 0
         assert np.abs(J - Jr).max() <= 1e-12 * scale and np.abs(K - Kr).max() <= 1e-12 * scale, (cls, split)
     assert host_jk[k].host_jk_nchunk() >= 1
+
+
+@pytest.mark.parametrize("k", range(21))
+def test_jk_kernels_on_a_work_list(k, host_classes, host_jk):
+    """The library's jk_kernel (1 and 3 quartets per lane, one and two blocks) and jk_split_kernel run on
+    the host over every canonical quartet of one class in a six-shell basis (two s, two p, two d, contracted):
+    J' and K' equal the digestion of each quartet's ERI block with its symmetry weight."""
+    X = next(x for x in range(6) if (x + 1) * (x + 2) // 2 > k)
+    Y = k - X * (X + 1) // 2
+    pair_L = [(0, 0), (1, 0), (1, 1), (2, 0), (2, 1), (2, 2)]
+    npool = 16
+    pool = W.shell_pool(npool, seed=W.SEED0 + 2300, box=3.0)
+    basis = [L * npool + i for L in range(3) for i in range(2)]          # pool indices, s s p p d d
+    Ls = [pool[b].L for b in basis]
+    nf = [(L + 1) * (L + 2) // 2 for L in Ls]
+    f0 = np.concatenate([[0], np.cumsum(nf)[:-1]]).astype(np.int32)
+    n = int(sum(nf))
+
+    def pairs_of(cls_idx):
+        la, lb = pair_L[cls_idx]
+        return [(a, b) for a in range(6) for b in range(6)
+                if Ls[a] == la and Ls[b] == lb and (la > lb or a >= b)]
+
+    bra_pairs, ket_pairs = pairs_of(X), pairs_of(Y)
+    same = X == Y
+    p = lambda a, t: a.ctypes.data_as(ctypes.POINTER(t))
+    # primitive pairs of every bra and ket pair in one table
+    rows, ppo, npp = [], {}, {}
+    for (a, b) in sorted(set(bra_pairs) | set(ket_pairs)):
+        sa, sb = pool[basis[a]], pool[basis[b]]
+        wa, wb = _norm_coefs(sa), _norm_coefs(sb)
+        ppo[(a, b)] = len(rows)
+        for i, ea in enumerate(sa.exps):
+            for j, eb in enumerate(sb.exps):
+                row = np.zeros(11)
+                host_jk[k].host_prim_pair(ctypes.c_double(ea), p(np.asarray(sa.centre, dtype=float), ctypes.c_double),
+                                          ctypes.c_double(wa[i]), ctypes.c_double(eb),
+                                          p(np.asarray(sb.centre, dtype=float), ctypes.c_double),
+                                          ctypes.c_double(wb[j]), p(row, ctypes.c_double))
+                rows.append(row)
+        npp[(a, b)] = len(rows) - ppo[(a, b)]
+    P = np.ascontiguousarray(np.array(rows).T)                            # 11 arrays of np entries
+
+    def lists(prs):
+        return (np.array([a for a, _ in prs], dtype=np.int32), np.array([b for _, b in prs], dtype=np.int32),
+                np.array([ppo[x] for x in prs], dtype=np.int32), np.array([npp[x] for x in prs], dtype=np.int32),
+                np.ones(len(prs)))
+
+    bra, ket = lists(bra_pairs), lists(ket_pairs)
+    counts = [i + 1 if same else len(ket_pairs) for i in range(len(bra_pairs))]
+    offs = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    rng = np.random.default_rng(100 + k)
+    D = rng.normal(size=(n, n))
+    D = D + D.T
+    # reference: every canonical quartet's ERI block, digested with its weight
+    Jr, Kr = np.zeros((n, n)), np.zeros((n, n))
+    for i, (a, b) in enumerate(bra_pairs):
+        for j in range(counts[i]):
+            c, d = ket_pairs[j]
+            L4, npr, ex, co, cen = _pack(pool, np.asarray([[basis[a], basis[b], basis[c], basis[d]]]))
+            blk = np.zeros(nf[a] * nf[b] * nf[c] * nf[d])
+            assert host_classes[k].host_md_eri(ctypes.c_longlong(1), p(L4, ctypes.c_int), p(npr, ctypes.c_int),
+                                               p(ex, ctypes.c_double), p(co, ctypes.c_double),
+                                               p(cen, ctypes.c_double), p(blk, ctypes.c_double)) == 0
+            blk = blk.reshape(nf[a], nf[b], nf[c], nf[d])
+            s = (0.5 if a == b else 1.0) * (0.5 if c == d else 1.0) * (0.5 if same and i == j else 1.0)
+            for x in range(nf[a]):
+                for y in range(nf[b]):
+                    for z in range(nf[c]):
+                        for t in range(nf[d]):
+                            mu, nu, la, si = f0[a] + x, f0[b] + y, f0[c] + z, f0[d] + t
+                            wv = s * blk[x, y, z, t]
+                            Jr[mu, nu] += 2 * wv * D[la, si]
+                            Jr[la, si] += 2 * wv * D[mu, nu]
+                            Kr[mu, la] += wv * D[nu, si]
+                            Kr[nu, la] += wv * D[mu, si]
+                            Kr[mu, si] += wv * D[nu, la]
+                            Kr[nu, si] += wv * D[mu, la]
+    scale = max(np.abs(Jr).max(), np.abs(Kr).max())
+    for split, run, grid in ((0, 1, 1), (0, 3, 2), (1, 1, 2)):
+        J, K = np.zeros((n, n)), np.zeros((n, n))
+        rc = host_jk[k].host_jk_kernel(split, run, grid, len(bra_pairs), *(p(x, ctypes.c_int) for x in bra[:4]),
+                                       p(bra[4], ctypes.c_double), len(ket_pairs),
+                                       *(p(x, ctypes.c_int) for x in ket[:4]), p(ket[4], ctypes.c_double),
+                                       p(P, ctypes.c_double), P.shape[1], p(offs, ctypes.c_longlong), int(same),
+                                       p(f0, ctypes.c_int), p(D, ctypes.c_double), p(J, ctypes.c_double),
+                                       p(K, ctypes.c_double), n)
+        assert rc == 0
+        assert np.abs(J - Jr).max() <= 1e-12 * scale and np.abs(K - Kr).max() <= 1e-12 * scale, (k, split, run, grid)
