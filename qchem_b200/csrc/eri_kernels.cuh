@@ -135,6 +135,57 @@ __global__ void __launch_bounds__(THREADS) eri_batch_lockstep_kernel(BasisDev bs
     }
 }
 
+// Cartesian ERI batch in horizontal-recurrence form; the library does not instantiate it yet, and the
+// host tests run it.  Cls provides the generated HRR functions (gen_md.main_hrr): quartet_hrr adds a
+// primitive quartet's [e0|f0] block (e over L = LA..LA+LB on centre A, f over L = LC..LC+LD on centre C)
+// into the zeroed output block at row stride n_c n_d with red.global.  After the primitives, hrr_ket
+// carries each e row to [e0|cd] in place, and hrr_bra carries each (c d) column to (ab|cd) in place.  The
+// recurrences read back through L2 (ld_l2), where the red.global updates are.  The block always has room:
+// |E| <= n_a n_b and |F| <= n_c n_d.
+template <class RT, int NCD>
+struct HrrRowSink
+{
+    RT* o;
+    __device__ __forceinline__ void operator()(int ie, int jf, RT v) { atomicAdd(o + ie * NCD + jf, v); }
+};
+
+template <class Cls, int THREADS, class RT>
+__global__ void __launch_bounds__(THREADS) eri_batch_hrr_kernel(BasisDev bs, const int4* __restrict__ quartets,
+                                                                const int* __restrict__ order, long long nq,
+                                                                RT* __restrict__ out,
+                                                                const double* __restrict__ boys_table)
+{
+    constexpr int NCD = ncart(Cls::LC) * ncart(Cls::LD);
+    constexpr long long BLK = (long long)ncart(Cls::LA) * ncart(Cls::LB) * NCD;
+    static_assert(Cls::kHrrE <= ncart(Cls::LA) * ncart(Cls::LB) && Cls::kHrrF <= NCD, "[e0|f0] fits the block");
+    RT* rs = r_slice<RT>();
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < nq; g += (long long)gridDim.x * blockDim.x)
+    {
+        const long long q = order ? order[g] : g;
+        const int4 s = quartets[q];
+        RT* o = out + q * BLK;
+        for (int k = 0; k < (int)BLK; ++k) o[k] = RT(0);
+        HrrRowSink<RT, NCD> sink{o};
+        const int ni = bs.nprim[s.x], nj = bs.nprim[s.y], nk = bs.nprim[s.z], nl = bs.nprim[s.w];
+        const int nket = nk * nl, ntot = ni * nj * nket;
+        for (int x = 0; x < ntot; ++x)
+        {
+            const int ij = x / nket, kl = x - ij * nket;
+            const PrimPairData ab = shell_prim_pair(bs, s.x, ij / nj, s.y, ij % nj);
+            const PrimPairData cd = shell_prim_pair(bs, s.z, kl / nl, s.w, kl % nl);
+            Cls::template quartet_hrr<RT>(ab, cd, boys_table, rs, THREADS, sink);
+        }
+        const double* A = bs.cen + 3 * s.x;
+        const double* B = bs.cen + 3 * s.y;
+        const double* C = bs.cen + 3 * s.z;
+        const double* D = bs.cen + 3 * s.w;
+        const RT CDx = RT(C[0] - D[0]), CDy = RT(C[1] - D[1]), CDz = RT(C[2] - D[2]);
+        const RT ABx = RT(A[0] - B[0]), ABy = RT(A[1] - B[1]), ABz = RT(A[2] - B[2]);
+        for (int e = 0; e < Cls::kHrrE; ++e) Cls::template hrr_ket<RT>(o + e * NCD, o + e * NCD, CDx, CDy, CDz);
+        for (int cd = 0; cd < NCD; ++cd) Cls::template hrr_bra<RT>(o + cd, NCD, o + cd, NCD, ABx, ABy, ABz);
+    }
+}
+
 // ------------------------------------------------------------------------------------------------
 // Pair lists: pair class X holds shell pairs (a,b) with L_a >= L_b, sorted by Schwarz bound
 // descending; the primitive pairs of pair i are P[ppo[i] .. ppo[i]+npp[i]).

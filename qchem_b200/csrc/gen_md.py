@@ -425,7 +425,7 @@ def gen_class_hrr(LA, LB, LC, LD, idx):
     w(f"__device__ __forceinline__ void hrr_ket_{idx}(const RT* p, RT* y, const RT CDx,")
     w("    const RT CDy, const RT CDz)")
     w("{")
-    hrr_code(LC, LD, lambda k: f"p[{k}]", lambda ix, iy, v, nrm: f"    y[{ix * nd + iy}] = {v} * RT({lit(nrm)});",
+    hrr_code(LC, LD, lambda k: f"ld_l2(p + {k})", lambda ix, iy, v, nrm: f"    y[{ix * nd + iy}] = {v} * RT({lit(nrm)});",
              ("CDx", "CDy", "CDz"), w, "t")
     w("}")
     # bra HRR of one (c, d) column: y[e * ys] -> o[(a * NB + b) * os], times the (a, b) component norms
@@ -435,7 +435,7 @@ def gen_class_hrr(LA, LB, LC, LD, idx):
     w(f"__device__ __forceinline__ void hrr_bra_{idx}(const RT* y, const int ys, RT* o,")
     w("    const int os, const RT ABx, const RT ABy, const RT ABz)")
     w("{")
-    hrr_code(LA, LB, lambda k: f"y[{k} * ys]",
+    hrr_code(LA, LB, lambda k: f"ld_l2(y + {k} * ys)",
              lambda ix, iy, v, nrm: f"    o[{ix * nb + iy} * os] = {v} * RT({lit(nrm)});", ("ABx", "ABy", "ABz"), w,
              "t")
     w("}")

@@ -160,6 +160,14 @@ __device__ __forceinline__ void boys(double T, const double* __restrict__ table,
 }
 
 // fused multiply-add in the generated code's arithmetic type
+// a load served by L2 (bypassing L1): for values this thread accumulated with red.global, which L1 does
+// not see
+template <class T>
+__device__ __forceinline__ T ld_l2(const T* p)
+{
+    return __ldcg(p);
+}
+
 __device__ __forceinline__ double qfma(double a, double b, double c) { return fma(a, b, c); }
 __device__ __forceinline__ float qfma(float a, float b, float c) { return fmaf(a, b, c); }
 

@@ -156,3 +156,53 @@ extern "C" int host_jk_kernel(int split, int run, int grid, int nbra, const int*
         }
     return 0;
 }
+
+#ifdef HJ_HRR
+// the HRR form of the class (gen_md.main_hrr) and the library's eri_batch_hrr_kernel over a batch of quartets
+#include HJ_STR(gen_hrr/HJ_CAT(md_hrr_, QCG_CLASS).cuh)
+
+namespace {
+struct ClsH
+{
+    static constexpr int LA = ::LA, LB = ::LB, LC = ::LC, LD = ::LD;
+    static constexpr int kHrrE = HJ_CAT(qcg::gen::kHrrE, QCG_CLASS), kHrrF = HJ_CAT(qcg::gen::kHrrF, QCG_CLASS);
+    template <class RT, class S>
+    static void quartet_hrr(const qcg::PrimPairData& ab, const qcg::PrimPairData& cd, const double* bt, RT* rs,
+                            int stride, S& sink)
+    {
+        HJ_CAT(qcg::gen::prim_quartet_hrr_, QCG_CLASS)<RT, S>(ab, cd, bt, rs, stride, sink);
+    }
+    template <class RT>
+    static void hrr_ket(const RT* p, RT* y, RT CDx, RT CDy, RT CDz)
+    {
+        HJ_CAT(qcg::gen::hrr_ket_, QCG_CLASS)<RT>(p, y, CDx, CDy, CDz);
+    }
+    template <class RT>
+    static void hrr_bra(const RT* y, int ys, RT* o, int os, RT ABx, RT ABy, RT ABz)
+    {
+        HJ_CAT(qcg::gen::hrr_bra_, QCG_CLASS)<RT>(y, ys, o, os, ABx, ABy, ABz);
+    }
+};
+}   // namespace
+
+// basis arrays as the library's device basis holds them (coefficients already normalised), nq quartets of
+// shell indices; every (block, thread) of a grid of `grid` blocks of 64 threads run in turn
+extern "C" int host_eri_hrr_kernel(int grid, int nshell, const int* L, const int* nprim, const int* prim0,
+                                   const double* cen, const double* alpha, const double* coef, long long nq,
+                                   const int* quartets, double* out)
+{
+    qcg::BasisDev bs{nshell, L, nprim, prim0, cen, alpha, coef};
+    constexpr int T = 64;
+    blockDim.x = T;
+    gridDim.x = grid;
+    for (int b = 0; b < grid; ++b)
+        for (int t = 0; t < T; ++t)
+        {
+            blockIdx.x = b;
+            threadIdx.x = t;
+            qcg::eri_batch_hrr_kernel<ClsH, T, double>(bs, reinterpret_cast<const int4*>(quartets), nullptr, nq, out,
+                                                      kBoysTable);
+        }
+    return 0;
+}
+#endif

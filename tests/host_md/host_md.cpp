@@ -16,6 +16,11 @@ static inline T __ldg(const T* p)
 {
     return *p;
 }
+template <class T>
+static inline T __ldcg(const T* p)
+{
+    return *p;
+}
 static inline void __syncthreads() {}   // the lock-step variant is not instantiated here
 
 #include "md_core.cuh"

@@ -28,6 +28,11 @@ inline T __ldg(const T* p)
 {
     return *p;
 }
+template <class T>
+inline T __ldcg(const T* p)
+{
+    return *p;
+}
 inline double atomicAdd(double* p, double v)
 {
     const double o = *p;

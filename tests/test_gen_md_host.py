@@ -153,6 +153,7 @@ def host_jk(tmp_path_factory):
     finally:
         sys.path.pop(0)
     gen_md.main(os.path.join(tmp, "gen"))
+    gen_md.main_hrr(os.path.join(tmp, "gen_hrr"))
     for name in ("md_core.cuh", "boys_table.h", "eri_kernels.cuh", "qcg_internal.h"):
         shutil.copy(os.path.join(CSRC, name), tmp)
     src = os.path.join(HERE, "host_md", "host_jk.cpp")
@@ -160,13 +161,14 @@ def host_jk(tmp_path_factory):
 
     def compile_class(k):
         out = os.path.join(tmp, f"host_jk_{k}.so")
-        r = subprocess.run(["g++", "-std=c++17", "-O1", "-fPIC", "-shared", f"-DQCG_CLASS={k}", "-I", shim, "-I", tmp,
-                            src, "-o", out], capture_output=True, text=True)
+        r = subprocess.run(["g++", "-std=c++17", "-O1", "-fPIC", "-shared", f"-DQCG_CLASS={k}", "-DHJ_HRR", "-I", shim,
+                            "-I", tmp, src, "-o", out], capture_output=True, text=True)
         assert r.returncode == 0, r.stderr[-3000:]
         lib = ctypes.CDLL(out)
         lib.host_jk_quartet.restype = ctypes.c_int
         lib.host_jk_nchunk.restype = ctypes.c_int
         lib.host_jk_kernel.restype = ctypes.c_int
+        lib.host_eri_hrr_kernel.restype = ctypes.c_int
         return k, lib
 
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
@@ -336,3 +338,29 @@ def test_jk_kernels_on_a_work_list(k, host_classes, host_jk):
                                        p(K, ctypes.c_double), n)
         assert rc == 0
         assert np.abs(J - Jr).max() <= 1e-12 * scale and np.abs(K - Kr).max() <= 1e-12 * scale, (k, split, run, grid)
+
+
+@pytest.mark.parametrize("k", range(21))
+def test_eri_batch_hrr_kernel(k, host_jk, oracle_mod):
+    """eri_batch_hrr_kernel (the HRR form of the ERI-batch kernel, not yet instantiated by the library) run on
+    the host over a batch of contracted quartets on two blocks: the oracle's integrals to 1e-12."""
+    cls = W.quartet_classes()[k]
+    npool = 16
+    pool = W.shell_pool(npool, seed=W.SEED0 + 2400, box=3.0)
+    q = np.ascontiguousarray(W.eri_class_batch(cls, 150, npool, seed=W.SEED0 + 2400 + k), dtype=np.int32)
+    L = np.array([sh.L for sh in pool], dtype=np.int32)
+    nprim = np.array([len(sh.exps) for sh in pool], dtype=np.int32)
+    prim0 = np.concatenate([[0], np.cumsum(nprim)[:-1]]).astype(np.int32)
+    cen = np.ascontiguousarray(np.array([sh.centre for sh in pool], dtype=float).reshape(-1))
+    alpha = np.concatenate([np.asarray(sh.exps, dtype=float) for sh in pool])
+    coef = np.concatenate([_norm_coefs(sh) for sh in pool])
+    blk = int(np.prod([(l + 1) * (l + 2) // 2 for l in cls]))
+    out = np.full(len(q) * blk, np.nan)
+    p = lambda a, t: a.ctypes.data_as(ctypes.POINTER(t))
+    assert host_jk[k].host_eri_hrr_kernel(2, len(pool), p(L, ctypes.c_int), p(nprim, ctypes.c_int),
+                                          p(prim0, ctypes.c_int), p(cen, ctypes.c_double), p(alpha, ctypes.c_double),
+                                          p(coef, ctypes.c_double), ctypes.c_longlong(len(q)), p(q, ctypes.c_int),
+                                          p(out, ctypes.c_double)) == 0
+    ref = oracle_mod.OracleBasis(pool).eri_batch(q).reshape(-1)
+    err = np.abs(out - ref).max()
+    assert err <= ERI_ABS and err <= 1e-12 * np.abs(ref).max(), (cls, err)
