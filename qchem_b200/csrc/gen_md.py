@@ -362,33 +362,12 @@ def hrr_code(Lx, Ly, src, dst, D, w, prefix):
             w(dst(ix, iy, node(x, y), comp_norm(x) * comp_norm(y)))
 
 
-def gen_class_hrr(LA, LB, LC, LD, idx):
-    L = LA + LB + LC + LD
-    LAB, LCD = LA + LB, LC + LD
-    E, F = comps_range(LA, LAB), comps_range(LC, LCD)
+def hrr_f_blocks(LAB, L, E, F, fsel, w):
+    """[e0|f0] for the f of F listed in fsel (indices into F), every e of E; R read through RR()."""
     HAB = herm_list(LAB)
     NX = len(HAB)
-    rsm = L >= R_SMEM_MIN_L
-    o = []
-    w = o.append
-    w(f"// class {idx} in HRR form: [e0|f0] has {len(E)} x {len(F)} entries")
-    w(f"constexpr int kHrrE{idx} = {len(E)};")
-    w(f"constexpr int kHrrF{idx} = {len(F)};")
-    # primitive quartet -> sink(ie, if, value)
-    w("template <class RT, class Sink>")
-    w(f"__device__ __forceinline__ void prim_quartet_hrr_{idx}(const PrimPairData& ab, const PrimPairData& cd,")
-    w("    const double* __restrict__ bt, RT* __restrict__ rs, const int rstride, Sink& sink)")
-    w("{")
-    w("    (void)rs; (void)rstride;")
-    r_prologue(L, rsm, w)
-    w("    const RT bPAx = RT(ab.PAx), bPAy = RT(ab.PAy), bPAz = RT(ab.PAz);")
-    w("    const RT kPAx = RT(cd.PAx), kPAy = RT(cd.PAy), kPAz = RT(cd.PAz);")
-    for dname, Lmax, PA, a12 in (("ebx", LAB, "bPAx", "a12b"), ("eby", LAB, "bPAy", "a12b"),
-                                 ("ebz", LAB, "bPAz", "a12b"), ("ekx", LCD, "kPAx", "a12k"),
-                                 ("eky", LCD, "kPAy", "a12k"), ("ekz", LCD, "kPAz", "a12k")):
-        for s_ in gen_E(dname, Lmax, 0, PA, "0", a12):
-            w("    " + s_)
-    for jf, f in enumerate(F):
+    for jf in fsel:
+        f = F[jf]
         w(f"    {{ // f = {f}")
         supp = [(tp, up, vp) for tp in range(f[0] + 1) for up in range(f[1] + 1) for vp in range(f[2] + 1)]
         for (tp, up, vp) in supp:
@@ -417,6 +396,63 @@ def gen_class_hrr(LA, LB, LC, LD, idx):
             w(f"      sink({je}, {jf}, sx * lambda);")
             w("    }")
         w("    }")
+
+
+def hrr_e_tables(LAB, LCD):
+    out = []
+    for dname, Lmax, PA, a12 in (("ebx", LAB, "bPAx", "a12b"), ("eby", LAB, "bPAy", "a12b"),
+                                 ("ebz", LAB, "bPAz", "a12b"), ("ekx", LCD, "kPAx", "a12k"),
+                                 ("eky", LCD, "kPAy", "a12k"), ("ekz", LCD, "kPAz", "a12k")):
+        out.extend(gen_E(dname, Lmax, 0, PA, "0", a12))
+    return out
+
+
+def gen_class_hrr(LA, LB, LC, LD, idx):
+    L = LA + LB + LC + LD
+    LAB, LCD = LA + LB, LC + LD
+    E, F = comps_range(LA, LAB), comps_range(LC, LCD)
+    chunked = len(E) * len(F) > CHUNK_ABOVE
+    rsm = L >= R_SMEM_MIN_L or chunked
+    o = []
+    w = o.append
+    w(f"// class {idx} in HRR form: [e0|f0] has {len(E)} x {len(F)} entries"
+      f"{'; f split into __noinline__ chunks' if chunked else ''}")
+    w(f"constexpr int kHrrE{idx} = {len(E)};")
+    w(f"constexpr int kHrrF{idx} = {len(F)};")
+    chunk_names = []
+    if chunked:
+        per = max(1, CHUNK_OUTPUTS // len(E))
+        groups = [list(range(len(F)))[i:i + per] for i in range(0, len(F), per)]
+        for ci, fsel in enumerate(groups):
+            fn = f"prim_quartet_hrr_{idx}_chunk{ci}"
+            chunk_names.append(fn)
+            w("template <class RT, class Sink>")
+            w(f"__device__ __noinline__ void {fn}(const RT* __restrict__ rs, const int rstride, const RT a12b,")
+            w("    const RT bPAx, const RT bPAy, const RT bPAz, const RT a12k, const RT kPAx, const RT kPAy,")
+            w("    const RT kPAz, const RT lambda, typename SinkArg<Sink>::type sink)")
+            w("{")
+            for s_ in hrr_e_tables(LAB, LCD):
+                w("    " + s_)
+            w("#define RR(i) rs[(i) * rstride]")
+            hrr_f_blocks(LAB, L, E, F, fsel, w)
+            w("#undef RR")
+            w("}")
+    # primitive quartet -> sink(ie, if, value)
+    w("template <class RT, class Sink>")
+    w(f"__device__ __forceinline__ void prim_quartet_hrr_{idx}(const PrimPairData& ab, const PrimPairData& cd,")
+    w("    const double* __restrict__ bt, RT* __restrict__ rs, const int rstride, Sink& sink)")
+    w("{")
+    w("    (void)rs; (void)rstride;")
+    r_prologue(L, rsm, w)
+    w("    const RT bPAx = RT(ab.PAx), bPAy = RT(ab.PAy), bPAz = RT(ab.PAz);")
+    w("    const RT kPAx = RT(cd.PAx), kPAy = RT(cd.PAy), kPAz = RT(cd.PAz);")
+    if chunked:
+        for fn in chunk_names:
+            w(f"    {fn}<RT, Sink>(rs, rstride, a12b, bPAx, bPAy, bPAz, a12k, kPAx, kPAy, kPAz, lambda, sink);")
+    else:
+        for s_ in hrr_e_tables(LAB, LCD):
+            w("    " + s_)
+        hrr_f_blocks(LAB, L, E, F, range(len(F)), w)
     w("#undef RR")
     w("}")
     # ket HRR of one e row: p[f] -> y[c * ND + d], times the (c, d) component norms (y may be p)
