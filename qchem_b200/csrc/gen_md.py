@@ -327,6 +327,12 @@ if __name__ == "__main__":
 # once per contracted quartet instead of once per primitive quartet.  The library's kernels do not use it
 # yet; tests/test_gen_md_host.py checks it against the oracle on the host.
 # ------------------------------------------------------------------------------------------------------
+# f components per chunk of the chunked HRR classes: with one, no (dd|dd) chunk spills under ptxas for
+# sm_100a (two spill 2.3 KB over the class); each chunk rebuilds its E tables (~90 operations against
+# ~500 for one f of (dd|dd)), which a B200 measurement has to weigh
+HRR_F_PER_CHUNK = 1
+
+
 def comps_range(L0, L1):
     return [c for L in range(L0, L1 + 1) for c in comps(L)]
 
@@ -421,7 +427,7 @@ def gen_class_hrr(LA, LB, LC, LD, idx):
     w(f"constexpr int kHrrF{idx} = {len(F)};")
     chunk_names = []
     if chunked:
-        per = max(1, CHUNK_OUTPUTS // len(E))
+        per = HRR_F_PER_CHUNK
         groups = [list(range(len(F)))[i:i + per] for i in range(0, len(F), per)]
         for ci, fsel in enumerate(groups):
             fn = f"prim_quartet_hrr_{idx}_chunk{ci}"
