@@ -157,6 +157,49 @@ extern "C" int host_jk_kernel(int split, int run, int grid, int nbra, const int*
     return 0;
 }
 
+// Schwarz diagonals of a pair list of a diagonal class (Q_i = sqrt(max |(ab|ab)|)): split = 0 runs
+// schwarz_kernel, split = 1 schwarz_split_kernel (Q zeroed first, as the launcher does)
+extern "C" int host_schwarz_kernel(int split, int grid, int npair, const int* sa, const int* sb, const int* ppo,
+                                   const int* npp, const double* P, int np, double* Q)
+{
+    if (kX != kY) return 1;
+    qcg::PairListDev pl{npair, sa, sb, ppo, npp, nullptr, nullptr};
+    qcg::PrimPairsDev pp{P, P + np, P + 2 * np, P + 3 * np, P + 4 * np, P + 5 * np, P + 6 * np, P + 7 * np,
+                         P + 8 * np, P + 9 * np, P + 10 * np};
+    if (split)
+        for (int i = 0; i < npair; ++i) Q[i] = 0.0;
+    blockDim.x = kThreads;
+    gridDim.x = grid;
+    for (int b = 0; b < grid; ++b)
+        for (int t = 0; t < kThreads; ++t)
+        {
+            blockIdx.x = b;
+            threadIdx.x = t;
+            if (split) qcg::schwarz_split_kernel<Cls, kThreads>(pl, pp, Q, kBoysTable);
+            else qcg::schwarz_kernel<Cls, kThreads>(pl, pp, Q, kBoysTable);
+        }
+    return 0;
+}
+
+// the library's direct ERI-batch kernel (eri_batch_kernel) over a batch of quartets, in input order
+extern "C" int host_eri_batch_kernel(int grid, int nshell, const int* L, const int* nprim, const int* prim0,
+                                     const double* cen, const double* alpha, const double* coef, long long nq,
+                                     const int* quartets, double* out)
+{
+    qcg::BasisDev bs{nshell, L, nprim, prim0, cen, alpha, coef};
+    blockDim.x = kThreads;
+    gridDim.x = grid;
+    for (int b = 0; b < grid; ++b)
+        for (int t = 0; t < kThreads; ++t)
+        {
+            blockIdx.x = b;
+            threadIdx.x = t;
+            qcg::eri_batch_kernel<Cls, kThreads, double>(bs, reinterpret_cast<const int4*>(quartets), nullptr, nq, out,
+                                                        kBoysTable);
+        }
+    return 0;
+}
+
 #ifdef HJ_HRR
 // the HRR form of the class (gen_md.main_hrr) and the library's eri_batch_hrr_kernel over a batch of quartets
 #include HJ_STR(gen_hrr/HJ_CAT(md_hrr_, QCG_CLASS).cuh)

@@ -169,6 +169,8 @@ def host_jk(tmp_path_factory):
         lib.host_jk_nchunk.restype = ctypes.c_int
         lib.host_jk_kernel.restype = ctypes.c_int
         lib.host_eri_hrr_kernel.restype = ctypes.c_int
+        lib.host_schwarz_kernel.restype = ctypes.c_int
+        lib.host_eri_batch_kernel.restype = ctypes.c_int
         return k, lib
 
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
@@ -338,6 +340,81 @@ def test_jk_kernels_on_a_work_list(k, host_classes, host_jk):
                                        p(K, ctypes.c_double), n)
         assert rc == 0
         assert np.abs(J - Jr).max() <= 1e-12 * scale and np.abs(K - Kr).max() <= 1e-12 * scale, (k, split, run, grid)
+
+
+def _device_basis(pool):
+    """The pool as the library's device basis holds it (normalised coefficients)."""
+    L = np.array([sh.L for sh in pool], dtype=np.int32)
+    nprim = np.array([len(sh.exps) for sh in pool], dtype=np.int32)
+    prim0 = np.concatenate([[0], np.cumsum(nprim)[:-1]]).astype(np.int32)
+    cen = np.ascontiguousarray(np.array([sh.centre for sh in pool], dtype=float).reshape(-1))
+    alpha = np.concatenate([np.asarray(sh.exps, dtype=float) for sh in pool])
+    coef = np.concatenate([_norm_coefs(sh) for sh in pool])
+    return L, nprim, prim0, cen, alpha, coef
+
+
+@pytest.mark.parametrize("k", range(21))
+def test_eri_batch_kernel(k, host_jk, oracle_mod):
+    """eri_batch_kernel, the library's direct ERI-batch kernel, run on the host over a contracted batch on
+    two blocks: the oracle's integrals to 1e-12."""
+    cls = W.quartet_classes()[k]
+    npool = 16
+    pool = W.shell_pool(npool, seed=W.SEED0 + 2500, box=3.0)
+    q = np.ascontiguousarray(W.eri_class_batch(cls, 300, npool, seed=W.SEED0 + 2500 + k), dtype=np.int32)
+    L, nprim, prim0, cen, alpha, coef = _device_basis(pool)
+    blk = int(np.prod([(l + 1) * (l + 2) // 2 for l in cls]))
+    out = np.full(len(q) * blk, np.nan)
+    p = lambda a, t: a.ctypes.data_as(ctypes.POINTER(t))
+    assert host_jk[k].host_eri_batch_kernel(2, len(pool), p(L, ctypes.c_int), p(nprim, ctypes.c_int),
+                                            p(prim0, ctypes.c_int), p(cen, ctypes.c_double),
+                                            p(alpha, ctypes.c_double), p(coef, ctypes.c_double),
+                                            ctypes.c_longlong(len(q)), p(q, ctypes.c_int), p(out, ctypes.c_double)) == 0
+    ref = oracle_mod.OracleBasis(pool).eri_batch(q).reshape(-1)
+    err = np.abs(out - ref).max()
+    assert err <= ERI_ABS and err <= 1e-12 * np.abs(ref).max(), (cls, err)
+
+
+@pytest.mark.parametrize("k", [0, 2, 5, 9, 14, 20])
+def test_schwarz_kernels(k, host_jk, oracle_mod):
+    """schwarz_kernel and schwarz_split_kernel (per-chunk maxima merged with an atomic max on the bit
+    pattern) give the same Schwarz bounds, equal to sqrt(max |(ab|ab)|) of the oracle's diagonal quartets."""
+    X = next(x for x in range(6) if (x + 1) * (x + 2) // 2 > k)
+    la, lb = [(0, 0), (1, 0), (1, 1), (2, 0), (2, 1), (2, 2)][X]
+    npool = 16
+    pool = W.shell_pool(npool, seed=W.SEED0 + 2600, box=3.0)
+    pairs = [(la * npool + a, lb * npool + b) for a in range(4) for b in range(4) if la > lb or a >= b]
+    p = lambda a, t: a.ctypes.data_as(ctypes.POINTER(t))
+    rows, ppo, npp = [], [], []
+    for (a, b) in pairs:
+        sa, sb = pool[a], pool[b]
+        wa, wb = _norm_coefs(sa), _norm_coefs(sb)
+        ppo.append(len(rows))
+        for i, ea in enumerate(sa.exps):
+            for j, eb in enumerate(sb.exps):
+                row = np.zeros(11)
+                host_jk[k].host_prim_pair(ctypes.c_double(ea), p(np.asarray(sa.centre, dtype=float), ctypes.c_double),
+                                          ctypes.c_double(wa[i]), ctypes.c_double(eb),
+                                          p(np.asarray(sb.centre, dtype=float), ctypes.c_double),
+                                          ctypes.c_double(wb[j]), p(row, ctypes.c_double))
+                rows.append(row)
+        npp.append(len(rows) - ppo[-1])
+    P = np.ascontiguousarray(np.array(rows).T)
+    sa_ = np.array([a for a, _ in pairs], dtype=np.int32)
+    sb_ = np.array([b for _, b in pairs], dtype=np.int32)
+    ppo, npp = np.array(ppo, dtype=np.int32), np.array(npp, dtype=np.int32)
+    Qs = []
+    for split in (0, 1):
+        Q = np.full(len(pairs), np.nan)
+        assert host_jk[k].host_schwarz_kernel(split, 2, len(pairs), p(sa_, ctypes.c_int), p(sb_, ctypes.c_int),
+                                              p(ppo, ctypes.c_int), p(npp, ctypes.c_int), p(P, ctypes.c_double),
+                                              P.shape[1], p(Q, ctypes.c_double)) == 0
+        Qs.append(Q)
+    q = np.array([[a, b, a, b] for a, b in pairs], dtype=np.int32)
+    na, nb = (la + 1) * (la + 2) // 2, (lb + 1) * (lb + 2) // 2
+    ref = oracle_mod.OracleBasis(pool).eri_batch(q).reshape(len(pairs), na, nb, na, nb)
+    Qref = np.sqrt(np.abs(np.einsum("iabab->iab", ref)).reshape(len(pairs), -1).max(axis=1))
+    np.testing.assert_allclose(Qs[0], Qref, rtol=1e-12, atol=1e-14)
+    np.testing.assert_allclose(Qs[1], Qs[0], rtol=1e-13, atol=1e-15)
 
 
 @pytest.mark.parametrize("k", range(21))
