@@ -157,6 +157,47 @@ extern "C" int host_jk_kernel(int split, int run, int grid, int nbra, const int*
     return 0;
 }
 
+// The same kernels on several molecules packed in one work list (as a batch handle builds it): bmol/kmol
+// give each pair's molecule, kbase[i] the first ket of bra pair i's molecule, mol_off/mol_n the packed
+// layout of D, J', K', and mol_active (or null) the molecules still iterating.
+extern "C" int host_jk_kernel_batch(int split, int run, int grid, int nbra, const int* bsa, const int* bsb,
+                                    const int* bppo, const int* bnpp, const double* bQ, const int* bmol, int nket,
+                                    const int* ksa, const int* ksb, const int* kppo, const int* knpp,
+                                    const double* kQ, const int* kmol, const double* P, int np,
+                                    const long long* offs, const int* kbase, int same_class, const int* f0,
+                                    int nmol, const long long* mol_off, const int* mol_n, const int* mol_active,
+                                    const double* D, double* J, double* K)
+{
+    if (kThreads * Cls::kRSize > 128 * 165) return 1;
+    qcg::PairListDev bra{nbra, bsa, bsb, bppo, bnpp, bQ, bmol}, ket{nket, ksa, ksb, kppo, knpp, kQ, kmol};
+    qcg::PrimPairsDev pp{P, P + np, P + 2 * np, P + 3 * np, P + 4 * np, P + 5 * np, P + 6 * np, P + 7 * np,
+                         P + 8 * np, P + 9 * np, P + 10 * np};
+    qcg::JKWorkDev w{};
+    w.total = offs[nbra];
+    w.gbeg = 0;
+    w.gend = w.total;
+    w.offs = offs;
+    w.kbase = kbase;
+    w.same_class = same_class;
+    w.lo = 0.0;
+    w.hi = HUGE_VAL;
+    w.mols = qcg::MolLayoutDev{nmol, mol_off, mol_n};
+    w.mol_active = mol_active;
+    blockDim.x = kThreads;
+    gridDim.x = grid;
+    for (int b = 0; b < grid; ++b)
+        for (int t = 0; t < kThreads; ++t)
+        {
+            blockIdx.x = b;
+            threadIdx.x = t;
+            if (split)
+                qcg::jk_split_kernel<Cls, kThreads, double>(w, bra, ket, pp, f0, D, J, K, 0, kBoysTable);
+            else
+                qcg::jk_kernel<Cls, kThreads, double>(w, bra, ket, pp, f0, D, J, K, 0, kBoysTable, run);
+        }
+    return 0;
+}
+
 // Schwarz diagonals of a pair list of a diagonal class (Q_i = sqrt(max |(ab|ab)|)): split = 0 runs
 // schwarz_kernel, split = 1 schwarz_split_kernel (Q zeroed first, as the launcher does)
 extern "C" int host_schwarz_kernel(int split, int grid, int npair, const int* sa, const int* sb, const int* ppo,

@@ -168,6 +168,7 @@ def host_jk(tmp_path_factory):
         lib.host_jk_quartet.restype = ctypes.c_int
         lib.host_jk_nchunk.restype = ctypes.c_int
         lib.host_jk_kernel.restype = ctypes.c_int
+        lib.host_jk_kernel_batch.restype = ctypes.c_int
         lib.host_eri_hrr_kernel.restype = ctypes.c_int
         lib.host_schwarz_kernel.restype = ctypes.c_int
         lib.host_eri_batch_kernel.restype = ctypes.c_int
@@ -441,3 +442,119 @@ def test_eri_batch_hrr_kernel(k, host_jk, oracle_mod):
     ref = oracle_mod.OracleBasis(pool).eri_batch(q).reshape(-1)
     err = np.abs(out - ref).max()
     assert err <= ERI_ABS and err <= 1e-12 * np.abs(ref).max(), (cls, err)
+
+
+@pytest.mark.parametrize("k", [0, 4, 8, 13, 17, 20])
+def test_jk_kernels_on_a_batch_work_list(k, host_classes, host_jk):
+    """The J/K kernels on two molecules packed in one work list (per-pair molecules, kets from the bra's
+    molecule segment, packed D/J'/K'), with both molecules active and with one switched off as a batched
+    SCF does when it converges: each molecule's block equals its own quartets' digestion, and a switched-off
+    molecule's block stays zero."""
+    X = next(x for x in range(6) if (x + 1) * (x + 2) // 2 > k)
+    Y = k - X * (X + 1) // 2
+    pair_L = [(0, 0), (1, 0), (1, 1), (2, 0), (2, 1), (2, 2)]
+    npool = 16
+    pool = W.shell_pool(npool, seed=W.SEED0 + 2700, box=3.0)
+    mols = [[L * npool + 2 * m + i for L in range(3) for i in range(2)] for m in range(2)]   # pool indices
+    Ls = [pool[b].L for b in mols[0]]
+    nf = [(L + 1) * (L + 2) // 2 for L in Ls]
+    f0_local = np.concatenate([[0], np.cumsum(nf)[:-1]]).astype(int)
+    nm = int(sum(nf))
+    shells = [b for m in mols for b in m]                 # global shell order: molecule 0, then 1
+    f0 = np.array([f0_local[i % 6] for i in range(12)], dtype=np.int32)
+    mol_of = [i // 6 for i in range(12)]
+    mol_off = np.array([0, nm * nm, 2 * nm * nm], dtype=np.int64)
+    mol_n = np.array([nm, nm], dtype=np.int32)
+
+    def pairs_of(cls_idx):
+        la, lb = pair_L[cls_idx]
+        out = []
+        for m in range(2):
+            loc = range(6 * m, 6 * m + 6)
+            out += [(a, b) for a in loc for b in loc if Ls[a % 6] == la and Ls[b % 6] == lb and (la > lb or a >= b)]
+        return out
+
+    bra_pairs, ket_pairs = pairs_of(X), pairs_of(Y)
+    same = X == Y
+    p = lambda a, t: a.ctypes.data_as(ctypes.POINTER(t))
+    rows, ppo, npp = [], {}, {}
+    for (a, b) in sorted(set(bra_pairs) | set(ket_pairs)):
+        sa, sb = pool[shells[a]], pool[shells[b]]
+        wa, wb = _norm_coefs(sa), _norm_coefs(sb)
+        ppo[(a, b)] = len(rows)
+        for i, ea in enumerate(sa.exps):
+            for j, eb in enumerate(sb.exps):
+                row = np.zeros(11)
+                host_jk[k].host_prim_pair(ctypes.c_double(ea), p(np.asarray(sa.centre, dtype=float), ctypes.c_double),
+                                          ctypes.c_double(wa[i]), ctypes.c_double(eb),
+                                          p(np.asarray(sb.centre, dtype=float), ctypes.c_double),
+                                          ctypes.c_double(wb[j]), p(row, ctypes.c_double))
+                rows.append(row)
+        npp[(a, b)] = len(rows) - ppo[(a, b)]
+    P = np.ascontiguousarray(np.array(rows).T)
+
+    def lists(prs):
+        return (np.array([a for a, _ in prs], dtype=np.int32), np.array([b for _, b in prs], dtype=np.int32),
+                np.array([ppo[x] for x in prs], dtype=np.int32), np.array([npp[x] for x in prs], dtype=np.int32),
+                np.ones(len(prs)), np.array([mol_of[a] for a, _ in prs], dtype=np.int32))
+
+    bra, ket = lists(bra_pairs), lists(ket_pairs)
+    seg = {m: [j for j, (a, _) in enumerate(ket_pairs) if mol_of[a] == m] for m in range(2)}
+    kbase = np.array([seg[mol_of[a]][0] for a, _ in bra_pairs], dtype=np.int32)
+    counts = [(i - kbase[i] + 1) if same else len(seg[mol_of[a]]) for i, (a, _) in enumerate(bra_pairs)]
+    offs = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    rng = np.random.default_rng(200 + k)
+    Dm = []
+    for m in range(2):
+        x = rng.normal(size=(nm, nm))
+        Dm.append(x + x.T)
+    D = np.concatenate([d.reshape(-1) for d in Dm])
+    refs = [(np.zeros((nm, nm)), np.zeros((nm, nm))) for _ in range(2)]
+    for i, (a, b) in enumerate(bra_pairs):
+        m = mol_of[a]
+        Jr, Kr = refs[m]
+        Dl = Dm[m]
+        for jj in range(counts[i]):
+            j = kbase[i] + jj
+            c, d = ket_pairs[j]
+            L4, npr, ex, co, cen = _pack(pool, np.asarray([[shells[a], shells[b], shells[c], shells[d]]]))
+            na, nb, nc, nd = (nf[a % 6], nf[b % 6], nf[c % 6], nf[d % 6])
+            blk = np.zeros(na * nb * nc * nd)
+            assert host_classes[k].host_md_eri(ctypes.c_longlong(1), p(L4, ctypes.c_int), p(npr, ctypes.c_int),
+                                               p(ex, ctypes.c_double), p(co, ctypes.c_double),
+                                               p(cen, ctypes.c_double), p(blk, ctypes.c_double)) == 0
+            blk = blk.reshape(na, nb, nc, nd)
+            s_ = (0.5 if a == b else 1.0) * (0.5 if c == d else 1.0) * (0.5 if same and i == j else 1.0)
+            for x in range(na):
+                for y in range(nb):
+                    for z in range(nc):
+                        for t in range(nd):
+                            mu, nu, la, si = f0[a] + x, f0[b] + y, f0[c] + z, f0[d] + t
+                            wv = s_ * blk[x, y, z, t]
+                            Jr[mu, nu] += 2 * wv * Dl[la, si]
+                            Jr[la, si] += 2 * wv * Dl[mu, nu]
+                            Kr[mu, la] += wv * Dl[nu, si]
+                            Kr[nu, la] += wv * Dl[mu, si]
+                            Kr[mu, si] += wv * Dl[nu, la]
+                            Kr[nu, si] += wv * Dl[mu, la]
+    scale = max(max(np.abs(r).max() for r in pair) for pair in refs)
+    for active in (None, (1, 1), (1, 0), (0, 1)):
+        act = None if active is None else np.array(active, dtype=np.int32)
+        for split, run, grid in ((0, 1, 1), (0, 3, 2), (1, 1, 2)):
+            J, K = np.zeros_like(D), np.zeros_like(D)
+            rc = host_jk[k].host_jk_kernel_batch(
+                split, run, grid, len(bra_pairs), *(p(x, ctypes.c_int) for x in bra[:4]), p(bra[4], ctypes.c_double),
+                p(bra[5], ctypes.c_int), len(ket_pairs), *(p(x, ctypes.c_int) for x in ket[:4]),
+                p(ket[4], ctypes.c_double), p(ket[5], ctypes.c_int), p(P, ctypes.c_double), P.shape[1],
+                p(offs, ctypes.c_longlong), p(kbase, ctypes.c_int), int(same), p(f0, ctypes.c_int), 2,
+                p(mol_off, ctypes.c_longlong), p(mol_n, ctypes.c_int),
+                p(act, ctypes.c_int) if act is not None else None, p(D, ctypes.c_double), p(J, ctypes.c_double),
+                p(K, ctypes.c_double))
+            assert rc == 0
+            for m in range(2):
+                Jm = J[mol_off[m]:mol_off[m + 1]].reshape(nm, nm)
+                Km = K[mol_off[m]:mol_off[m + 1]].reshape(nm, nm)
+                on = active is None or active[m] == 1
+                Jr, Kr = refs[m] if on else (np.zeros((nm, nm)), np.zeros((nm, nm)))
+                assert np.abs(Jm - Jr).max() <= 1e-12 * scale and np.abs(Km - Kr).max() <= 1e-12 * scale, \
+                    (k, active, split, run, m)
