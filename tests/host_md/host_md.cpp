@@ -206,6 +206,13 @@ extern "C" int host_md_eri_hrr(long long nq, const int* L, const int* np, const 
     return host_eri_hrr<double>(nq, L, np, exps, coefs, cen, out);
 }
 
+// the HRR form in FP32 (primitive code and both recurrences in float)
+extern "C" int host_md_eri_hrr_f32(long long nq, const int* L, const int* np, const double* exps,
+                                   const double* coefs, const double* cen, float* out)
+{
+    return host_eri_hrr<float>(nq, L, np, exps, coefs, cen, out);
+}
+
 // The data flow planned for the GPU kernel, inside each quartet's own output block (n_a n_b rows of
 // n_c n_d): [e0|f0] accumulated at o[e * ncd + f], the ket recurrence in place per e row, then the bra
 // recurrence in place per (c d) column.

@@ -51,6 +51,7 @@ def host_classes(tmp_path_factory):
         lib.host_md_eri_f32.restype = ctypes.c_int
         lib.host_md_eri_hrr.restype = ctypes.c_int
         lib.host_md_eri_hrr_inplace.restype = ctypes.c_int
+        lib.host_md_eri_hrr_f32.restype = ctypes.c_int
         assert lib.host_md_class() == k
         return k, lib
 
@@ -558,3 +559,25 @@ def test_jk_kernels_on_a_batch_work_list(k, host_classes, host_jk):
                 Jr, Kr = refs[m] if on else (np.zeros((nm, nm)), np.zeros((nm, nm)))
                 assert np.abs(Jm - Jr).max() <= 1e-12 * scale and np.abs(Km - Kr).max() <= 1e-12 * scale, \
                     (k, active, split, run, m)
+
+
+@pytest.mark.parametrize("k", range(21))
+def test_generated_class_hrr_form_fp32(k, host_classes, oracle_mod):
+    """The HRR form in FP32 (recurrences included), on the 12-bohr box of the benchmark's shells, where the
+    displacements A - B and C - D that the recurrences multiply by are largest.  The recurrences amplify
+    FP32 rounding: (dd|pp) and (dd|dd) reach 2.6e-5 and 3.2e-5 of the batch's largest integral, above the
+    2e-5 bar the direct FP32 form meets (it stays within 3.3e-7), so the FP32 form keeps the direct
+    evaluation; this test records the bound (1e-4) that the FP32 HRR numbers stay within."""
+    cls = W.quartet_classes()[k]
+    pool = W.shell_pool(16, seed=W.SEED0 + 2800)
+    q = W.eri_class_batch(cls, NQ, 16, seed=W.SEED0 + 2800 + k)
+    L, npr, ex, co, cen = _pack(pool, q)
+    blk = int(np.prod([(l + 1) * (l + 2) // 2 for l in cls]))
+    out = np.zeros(NQ * blk, dtype=np.float32)
+    p = lambda a, t: a.ctypes.data_as(ctypes.POINTER(t))
+    assert host_classes[k].host_md_eri_hrr_f32(ctypes.c_longlong(NQ), p(L, ctypes.c_int), p(npr, ctypes.c_int),
+                                               p(ex, ctypes.c_double), p(co, ctypes.c_double),
+                                               p(cen, ctypes.c_double), p(out, ctypes.c_float)) == 0
+    ref = oracle_mod.OracleBasis(pool).eri_batch(q).reshape(-1)
+    rel = np.abs(out.astype(np.float64) - ref).max() / np.abs(ref).max()
+    assert rel <= 1e-4, (cls, rel)
