@@ -120,12 +120,14 @@ def test_generated_class_fp32_form(k, host_classes, oracle_mod):
     assert 0 < rel <= 2e-5, (cls, rel)
 
 
+@pytest.mark.parametrize("box", [3.0, 12.0])
 @pytest.mark.parametrize("k", range(21))
-def test_generated_class_hrr_form(k, host_classes, oracle_mod):
+def test_generated_class_hrr_form(k, box, host_classes, oracle_mod):
     """[e0|f0] accumulated over the primitives, then the ket and bra horizontal recurrences: the same
-    integrals as the direct form, to 1e-12 absolute and relative to the largest integral."""
+    integrals as the direct form, to 1e-12 absolute and relative to the largest integral, on compact shells
+    and on the benchmark's 12-bohr box (large A - B, C - D)."""
     cls = W.quartet_classes()[k]
-    pool = W.shell_pool(16, seed=W.SEED0 + 2100, box=3.0)
+    pool = W.shell_pool(16, seed=W.SEED0 + 2100, box=box)
     q = W.eri_class_batch(cls, NQ, 16, seed=W.SEED0 + 2100 + k)
     L, npr, ex, co, cen = _pack(pool, q)
     blk = int(np.prod([(l + 1) * (l + 2) // 2 for l in cls]))
