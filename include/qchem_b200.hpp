@@ -104,4 +104,9 @@ private:
     std::vector<double> D_, J_, K_;
 };
 
+// Frees the device slabs, pinned staging, streams and events that destroyed engines left for reuse by the
+// next engine on the same device (qcg_release_cache): call it before cudaDeviceReset, or when the memory is
+// wanted back.
+inline void release_cache() { qcg_release_cache(); }
+
 }   // namespace qcg

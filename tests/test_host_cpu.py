@@ -243,8 +243,10 @@ def test_cpp_adapter_builds_and_fails_loudly_without_a_device(tmp_path):
         pytest.skip("no g++")
     src = tmp_path / "t.cpp"
     src.write_text('#include "qchem_b200.hpp"\nint main(){std::vector<qcg::ShellSpec> s{{0,{0,0,0},{1.0},{1.0}}};\n'
-                   'try { qcg::FockEngine e(s); return e.AODimension() == 1 ? 0 : 3; }\n'
-                   'catch (const qcg::Error& err) { return err.code == QCG_ERR_CUDA ? 10 : 11; }}\n')
+                   'int rc;\n'
+                   'try { qcg::FockEngine e(s); rc = e.AODimension() == 1 ? 0 : 3; }\n'
+                   'catch (const qcg::Error& err) { rc = err.code == QCG_ERR_CUDA ? 10 : 11; }\n'
+                   'qcg::release_cache(); return rc; }\n')
     libdir = os.path.dirname(api.library_path())
     exe = tmp_path / "t"
     subprocess.run(["g++", "-std=c++17", "-I", os.path.join(REPO, "include"), str(src), "-L", libdir, "-lqchem_b200",
