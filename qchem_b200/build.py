@@ -47,6 +47,12 @@ def _headers(names):
     return [_read(os.path.join(CSRC, n)) for n in names]
 
 
+def _eri_hrr() -> bool:
+    """QCG_ERI_HRR=1 in the environment builds the FP64 ERI batches in the horizontal-recurrence form
+    (off by default: it matches the oracle on the host and is still to be timed on a B200)."""
+    return os.environ.get("QCG_ERI_HRR", "0") == "1"
+
+
 def _jobs():
     core = _headers(["md_core.cuh", "qcg_internal.h"])
     jobs = []
@@ -54,8 +60,11 @@ def _jobs():
     for prec in (64, 32):
         for k in range(NCLASS):
             defs = [f"-DQCG_CLASS={k}", f"-DQCG_PREC={prec}"]
-            key = _hash([_read(src), _read(os.path.join(GEN, f"md_class_{k}.cuh"))] + core
-                        + _headers(["eri_kernels.cuh"]) + FLAGS + defs)
+            parts = [_read(src), _read(os.path.join(GEN, f"md_class_{k}.cuh"))]
+            if _eri_hrr() and prec == 64:
+                defs.append("-DQCG_ERI_HRR=1")
+                parts.append(_read(os.path.join(GEN, f"md_hrr_{k}.cuh")))
+            key = _hash(parts + core + _headers(["eri_kernels.cuh"]) + FLAGS + defs)
             jobs.append((src, defs, os.path.join(BUILD, f"eri_class_{k}_f{prec}_{key}.o")))
     extra = {"runtime.cu": _headers(["boys_table.h"]) + [_read(os.path.join(INCLUDE, "qchem_b200.h"))],
              "mlp.cu": [_read(os.path.join(INCLUDE, "qchem_b200.h"))]}
@@ -87,6 +96,8 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
     finally:
         sys.path.pop(0)
     gen_md.main(GEN)
+    if _eri_hrr():
+        gen_md.main_hrr(GEN)
     if not os.path.exists(os.path.join(CSRC, "boys_table.h")):
         raise RuntimeError("csrc/boys_table.h is missing (python csrc/gen_boys_table.py regenerates it)")
     os.makedirs(BUILD, exist_ok=True)

@@ -18,6 +18,15 @@
 #define QCG_CAT2(a, b) a##b
 #define QCG_CAT(a, b) QCG_CAT2(a, b)
 #include QCG_STR(gen/QCG_CAT(md_class_, QCG_CLASS).cuh)
+// QCG_ERI_HRR=1 (FP64 objects only; off by default): the ERI batches use the horizontal-recurrence form
+// (gen/md_hrr_<k>.cuh, eri_batch_hrr_kernel).  It matches the oracle on the host; its B200 timing is still
+// to be taken.
+#ifndef QCG_ERI_HRR
+#define QCG_ERI_HRR 0
+#endif
+#if QCG_ERI_HRR && QCG_PREC == 64
+#include QCG_STR(gen/QCG_CAT(md_hrr_, QCG_CLASS).cuh)
+#endif
 #if QCG_PREC == 64
 #define QCG_NAME(base) QCG_CAT(QCG_CAT(base, _), QCG_CLASS)
 #elif QCG_PREC == 32
@@ -61,6 +70,30 @@ struct Cls
     {
         gen::QCG_CAT(prim_quartet_chunk_, QCG_CLASS)<RT, Sink>(c, ab, cd, bt, rs, stride, sink);
     }
+#if QCG_ERI_HRR && QCG_PREC == 64
+    // the horizontal-recurrence form (eri_batch_hrr_kernel)
+    static constexpr int kHrrE = gen::QCG_CAT(kHrrE, QCG_CLASS), kHrrF = gen::QCG_CAT(kHrrF, QCG_CLASS);
+    template <class RT, class Sink>
+    static __device__ __forceinline__ void quartet_hrr(const PrimPairData& ab, const PrimPairData& cd,
+                                                       const double* __restrict__ bt, RT* __restrict__ rs, int stride,
+                                                       Sink& sink)
+    {
+        gen::QCG_CAT(prim_quartet_hrr_, QCG_CLASS)<RT, Sink>(ab, cd, bt, rs, stride, sink);
+    }
+    template <class RT>
+    static __device__ __forceinline__ void hrr_ket(const RT* p, RT* y, RT CDx, RT CDy, RT CDz)
+    {
+        gen::QCG_CAT(hrr_ket_, QCG_CLASS)<RT>(p, y, CDx, CDy, CDz);
+    }
+    template <class RT>
+    static __device__ __forceinline__ void hrr_bra(const RT* y, int ys, RT* o, int os, RT ABx, RT ABy, RT ABz)
+    {
+        gen::QCG_CAT(hrr_bra_, QCG_CLASS)<RT>(y, ys, o, os, ABx, ABy, ABz);
+    }
+    // the HRR code keeps R in the per-thread shared-memory slice only where the direct code does too, so the
+    // direct form's block size and shared memory serve both
+    static_assert(!gen::QCG_CAT(kHrrRShared, QCG_CLASS) || kRShared, "HRR R slice needs shared memory");
+#endif
 };
 
 // classes whose R table lives in shared memory run 64-thread blocks (per-thread R slice); the others 128
@@ -99,6 +132,17 @@ void QCG_NAME(launch_eri_batch)(const BasisDev& bs, const int4* q, const int* or
                                 const double* boys, cudaStream_t st, int nsm)
 {
     if (nq <= 0) return;
+#if QCG_ERI_HRR && QCG_PREC == 64
+    {
+        auto k = eri_batch_hrr_kernel<Cls, kThreads, Real>;
+        static bool hrr_ready = false;   // its own flag: prepare() keys on the kernel's type
+        if (!hrr_ready && kSmem > 48 * 1024)
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem);
+        hrr_ready = true;
+        k<<<(unsigned)grid_for(nq, nsm), kThreads, kSmem, st>>>(bs, q, order, nq, out, boys);
+        return;
+    }
+#endif
     if constexpr (kUseLockstep)
     {
         auto k = eri_batch_lockstep_kernel<Cls, kLockThreads, Real>;

@@ -425,6 +425,7 @@ def gen_class_hrr(LA, LB, LC, LD, idx):
       f"{'; f split into __noinline__ chunks' if chunked else ''}")
     w(f"constexpr int kHrrE{idx} = {len(E)};")
     w(f"constexpr int kHrrF{idx} = {len(F)};")
+    w(f"constexpr bool kHrrRShared{idx} = {'true' if rsm else 'false'};")
     chunk_names = []
     if chunked:
         per = HRR_F_PER_CHUNK
