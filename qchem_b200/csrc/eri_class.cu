@@ -18,9 +18,8 @@
 #define QCG_CAT2(a, b) a##b
 #define QCG_CAT(a, b) QCG_CAT2(a, b)
 #include QCG_STR(gen/QCG_CAT(md_class_, QCG_CLASS).cuh)
-// QCG_ERI_HRR=1 (FP64 objects only; off by default): the ERI batches use the horizontal-recurrence form
-// (gen/md_hrr_<k>.cuh, eri_batch_hrr_kernel).  It matches the oracle on the host; its B200 timing is still
-// to be taken.
+// QCG_ERI_HRR=1 (FP64 objects only; build.py sets it for the classes where it measured faster): the ERI
+// batches use the horizontal-recurrence form (gen/md_hrr_<k>.cuh, eri_batch_hrr_kernel).
 #ifndef QCG_ERI_HRR
 #define QCG_ERI_HRR 0
 #endif
