@@ -253,3 +253,16 @@ def test_cpp_adapter_builds_and_fails_loudly_without_a_device(tmp_path):
                     f"-Wl,-rpath,{libdir}", "-o", str(exe)], check=True)
     rc = subprocess.run([str(exe)]).returncode
     assert rc == (0 if torch.cuda.is_available() else 10)
+
+
+def test_hrr_class_selection(monkeypatch):
+    """The FP64 ERI batches use the horizontal-recurrence form for (dp|dp), (dd|pp), (dd|dp) and (dd|dd) by
+    default; QCG_ERI_HRR=1 / =0 switch every class."""
+    from qchem_b200 import build as qb
+    monkeypatch.delenv("QCG_ERI_HRR", raising=False)
+    picked = [W.quartet_classes()[k] for k in range(21) if qb._eri_hrr(k)]
+    assert picked == [(2, 1, 2, 1), (2, 2, 1, 1), (2, 2, 2, 1), (2, 2, 2, 2)]
+    monkeypatch.setenv("QCG_ERI_HRR", "1")
+    assert all(qb._eri_hrr(k) for k in range(21))
+    monkeypatch.setenv("QCG_ERI_HRR", "0")
+    assert not any(qb._eri_hrr(k) for k in range(21))
