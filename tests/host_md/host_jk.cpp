@@ -157,6 +157,43 @@ extern "C" int host_jk_kernel(int split, int run, int grid, int nbra, const int*
     return 0;
 }
 
+// jk_kernel over the quartets whose bound Q_ab Q_cd lies in [lo, hi) (one launch of a mixed-precision
+// build), in FP64 (fp32 = 0) or FP32 (fp32 = 1) arithmetic; one block-sized grid, runs of one quartet
+extern "C" int host_jk_kernel_band(int fp32, double lo, double hi, int nbra, const int* bsa, const int* bsb,
+                                   const int* bppo, const int* bnpp, const double* bQ, int nket, const int* ksa,
+                                   const int* ksb, const int* kppo, const int* knpp, const double* kQ,
+                                   const double* P, int np, const long long* offs, int same_class, const int* f0,
+                                   const double* D, double* J, double* K, int n)
+{
+    if (kThreads * Cls::kRSize > 128 * 165) return 1;
+    qcg::PairListDev bra{nbra, bsa, bsb, bppo, bnpp, bQ, nullptr}, ket{nket, ksa, ksb, kppo, knpp, kQ, nullptr};
+    qcg::PrimPairsDev pp{P, P + np, P + 2 * np, P + 3 * np, P + 4 * np, P + 5 * np, P + 6 * np, P + 7 * np,
+                         P + 8 * np, P + 9 * np, P + 10 * np};
+    qcg::JKWorkDev w{};
+    w.total = offs[nbra];
+    w.gbeg = 0;
+    w.gend = w.total;
+    w.offs = offs;
+    w.same_class = same_class;
+    w.lo = lo;
+    w.hi = hi;
+    w.mols = qcg::MolLayoutDev{1, nullptr, nullptr};
+    const int grid = (int)((w.total + kThreads - 1) / kThreads);
+    blockDim.x = kThreads;
+    gridDim.x = grid;
+    for (int b = 0; b < grid; ++b)
+        for (int t = 0; t < kThreads; ++t)
+        {
+            blockIdx.x = b;
+            threadIdx.x = t;
+            if (fp32)
+                qcg::jk_kernel<Cls, kThreads, float>(w, bra, ket, pp, f0, D, J, K, n, kBoysTable, 1);
+            else
+                qcg::jk_kernel<Cls, kThreads, double>(w, bra, ket, pp, f0, D, J, K, n, kBoysTable, 1);
+        }
+    return 0;
+}
+
 // The same kernels on several molecules packed in one work list (as a batch handle builds it): bmol/kmol
 // give each pair's molecule, kbase[i] the first ket of bra pair i's molecule, mol_off/mol_n the packed
 // layout of D, J', K', and mol_active (or null) the molecules still iterating.

@@ -172,6 +172,7 @@ def host_jk(tmp_path_factory):
         lib.host_jk_nchunk.restype = ctypes.c_int
         lib.host_jk_kernel.restype = ctypes.c_int
         lib.host_jk_kernel_batch.restype = ctypes.c_int
+        lib.host_jk_kernel_band.restype = ctypes.c_int
         lib.host_eri_hrr_kernel.restype = ctypes.c_int
         lib.host_schwarz_kernel.restype = ctypes.c_int
         lib.host_eri_batch_kernel.restype = ctypes.c_int
@@ -583,3 +584,81 @@ def test_generated_class_hrr_form_fp32(k, host_classes, oracle_mod):
     ref = oracle_mod.OracleBasis(pool).eri_batch(q).reshape(-1)
     rel = np.abs(out.astype(np.float64) - ref).max() / np.abs(ref).max()
     assert rel <= 1e-4, (cls, rel)
+
+
+@pytest.mark.parametrize("k", [2, 5, 12, 14, 20])
+def test_jk_precision_bands_partition_the_build(k, host_jk):
+    """A mixed-precision build is two launches per class: FP64 over the quartets with bound Q_ab Q_cd in
+    [t, inf) and FP32 over [0, t).  With unequal Schwarz bounds, the two FP64 halves add up to the whole FP64
+    build (every quartet in exactly one band), and the mixed and the all-FP32 builds stay within the FP32
+    bar of it."""
+    X = next(x for x in range(6) if (x + 1) * (x + 2) // 2 > k)
+    Y = k - X * (X + 1) // 2
+    pair_L = [(0, 0), (1, 0), (1, 1), (2, 0), (2, 1), (2, 2)]
+    npool = 16
+    pool = W.shell_pool(npool, seed=W.SEED0 + 2900, box=3.0)
+    basis = [L * npool + i for L in range(3) for i in range(2)]
+    Ls = [pool[b].L for b in basis]
+    nf = [(L + 1) * (L + 2) // 2 for L in Ls]
+    f0 = np.concatenate([[0], np.cumsum(nf)[:-1]]).astype(np.int32)
+    n = int(sum(nf))
+
+    def pairs_of(c):
+        la, lb = pair_L[c]
+        return [(a, b) for a in range(6) for b in range(6) if Ls[a] == la and Ls[b] == lb and (la > lb or a >= b)]
+
+    bra_pairs, ket_pairs = pairs_of(X), pairs_of(Y)
+    same = X == Y
+    p = lambda a, t: a.ctypes.data_as(ctypes.POINTER(t))
+    rows, ppo, npp = [], {}, {}
+    for (a, b) in sorted(set(bra_pairs) | set(ket_pairs)):
+        sa, sb = pool[basis[a]], pool[basis[b]]
+        wa, wb = _norm_coefs(sa), _norm_coefs(sb)
+        ppo[(a, b)] = len(rows)
+        for i, ea in enumerate(sa.exps):
+            for j, eb in enumerate(sb.exps):
+                row = np.zeros(11)
+                host_jk[k].host_prim_pair(ctypes.c_double(ea), p(np.asarray(sa.centre, dtype=float), ctypes.c_double),
+                                          ctypes.c_double(wa[i]), ctypes.c_double(eb),
+                                          p(np.asarray(sb.centre, dtype=float), ctypes.c_double),
+                                          ctypes.c_double(wb[j]), p(row, ctypes.c_double))
+                rows.append(row)
+        npp[(a, b)] = len(rows) - ppo[(a, b)]
+    P = np.ascontiguousarray(np.array(rows).T)
+    rng = np.random.default_rng(300 + k)
+    Qof = {x: float(rng.uniform(0.1, 10.0)) for x in set(bra_pairs) | set(ket_pairs)}
+
+    def lists(prs):
+        return (np.array([a for a, _ in prs], dtype=np.int32), np.array([b for _, b in prs], dtype=np.int32),
+                np.array([ppo[x] for x in prs], dtype=np.int32), np.array([npp[x] for x in prs], dtype=np.int32),
+                np.array([Qof[x] for x in prs]))
+
+    bra, ket = lists(bra_pairs), lists(ket_pairs)
+    counts = [i + 1 if same else len(ket_pairs) for i in range(len(bra_pairs))]
+    offs = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    bounds = [bra[4][i] * ket[4][j] for i in range(len(bra_pairs)) for j in range(counts[i])]
+    t = float(np.median(bounds))
+    D = rng.normal(size=(n, n))
+    D = D + D.T
+
+    def build(fp32, lo, hi):
+        J, K = np.zeros((n, n)), np.zeros((n, n))
+        assert host_jk[k].host_jk_kernel_band(fp32, ctypes.c_double(lo), ctypes.c_double(hi), len(bra_pairs),
+                                              *(p(x, ctypes.c_int) for x in bra[:4]), p(bra[4], ctypes.c_double),
+                                              len(ket_pairs), *(p(x, ctypes.c_int) for x in ket[:4]),
+                                              p(ket[4], ctypes.c_double), p(P, ctypes.c_double), P.shape[1],
+                                              p(offs, ctypes.c_longlong), int(same), p(f0, ctypes.c_int),
+                                              p(D, ctypes.c_double), p(J, ctypes.c_double), p(K, ctypes.c_double),
+                                              n) == 0
+        return J, K
+
+    inf = float("inf")
+    J, K = build(0, 0.0, inf)
+    scale = max(np.abs(J).max(), np.abs(K).max())
+    lo64, hi64 = build(0, 0.0, t), build(0, t, inf)
+    assert np.abs(lo64[0]).max() > 0 and np.abs(hi64[0]).max() > 0           # both bands hold quartets
+    assert np.abs(lo64[0] + hi64[0] - J).max() <= 1e-13 * scale
+    assert np.abs(lo64[1] + hi64[1] - K).max() <= 1e-13 * scale
+    lo32 = build(1, 0.0, t)
+    for Jm, Km in ((lo32[0] + hi64[0], lo32[1] + hi64[1]), build(1, 0.0, inf)):
+        assert 0 < max(np.abs(Jm - J).max(), np.abs(Km - K).max()) <= 2e-5 * scale
