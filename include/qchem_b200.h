@@ -188,9 +188,12 @@ int qcg_autotune_jk(qcg_handle* h, const double* d_D, int reps, int* run_out, in
  * other allocating call: its J'/K' accumulators live in a file-scope device array of the library, sized
  * for at most 512 basis functions (larger bases are rejected with QCG_ERR_ARG).  qcg_basis_create and
  * qcg_schwarz, which do allocate, must have run before.  The first call on a device looks up the array's
- * device address; make that first call before any stream capture.  All calls share the one array (it
- * keeps the last call's contents and is cleared at the start of each call), so calls that overlap on the
- * GPU race: issue them in order on one stream.  No validation of D.  Has no counterpart in the reference. */
+ * device address; make that first call before any stream capture (qcg_release_cache forgets the address,
+ * so the first call after it looks it up again).  All calls share the one array (it keeps the last call's
+ * contents and is cleared at the start of each call), so calls that overlap on the GPU race: issue them in
+ * order on one stream.  It evaluates this rank's slice after qcg_set_shard and uses the autotuned launch
+ * shape, like qcg_fock_jk_device, but always in FP64 (qcg_set_fp32_bound does not apply).  No validation of
+ * D, and no report of non-finite results.  Has no counterpart in the reference. */
 int qcg_fock_jk_device_noalloc(qcg_handle* h, const double* d_D, double* d_J, double* d_K);
 
 /* Real solid-harmonic (spherical) functions, the reference's PG_Spherical basis: per shell 2L+1 components

@@ -2,9 +2,11 @@
 // -DQCG_CLASS=k (k = X(X+1)/2 + Y for pair classes X >= Y) and -DQCG_PREC=64 or 32, so that the 21 classes
 // of both forms build in parallel.  The FP64 objects define launch_eri_batch_k, launch_jk_k and
 // launch_schwarz_k; the FP32 objects launch_eri_batch32_k and launch_jk32_k.
+#include <atomic>
 #include <type_traits>
 
 #include "eri_kernels.cuh"
+#include "smem_attr.h"
 
 #ifndef QCG_CLASS
 #error "compile with -DQCG_CLASS=<0..20>"
@@ -104,10 +106,8 @@ constexpr size_t kSmem64 = Cls::kRShared ? (size_t)kThreads * Cls::kRSize * size
 template <class KernelPtr>
 void prepare(KernelPtr k, size_t smem = kSmem)
 {
-    static bool done = false;
-    if (!done && smem > 48 * 1024)
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    done = true;
+    static std::atomic<unsigned long long> ready{0};
+    ensure_smem(k, smem, ready);
 }
 
 long long grid_for(long long work, int nsm)
@@ -134,10 +134,8 @@ void QCG_NAME(launch_eri_batch)(const BasisDev& bs, const int4* q, const int* or
 #if QCG_ERI_HRR && QCG_PREC == 64
     {
         auto k = eri_batch_hrr_kernel<Cls, kThreads, Real>;
-        static bool hrr_ready = false;   // its own flag: prepare() keys on the kernel's type
-        if (!hrr_ready && kSmem > 48 * 1024)
-            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem);
-        hrr_ready = true;
+        static std::atomic<unsigned long long> hrr_ready{0};
+        ensure_smem(k, kSmem, hrr_ready);
         k<<<(unsigned)grid_for(nq, nsm), kThreads, kSmem, st>>>(bs, q, order, nq, out, boys);
         return;
     }
@@ -145,10 +143,8 @@ void QCG_NAME(launch_eri_batch)(const BasisDev& bs, const int4* q, const int* or
     if constexpr (kUseLockstep)
     {
         auto k = eri_batch_lockstep_kernel<Cls, kLockThreads, Real>;
-        static bool done = false;
-        if (!done && kLockSmem > 48 * 1024)
-            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLockSmem);
-        done = true;
+        static std::atomic<unsigned long long> lock_ready{0};
+        ensure_smem(k, kLockSmem, lock_ready);
         long long blocks = (nq + kLockThreads - 1) / kLockThreads;
         const long long cap = (long long)nsm * 2;
         if (blocks > cap) blocks = cap;
@@ -175,10 +171,8 @@ void QCG_NAME(launch_jk)(const JKWorkDev& w, const PairListDev& bra, const PairL
         if (span <= (long long)nsm * kThreads)
         {
             auto ks = jk_split_kernel<Cls, kThreads, Real>;
-            static bool split_ready = false;
-            if (!split_ready && kSmem > 48 * 1024)
-                cudaFuncSetAttribute(ks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem);
-            split_ready = true;
+            static std::atomic<unsigned long long> split_ready{0};
+            ensure_smem(ks, kSmem, split_ready);
             const long long items = ((span + 31) & ~31LL) * Cls::kNChunk;
             const long long blocks = (items + kThreads - 1) / kThreads;
             ks<<<(unsigned)blocks, kThreads, kSmem, st>>>(w, bra, ket, P, f0, D, J, K, n, boys);
@@ -216,10 +210,8 @@ void QCG_CAT(launch_schwarz_, QCG_CLASS)(const PairListDev& pl, const PrimPairsD
             if ((long long)pl.n <= (long long)nsm * kThreads)
             {
                 auto ks = schwarz_split_kernel<Cls, kThreads>;
-                static bool split_ready = false;
-                if (!split_ready && kSmem64 > 48 * 1024)
-                    cudaFuncSetAttribute(ks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem64);
-                split_ready = true;
+                static std::atomic<unsigned long long> split_ready{0};
+                ensure_smem(ks, kSmem64, split_ready);
                 cudaMemsetAsync(Q, 0, (size_t)pl.n * sizeof(double), st);
                 const long long items = (((long long)pl.n + 31) & ~31LL) * Cls::kNChunk;
                 ks<<<(unsigned)((items + kThreads - 1) / kThreads), kThreads, kSmem64, st>>>(pl, P, Q, boys);

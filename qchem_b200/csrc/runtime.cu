@@ -2196,7 +2196,15 @@ int qcg_basis_create_batch(const int* shell_L, const int* shell_nprim, const dou
 
 void qcg_destroy(qcg_handle* h) { delete h; }
 
-void qcg_release_cache(void) { ResourceCache::get().release_all(); }
+namespace {
+void noalloc_forget_addresses();   // defined with the allocation-free J/K build below
+}
+
+void qcg_release_cache(void)
+{
+    ResourceCache::get().release_all();
+    noalloc_forget_addresses();
+}
 
 const char* qcg_last_error(const qcg_handle* h) { return h ? h->last_error.c_str() : "null handle"; }
 
@@ -3002,11 +3010,13 @@ static __device__ __align__(256) double qcg_noalloc_scratch[kNoAllocScratchDoubl
 
 namespace {
 constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
 double* g_noalloc_scratch[kNoAllocMaxDevices] = {};
 
 double* noalloc_scratch_for(int device)
 {
     require(device >= 0 && device < kNoAllocMaxDevices, "device index out of range");
+    std::lock_guard<std::mutex> g(g_noalloc_mu);
     if (!g_noalloc_scratch[device])
     {
         int cur = -1;
@@ -3017,6 +3027,14 @@ double* noalloc_scratch_for(int device)
         g_noalloc_scratch[device] = (double*)p;
     }
     return g_noalloc_scratch[device];
+}
+
+// qcg_release_cache runs before a cudaDeviceReset: the array's address may change when the module is loaded
+// again, so the next allocation-free call looks it up anew
+void noalloc_forget_addresses()
+{
+    std::lock_guard<std::mutex> g(g_noalloc_mu);
+    for (double*& p : g_noalloc_scratch) p = nullptr;
 }
 }   // namespace
 
@@ -3040,11 +3058,21 @@ extern "C" int qcg_fock_jk_device_noalloc(qcg_handle* h, const double* d_D, doub
         CK(cudaMemsetAsync(scratch, 0, (2 * nn + 1) * sizeof(double), h->stream));
         for (int k = kNumQuartetClasses - 1; k >= 0; --k)
         {
+            if (h->work[k].total <= 0) continue;
             int X = 0;
             while ((X + 1) * (X + 2) / 2 <= k) ++X;
             const int Y = k - X * (X + 1) / 2;
-            kJKLaunchers[k](h->work[k], h->pl_dev[X], h->pl_dev[Y], h->pp_dev, h->d_f0, d_D, Jp, Kp, n, h->d_boys,
-                            h->stream, h->nsm);
+            // the same slice and launch shape as qcg_fock_jk_device: this rank's shard (qcg_set_shard) and the
+            // autotuned run and grid cap; the build is always FP64 (qcg_set_fp32_bound does not apply)
+            JKWorkDev wk = h->work[k];
+            wk.run = h->tuned_run[k];
+            wk.cap = h->tuned_cap[k];
+            wk.mol_active = h->d_mol_active;
+            wk.gbeg = wk.total * h->shard_rank / h->shard_world;
+            wk.gend = wk.total * (h->shard_rank + 1) / h->shard_world;
+            if (wk.gend <= wk.gbeg) continue;
+            kJKLaunchers[k](wk, h->pl_dev[X], h->pl_dev[Y], h->pp_dev, h->d_f0, d_D, Jp, Kp, n, h->d_boys, h->stream,
+                            h->nsm);
         }
         CK(cudaGetLastError());
         launch_symmetrize(Jp, Kp, d_J, d_K, (long long)nn, n, MolLayoutDev{1, nullptr, nullptr}, flag, h->stream,

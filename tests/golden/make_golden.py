@@ -1,7 +1,7 @@
 """Write the golden fixtures of tests/golden/ from the reference sources (JanReimers/qchem).
 
-Run in a container where the reference is mounted (default /root/reference; override with QCHEM_REF):
-    python tests/golden/make_golden.py
+Run where the reference source tree is available, naming its root in QCHEM_REF:
+    QCHEM_REF=<path to the qchem checkout> python tests/golden/make_golden.py
 
 Outputs (committed):
   boys_reference_sample.json  -- entries of the reference's Boys table (Internal/Boys/Imp/AuxillaryData.C)
@@ -19,7 +19,9 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REF = os.environ.get("QCHEM_REF", "/root/reference")
+REF = os.environ.get("QCHEM_REF")
+if not REF:
+    sys.exit("set QCHEM_REF to the root of the qchem source tree")
 
 
 def reference_boys_table():
