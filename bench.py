@@ -114,19 +114,62 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_baseline(classes, pool, sample_per_class, threads):
-    """Oracle eri_batch on a bounded sample per class; quartets/s for the full class mix."""
+def team_flops(cls, kab, kcd):
+    """Operations the team-form kernel executes for one contracted quartet with kab bra and kcd ket primitive
+    pairs (2 per fused multiply-add): per primitive quartet the Boys function and the R recursion, the Hermite
+    tables and the ket step of every ket component; per bra primitive pair the bra step; per contracted
+    quartet the two recurrences.  Beside the fixed algorithmic count (class_flops, the direct form), it shows
+    how much of the measured rate is arithmetic the kernel actually performs."""
+    sys.path.insert(0, os.path.join(REPO, "qchem_b200", "csrc"))
+    try:
+        import gen_md as G
+    finally:
+        sys.path.pop(0)
+    la, lb, lc, ld = cls
+    L, lab, lcd = la + lb + lc + ld, la + lb, lc + ld
+    H = lambda n: (n + 1) * (n + 2) * (n + 3) // 6
+    E, F = G.comps_range(la, lab), G.comps_range(lc, lcd)
+    nh = H(lab)
+    r = (20 + 3 * L) + 2 * sum(H(j) for j in range(L + 1)) + 4 * (G.ne1(lab) + G.ne1(lcd)) * 3
+    ket = sum(2 * nh * (f[0] + 1) * (f[1] + 1) * (f[2] + 1) + 2 * (f[0] + 1) * (f[1] + 1) * (f[2] + 1) for f in F)
+    bra = 2 * len(F) * sum((e[0] + 1) * (e[1] + 1) * (e[2] + 1) + (e[0] + 1) * (e[1] + 1) + (e[0] + 1) for e in E)
+    nc = lambda l: (l + 1) * (l + 2) // 2
+
+    def hrr_ops(lx, ly):   # one fused multiply-add per generated recurrence node, one multiply per output norm
+        lines = []
+        G.hrr_code(lx, ly, lambda k: "s", lambda ix, iy, v, nrm: "o", ("Dx", "Dy", "Dz"), lines.append, "t")
+        return 2 * sum("qfma(" in ln for ln in lines) + nc(lx) * nc(ly)
+
+    hrr = len(E) * hrr_ops(lc, ld) + nc(lc) * nc(ld) * hrr_ops(la, lb)
+    return kab * kcd * (r + ket) + kab * bra + hrr
+
+
+def team_flops_batch(cls, q, nprim):
+    """team_flops summed over the quartets q (rows of shell indices) with primitive counts nprim per shell."""
+    kab = nprim[q[:, 0]] * nprim[q[:, 1]]
+    kcd = nprim[q[:, 2]] * nprim[q[:, 3]]
+    per_prim = team_flops(cls, 1, 1) - team_flops(cls, 1, 0)          # r + ket
+    per_bra = team_flops(cls, 1, 0) - team_flops(cls, 0, 0)           # bra
+    per_quartet = team_flops(cls, 0, 0)                               # recurrences
+    return float(per_prim * (kab * kcd).sum() + per_bra * kab.sum() + per_quartet * len(q))
+
+
+def oracle_rate(classes, pool, sample, threads, steps=1):
+    """The CPU oracle's eri_batch on `sample` quartets of every class (the same seeded quartets in the
+    cpu_baseline leg and in --impl reference), all `threads` host threads: quartets/s over the class mix
+    and the per-step wall times."""
     from oracle.oracle import OracleBasis
     from qchem_b200 import workloads as W
     ob = OracleBasis(pool)
-    t_total = 0.0
-    for k, cls in enumerate(classes):
-        q = W.eri_class_batch(cls, sample_per_class, NPOOL, seed=W.SEED0 + 2500 + k)
+    qs = [W.eri_class_batch(cls, sample, NPOOL, seed=W.SEED0 + 2600 + k) for k, cls in enumerate(classes)]
+    ob.eri_batch(qs[0][:64], nthreads=threads)   # warm-up (thread pool, first-touch)
+    times = []
+    for _ in range(steps):
         t0 = time.perf_counter()
-        ob.eri_batch(q, nthreads=threads)
-        dt = time.perf_counter() - t0
-        t_total += dt * (Q_PER_CLASS / sample_per_class)
-    return len(classes) * Q_PER_CLASS / t_total
+        for q in qs:
+            ob.eri_batch(q, nthreads=threads)
+        times.append(time.perf_counter() - t0)
+    return len(classes) * sample * steps / sum(times), times
 
 
 def run_reference(args, rank, world):
@@ -134,21 +177,13 @@ def run_reference(args, rank, world):
     if rank != 0:
         return
     from qchem_b200 import workloads as W
-    from oracle.oracle import OracleBasis
     threads = os.cpu_count() or 1
     classes = W.quartet_classes()
     pool = W.shell_pool(NPOOL, seed=W.SEED0 + 2000)
-    ob = OracleBasis(pool)
     sample = args.ref_sample
-    qs = [W.eri_class_batch(cls, sample, NPOOL, seed=W.SEED0 + 2600 + k) for k, cls in enumerate(classes)]
-    for _ in range(args.warmup):
-        ob.eri_batch(qs[0][:64], nthreads=threads)
-    times = []
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        for q in qs:
-            ob.eri_batch(q, nthreads=threads)
-        times.append(time.perf_counter() - t0)
+    for _ in range(max(0, args.warmup - 1)):
+        oracle_rate(classes[:1], pool, 64, threads)
+    value, times = oracle_rate(classes, pool, sample, threads, steps=args.steps)
     dt = sum(times)
     value = len(classes) * sample * args.steps / dt
     line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world,
@@ -174,7 +209,6 @@ def main():
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--ref-sample", type=int, default=2000)
-    ap.add_argument("--cpu-sample", type=int, default=1000)
     ap.add_argument("--workload", default="eri", choices=["eri", "fock_config3", "rhf_config1", "rhf_learned", "rhf_batch"],
                     help="eri: the headline ERI microbenchmark; fock_config3: one direct J/K build of the "
                          "32-water cluster per step; rhf_config1: one water RHF to convergence per step; "
@@ -213,7 +247,7 @@ def main():
     nprim = np.array([s.nprim for s in pool], dtype=np.int64)
 
     # per-rank quartet lists (weak scaling: every rank its own 21 x nq_cls quartets), pinned host + device
-    h_q, d_q, prim_q = [], [], []
+    h_q, d_q, prim_q, exec_q = [], [], [], []
     for k, cls in enumerate(classes):
         q = W.eri_class_batch(cls, nq_cls, NPOOL, seed=W.SEED0 + 2000 + 97 * rank + k)
         t = torch.from_numpy(q).pin_memory()
@@ -221,6 +255,7 @@ def main():
         d_q.append(t.to(dev, non_blocking=True))
         pr = nprim[q].prod(axis=1)
         prim_q.append([int(pr[c:c + CHUNK].sum()) for c in range(0, nq_cls, CHUNK)])
+        exec_q.append(team_flops_batch(cls, q, nprim))
     max_blk = max(class_block(c) for c in classes)
     d_out = torch.empty(min(CHUNK, nq_cls) * max_blk, dtype=torch.float64, device=dev)
     torch.cuda.synchronize()
@@ -280,19 +315,27 @@ def main():
                                                   (cls_ms[k] / args.steps * 1e-3) / 1e12}
                  for k, c in enumerate(classes)}
     from qchem_b200 import build as qbuild
-    # the dominant class's kernel: the horizontal-recurrence form where the library builds it (HRR_CLASSES)
-    dom_hrr = qbuild._eri_hrr(W.quartet_classes().index(tuple(classes[kdom])))
-    dom_kernel = ("eri_batch_hrr_kernel" if dom_hrr else "eri_batch_kernel") + " class " + \
-        "".join("spd"[l] for l in classes[kdom])
+    # the dominant class's kernel: the team form where the library runs it (TEAM_CLASSES, or the mask in
+    # QCG_ERI_TEAM_MASK), else the horizontal-recurrence or direct form
+    env_mask = os.environ.get("QCG_ERI_TEAM_MASK")
+    team_mask = int(env_mask, 0) if env_mask else qbuild._team_mask()
+    kname = "".join("spd"[l] for l in classes[kdom])
+    if (team_mask >> kdom) & 1:
+        dom_kernel = "eri_batch_team_kernel"
+    else:
+        dom_kernel = "eri_batch_hrr_kernel" if qbuild._eri_hrr(kdom) else "eri_batch_kernel"
+    # executed operations of the team form (team_flops) over the same device time
+    executed_tf = exec_q[kdom] / (cls_ms[kdom] / args.steps * 1e-3) / 1e12 if (team_mask >> kdom) & 1 else None
+    # DRAM bytes per launch from a committed ncu capture of this kernel and class (profiles/dram_traffic.json)
     traffic = None
     prof = os.path.join(REPO, "profiles", "dram_traffic.json")
-    # the committed DRAM figures are an ncu capture of the direct kernel; the HRR kernel has none yet
-    if os.path.exists(prof) and not dom_hrr:
+    if os.path.exists(prof):
         with open(prof) as f:
             tr = json.load(f)
-        key = "".join("spd"[l] for l in classes[kdom])
-        if key in tr.get("bytes_per_launch", {}):
-            traffic = tr["bytes_per_launch"][key]
+        ent = tr.get("bytes_per_launch", {}).get(f"{dom_kernel} {kname}")
+        if ent is not None:
+            traffic = ent
+    dom_kernel += " class " + kname
 
     # end to end through the host-buffer C ABI call (pinned host memory, copies inside the timed region)
     e2e = None
@@ -346,6 +389,12 @@ def main():
             "roofline": {"bound": "fp64", "achieved": achieved_tf, "peak": peak_tf, "unit": "TFLOP/s",
                          "frac": achieved_tf / peak_tf, "traffic": traffic,
                          "kernel": dom_kernel,
+                         "achieved_note": "algorithmic FLOPs (the fixed direct-form count per primitive quartet) "
+                                          "over the class's device time: pattern sort + ERI kernel",
+                         "executed": executed_tf,
+                         "executed_frac": None if executed_tf is None else executed_tf / peak_tf,
+                         "executed_note": "operations the team form performs (HRR: bra step once per bra "
+                                          "primitive pair, recurrences once per quartet) over the same time",
                          "peak_source": "measured here: library DFMA probe (MEASURED_PEAKS.json has no FP64 figure)"},
             "per_class": per_class,
             "e2e": e2e}
@@ -354,10 +403,10 @@ def main():
         line["fp32"] = fp32_pass(torch, stream, eng, classes, d_q, prim_q, step, args)
     if rank == 0 and world == 1:
         threads = os.cpu_count() or 1
-        cb = cpu_baseline(classes, pool, args.cpu_sample, threads)
+        cb, _ = oracle_rate(classes, pool, args.ref_sample, threads)
         line["cpu_baseline"] = {"value": cb, "unit": UNIT, "cores": threads, "kind": "port",
-                                "sample": f"{args.cpu_sample} quartets per class (21 classes), extrapolated to "
-                                          f"{nq_cls} per class"}
+                                "sample": f"{args.ref_sample} seeded quartets per class x 21 classes, the same "
+                                          f"quartets and procedure as --impl reference"}
     if rank == 0 and not args.no_extras:
         line["extras"] = extras(torch, dev)
     if rank == 0:
@@ -416,6 +465,40 @@ def fp32_pass(torch, stream, eng, classes, d_q, prim_q, step, args):
             "error_vs_fp64": errs}
 
 
+def rhf_solve(api, mol, sh, steps, warmup, **kw):
+    """median wall time (engine set-up + SCF) over `steps` runs, and the last result; host timing on a shared
+    machine has outliers, the median is what is reported"""
+    for _ in range(warmup):
+        api.Engine(sh).rhf(mol, **kw)
+    walls, res = [], None
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        res = api.Engine(sh).rhf(mol, **kw)
+        walls.append(time.perf_counter() - t0)
+    return statistics.median(walls), res
+
+
+# the chosen form at a fixed geometry (no learned guess): incremental builds and DIIS from the first iteration;
+# FP32 quartets do not pay at 57 functions (two launches per class on a ~0.5 ms build)
+CHOSEN_FIXED = dict(incremental=True, diis_fdmax=1e6)
+
+
+def rhf_config1_summary(api, B, W, nrep, warmup, dimer=False):
+    """Config-1 water RHF to dE < 1e-10: plain FP64 GPU (core guess, the reference's DIIS rules) against the
+    chosen form, medians of nrep runs each; with dimer=True also the water dimer (114 functions)."""
+    mol = W.water()
+    sh = B.even_tempered(mol)
+    wall, res = rhf_solve(api, mol, sh, nrep, warmup)
+    wall_c, res_c = rhf_solve(api, mol, sh, nrep, warmup, **CHOSEN_FIXED)
+    out = {"_plain_wall": wall, "_plain": res, "_chosen_wall": wall_c, "_chosen": res_c}
+    if dimer:
+        mol8 = W.water_cluster(nx=2, ny=1, nz=1, seed=W.SEED0 + 3300)
+        sh8 = B.even_tempered(mol8)
+        out["_w8"], out["_r8"] = rhf_solve(api, mol8, sh8, 5, 1)
+        out["_w8c"], out["_r8c"] = rhf_solve(api, mol8, sh8, 5, 1, **CHOSEN_FIXED)
+    return out
+
+
 def run_secondary(args):
     """Secondary workloads: the config-3 Fock build (any number of ranks), the RHF workloads (one GPU)."""
     import torch
@@ -433,31 +516,10 @@ def run_secondary(args):
     elif args.workload == "rhf_batch":
         line = run_batch(args, api, B, W)
     else:
-        def solve(mol, sh, steps, warmup, **kw):
-            """median wall time (engine set-up + SCF) over `steps` runs; host timing on a shared machine
-            has outliers, the median is what is reported"""
-            for _ in range(warmup):
-                api.Engine(sh).rhf(mol, **kw)
-            walls, res = [], None
-            for _ in range(steps):
-                t0 = time.perf_counter()
-                res = api.Engine(sh).rhf(mol, **kw)
-                walls.append(time.perf_counter() - t0)
-            return statistics.median(walls), res
-
-        # chosen form at a fixed geometry (no learned guess): incremental builds and DIIS from the first
-        # iteration; FP32 quartets do not pay at 57 functions (two launches per class on a ~0.5 ms build)
-        chosen = dict(incremental=True, diis_fdmax=1e6)
-        mol = W.water()
-        sh = B.even_tempered(mol)
         nrep = max(args.steps, 9)
-        wall, res = solve(mol, sh, nrep, max(args.warmup, 3))
-        wall_c, res_c = solve(mol, sh, nrep, 3, **chosen)
-        # a larger system where the Fock build weighs more: the water dimer, 114 functions
-        mol8 = W.water_cluster(nx=2, ny=1, nz=1, seed=W.SEED0 + 3300)
-        sh8 = B.even_tempered(mol8)
-        w8, r8 = solve(mol8, sh8, 5, 1)
-        w8c, r8c = solve(mol8, sh8, 5, 1, **chosen)
+        rc1 = rhf_config1_summary(api, B, W, nrep, max(args.warmup, 3), dimer=True)
+        wall, res, wall_c, res_c = rc1["_plain_wall"], rc1["_plain"], rc1["_chosen_wall"], rc1["_chosen"]
+        w8, r8, w8c, r8c = rc1["_w8"], rc1["_r8"], rc1["_w8c"], rc1["_r8c"]
         line = {"metric": "RHF time-to-solution (water, even-tempered 57 functions, dE < 1e-10), plain FP64 GPU",
                 "value": wall, "unit": "s", "n_gpus": 1, "steps": nrep, "warmup": max(args.warmup, 3),
                 "ms_per_step": 1e3 * wall, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
@@ -675,6 +737,30 @@ def run_learned(args, api, B, W, peak_tf):
                     "d2h_bytes_per_step": None}}
 
 
+def learned_summary(api, B, W, train, held_out):
+    """A reduced learned-guess run for the default bench line (the full one is --workload rhf_learned):
+    train on `train` conformers, then time held-out RHFs from the core guess (plain) and the learned guess
+    (chosen), with the energy error of both against the FP64 CPU oracle on the first three."""
+    from oracle.oracle import OracleBasis
+    ns = argparse.Namespace(train=train, held_out=held_out, warmup=2)
+    full = run_learned(ns, api, B, W, None)
+    from qchem_b200 import guess as G
+    test = G.conformers(W.water(), held_out, seed=W.SEED0 + 5001)
+    e_or = [OracleBasis(B.even_tempered(m)).rhf(m, nthreads=os.cpu_count() or 1)["energy"] for m in test[:3]]
+    e_pl = [api.Engine(B.even_tempered(m)).rhf(m)["energy"] for m in test[:3]]
+    return {"train_conformers": train, "held_out": held_out,
+            "plain": {k: full["plain"][k] for k in ("wall_s_median", "iterations_mean", "all_converged")},
+            "chosen": {k: full["chosen"][k] for k in ("wall_s_median", "iterations_mean", "all_converged",
+                                                      "max_abs_dE")},
+            "chosen_settings": full["chosen_settings"],
+            "speedup_chosen_vs_plain": full["speedup_chosen_vs_plain"],
+            "chosen_batched_wall_s_per_molecule": full["chosen_batched"]["wall_s_per_molecule"],
+            "max_abs_dE_chosen_vs_plain_eh": full["chosen"]["max_abs_dE"],
+            "plain_vs_oracle_max_abs_dE_eh_first3": max(abs(a - b) for a, b in zip(e_pl, e_or)),
+            "note": "chosen energies are compared with the plain FP64 GPU energies of every held-out conformer; "
+                    "the plain energies with the CPU oracle on the first three"}
+
+
 def extras(torch, dev):
     """RHF time-to-solution (config-1 water) and one config-3 direct J/K build, GPU vs CPU oracle."""
     from oracle.oracle import OracleBasis
@@ -690,6 +776,24 @@ def extras(torch, dev):
                                 "gpu_fock_ms_total": r["fock_ms"], "oracle_energy": ro["energy"],
                                 "abs_diff_eh": abs(r["energy"] - ro["energy"]), "cpu_oracle_wall_s": ro["wall_s"],
                                 "cpu_threads": os.cpu_count()}
+    # the reference's own cost structure on one thread: ERI4 supermatrices filled element by element, then
+    # contracted with D every iteration (qchem IrrepBasisSet.C:138-183, ERI4.C:10-17)
+    rs = OracleBasis(sh).rhf(mol, jk_mode=1)
+    out["ref_faithful_serial_config1"] = {"wall_s": rs["wall_s"], "energy": rs["energy"], "iterations": rs["iterations"],
+                                          "threads": 1, "abs_diff_vs_gpu_eh": abs(rs["energy"] - r["energy"]),
+                                          "note": "CPU oracle, ERI4 supermatrix build + MatMul per iteration"}
+    # RHF time-to-solution, chosen form against plain FP64 GPU, with each arm's iterations and its energy
+    # error against the FP64 CPU oracle
+    rc1 = rhf_config1_summary(api, B, W, 7, 3)
+    arm = lambda wall, res: {"wall_s_median": wall, "iterations": res["iterations"], "energy": res["energy"],
+                             "converged": bool(res["converged"]), "abs_dE_vs_oracle_eh": abs(res["energy"] - ro["energy"]),
+                             "full_builds": res["full_builds"], "incremental_builds": res["incremental_builds"]}
+    tts = {"water_config1": {"plain": arm(rc1["_plain_wall"], rc1["_plain"]),
+                             "chosen": arm(rc1["_chosen_wall"], rc1["_chosen"]),
+                             "chosen_settings": CHOSEN_FIXED,
+                             "speedup_chosen_vs_plain": rc1["_plain_wall"] / rc1["_chosen_wall"]}}
+    tts["held_out_learned_guess"] = learned_summary(api, B, W, train=300, held_out=30)
+    out["rhf_time_to_solution"] = tts
     mol3 = W.water_cluster()
     sh3 = B.even_tempered(mol3)
     D = W.cluster_density(B.nbf(sh3))

@@ -169,6 +169,12 @@ int qcg_set_fp32_bound(qcg_handle* h, double bound);
  * Also switched on by the environment variable QCG_GRAPHS=1.  The handle's stream must not be the legacy
  * default stream for capture to happen. */
 int qcg_set_graphs(qcg_handle* h, int enable);
+/* Which FP64 ERI-batch classes (bit k: class k of qcg_eri_batch*) run in the team form -- a warp-specialised
+ * kernel that shares each primitive quartet's R table among the warps of a CTA and transfers to (ab|cd) once
+ * per contracted quartet -- rather than the one-thread-per-quartet form.  -1 (default): the library's own
+ * choice, or the mask in the environment variable QCG_ERI_TEAM_MASK.  Both forms give the same integrals
+ * to rounding.  No reference counterpart. */
+int qcg_set_eri_team_classes(qcg_handle* h, long long mask);
 /* Several GPUs on one J/K build: with (rank, world) set, later qcg_fock_jk* calls evaluate only this rank's
  * contiguous slice (1/world of the screened quartets of every class) and return the rank's PARTIAL J and K;
  * the sum over ranks (one all-reduce) is the full J and K.  (0, 1), the default, is the whole build.  The

@@ -41,7 +41,8 @@ EXPORTS = ["qcg_basis_create", "qcg_destroy", "qcg_last_error", "qcg_set_stream"
            "qcg_mlp_nparams", "qcg_mlp_params", "qcg_mlp_set_params", "qcg_mlp_forward", "qcg_mlp_loss_grad",
            "qcg_mlp_adam", "qcg_basis_create_batch", "qcg_nmol", "qcg_mol_nbf", "qcg_one_electron_batch",
            "qcg_rhf_batch", "qcg_set_graphs", "qcg_set_shard", "qcg_autotune_jk", "qcg_eri3_batch",
-           "qcg_nbf_spherical", "qcg_spherical_transform", "qcg_fock_jk_spherical", "qcg_release_cache"]
+           "qcg_nbf_spherical", "qcg_spherical_transform", "qcg_fock_jk_spherical", "qcg_release_cache",
+           "qcg_set_eri_team_classes"]
 
 
 class QcgError(RuntimeError):
@@ -98,6 +99,7 @@ def lib():
     L.qcg_last_error.argtypes = [vp]
     L.qcg_last_error.restype = ctypes.c_char_p
     L.qcg_set_stream.argtypes = [vp, vp]
+    L.qcg_set_eri_team_classes.argtypes = [vp, i64]
     L.qcg_set_memory_limit.argtypes = [vp, i64]
     L.qcg_nbf.argtypes = [vp, P(i32)]
     L.qcg_nshell.argtypes = [vp, P(i32)]
@@ -327,6 +329,10 @@ class Engine:
     def set_graphs(self, enable: bool):
         """Replay repeated J/K builds as CUDA graphs (off by default)."""
         self._check(lib().qcg_set_graphs(self._h, int(bool(enable))))
+
+    def set_eri_team_classes(self, mask: int):
+        """FP64 ERI-batch classes (bit k: class k) evaluated by the team-form kernel; -1 restores the default."""
+        self._check(lib().qcg_set_eri_team_classes(self._h, ctypes.c_longlong(mask)))
 
     def set_fp32_bound(self, bound: float):
         """Later J/K builds evaluate quartets with Q_ab Q_cd < bound in FP32 (FP64 accumulation)."""

@@ -1,0 +1,109 @@
+// eri_team.cu -- the team form of the FP64 ERI batches (eri_team.cuh) for ONE quartet class; compiled with
+// -DQCG_CLASS=k for every class, defining launch_eri_team_k and team_shape_k.  The generated code comes from
+// gen/md_team_<k>.cuh (stage tables, ket and bra steps, recurrences).
+#include <atomic>
+
+#include "eri_kernels.cuh"
+#include "eri_team.cuh"
+#include "smem_attr.h"
+
+#ifndef QCG_CLASS
+#error "compile with -DQCG_CLASS=<0..20>"
+#endif
+
+#define QCG_STR2(x) #x
+#define QCG_STR(x) QCG_STR2(x)
+#define QCG_CAT2(a, b) a##b
+#define QCG_CAT(a, b) QCG_CAT2(a, b)
+#include QCG_STR(gen/QCG_CAT(md_team_, QCG_CLASS).cuh)
+
+namespace qcg {
+
+namespace {
+constexpr int cls_X()
+{
+    int X = 0;
+    while ((X + 1) * (X + 2) / 2 <= QCG_CLASS) ++X;
+    return X;
+}
+constexpr int kX = cls_X();
+constexpr int kY = QCG_CLASS - kX * (kX + 1) / 2;
+
+// Warps: passes of at most 8, every warp a consumer.  The SM's registers are split among its four
+// schedulers: 8 warps (two per scheduler) leave each thread up to 255 registers, which the (dd|dd) steps
+// need without spilling; a ninth warp would cap every thread at 168.
+constexpr int team_warps(int nf)
+{
+    const int npass = (nf + 7) / 8;
+    return (nf + npass - 1) / npass;
+}
+
+struct Cls
+{
+    static constexpr int LA = kPairLA[kX], LB = kPairLB[kX], LC = kPairLA[kY], LD = kPairLB[kY];
+    static constexpr int kNF = gen::QCG_CAT(kTeamNF, QCG_CLASS), kNE = gen::QCG_CAT(kTeamNE, QCG_CLASS);
+    static constexpr int kNH = gen::QCG_CAT(kTeamNH, QCG_CLASS), kStage = gen::QCG_CAT(kTeamStage, QCG_CLASS);
+#ifdef QCG_TEAM_NW
+    static constexpr int kNW = QCG_TEAM_NW;
+#else
+    static constexpr int kNW = team_warps(kNF);
+#endif
+    static __device__ __forceinline__ void produce(double* st, const PrimPairData& ab, const PrimPairData& cd,
+                                                   const double* __restrict__ bt, bool bra_e)
+    {
+        gen::QCG_CAT(team_produce_, QCG_CLASS)<double>(st, ab, cd, bt, bra_e);
+    }
+    static __device__ __forceinline__ void ket(int jf, const double* st, double (&Y)[kNH])
+    {
+        gen::QCG_CAT(team_ket_, QCG_CLASS)<double>(jf, st, Y);
+    }
+    static __device__ __forceinline__ void bra(const double* st, const double (&Y)[kNH], double (&acc)[kNE])
+    {
+        gen::QCG_CAT(team_bra_, QCG_CLASS)<double>(st, Y, acc);
+    }
+    static __device__ __forceinline__ void hrr_ket(const double* p, double* y, double CDx, double CDy, double CDz)
+    {
+        gen::QCG_CAT(team_hrr_ket_, QCG_CLASS)<double>(p, y, CDx, CDy, CDz);
+    }
+    static __device__ __forceinline__ void hrr_bra(const double* y, double* o, int os, double ABx, double ABy,
+                                                   double ABz)
+    {
+        gen::QCG_CAT(team_hrr_bra_, QCG_CLASS)<double>(y, o, os, ABx, ABy, ABz);
+    }
+};
+
+constexpr int kThreads = Cls::kNW * 32;
+constexpr int kNCD = ncart(Cls::LC) * ncart(Cls::LD);
+constexpr size_t kSmem = 3 * (size_t)Cls::kStage * 32 * sizeof(double);   // three stages
+std::atomic<unsigned long long> g_smem_ready{0};
+}   // namespace
+
+TeamShape QCG_CAT(team_shape_, QCG_CLASS)(int nsm)
+{
+    auto k = eri_batch_team_kernel<Cls>;
+    ensure_smem(k, kSmem, g_smem_ready);
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kThreads, kSmem) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    TeamShape sh;
+    sh.grid = nsm * per_sm;
+    sh.threads = kThreads;
+    sh.slot_doubles = (long long)Cls::kStage * 32;
+    sh.hrr_doubles = (long long)(Cls::kNE * Cls::kNF + Cls::kNE * kNCD) * 32;
+    return sh;
+}
+
+void QCG_CAT(launch_eri_team_, QCG_CLASS)(const BasisDev& bs, const int4* q, const int* order, long long nq,
+                                          double* out, const double* boys, const TeamScratchDev& scr,
+                                          const TeamShape& sh, cudaStream_t st)
+{
+    if (nq <= 0) return;
+    auto k = eri_batch_team_kernel<Cls>;
+    ensure_smem(k, kSmem, g_smem_ready);
+    // one wave of CTAs, each walking groups of 32 quartets; the scratch has room for sh.grid CTAs
+    const long long ngroups = (nq + 31) / 32;
+    const long long blocks = ngroups < sh.grid ? ngroups : sh.grid;
+    k<<<(unsigned)blocks, kThreads, kSmem, st>>>(bs, q, order, nq, out, boys, scr);
+}
+
+}   // namespace qcg

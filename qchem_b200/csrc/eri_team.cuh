@@ -1,0 +1,227 @@
+// eri_team.cuh -- warp-specialised ERI-batch kernel for the high-L classes (team form).
+//
+// A CTA takes 32 contracted quartets at a time (a "group": 32 consecutive entries of the batch's visiting
+// order, which groups equal contraction patterns), one per lane, and works through them in three phases.
+//
+//  1. Stage tables.  For every primitive quartet x of the group (bra primitive pair outer, ket inner) and
+//     every lane, a "stage" holds R^0_{tuv} scaled by the prefactor lambda and the single-centre Hermite
+//     tables E^{i0}_t of the ket pair (and, after the last ket primitive of a bra primitive pair, of the bra
+//     pair) -- generated code, team_produce_<k>.  All warps compute stages, warp w taking x = w, w + nwarps,
+//     ..., and write them once to the CTA's slots of the R cache in global memory (entry-major, lane-minor).
+//  2. Contraction.  Warp w owns one component f of the ket range of the horizontal-recurrence form (f over
+//     L = LC..LC+LD on centre C) per pass.  It keeps in registers Y_f -- the ket step summed over the ket
+//     primitives of the current bra primitive pair -- and acc_f = [e0|f] for every e, adding the bra step
+//     of Y_f to acc_f after the bra pair's last ket primitive (team_ket_<k>, team_bra_<k>).  The stages
+//     stream from the R cache into shared memory, three deep, by bulk copies (cp.async.bulk, the Tensor
+//     Memory Accelerator's untiled form) that one thread issues on an mbarrier; one barrier per primitive
+//     quartet.  With more ket components than warps the group is walked in passes, each pass reading the
+//     stages again (from L2 or HBM) instead of recomputing them.
+//  3. Recurrences.  acc_f goes to the CTA's scratch as [e0|f0] (lane-minor, so every access of a warp is
+//     one coalesced line); the ket recurrence per e row gives [e0|cd] there, and the bra recurrence per
+//     (c d) column writes (ab|cd) into the quartet's output block (generated team_hrr_ket_<k>,
+//     team_hrr_bra_<k>).  No atomics: every output element is written once by one thread.
+//
+// This is the arithmetic of qchem's PrimGaussian::Repulsion4C (PG_Cart_MnD/Imp/GaussianRF.C:446-483) and
+// its contraction (GaussianRF.C:726-752), with the bra and ket transfers done once per contracted quartet
+// (horizontal recurrence) and the bra Hermite contraction once per bra primitive pair.
+#pragma once
+#include <cstdint>
+
+#include "eri_team_iface.h"
+#include "md_core.cuh"
+
+namespace qcg {
+
+extern __shared__ __align__(128) double qcg_team_smem[];
+
+namespace team {
+
+// a wait for a bulk copy gives up after this many polls (each poll may suspend the thread for a while)
+constexpr long long kWaitPolls = 1ll << 24;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_init_fence()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// bulk copy of `bytes` (a multiple of 16; both addresses 16-byte aligned) from global to shared memory,
+// completing a phase of `bar`
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
+// bounded wait for phase `parity` of `bar`; false when it gave up
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
+{
+    for (long long n = 0; n < kWaitPolls; ++n)
+    {
+        uint32_t done;
+        asm volatile(
+            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+            : "=r"(done)
+            : "r"(smem_addr(bar)), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// this thread's generic-proxy writes to global memory become visible to later bulk copies (async proxy)
+__device__ __forceinline__ void fence_async_global()
+{
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+
+}   // namespace team
+
+template <class Cls>
+__global__ void __launch_bounds__(Cls::kNW * 32, 1)
+    eri_batch_team_kernel(BasisDev bs, const int4* __restrict__ quartets, const int* __restrict__ order, long long nq,
+                          double* __restrict__ out, const double* __restrict__ boys_table, TeamScratchDev scr)
+{
+    constexpr int NW = Cls::kNW;                   // warps; warp w owns ket component pass * NW + w
+    constexpr int NF = Cls::kNF, NE = Cls::kNE, NH = Cls::kNH;
+    constexpr int NPASS = (NF + NW - 1) / NW;
+    constexpr int STAGE = Cls::kStage * 32;        // doubles per stage (entry-major, lane-minor)
+    constexpr uint32_t STAGE_BYTES = STAGE * sizeof(double);
+    constexpr int NCD = ncart(Cls::LC) * ncart(Cls::LD);
+    constexpr long long BLK = (long long)ncart(Cls::LA) * ncart(Cls::LB) * NCD;
+    static_assert(NE <= ncart(Cls::LA) * ncart(Cls::LB) && NF <= NCD, "[e0|f0] fits the output block");
+    __shared__ uint64_t full[3];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const bool leader = threadIdx.x == 0;
+    if (leader)
+    {
+        for (int s = 0; s < 3; ++s) team::mbar_init(&full[s]);
+        team::mbar_init_fence();
+    }
+    __syncthreads();
+    double* const rc = scr.rcache + (long long)blockIdx.x * scr.kmax * STAGE;   // this CTA's stage slots
+    double* const hA = scr.hrr + (long long)blockIdx.x * (NE * NF + NE * NCD) * 32;
+    double* const hB = hA + NE * NF * 32;
+    unsigned long long G = 0;   // steps streamed so far: step G uses stage G % 3, phase (G / 3) & 1
+    bool ok = true;             // the leader's waits all completed
+    const long long ngroups = (nq + 31) >> 5;
+    for (long long g = blockIdx.x; g < ngroups; g += gridDim.x)
+    {
+        // every warp reads the same 32 quartets: lane l of every warp holds quartet l of the group
+        const long long gi = g * 32 + lane;
+        const bool valid = gi < nq;
+        const long long q = valid ? (order ? (long long)order[gi] : gi) : 0;
+        const int4 s = quartets[q];
+        int ni = 0, nj = 0, nk = 0, nl = 0;
+        if (valid)
+        {
+            ni = bs.nprim[s.x];
+            nj = bs.nprim[s.y];
+            nk = bs.nprim[s.z];
+            nl = bs.nprim[s.w];
+        }
+        const int Kcd = nk * nl, K = ni * nj * Kcd;
+        const int Kg = __reduce_max_sync(0xffffffffu, K);   // the group's longest primitive loop (CTA-uniform)
+        if (Kg > scr.kmax)
+        {
+            if (leader) atomicOr(scr.err, 2);
+            continue;
+        }
+        // 1. stage tables of every primitive quartet, written once to the R cache
+        for (int x = warp; x < Kg; x += NW)
+            if (x < K)
+            {
+                const int ij = x / Kcd, kl = x - ij * Kcd;
+                const PrimPairData ab = shell_prim_pair(bs, s.x, ij / nj, s.y, ij % nj);
+                const PrimPairData cd = shell_prim_pair(bs, s.z, kl / nl, s.w, kl % nl);
+                Cls::produce(rc + (long long)x * STAGE + lane, ab, cd, boys_table, kl == Kcd - 1);
+            }
+        team::fence_async_global();
+        __syncthreads();
+        // 2. contraction, the stages streamed back through shared memory three deep
+        for (int pass = 0; pass < NPASS; ++pass)
+        {
+            const int jf = pass * NW + warp;
+            auto issue = [&](int x) {
+                const unsigned long long gs = G + x;
+                team::bulk_load(qcg_team_smem + (gs % 3) * STAGE, rc + (long long)x * STAGE, STAGE_BYTES,
+                                &full[gs % 3]);
+            };
+            if (leader)
+            {
+                issue(0);
+                if (Kg > 1) issue(1);
+            }
+            double Y[NH], acc[NE];
+#pragma unroll
+            for (int h = 0; h < NH; ++h) Y[h] = 0.0;
+#pragma unroll
+            for (int e = 0; e < NE; ++e) acc[e] = 0.0;
+            int kl = 0;
+            for (int i = 0; i < Kg; ++i)
+            {
+                const unsigned long long gs = G + i;
+                if (leader) ok = team::mbar_wait(&full[gs % 3], (uint32_t)((gs / 3) & 1)) && ok;
+                __syncthreads();   // stage i is in shared memory; every warp has left step i - 1
+                if (leader && i + 2 < Kg) issue(i + 2);   // into the stage step i - 1 used
+                if (jf < NF && i < K)
+                {
+                    const double* st = qcg_team_smem + (gs % 3) * STAGE + lane;
+                    Cls::ket(jf, st, Y);
+                    if (kl == Kcd - 1)
+                    {
+                        Cls::bra(st, Y, acc);
+#pragma unroll
+                        for (int h = 0; h < NH; ++h) Y[h] = 0.0;
+                        kl = 0;
+                    }
+                    else
+                        ++kl;
+                }
+            }
+            G += Kg;
+            if (jf < NF)
+            {
+#pragma unroll
+                for (int e = 0; e < NE; ++e) hA[(e * NF + jf) * 32 + lane] = acc[e];
+            }
+            __syncthreads();   // the pass's stages are no longer read; its [e0|f] columns are written
+        }
+        // 3. recurrences: ket per e row into [e0|cd], bra per (c d) column into the output block
+        const double* A = bs.cen + 3 * s.x;
+        const double* B = bs.cen + 3 * s.y;
+        const double* C = bs.cen + 3 * s.z;
+        const double* D = bs.cen + 3 * s.w;
+        if (valid)
+        {
+            const double CDx = C[0] - D[0], CDy = C[1] - D[1], CDz = C[2] - D[2];
+            for (int e = warp; e < NE; e += NW)
+                Cls::hrr_ket(hA + e * NF * 32 + lane, hB + e * NCD * 32 + lane, CDx, CDy, CDz);
+        }
+        __syncthreads();
+        if (valid)
+        {
+            const double ABx = A[0] - B[0], ABy = A[1] - B[1], ABz = A[2] - B[2];
+            double* const o = out + q * BLK;
+            for (int cd = warp; cd < NCD; cd += NW) Cls::hrr_bra(hB + cd * 32 + lane, o + cd, NCD, ABx, ABy, ABz);
+        }
+        __syncthreads();   // the scratch and the R cache are free for the next group
+    }
+    if (leader && !ok) atomicOr(scr.err, 1);
+}
+
+}   // namespace qcg

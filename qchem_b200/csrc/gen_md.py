@@ -494,3 +494,212 @@ def main_hrr(outdir):
                 "namespace qcg {\nnamespace gen {\n" + "\n".join(body) + "\n}  // namespace gen\n}  // namespace qcg\n")
         with open(os.path.join(outdir, f"md_hrr_{k}.cuh"), "w") as f:
             f.write(text)
+
+
+# ------------------------------------------------------------------------------------------------------
+# Team form (main_team): the code of the warp-specialised ERI-batch kernel (eri_team.cuh).  A CTA holds 32
+# contracted quartets, one per lane.  Per primitive quartet a producer warp writes a shared-memory stage
+# per lane: R^0_{tuv} scaled by the prefactor lambda, and the single-centre Hermite tables E^{i0}_t of the
+# ket pair (and, after the last ket primitive of a bra primitive pair, of the bra pair).  Consumer warp w
+# owns one ket component f of the HRR form ([e0|f0], f over L = LC..LC+LD on centre C) and keeps in
+# registers
+#     Y_f[h] = sum over the ket primitives of sum_{h' in supp(f)} (-1)^{|h'|} E^{f0}_{h'} R_{h+h'}
+# for h over the bra's Hermite indices, and, once per bra primitive pair, adds
+#     acc_f[e] += sum_t E^{ex 0}_t sum_u E^{ey 0}_u sum_v E^{ez 0}_v Y_f[tuv]
+# so the bra contraction runs once per bra primitive pair instead of once per primitive quartet.  The
+# ket and bra horizontal recurrences of the HRR form then give (ab|cd).  All indices are literals.
+# ------------------------------------------------------------------------------------------------------
+def ne1(Lmax):
+    """stored 1-D entries E^{i0}_t, 1 <= i <= Lmax, t <= i (E^{00}_0 = 1 is not stored)"""
+    return (Lmax + 1) * (Lmax + 2) // 2 - 1
+
+
+def e1_slot(i, t):
+    return i * (i + 1) // 2 - 1 + t
+
+
+def r_stream(L, w, store):
+    """Boys -> R^0_{tuv} for t+u+v <= L, each stored once through store(H, name) as soon as it exists.
+    Same recursion and branch order as r_prologue (x first, then y, then z), evaluated column by column
+    (v, then u, then t) so that only the columns the next ones need stay live; lambda is folded into
+    R^n_{000}, so every R value carries it."""
+    w("    const double p = ab.p, q = cd.p, pq = p + q;")
+    w("    const double alpha = p * q / pq;")
+    w("    const double Xd = ab.Px - cd.Px, Yd = ab.Py - cd.Py, Zd = ab.Pz - cd.Pz;")
+    w(f"    RT F[{L + 1}];")
+    w(f"    boys<{L}>(alpha * (Xd * Xd + Yd * Yd + Zd * Zd), bt, F);")
+    w("    const RT X = RT(Xd), Y = RT(Yd), Z = RT(Zd);")
+    w("    const RT m2a = RT(-2.0 * alpha);")
+    w("    const RT lambda = RT(34.986836655249725693 / (p * q * sqrt(pq)) * ab.K * cd.K);")
+    w("    const RT g0 = lambda;")
+    for n in range(1, L + 1):
+        w(f"    const RT g{n} = g{n - 1} * m2a;")
+
+    def nm(n, t, u, v):
+        return f"r{n}_{t}_{u}_{v}"
+
+    for v in range(L + 1):
+        for n in range(L - v + 1):
+            if v == 0:
+                w(f"    const RT {nm(n, 0, 0, 0)} = g{n} * F[{n}];")
+            else:
+                e = f"Z * {nm(n + 1, 0, 0, v - 1)}"
+                if v > 1:
+                    e += f" + RT({v - 1}) * {nm(n + 1, 0, 0, v - 2)}"
+                w(f"    const RT {nm(n, 0, 0, v)} = {e};")
+        for u in range(L - v + 1):
+            if u >= 1:
+                for n in range(L - u - v + 1):
+                    e = f"Y * {nm(n + 1, 0, u - 1, v)}"
+                    if u > 1:
+                        e += f" + RT({u - 1}) * {nm(n + 1, 0, u - 2, v)}"
+                    w(f"    const RT {nm(n, 0, u, v)} = {e};")
+            for t in range(L - u - v + 1):
+                if t >= 1:
+                    for n in range(L - t - u - v + 1):
+                        e = f"X * {nm(n + 1, t - 1, u, v)}"
+                        if t > 1:
+                            e += f" + RT({t - 1}) * {nm(n + 1, t - 2, u, v)}"
+                        w(f"    const RT {nm(n, t, u, v)} = {e};")
+                w(store(hidx(L, t, u, v), nm(0, t, u, v)))
+
+
+def gen_class_team(LA, LB, LC, LD, idx):
+    L = LA + LB + LC + LD
+    LAB, LCD = LA + LB, LC + LD
+    E, F = comps_range(LA, LAB), comps_range(LC, LCD)
+    HAB = herm_list(LAB)
+    NR, NH = nherm(L), nherm(LAB)
+    NEB, NEK = 3 * ne1(LAB), 3 * ne1(LCD)
+    BOFF, KOFF = NR, NR + NEB
+    o = []
+    w = o.append
+    w(f"// class {idx} in team form: R has {NR} entries, Y_f {NH}, [e0|f0] {len(E)} x {len(F)}")
+    w(f"constexpr int kTeamNR{idx} = {NR};")
+    w(f"constexpr int kTeamNH{idx} = {NH};")
+    w(f"constexpr int kTeamNE{idx} = {len(E)};")
+    w(f"constexpr int kTeamNF{idx} = {len(F)};")
+    w(f"constexpr int kTeamStage{idx} = {NR + NEB + NEK};   // stage entries per lane")
+    # producer
+    w("// one lane's stage for one primitive quartet: entry i at st[i * 32]; the bra tables only when bra_e")
+    w("template <class RT>")
+    w(f"__device__ __forceinline__ void team_produce_{idx}(RT* __restrict__ st, const PrimPairData& ab,")
+    w("    const PrimPairData& cd, const double* __restrict__ bt, const bool bra_e)")
+    w("{")
+    r_stream(L, w, lambda H, name: f"    st[{H} * 32] = {name};")
+    if LCD > 0:
+        w("    {")
+        w("    const RT a12k = RT(0.5 / cd.p);")
+        w("    const RT kPAx = RT(cd.PAx), kPAy = RT(cd.PAy), kPAz = RT(cd.PAz);")
+        for d, (dn, PA) in enumerate((("ekx", "kPAx"), ("eky", "kPAy"), ("ekz", "kPAz"))):
+            for s_ in gen_E(dn, LCD, 0, PA, "0", "a12k"):
+                w("    " + s_)
+            for i in range(1, LCD + 1):
+                for t in range(i + 1):
+                    w(f"    st[{KOFF + d * ne1(LCD) + e1_slot(i, t)} * 32] = {dn}_{i}_0_{t};")
+        w("    }")
+    if LAB > 0:
+        w("    if (bra_e)")
+        w("    {")
+        w("    const RT a12b = RT(0.5 / ab.p);")
+        w("    const RT bPAx = RT(ab.PAx), bPAy = RT(ab.PAy), bPAz = RT(ab.PAz);")
+        for d, (dn, PA) in enumerate((("ebx", "bPAx"), ("eby", "bPAy"), ("ebz", "bPAz"))):
+            for s_ in gen_E(dn, LAB, 0, PA, "0", "a12b"):
+                w("    " + s_)
+            for i in range(1, LAB + 1):
+                for t in range(i + 1):
+                    w(f"    st[{BOFF + d * ne1(LAB) + e1_slot(i, t)} * 32] = {dn}_{i}_0_{t};")
+        w("    }")
+    else:
+        w("    (void)bra_e;")
+    w("}")
+    # consumer: ket step of component jf
+    w("// Y_f[h] += sum_{h' in supp(f)} (-1)^{|h'|} E^{f0}_{h'} R_{h+h'} for ket component jf (warp-uniform)")
+    w("template <class RT>")
+    w(f"__device__ __forceinline__ void team_ket_{idx}(const int jf, const RT* __restrict__ st, RT (&Yf)[{NH}])")
+    w("{")
+    w("    switch (jf)")
+    w("    {")
+    for jf, f in enumerate(F):
+        w(f"    case {jf}: {{ // f = {f}")
+        for d, dn in enumerate(("ekx", "eky", "ekz")):
+            for t in range(f[d] + 1):
+                if f[d] == 0:
+                    w(f"    const RT {dn}_0_0_0 = RT(1);")
+                else:
+                    w(f"    const RT {dn}_{f[d]}_0_{t} = st[{KOFF + d * ne1(LCD) + e1_slot(f[d], t)} * 32];")
+        supp = [(tp, up, vp) for tp in range(f[0] + 1) for up in range(f[1] + 1) for vp in range(f[2] + 1)]
+        for (tp, up, vp) in supp:
+            sgn = "-" if (tp + up + vp) & 1 else ""
+            w(f"    const RT s{tp}{up}{vp} = {sgn}ekx_{f[0]}_0_{tp} * eky_{f[1]}_0_{up} * ekz_{f[2]}_0_{vp};")
+        contrib = {}
+        for h in HAB:
+            for hp in supp:
+                H = hidx(L, h[0] + hp[0], h[1] + hp[1], h[2] + hp[2])
+                contrib.setdefault(H, []).append((hidx(LAB, *h), hp))
+        for H in sorted(contrib):
+            body = " ".join(f"Yf[{xi}] = qfma(s{hp[0]}{hp[1]}{hp[2]}, r, Yf[{xi}]);" for (xi, hp) in contrib[H])
+            w(f"    {{ const RT r = st[{H} * 32]; {body} }}")
+        w("    } break;")
+    w("    default: break;")
+    w("    }")
+    w("}")
+    # consumer: bra step (the same for every f)
+    w("// acc[e] += sum_t E^{ex 0}_t sum_u E^{ey 0}_u sum_v E^{ez 0}_v Y_f[tuv], bra tables from the stage")
+    w("template <class RT>")
+    w(f"__device__ __forceinline__ void team_bra_{idx}(const RT* __restrict__ st, const RT (&Yf)[{NH}],")
+    w(f"    RT (&acc)[{len(E)}])")
+    w("{")
+    for d, dn in enumerate(("ebx", "eby", "ebz")):
+        w(f"    const RT {dn}_0_0_0 = RT(1);")
+        for i in range(1, LAB + 1):
+            for t in range(i + 1):
+                w(f"    const RT {dn}_{i}_0_{t} = st[{BOFF + d * ne1(LAB) + e1_slot(i, t)} * 32];")
+    for je, e in enumerate(E):
+        w("    {")
+        w("      RT sx = RT(0);")
+        for t in range(e[0] + 1):
+            w("      { RT sy = RT(0);")
+            for u in range(e[1] + 1):
+                zs = f"ebz_{e[2]}_0_0 * Yf[{hidx(LAB, t, u, 0)}]"
+                for v in range(1, e[2] + 1):
+                    zs = f"qfma(ebz_{e[2]}_0_{v}, Yf[{hidx(LAB, t, u, v)}], {zs})"
+                w(f"        sy = qfma(eby_{e[1]}_0_{u}, {zs}, sy);")
+            w(f"        sx = qfma(ebx_{e[0]}_0_{t}, sy, sx); }}")
+        w(f"      acc[{je}] += sx;")
+        w("    }")
+    w("}")
+    # the recurrences on the per-CTA scratch, whose layout is lane-minor (element k of lane l at [k * 32 + l]):
+    # ket of one e row: p[f] -> y[c * ND + d]; bra of one (c d) column: y[e * NCD] -> o[(a * NB + b) * os]
+    nd, nb, ncd = len(comps(LD)), len(comps(LB)), len(comps(LC)) * len(comps(LD))
+    w("template <class RT>")
+    w(f"__device__ __forceinline__ void team_hrr_ket_{idx}(const RT* p, RT* y, const RT CDx, const RT CDy,")
+    w("    const RT CDz)")
+    w("{")
+    hrr_code(LC, LD, lambda k: f"p[{k} * 32]", lambda ix, iy, v, nrm: f"    y[{ix * nd + iy} * 32] = {v} * RT({lit(nrm)});",
+             ("CDx", "CDy", "CDz"), w, "t")
+    w("}")
+    w("template <class RT>")
+    w(f"__device__ __forceinline__ void team_hrr_bra_{idx}(const RT* y, RT* o, const int os, const RT ABx,")
+    w("    const RT ABy, const RT ABz)")
+    w("{")
+    hrr_code(LA, LB, lambda k: f"y[{k * ncd} * 32]",
+             lambda ix, iy, v, nrm: f"    o[{ix * nb + iy} * os] = {v} * RT({lit(nrm)});", ("ABx", "ABy", "ABz"), w, "t")
+    w("}")
+    return o
+
+
+def main_team(outdir, classes_=None):
+    """Writes md_team_<k>.cuh (the team form of class k) for the classes listed (default: all 21)."""
+    os.makedirs(outdir, exist_ok=True)
+    for k, (la, lb, lc, ld) in enumerate(classes()):
+        if classes_ is not None and k not in classes_:
+            continue
+        body = gen_class_team(la, lb, lc, ld, k)
+        text = ("// generated by gen_md.py (team form) -- do not edit\n#pragma once\n#include \"../md_core.cuh\"\n"
+                "namespace qcg {\nnamespace gen {\n" + "\n".join(body) + "\n}  // namespace gen\n}  // namespace qcg\n")
+        path = os.path.join(outdir, f"md_team_{k}.cuh")
+        old = open(path).read() if os.path.exists(path) else None
+        if old != text:
+            with open(path, "w") as f:
+                f.write(text)

@@ -1,4 +1,6 @@
-// registry.cu -- tables of the per-class launchers compiled in the 42 eri_class objects (21 classes x FP64/FP32).
+// registry.cu -- tables of the per-class launchers compiled in the 42 eri_class objects (21 classes x FP64/FP32)
+// and the 21 eri_team objects (the team form of the FP64 ERI batches).
+#include "eri_team_iface.h"
 #include "qcg_internal.h"
 
 namespace qcg {
@@ -12,7 +14,10 @@ namespace qcg {
     void launch_eri_batch32_##k(const BasisDev&, const int4*, const int*, long long, float*, const double*,        \
                                 cudaStream_t, int);                                                                 \
     void launch_jk32_##k(const JKWorkDev&, const PairListDev&, const PairListDev&, const PrimPairsDev&, const int*,  \
-                         const double*, double*, double*, int, const double*, cudaStream_t, int);
+                         const double*, double*, double*, int, const double*, cudaStream_t, int);                    \
+    void launch_eri_team_##k(const BasisDev&, const int4*, const int*, long long, double*, const double*,            \
+                             const TeamScratchDev&, const TeamShape&, cudaStream_t);                                 \
+    TeamShape team_shape_##k(int);
 QCG_DECL(0) QCG_DECL(1) QCG_DECL(2) QCG_DECL(3) QCG_DECL(4) QCG_DECL(5) QCG_DECL(6) QCG_DECL(7) QCG_DECL(8)
 QCG_DECL(9) QCG_DECL(10) QCG_DECL(11) QCG_DECL(12) QCG_DECL(13) QCG_DECL(14) QCG_DECL(15) QCG_DECL(16)
 QCG_DECL(17) QCG_DECL(18) QCG_DECL(19) QCG_DECL(20)
@@ -24,6 +29,16 @@ const EriBatchLauncher kEriBatchLaunchers[kNumQuartetClasses] = {
     launch_eri_batch_10, launch_eri_batch_11, launch_eri_batch_12, launch_eri_batch_13, launch_eri_batch_14,
     launch_eri_batch_15, launch_eri_batch_16, launch_eri_batch_17, launch_eri_batch_18, launch_eri_batch_19,
     launch_eri_batch_20};
+const EriTeamShapeFn kEriTeamShapes[kNumQuartetClasses] = {
+    team_shape_0,  team_shape_1,  team_shape_2,  team_shape_3,  team_shape_4,  team_shape_5,  team_shape_6,
+    team_shape_7,  team_shape_8,  team_shape_9,  team_shape_10, team_shape_11, team_shape_12, team_shape_13,
+    team_shape_14, team_shape_15, team_shape_16, team_shape_17, team_shape_18, team_shape_19, team_shape_20};
+const EriTeamLauncher kEriTeamLaunchers[kNumQuartetClasses] = {
+    launch_eri_team_0,  launch_eri_team_1,  launch_eri_team_2,  launch_eri_team_3,  launch_eri_team_4,
+    launch_eri_team_5,  launch_eri_team_6,  launch_eri_team_7,  launch_eri_team_8,  launch_eri_team_9,
+    launch_eri_team_10, launch_eri_team_11, launch_eri_team_12, launch_eri_team_13, launch_eri_team_14,
+    launch_eri_team_15, launch_eri_team_16, launch_eri_team_17, launch_eri_team_18, launch_eri_team_19,
+    launch_eri_team_20};
 const JKLauncher kJKLaunchers[kNumQuartetClasses] = {
     launch_jk_0,  launch_jk_1,  launch_jk_2,  launch_jk_3,  launch_jk_4,  launch_jk_5,  launch_jk_6,
     launch_jk_7,  launch_jk_8,  launch_jk_9,  launch_jk_10, launch_jk_11, launch_jk_12, launch_jk_13,

@@ -24,6 +24,7 @@
 #include <cusolverDn.h>
 
 #include "../../include/qchem_b200.h"
+#include "eri_team_iface.h"
 #include "md_core.cuh"
 #include "qcg_internal.h"
 #include "boys_table.h"
@@ -340,6 +341,12 @@ struct qcg_handle
     unsigned char* d_key = nullptr;
     int *d_order = nullptr, *d_hist = nullptr, *d_cursor = nullptr;
 
+    // team-form ERI batches (eri_team.cu): per-CTA R cache and recurrence scratch (grow only), error word
+    double* d_team = nullptr;
+    long long team_cap = 0;   // doubles
+    int* d_team_err = nullptr;
+    int maxnp[kMaxL + 1] = {};   // largest contraction length per angular momentum (0: not yet computed)
+
     // host-buffer ERI batches: two quartet/output buffer pairs (grow only) and a copy-out stream
     void* hb_q[2] = {nullptr, nullptr};
     void* hb_out[2] = {nullptr, nullptr};
@@ -358,6 +365,7 @@ struct qcg_handle
     cudaEvent_t fork = nullptr, join[kSide] = {};
     // J/K builds replayed as CUDA graphs, keyed by their arguments and the screening generation
     bool use_graphs = false;
+    long long team_mask = -1;   // qcg_set_eri_team_classes; -1: the process default (eri_team_mask)
     int screen_gen = 0;
     QcgGraphKey last_key{};
     std::vector<std::pair<QcgGraphKey, cudaGraphExec_t>> graphs;
@@ -2261,12 +2269,94 @@ int qcg_norms(const qcg_handle* h, double* ns)
 
 extern "C++" {
 namespace {
+#ifndef QCG_TEAM_DEFAULT_MASK
+#define QCG_TEAM_DEFAULT_MASK 0u
+#endif
+// The FP64 classes whose ERI batches run in the team form (bit k: class k): the build's choice
+// (QCG_TEAM_DEFAULT_MASK, the classes measured faster in that form), unless QCG_ERI_TEAM_MASK in the
+// environment names other classes (hexadecimal or decimal bit mask; read once per process).
+unsigned eri_team_mask()
+{
+    static const unsigned mask = [] {
+        const char* e = std::getenv("QCG_ERI_TEAM_MASK");
+        if (!e || !*e) return (unsigned)(QCG_TEAM_DEFAULT_MASK);
+        return (unsigned)std::strtoul(e, nullptr, 0);
+    }();
+    return mask;
+}
+
+// the team form's scratch for class k: one wave of CTAs, each with stage slots for the class's longest
+// primitive loop in this basis (the product of the largest contraction lengths of the four angular
+// momenta) and its recurrence blocks.  Null when that exceeds kTeamScratchMax bytes; the batch then runs in
+// the thread-per-quartet form.
+constexpr long long kTeamScratchMax = 4LL << 30;
+
+bool team_scratch(qcg_handle* h, int k, TeamScratchDev& scr, TeamShape& sh)
+{
+    int X = 0;
+    while ((X + 1) * (X + 2) / 2 <= k) ++X;
+    const int Y = k - X * (X + 1) / 2;
+    const int Ls[4] = {kPairLA[X], kPairLB[X], kPairLA[Y], kPairLB[Y]};
+    if (!h->maxnp[0])
+        for (int l = 0; l <= kMaxL; ++l)
+        {
+            int mx = 1;
+            for (int i = 0; i < h->nshell; ++i)
+                if (h->L[i] == l) mx = std::max(mx, h->nprim[i]);
+            h->maxnp[l] = mx;
+        }
+    long long kmax = 1;
+    for (int l : Ls) kmax *= h->maxnp[l];
+    sh = kEriTeamShapes[k](h->nsm);
+    const long long need = (long long)sh.grid * (kmax * sh.slot_doubles + sh.hrr_doubles);
+    if (need * (long long)sizeof(double) > kTeamScratchMax) return false;
+    if (need > h->team_cap)
+    {
+        if (h->d_team) h->release(h->d_team);
+        h->d_team = nullptr;
+        h->team_cap = 0;
+        h->d_team = h->alloc<double>((size_t)need);
+        h->team_cap = need;
+    }
+    if (!h->d_team_err)
+    {
+        h->d_team_err = h->alloc<int>(1);
+        CK(cudaMemsetAsync(h->d_team_err, 0, sizeof(int), h->stream));
+    }
+    scr.rcache = h->d_team;
+    scr.kmax = (int)kmax;
+    scr.hrr = h->d_team + (long long)sh.grid * kmax * sh.slot_doubles;
+    scr.err = h->d_team_err;
+    return true;
+}
+
+// the team kernels' error word (a bulk-copy wait that gave up, or a group longer than the stage slots):
+// read after a synchronising call, then cleared
+void check_team_error(qcg_handle* h)
+{
+    if (!h->d_team_err) return;
+    int e = 0;
+    CK(cudaMemcpy(&e, h->d_team_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (!e) return;
+    CK(cudaMemset(h->d_team_err, 0, sizeof(int)));
+    throw Error{QCG_ERR_CUDA, e & 1 ? "ERI batch: a bulk-copy wait gave up; the results are not valid"
+                                    : "ERI batch: a primitive loop longer than the stage slots"};
+}
+
 template <class T>
 void eri_batch_launch(qcg_handle* h, int k, const int* dq, long long m, T* dout)
 {
     const int* order = batch_order(h, dq, m);
     if constexpr (std::is_same_v<T, double>)
-        kEriBatchLaunchers[k](h->bs, (const int4*)dq, order, m, dout, h->d_boys, h->stream, h->nsm);
+    {
+        const unsigned mask = h->team_mask >= 0 ? (unsigned)h->team_mask : eri_team_mask();
+        TeamScratchDev scr{};
+        TeamShape sh{};
+        if (((mask >> k) & 1u) && team_scratch(h, k, scr, sh))
+            kEriTeamLaunchers[k](h->bs, (const int4*)dq, order, m, dout, h->d_boys, scr, sh, h->stream);
+        else
+            kEriBatchLaunchers[k](h->bs, (const int4*)dq, order, m, dout, h->d_boys, h->stream, h->nsm);
+    }
     else
         kEriBatch32Launchers[k](h->bs, (const int4*)dq, order, m, dout, h->d_boys, h->stream, h->nsm);
     CK(cudaGetLastError());
@@ -2386,6 +2476,7 @@ void eri_batch_run(qcg_handle* h, int la, int lb, int lc, int ld, long long nq, 
         }
         CK(cudaStreamSynchronize(h->copy_stream));
         CK(cudaStreamSynchronize(h->stream));
+        check_team_error(h);
     }
 }
 }   // namespace
@@ -2577,6 +2668,15 @@ int qcg_set_graphs(qcg_handle* h, int enable)
     h->use_graphs = enable != 0;
     if (!h->use_graphs) h->drop_graphs();
     return QCG_OK;
+}
+
+int qcg_set_eri_team_classes(qcg_handle* h, long long mask)
+{
+    if (!h) return QCG_ERR_ARG;
+    return guarded(h, [&] {
+        require(mask >= -1 && mask < (1LL << kNumQuartetClasses), "mask must be -1 or a 21-bit class mask");
+        h->team_mask = mask;
+    });
 }
 
 int qcg_set_fp32_bound(qcg_handle* h, double bound)

@@ -270,3 +270,75 @@ extern "C" int host_md_eri_hrr_inplace(long long nq, const int* L, const int* np
     return 0;
 }
 #endif
+
+#ifdef HM_TEAM
+// The team form (gen_md.main_team writes gen_team/md_team_<k>.cuh): the arithmetic of eri_batch_team_kernel
+// for one quartet on lane 0 of a stage, in the kernel's order -- per ket component f, over the primitive
+// quartets (bra primitive pair outer, ket inner) the stage tables, the ket step into Y_f, and after the last
+// ket primitive the bra step into acc_f; then [e0|f0] in a lane-minor scratch, the ket recurrence per e row
+// into [e0|cd] there, and the bra recurrence per (c d) column into the output block, as the kernel does.
+#include HM_STR(gen_team/HM_CAT(md_team_, QCG_CLASS).cuh)
+
+extern "C" int host_md_eri_team(long long nq, const int* L, const int* np, const double* exps, const double* coefs,
+                                const double* cen, double* out)
+{
+    constexpr int NE = HM_CAT(qcg::gen::kTeamNE, QCG_CLASS), NF = HM_CAT(qcg::gen::kTeamNF, QCG_CLASS);
+    constexpr int NH = HM_CAT(qcg::gen::kTeamNH, QCG_CLASS), NS = HM_CAT(qcg::gen::kTeamStage, QCG_CLASS);
+    std::vector<double> stage((size_t)NS * 32);
+    for (long long q = 0; q < nq; ++q)
+    {
+        int l[4], n[4];
+        std::vector<double> w[4];
+        for (int s = 0; s < 4; ++s)
+        {
+            const long long r = 4 * q + s;
+            l[s] = L[r];
+            n[s] = np[r];
+            if (n[s] < 1 || n[s] > 8) return 1;
+            w[s] = shell_coefs(l[s], n[s], exps + 8 * r, coefs + 8 * r);
+        }
+        const int na = qcg::ncart(l[0]), nb = qcg::ncart(l[1]), ncd = qcg::ncart(l[2]) * qcg::ncart(l[3]);
+        if (NE > na * nb || NF > ncd) return 2;
+        double* o = out + q * (long long)na * nb * ncd;
+        for (int k = 0; k < na * nb * ncd; ++k) o[k] = std::nan("");
+        std::vector<double> hA((size_t)NE * NF * 32, std::nan("")), hB((size_t)NE * ncd * 32, std::nan(""));
+        const double* c0 = cen + 12 * q;
+        auto pair = [&](int s0, int i, int s1, int j) {
+            return qcg::make_prim_pair(exps[8 * (4 * q + s0) + i], c0[3 * s0], c0[3 * s0 + 1], c0[3 * s0 + 2],
+                                       w[s0][i], exps[8 * (4 * q + s1) + j], c0[3 * s1], c0[3 * s1 + 1],
+                                       c0[3 * s1 + 2], w[s1][j]);
+        };
+        const int Kcd = n[2] * n[3];
+        for (int jf = 0; jf < NF; ++jf)
+        {
+            double Y[NH] = {}, acc[NE] = {};
+            for (int ij = 0; ij < n[0] * n[1]; ++ij)
+            {
+                const qcg::PrimPairData pab = pair(0, ij / n[1], 1, ij % n[1]);
+                for (int kl = 0; kl < Kcd; ++kl)
+                {
+                    const qcg::PrimPairData pcd = pair(2, kl / n[3], 3, kl % n[3]);
+                    std::fill(stage.begin(), stage.end(), std::nan(""));
+                    HM_CAT(qcg::gen::team_produce_, QCG_CLASS)<double>(stage.data(), pab, pcd, kBoysTable,
+                                                                      kl == Kcd - 1);
+                    HM_CAT(qcg::gen::team_ket_, QCG_CLASS)<double>(jf, stage.data(), Y);
+                    if (kl == Kcd - 1)
+                    {
+                        HM_CAT(qcg::gen::team_bra_, QCG_CLASS)<double>(stage.data(), Y, acc);
+                        for (double& y : Y) y = 0.0;
+                    }
+                }
+            }
+            for (int e = 0; e < NE; ++e) hA[(size_t)(e * NF + jf) * 32] = acc[e];
+        }
+        for (int e = 0; e < NE; ++e)
+            HM_CAT(qcg::gen::team_hrr_ket_, QCG_CLASS)<double>(hA.data() + (size_t)e * NF * 32,
+                                                              hB.data() + (size_t)e * ncd * 32, c0[6] - c0[9],
+                                                              c0[7] - c0[10], c0[8] - c0[11]);
+        for (int cd = 0; cd < ncd; ++cd)
+            HM_CAT(qcg::gen::team_hrr_bra_, QCG_CLASS)<double>(hB.data() + (size_t)cd * 32, o + cd, ncd,
+                                                              c0[0] - c0[3], c0[1] - c0[4], c0[2] - c0[5]);
+    }
+    return 0;
+}
+#endif

@@ -37,14 +37,15 @@ def host_classes(tmp_path_factory):
         sys.path.pop(0)
     gen_md.main(os.path.join(tmp, "gen"))
     gen_md.main_hrr(os.path.join(tmp, "gen_hrr"))
+    gen_md.main_team(os.path.join(tmp, "gen_team"))
     for name in ("md_core.cuh", "boys_table.h"):
         shutil.copy(os.path.join(CSRC, name), tmp)
     src = os.path.join(HERE, "host_md", "host_md.cpp")
 
     def compile_class(k):
         out = os.path.join(tmp, f"host_md_{k}.so")
-        r = subprocess.run(["g++", "-std=c++17", "-O1", "-fPIC", "-shared", f"-DQCG_CLASS={k}", "-DHM_HRR", "-I", tmp,
-                            src, "-o", out], capture_output=True, text=True)
+        r = subprocess.run(["g++", "-std=c++17", "-O1", "-fPIC", "-shared", f"-DQCG_CLASS={k}", "-DHM_HRR", "-DHM_TEAM", "-I",
+                            tmp, src, "-o", out], capture_output=True, text=True)
         assert r.returncode == 0, r.stderr[-3000:]
         lib = ctypes.CDLL(out)
         lib.host_md_eri.restype = ctypes.c_int
@@ -52,6 +53,7 @@ def host_classes(tmp_path_factory):
         lib.host_md_eri_hrr.restype = ctypes.c_int
         lib.host_md_eri_hrr_inplace.restype = ctypes.c_int
         lib.host_md_eri_hrr_f32.restype = ctypes.c_int
+        lib.host_md_eri_team.restype = ctypes.c_int
         assert lib.host_md_class() == k
         return k, lib
 
@@ -142,6 +144,28 @@ def test_generated_class_hrr_form(k, box, host_classes, oracle_mod):
         assert rc == 0
         err = np.abs(out - ref).max()
         assert err <= ERI_ABS and err <= 1e-12 * np.abs(ref).max(), (cls, fn.__name__, err, np.abs(ref).max())
+
+
+@pytest.mark.parametrize("box", [3.0, 12.0])
+@pytest.mark.parametrize("k", range(21))
+def test_generated_class_team_form(k, box, host_classes, oracle_mod):
+    """The team form's arithmetic (producer stage, ket step per component f into Y_f summed over the ket
+    primitives, bra step once per bra primitive pair, then both recurrences in place in the output block):
+    the integrals of the direct form, to 1e-12 absolute and relative to the largest integral."""
+    cls = W.quartet_classes()[k]
+    pool = W.shell_pool(16, seed=W.SEED0 + 2100, box=box)
+    q = W.eri_class_batch(cls, NQ, 16, seed=W.SEED0 + 2100 + k)
+    L, npr, ex, co, cen = _pack(pool, q)
+    blk = int(np.prod([(l + 1) * (l + 2) // 2 for l in cls]))
+    out = np.full(NQ * blk, np.nan)
+    p = lambda a, t: a.ctypes.data_as(ctypes.POINTER(t))
+    rc = host_classes[k].host_md_eri_team(ctypes.c_longlong(NQ), p(L, ctypes.c_int), p(npr, ctypes.c_int),
+                                          p(ex, ctypes.c_double), p(co, ctypes.c_double), p(cen, ctypes.c_double),
+                                          p(out, ctypes.c_double))
+    assert rc == 0
+    ref = oracle_mod.OracleBasis(pool).eri_batch(q).reshape(-1)
+    err = np.abs(out - ref).max()
+    assert err <= ERI_ABS and err <= 1e-12 * np.abs(ref).max(), (cls, err, np.abs(ref).max())
 
 
 @pytest.fixture(scope="session")
