@@ -29,12 +29,20 @@ constexpr int cls_X()
 constexpr int kX = cls_X();
 constexpr int kY = QCG_CLASS - kX * (kX + 1) / 2;
 
-// Warps: passes of at most 8, every warp a consumer.  The SM's registers are split among its four
-// schedulers: 8 warps (two per scheduler) leave each thread up to 255 registers, which the (dd|dd) steps
-// need without spilling; a ninth warp would cap every thread at 168.
-constexpr int team_warps(int nf)
+// Warps per CTA, every warp a consumer of its own ket component per pass.  At most 8: the SM's registers are
+// split among its four schedulers, and 8 warps (two per scheduler) leave each thread up to 255 registers,
+// which the (dd|dd) steps need without spilling (a ninth warp caps every thread at 168).  Each component
+// has its own straight-line ket code, and the code of the components in flight must fit the instruction
+// cache.  Measured on a B200: on (dd|dd) 8 warps on 8 components ran at half the speed of 4 (and 3.4x slower
+// than 8 warps sharing one component's code), 2 warps were slower than 4, and 4 warps also beat 8 on (dd|dp),
+// (dd|pp) and (dp|dp), whose largest components have 220-570 instructions.  So: 8 warps where the largest
+// component has at most kSmallKet instructions, else 4.
+constexpr int kSmallKet = 150;
+
+constexpr int team_warps(int nf, int ket_instr)
 {
-    const int npass = (nf + 7) / 8;
+    const int maxw = ket_instr <= kSmallKet ? 8 : 4;
+    const int npass = (nf + maxw - 1) / maxw;
     return (nf + npass - 1) / npass;
 }
 
@@ -46,7 +54,7 @@ struct Cls
 #ifdef QCG_TEAM_NW
     static constexpr int kNW = QCG_TEAM_NW;
 #else
-    static constexpr int kNW = team_warps(kNF);
+    static constexpr int kNW = team_warps(kNF, gen::QCG_CAT(kTeamKetInstr, QCG_CLASS));
 #endif
     static __device__ __forceinline__ void produce(double* st, const PrimPairData& ab, const PrimPairData& cd,
                                                    const double* __restrict__ bt, bool bra_e)

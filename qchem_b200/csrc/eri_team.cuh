@@ -8,8 +8,13 @@
 //     tables E^{i0}_t of the ket pair (and, after the last ket primitive of a bra primitive pair, of the bra
 //     pair) -- generated code, team_produce_<k>.  All warps compute stages, warp w taking x = w, w + nwarps,
 //     ..., and write them once to the CTA's slots of the R cache in global memory (entry-major, lane-minor).
+//     Two variants were measured slower on a B200 and dropped: rebuilding the Hermite tables in the
+//     consumers to halve the stage (1.4x slower on (dd|dd): the contraction is bound by instruction issue),
+//     and walking the group one bra primitive pair at a time so that the cache stays in L2 (1.3x slower: a
+//     barrier, a pipeline restart and an accumulator save per window cost more than the HBM traffic saved).
 //  2. Contraction.  Warp w owns one component f of the ket range of the horizontal-recurrence form (f over
-//     L = LC..LC+LD on centre C) per pass.  It keeps in registers Y_f -- the ket step summed over the ket
+//     L = LC..LC+LD on centre C) per pass; each component has its own straight-line ket code, and the warp
+//     count is sized so that the code of the components in flight fits the SM's instruction cache.  It keeps in registers Y_f -- the ket step summed over the ket
 //     primitives of the current bra primitive pair -- and acc_f = [e0|f] for every e, adding the bra step
 //     of Y_f to acc_f after the bra pair's last ket primitive (team_ket_<k>, team_bra_<k>).  The stages
 //     stream from the R cache into shared memory, three deep, by bulk copies (cp.async.bulk, the Tensor

@@ -580,6 +580,15 @@ def gen_class_team(LA, LB, LC, LD, idx):
     w(f"constexpr int kTeamNE{idx} = {len(E)};")
     w(f"constexpr int kTeamNF{idx} = {len(F)};")
     w(f"constexpr int kTeamStage{idx} = {NR + NEB + NEK};   // stage entries per lane")
+    # ket-step instruction estimate (loads, products, fused multiply-adds) of the largest component: the
+    # launcher sizes its warp count so that the ket code running at once fits the instruction cache
+    sizes = []
+    for f in F:
+        supp = (f[0] + 1) * (f[1] + 1) * (f[2] + 1)
+        idxs = set((h[0] + a, h[1] + b, h[2] + c) for h in HAB for a in range(f[0] + 1) for b in range(f[1] + 1)
+                   for c in range(f[2] + 1))
+        sizes.append(len(HAB) * supp + len(idxs) + 2 * supp + sum(f) + 3)
+    w(f"constexpr int kTeamKetInstr{idx} = {max(sizes)};")
     # producer
     w("// one lane's stage for one primitive quartet: entry i at st[i * 32]; the bra tables only when bra_e")
     w("template <class RT>")

@@ -2287,7 +2287,7 @@ unsigned eri_team_mask()
 
 // the team form's scratch for class k: one wave of CTAs, each with stage slots for the class's longest
 // primitive loop in this basis (the product of the largest contraction lengths of the four angular
-// momenta) and its recurrence blocks.  Null when that exceeds kTeamScratchMax bytes; the batch then runs in
+// momenta) and its recurrence blocks.  False when that exceeds kTeamScratchMax bytes; the batch then runs in
 // the thread-per-quartet form.
 constexpr long long kTeamScratchMax = 4LL << 30;
 
