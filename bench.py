@@ -607,6 +607,25 @@ def run_fock3(args, torch, api, B, W, peak_tf, stream):
     e1.record(stream)
     torch.cuda.synchronize()
     ms_tuned = max_over_ranks(e0.elapsed_time(e1) / args.steps, dev)
+    # the chosen form's mixed precision on the same build: quartets whose density-weighted bound
+    # Q_ab Q_cd max|D| is below `bound` in FP32 (FP64 accumulation), the rest FP64; every rank takes the same
+    # collective steps
+    Jref, Kref = J.clone(), K.clone()
+    eng.set_fp32_bound(0.0)
+    mixed = {}
+    for bound in (1e-9, 1e-7, 1e-5):
+        eng.set_fp32_bound(bound)
+        step()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms_mixed = max_over_ranks(e0.elapsed_time(e1) / args.steps, dev)
+        mixed[f"{bound:g}"] = {"ms_per_step": ms_mixed, "speedup_vs_fp64": ms_tuned / ms_mixed,
+                               "max_abs_dJ": float((J - Jref).abs().max()), "max_abs_dK": float((K - Kref).abs().max())}
+    eng.set_fp32_bound(0.0)
     tf = st.flops / (ms * 1e-3) / 1e12
     line = {"metric": "direct J/K Fock build, shell quartets/s (32-water cluster, N=1824)",
             "value": st.quartets / (ms * 1e-3), "unit": "quartets/s", "n_gpus": world, "steps": args.steps,
@@ -622,7 +641,10 @@ def run_fock3(args, torch, api, B, W, peak_tf, stream):
             "e2e": {"value": st.quartets / e2e_s, "unit": "quartets/s", "h2d_bytes_per_step": 8 * n * n,
                     "d2h_bytes_per_step": 16 * n * n},
             "autotuned": {"value": st.quartets / (ms_tuned * 1e-3), "ms_per_step": ms_tuned, "tuning_s": t_tune,
-                          "shapes_run_cap_by_class": choice}}
+                          "shapes_run_cap_by_class": choice},
+            "mixed_fp32_fp64": {"by_fp32_bound": mixed,
+                                "note": "same build with the FP32 band below each bound (autotuned shapes); "
+                                        "errors are max |J - J_fp64|, |K - K_fp64| over the matrix"}}
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -803,8 +825,15 @@ def extras(torch, dev):
     setup_s = time.perf_counter() - t0
     J, K, st = e3.fock_jk(D)
     J, K, st = e3.fock_jk(D)
+    # the mixed FP32/FP64 build of the same density (quartets with Q_ab Q_cd max|D| < 1e-7 in FP32)
+    e3.set_fp32_bound(1e-7)
+    Jm, Km, stm = e3.fock_jk(D)
+    e3.set_fp32_bound(0.0)
     out["fock_jk_config3"] = {"nbf": B.nbf(sh3), "quartets": st.quartets, "ms": st.ms_total,
-                              "tflops_algorithmic": st.flops / (st.ms_eri * 1e-3) / 1e12, "setup_s": setup_s}
+                              "tflops_algorithmic": st.flops / (st.ms_eri * 1e-3) / 1e12, "setup_s": setup_s,
+                              "mixed_fp32_below_1e-7": {"ms": stm.ms_total, "speedup_vs_fp64": st.ms_total / stm.ms_total,
+                                                        "max_abs_dJ": float(np.abs(Jm - J).max()),
+                                                        "max_abs_dK": float(np.abs(Km - K).max())}}
     return out
 
 

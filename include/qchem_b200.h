@@ -175,6 +175,12 @@ int qcg_set_graphs(qcg_handle* h, int enable);
  * choice, or the mask in the environment variable QCG_ERI_TEAM_MASK.  Both forms give the same integrals
  * to rounding.  No reference counterpart. */
 int qcg_set_eri_team_classes(qcg_handle* h, long long mask);
+/* Restrict later J/K builds to a subset of shell pairs: mask (nshell x nshell bytes, row-major; pair (a,b) is
+ * in the subset when mask[a*nshell+b] or mask[b*nshell+a] is non-zero) selects the pairs, and a quartet
+ * (ab|cd) is evaluated only when both (a,b) and (c,d) are in it; J and K are then that sub-block's
+ * contribution.  NULL restores every quartet.  Single-molecule handles.  Used to check slices of a large
+ * build against the CPU oracle; no reference counterpart. */
+int qcg_set_pair_subset(qcg_handle* h, const unsigned char* mask);
 /* Several GPUs on one J/K build: with (rank, world) set, later qcg_fock_jk* calls evaluate only this rank's
  * contiguous slice (1/world of the screened quartets of every class) and return the rank's PARTIAL J and K;
  * the sum over ranks (one all-reduce) is the full J and K.  (0, 1), the default, is the whole build.  The

@@ -1,10 +1,12 @@
 // qchem_b200.hpp -- header-only C++ adapter over the C ABI (qchem_b200.h) for qchem's HF contraction face.
 //
-// qcg::FockEngine owns one qcg_handle and answers the two questions qchem's Hartree-Fock code asks of a
-// basis with the WholeSystemFock_IBS<double> face (src/BasisSet/Orbital_HF_IBS.C:75-87):
-//   MakeAOFock(Dao, exchange=false) -> J[Dao],  MakeAOFock(Dao, exchange=true) -> K[Dao]
+// qcg::FockEngine owns one qcg_handle and answers the questions qchem's Hartree-Fock code asks of a basis
+// with the WholeSystemFock_IBS<double> face (src/BasisSet/Orbital_HF_IBS.C:75-87):
+//   AODimension(), AddAODensity(Dao, D), MakeAOFock(Dao, exchange) -> J[Dao] or K[Dao], SliceAOFock(F, Fao)
 // and the Orbital_HF_IBS<double> contraction face (src/BasisSet/Orbital_HF_IBS.C:33-54) for a basis that is
-// one irrep: AccumulateDirect(S, D) adds J[D], AccumulateExchange(S, D) adds K[D].  qchem calls the
+// one irrep: AccumulateDirect(S, D, bs_cd) adds J[D], AccumulateExchange(S, D, bs_cd) adds K[D], and the
+// irrep-pair forms AccumulateDirectBoth / AccumulateExchangeBoth.  The engine is one irrep, so the partner
+// basis bs_cd must be the engine itself (or null); any other basis is rejected with QCG_ERR_ARG.  qchem calls the
 // Coulomb and the exchange face separately with the same density (Vee then Vxc, HF_HT.C:48-70); the
 // engine builds J and K together in one GPU pass and keeps them for the density it last saw, so the
 // second call costs nothing.  Status codes from the C ABI become qcg::Error exceptions here, the way the
@@ -72,9 +74,41 @@ public:
         const std::vector<double>& X = exchange ? K_ : J_;
         std::memcpy(out, X.data(), X.size() * sizeof(double));
     }
+    // Dao += D and F += Fao: the whole system is this one block, so the fold and the slice are identities
+    void AddAODensity(double* Dao, const double* D) const
+    {
+        for (size_t k = 0; k < (size_t)n_ * n_; ++k) Dao[k] += D[k];
+    }
+    void SliceAOFock(double* F, const double* Fao) const
+    {
+        for (size_t k = 0; k < (size_t)n_ * n_; ++k) F[k] += Fao[k];
+    }
     // S += J[D] and S += K[D] (qchem's AccumulateDirect / AccumulateExchange for a single-irrep basis)
-    void AccumulateDirect(double* S, const double* D) { add(S, D, false); }
-    void AccumulateExchange(double* S, const double* D) { add(S, D, true); }
+    void AccumulateDirect(double* S, const double* D, const FockEngine* bs_cd = nullptr)
+    {
+        partner(bs_cd);
+        add(S, D, false);
+    }
+    void AccumulateExchange(double* S, const double* D, const FockEngine* bs_cd = nullptr)
+    {
+        partner(bs_cd);
+        add(S, D, true);
+    }
+    // The irrep-pair forms, Ji += J(i,j) Dj and Jj += J(j,i) Di (and K alike), for the pair (this, cd); the
+    // engine is one irrep, so both blocks are its own J (K).  A zero density adds nothing, as in the
+    // reference, where either irrep of the pair may be empty.
+    void AccumulateDirectBoth(double* Ji, double* Jj, const double* Di, const double* Dj, const FockEngine* cd = nullptr)
+    {
+        partner(cd);
+        if (nonzero(Dj)) add(Ji, Dj, false);
+        if (nonzero(Di)) add(Jj, Di, false);
+    }
+    void AccumulateExchangeBoth(double* Ki, double* Kj, const double* Di, const double* Dj, const FockEngine* cd = nullptr)
+    {
+        partner(cd);
+        if (nonzero(Dj)) add(Ki, Dj, true);
+        if (nonzero(Di)) add(Kj, Di, true);
+    }
 
     qcg_handle* handle() { return h_; }
 
@@ -82,6 +116,16 @@ private:
     void check(int rc)
     {
         if (rc != QCG_OK) throw Error(rc, qcg_last_error(h_));
+    }
+    void partner(const FockEngine* cd) const
+    {
+        if (cd && cd != this) throw Error(QCG_ERR_ARG, "the partner basis must be this engine (one irrep)");
+    }
+    bool nonzero(const double* D) const
+    {
+        for (size_t k = 0; k < (size_t)n_ * n_; ++k)
+            if (D[k] != 0.0) return true;
+        return false;
     }
     void build(const double* D)
     {

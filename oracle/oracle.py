@@ -40,6 +40,8 @@ def lib():
         L.orc_jk_eri4.argtypes = [vp, P(f64), P(f64), P(f64)]
         L.orc_jk_direct_shard.argtypes = [vp, P(f64), P(f64), P(f64), f64, i32, i32, i32]
         L.orc_jk_direct_shard.restype = i64
+        L.orc_jk_direct_subset.argtypes = [vp, P(f64), P(f64), P(f64), f64, i32, vp]
+        L.orc_jk_direct_subset.restype = i64
         L.orc_rhf.argtypes = [vp, i32, P(f64), P(f64), i32, i32, f64, f64, i32, i32, P(f64), P(i32), P(f64),
                               P(f64)]
         L.orc_rhf.restype = i32
@@ -142,6 +144,17 @@ class OracleBasis:
         J, K = np.zeros((n, n)), np.zeros((n, n))
         lib().orc_jk_direct_shard(self.h, _p(D), _p(J), _p(K), float(thresh), int(nthreads), int(rank), int(world))
         return J, K
+
+    def jk_direct_subset(self, D, mask, thresh=1e-10, nthreads=0):
+        """The direct build restricted to the quartets whose two shell pairs are both in the subset (mask:
+        nshell x nshell booleans); returns J, K and the number of quartets evaluated."""
+        n = self.nbf
+        D = np.ascontiguousarray(D, dtype=np.float64)
+        m = np.ascontiguousarray(np.asarray(mask, dtype=np.uint8))
+        J, K = np.zeros((n, n)), np.zeros((n, n))
+        cnt = lib().orc_jk_direct_subset(self.h, _p(D), _p(J), _p(K), float(thresh), int(nthreads),
+                                         m.ctypes.data_as(ctypes.c_void_p))
+        return J, K, int(cnt)
 
     def jk_eri4(self, D):
         n = self.nbf

@@ -209,6 +209,50 @@ long long jk_direct(const Basis& bs, const std::vector<double>& Q, const double*
     return count;
 }
 
+// The direct build restricted to a subset of shell pairs: the quartets (ab|cd) of jk_direct's canonical
+// enumeration whose two pairs are both in the subset (pair (a,b), a >= b, is in it when in[a * ns + b] or
+// in[b * ns + a]), visiting only the subset's pairs.  Returns the number of quartets evaluated.
+long long jk_direct_subset(const Basis& bs, const std::vector<double>& Q, const double* D, double* Jout, double* Kout,
+                           double thresh, int nthreads, const unsigned char* in)
+{
+    const int ns = bs.shells.size(), n = bs.nbf;
+    std::vector<std::pair<int, int>> pairs;   // the subset's pairs in jk_direct's order (a, then b <= a)
+    for (int a = 0; a < ns; ++a)
+        for (int b = 0; b <= a; ++b)
+            if (in[(size_t)a * ns + b] || in[(size_t)b * ns + a]) pairs.push_back({a, b});
+    const long long np = pairs.size();
+    std::vector<double> Jt(n * n, 0.0), Kt(n * n, 0.0);
+    long long count = 0;
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel reduction(+ : count)
+    {
+        std::vector<double> J(n * n, 0.0), K(n * n, 0.0), buf(6 * 6 * 6 * 6);
+#pragma omp for schedule(dynamic, 1)
+        for (long long ij = np - 1; ij >= 0; --ij)
+        {
+            auto [a, b] = pairs[ij];
+            for (long long kl = 0; kl <= ij; ++kl)
+            {
+                auto [c, d] = pairs[kl];
+                if (Q[a * ns + b] * Q[c * ns + d] < thresh) continue;
+                shell_quartet(bs, a, b, c, d, buf.data());
+                double s = (a == b ? 0.5 : 1.0) * (c == d ? 0.5 : 1.0) * (ij == kl ? 0.5 : 1.0);
+                digest(bs, a, b, c, d, buf.data(), s, D, J.data(), K.data(), n);
+                ++count;
+            }
+        }
+#pragma omp critical
+        for (int i = 0; i < n * n; ++i) { Jt[i] += J[i]; Kt[i] += K[i]; }
+    }
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j)
+        {
+            Jout[i * n + j] = Jt[i * n + j] + Jt[j * n + i];
+            Kout[i * n + j] = Kt[i * n + j] + Kt[j * n + i];
+        }
+    return count;
+}
+
 // Reference cost structure: memoised Omega (primitive pair) and RNLM tables keyed like the reference's
 // Cache2, ERI4 element loops, then MatMul.
 struct Eri4Builder
@@ -424,6 +468,13 @@ long long orc_jk_direct_shard(void* h, const double* D, double* J, double* K, do
     auto* o = (OBasis*)h;
     if (o->Q.empty()) o->Q = schwarz(o->bs);
     return jk_direct(o->bs, o->Q, D, J, K, thresh, nthreads, rank, world);
+}
+long long orc_jk_direct_subset(void* h, const double* D, double* J, double* K, double thresh, int nthreads,
+                               const unsigned char* in)
+{
+    auto* o = (OBasis*)h;
+    if (o->Q.empty()) o->Q = schwarz(o->bs);
+    return jk_direct_subset(o->bs, o->Q, D, J, K, thresh, nthreads, in);
 }
 void orc_jk_eri4(void* h, const double* D, double* J, double* K)
 {

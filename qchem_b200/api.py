@@ -42,7 +42,7 @@ EXPORTS = ["qcg_basis_create", "qcg_destroy", "qcg_last_error", "qcg_set_stream"
            "qcg_mlp_adam", "qcg_basis_create_batch", "qcg_nmol", "qcg_mol_nbf", "qcg_one_electron_batch",
            "qcg_rhf_batch", "qcg_set_graphs", "qcg_set_shard", "qcg_autotune_jk", "qcg_eri3_batch",
            "qcg_nbf_spherical", "qcg_spherical_transform", "qcg_fock_jk_spherical", "qcg_release_cache",
-           "qcg_set_eri_team_classes"]
+           "qcg_set_eri_team_classes", "qcg_set_pair_subset"]
 
 
 class QcgError(RuntimeError):
@@ -100,6 +100,7 @@ def lib():
     L.qcg_last_error.restype = ctypes.c_char_p
     L.qcg_set_stream.argtypes = [vp, vp]
     L.qcg_set_eri_team_classes.argtypes = [vp, i64]
+    L.qcg_set_pair_subset.argtypes = [vp, vp]
     L.qcg_set_memory_limit.argtypes = [vp, i64]
     L.qcg_nbf.argtypes = [vp, P(i32)]
     L.qcg_nshell.argtypes = [vp, P(i32)]
@@ -333,6 +334,18 @@ class Engine:
     def set_eri_team_classes(self, mask: int):
         """FP64 ERI-batch classes (bit k: class k) evaluated by the team-form kernel; -1 restores the default."""
         self._check(lib().qcg_set_eri_team_classes(self._h, ctypes.c_longlong(mask)))
+
+    def set_pair_subset(self, mask):
+        """Later J/K builds evaluate only quartets whose two shell pairs are both in the subset (mask: nshell x
+        nshell booleans); None restores every quartet."""
+        if mask is None:
+            self._check(lib().qcg_set_pair_subset(self._h, None))
+            return
+        m = np.ascontiguousarray(np.asarray(mask, dtype=np.uint8))
+        ns = len(self.shells)
+        if m.shape != (ns, ns):
+            raise ValueError(f"mask must be {ns} x {ns}")
+        self._check(lib().qcg_set_pair_subset(self._h, m.ctypes.data_as(ctypes.c_void_p)))
 
     def set_fp32_bound(self, bound: float):
         """Later J/K builds evaluate quartets with Q_ab Q_cd < bound in FP32 (FP64 accumulation)."""

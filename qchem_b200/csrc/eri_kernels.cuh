@@ -135,8 +135,8 @@ __global__ void __launch_bounds__(THREADS) eri_batch_lockstep_kernel(BasisDev bs
     }
 }
 
-// Cartesian ERI batch in horizontal-recurrence form; the library does not instantiate it yet, and the
-// host tests run it.  Cls provides the generated HRR functions (gen_md.main_hrr): quartet_hrr adds a
+// Cartesian ERI batch in horizontal-recurrence form (the thread-per-quartet form of the classes build.py
+// lists in HRR_CLASSES, used when the team form is not; the host tests run it too).  Cls provides the generated HRR functions (gen_md.main_hrr): quartet_hrr adds a
 // primitive quartet's [e0|f0] block (e over L = LA..LA+LB on centre A, f over L = LC..LC+LD on centre C)
 // into the zeroed output block at row stride n_c n_d with red.global.  After the primitives, hrr_ket
 // carries each e row to [e0|cd] in place, and hrr_bra carries each (c d) column to (ab|cd) in place.  The
@@ -387,11 +387,13 @@ struct JKSink
     }
 };
 
-// true when quartet (bra pair i, ket pair j) is skipped: its density-weighted bound is below the density
-// threshold, or its bound lies outside this launch's precision band [w.lo, w.hi)
+// true when quartet (bra pair i, ket pair j) is skipped: one of its shell pairs is outside the pair subset,
+// its density-weighted bound is below the density threshold, or its bound lies outside this launch's
+// precision band [w.lo, w.hi)
 __device__ __forceinline__ bool jk_skip(const JKWorkDev& w, const PairListDev& bra, const PairListDev& ket, int i,
                                         int j, int sa, int sb, int sc, int sd)
 {
+    if (w.pmask && !(w.pmask[sa * w.nshell + sb] && w.pmask[sc * w.nshell + sd])) return true;
     const bool banded = w.lo > 0.0 || w.hi < 1e300;
     if (w.dmax)
     {

@@ -79,6 +79,9 @@ struct JKWorkDev
     // several molecules: mol_active[m] == 0 skips molecule m's quartets (a batched SCF's converged
     // molecules); null: every molecule
     const int* mol_active;
+    // a subset of shell pairs (qcg_set_pair_subset): a quartet is evaluated only when pmask[a * nshell + b]
+    // and pmask[c * nshell + d] are both set (the mask is symmetric); null: every quartet
+    const unsigned char* pmask;
 };
 
 void launch_block_max(const double* D, const int* shell_f0, const int* shell_L, int nshell, int n, double* dmax,

@@ -345,6 +345,7 @@ struct qcg_handle
     double* d_team = nullptr;
     long long team_cap = 0;   // doubles
     int* d_team_err = nullptr;
+    unsigned char* d_pmask = nullptr;   // qcg_set_pair_subset (null: every quartet)
     int maxnp[kMaxL + 1] = {};   // largest contraction length per angular momentum (0: not yet computed)
 
     // host-buffer ERI batches: two quartet/output buffer pairs (grow only) and a copy-out stream
@@ -1965,6 +1966,7 @@ void jk_device(qcg_handle* h, const double* dD, double* dJ, double* dK, int flag
             wk.dmax = dmax;
             wk.nshell = h->nshell;
             wk.dthr = dthr;
+            wk.pmask = h->d_pmask;
             if (fp32_below < HUGE_VAL)
             {
                 wk.lo = fp32_below;
@@ -2670,6 +2672,31 @@ int qcg_set_graphs(qcg_handle* h, int enable)
     return QCG_OK;
 }
 
+int qcg_set_pair_subset(qcg_handle* h, const unsigned char* mask)
+{
+    if (!h) return QCG_ERR_ARG;
+    return guarded(h, [&] {
+        require(h->nmol == 1, "a pair subset takes a single-molecule handle");
+        const int ns = h->nshell;
+        if (!mask)
+        {
+            if (h->d_pmask) h->release(h->d_pmask);
+            h->d_pmask = nullptr;
+        }
+        else
+        {
+            std::vector<unsigned char> m((size_t)ns * ns);
+            for (int a = 0; a < ns; ++a)
+                for (int b = 0; b < ns; ++b)
+                    m[(size_t)a * ns + b] = (mask[(size_t)a * ns + b] || mask[(size_t)b * ns + a]) ? 1 : 0;
+            if (!h->d_pmask) h->d_pmask = h->alloc<unsigned char>(m.size());
+            CK(cudaMemcpyAsync(h->d_pmask, m.data(), m.size(), cudaMemcpyHostToDevice, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+        }
+        ++h->screen_gen;   // recorded builds (CUDA graphs) no longer apply
+    });
+}
+
 int qcg_set_eri_team_classes(qcg_handle* h, long long mask)
 {
     if (!h) return QCG_ERR_ARG;
@@ -3171,6 +3198,8 @@ extern "C" int qcg_fock_jk_device_noalloc(qcg_handle* h, const double* d_D, doub
             wk.gbeg = wk.total * h->shard_rank / h->shard_world;
             wk.gend = wk.total * (h->shard_rank + 1) / h->shard_world;
             if (wk.gend <= wk.gbeg) continue;
+            wk.nshell = h->nshell;
+            wk.pmask = h->d_pmask;
             kJKLaunchers[k](wk, h->pl_dev[X], h->pl_dev[Y], h->pp_dev, h->d_f0, d_D, Jp, Kp, n, h->d_boys, h->stream,
                             h->nsm);
         }

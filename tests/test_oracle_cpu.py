@@ -262,3 +262,21 @@ def test_oracle_three_centre_closed_form_and_limit(oracle_mod):
         three = ob.eri3_batch(np.array([[0, 1, 2]]))[0]
         four = ob.eri_batch(np.array([[0, 1, 2, 3]]))[0] / norm(eps)
         assert np.abs(three - four).max() <= 1e-6 * np.abs(three).max(), (La, Lb, Lc)
+
+
+def test_oracle_pair_subset_of_every_pair_is_the_direct_build(oracle_mod):
+    """The subset build (the checker of sliced GPU builds) with every shell pair selected is the direct build,
+    quartet for quartet; with a proper subset it evaluates fewer quartets."""
+    from qchem_b200 import basis as B, workloads as W
+    sh = B.even_tempered(W.water())
+    ob = oracle_mod.OracleBasis(sh)
+    D = W.cluster_density(ob.nbf, nocc=5)
+    J, K, cnt = ob.jk_direct(D)
+    ns = len(sh)
+    Js, Ks, cnts = ob.jk_direct_subset(D, np.ones((ns, ns), bool))
+    assert cnts == cnt
+    assert np.abs(Js - J).max() <= 1e-13 and np.abs(Ks - K).max() <= 1e-13
+    m = np.zeros((ns, ns), bool)
+    m[::2, :] = True
+    _, _, cnt_half = ob.jk_direct_subset(D, m)
+    assert 0 < cnt_half < cnt
