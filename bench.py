@@ -626,6 +626,17 @@ def run_fock3(args, torch, api, B, W, peak_tf, stream):
         mixed[f"{bound:g}"] = {"ms_per_step": ms_mixed, "speedup_vs_fp64": ms_tuned / ms_mixed,
                                "max_abs_dJ": float((J - Jref).abs().max()), "max_abs_dK": float((K - Kref).abs().max())}
     eng.set_fp32_bound(0.0)
+    # the deterministic build (exact integer accumulation) of the same density
+    sharded_fock_jk(eng, D.data_ptr(), J.data_ptr(), K.data_ptr(), J, K, rank, world, deterministic=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        sharded_fock_jk(eng, D.data_ptr(), J.data_ptr(), K.data_ptr(), J, K, rank, world, deterministic=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_det = max_over_ranks(e0.elapsed_time(e1) / args.steps, dev)
+    det = {"ms_per_step": ms_det, "slowdown_vs_fp64": ms_det / ms_tuned,
+           "max_abs_dJ": float((J - Jref).abs().max()), "max_abs_dK": float((K - Kref).abs().max())}
     tf = st.flops / (ms * 1e-3) / 1e12
     line = {"metric": "direct J/K Fock build, shell quartets/s (32-water cluster, N=1824)",
             "value": st.quartets / (ms * 1e-3), "unit": "quartets/s", "n_gpus": world, "steps": args.steps,
@@ -642,6 +653,7 @@ def run_fock3(args, torch, api, B, W, peak_tf, stream):
                     "d2h_bytes_per_step": 16 * n * n},
             "autotuned": {"value": st.quartets / (ms_tuned * 1e-3), "ms_per_step": ms_tuned, "tuning_s": t_tune,
                           "shapes_run_cap_by_class": choice},
+            "deterministic": det,
             "mixed_fp32_fp64": {"by_fp32_bound": mixed,
                                 "note": "same build with the FP32 band below each bound (autotuned shapes); "
                                         "errors are max |J - J_fp64|, |K - K_fp64| over the matrix"}}

@@ -47,6 +47,11 @@ enum qcg_status {
 #define QCG_JK_SKIP_VALIDATION 1   /* do not check D for NaN/Inf and symmetry */
 #define QCG_JK_J_ONLY 2            /* reserved: both J and K are always built */
 #define QCG_JK_FP32 4              /* evaluate every quartet in FP32 (accumulation into J and K stays FP64) */
+/* accumulate J and K as exact 64-bit integer pairs (units of 2^-30 and 2^-70) instead of FP64 atomics, each
+ * quartet's contribution rounded alone: the result is the same bit for bit from build to build, whatever order
+ * the GPU's atomic updates take and whatever launch shapes the autotuner chose (for a given basis and shard);
+ * each contribution is represented to 2^-71, and |J|, |K| must stay below 2^32.  Not recorded as a CUDA graph. */
+#define QCG_JK_DETERMINISTIC 8
 
 typedef struct qcg_stats {
     double ms_total;          /* device time of the whole J/K build (CUDA events) */
@@ -175,6 +180,11 @@ int qcg_set_graphs(qcg_handle* h, int enable);
  * choice, or the mask in the environment variable QCG_ERI_TEAM_MASK.  Both forms give the same integrals
  * to rounding.  No reference counterpart. */
 int qcg_set_eri_team_classes(qcg_handle* h, long long mask);
+/* The same choice for the direct J/K build (bit k: class k of the work lists): the team kernel, whose CTAs
+ * digest each group's integral blocks into J and K, or the thread-per-quartet kernel; -1 (default): the
+ * library's choice, or QCG_JK_TEAM_MASK in the environment.  Same J and K to rounding (bit for bit under
+ * QCG_JK_DETERMINISTIC only within one form).  No reference counterpart. */
+int qcg_set_jk_team_classes(qcg_handle* h, long long mask);
 /* Restrict later J/K builds to a subset of shell pairs: mask (nshell x nshell bytes, row-major; pair (a,b) is
  * in the subset when mask[a*nshell+b] or mask[b*nshell+a] is non-zero) selects the pairs, and a quartet
  * (ab|cd) is evaluated only when both (a,b) and (c,d) are in it; J and K are then that sub-block's
@@ -267,6 +277,14 @@ int qcg_mlp_adam(qcg_mlp* m, float lr, float beta1, float beta2, float eps, floa
 int qcg_measure_fp64_peak(int reps, double* tflops, double* ms_per_launch);
 /* the same for FP32 fused multiply-adds: the roofline denominator of the FP32 ERI kernels */
 int qcg_measure_fp32_peak(int reps, double* tflops, double* ms_per_launch);
+
+/* ---- failure handling ------------------------------------------------------------------------ */
+/* Runs the team kernels' bounded mbarrier wait on its own, on the current device: one thread waits for the
+ * first phase of a barrier that expects one arrival.  arrive != 0: the arrival comes first and the wait
+ * completes (*gave_up = 0).  arrive == 0: nothing arrives; the wait gives up after `polls` polls and the
+ * kernel reports it (*gave_up = 1), leaving the context usable.  *ms (optional): the launch's duration.
+ * No reference counterpart. */
+int qcg_selftest_bounded_wait(long long polls, int arrive, int* gave_up, double* ms);
 
 #ifdef __cplusplus
 }

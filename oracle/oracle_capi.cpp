@@ -600,7 +600,7 @@ int orc_rhf(void* h, int natom, const double* Z, const double* R, int nelec, int
         diag_fill(Fuse);
     }
     *E_out = E;
-    *iters = it;
+    *iters = conv ? it : maxiter;   // iterations run (the loop exits at maxiter + 1)
     if (D_out) std::copy(D.begin(), D.end(), D_out);
     if (stats) { stats[0] = now() - t0; stats[1] = tjk; stats[2] = En; stats[3] = Enn; }
     return conv ? 0 : 1;

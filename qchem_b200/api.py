@@ -31,6 +31,7 @@ QCG_OK, QCG_ERR_ARG, QCG_ERR_CUDA, QCG_ERR_NONFINITE, QCG_ERR_ASYMMETRIC, QCG_ER
     QCG_ERR_NOCONV = range(8)
 QCG_JK_SKIP_VALIDATION = 1
 QCG_JK_FP32 = 4
+QCG_JK_DETERMINISTIC = 8
 
 # every symbol include/qchem_b200.h declares
 EXPORTS = ["qcg_basis_create", "qcg_destroy", "qcg_last_error", "qcg_set_stream", "qcg_set_memory_limit", "qcg_nbf",
@@ -42,7 +43,7 @@ EXPORTS = ["qcg_basis_create", "qcg_destroy", "qcg_last_error", "qcg_set_stream"
            "qcg_mlp_adam", "qcg_basis_create_batch", "qcg_nmol", "qcg_mol_nbf", "qcg_one_electron_batch",
            "qcg_rhf_batch", "qcg_set_graphs", "qcg_set_shard", "qcg_autotune_jk", "qcg_eri3_batch",
            "qcg_nbf_spherical", "qcg_spherical_transform", "qcg_fock_jk_spherical", "qcg_release_cache",
-           "qcg_set_eri_team_classes", "qcg_set_pair_subset"]
+           "qcg_set_eri_team_classes", "qcg_set_pair_subset", "qcg_set_jk_team_classes", "qcg_selftest_bounded_wait"]
 
 
 class QcgError(RuntimeError):
@@ -100,6 +101,7 @@ def lib():
     L.qcg_last_error.restype = ctypes.c_char_p
     L.qcg_set_stream.argtypes = [vp, vp]
     L.qcg_set_eri_team_classes.argtypes = [vp, i64]
+    L.qcg_set_jk_team_classes.argtypes = [vp, i64]
     L.qcg_set_pair_subset.argtypes = [vp, vp]
     L.qcg_set_memory_limit.argtypes = [vp, i64]
     L.qcg_nbf.argtypes = [vp, P(i32)]
@@ -129,6 +131,7 @@ def lib():
     L.qcg_internal_orthogonaliser.argtypes = [i32, P(f64), P(f64)]
     L.qcg_measure_fp64_peak.argtypes = [i32, P(f64), P(f64)]
     L.qcg_measure_fp32_peak.argtypes = [i32, P(f64), P(f64)]
+    L.qcg_selftest_bounded_wait.argtypes = [ctypes.c_longlong, i32, P(i32), P(f64)]
     f32 = ctypes.c_float
     L.qcg_mlp_create.argtypes = [i32, P(i32), ctypes.c_ulonglong, P(vp)]
     L.qcg_mlp_destroy.argtypes = [vp]
@@ -208,6 +211,16 @@ def measure_fp32_peak(reps: int = 20):
     if rc != QCG_OK:
         raise QcgError(rc, "fp32 peak probe failed")
     return tf.value, ms.value
+
+
+def selftest_bounded_wait(polls: int, arrive: bool):
+    """(gave_up, ms) of the team kernels' bounded mbarrier wait run on its own: with arrive the barrier's one
+    expected arrival comes first and the wait completes; without it the wait gives up after `polls` polls."""
+    gave, ms = ctypes.c_int(), ctypes.c_double()
+    rc = lib().qcg_selftest_bounded_wait(int(polls), 1 if arrive else 0, ctypes.byref(gave), ctypes.byref(ms))
+    if rc != QCG_OK:
+        raise QcgError(rc, "bounded-wait self-test failed")
+    return bool(gave.value), ms.value
 
 
 class Engine:
@@ -335,6 +348,10 @@ class Engine:
         """FP64 ERI-batch classes (bit k: class k) evaluated by the team-form kernel; -1 restores the default."""
         self._check(lib().qcg_set_eri_team_classes(self._h, ctypes.c_longlong(mask)))
 
+    def set_jk_team_classes(self, mask: int):
+        """J/K-build classes (bit k: class k) run by the team kernel; -1 restores the default."""
+        self._check(lib().qcg_set_jk_team_classes(self._h, ctypes.c_longlong(mask)))
+
     def set_pair_subset(self, mask):
         """Later J/K builds evaluate only quartets whose two shell pairs are both in the subset (mask: nshell x
         nshell booleans); None restores every quartet."""
@@ -358,8 +375,9 @@ class Engine:
         self._screen = thresh
         return Q
 
-    def fock_jk(self, D, validate: bool = True, fp32: bool = False):
-        """J[D], K[D] (unscaled) and the build's Stats; fp32=True evaluates every quartet in FP32."""
+    def fock_jk(self, D, validate: bool = True, fp32: bool = False, deterministic: bool = False):
+        """J[D], K[D] (unscaled) and the build's Stats; fp32=True evaluates every quartet in FP32;
+        deterministic=True accumulates in exact integer pairs (the same bits on every build)."""
         if self._screen is None:
             self.schwarz()
         D = _f64(D)
@@ -367,15 +385,18 @@ class Engine:
             raise QcgError(QCG_ERR_ARG, f"density must be {self.nbf}x{self.nbf}")
         J, K = np.zeros_like(D), np.zeros_like(D)
         st = Stats()
-        flags = (0 if validate else QCG_JK_SKIP_VALIDATION) | (QCG_JK_FP32 if fp32 else 0)
+        flags = ((0 if validate else QCG_JK_SKIP_VALIDATION) | (QCG_JK_FP32 if fp32 else 0) |
+                 (QCG_JK_DETERMINISTIC if deterministic else 0))
         self._check(lib().qcg_fock_jk(self._h, _p(D), _p(J), _p(K), flags, ctypes.byref(st)))
         return J, K, st
 
-    def fock_jk_device(self, d_D: int, d_J: int, d_K: int, validate: bool = False, fp32: bool = False) -> Stats:
+    def fock_jk_device(self, d_D: int, d_J: int, d_K: int, validate: bool = False, fp32: bool = False,
+                       deterministic: bool = False) -> Stats:
         if self._screen is None:
             self.schwarz()
         st = Stats()
-        flags = (0 if validate else QCG_JK_SKIP_VALIDATION) | (QCG_JK_FP32 if fp32 else 0)
+        flags = ((0 if validate else QCG_JK_SKIP_VALIDATION) | (QCG_JK_FP32 if fp32 else 0) |
+                 (QCG_JK_DETERMINISTIC if deterministic else 0))
         self._check(lib().qcg_fock_jk_device(self._h, ctypes.c_void_p(d_D), ctypes.c_void_p(d_J), ctypes.c_void_p(d_K),
                                              flags, ctypes.byref(st)))
         return st
@@ -464,13 +485,14 @@ class BatchEngine(Engine):
     def unpack(self, flat):
         return [flat[self.packed_off[m]:self.packed_off[m + 1]].reshape(n, n) for m, n in enumerate(self.mol_nbf)]
 
-    def fock_jk(self, Ds, validate: bool = True, fp32: bool = False):
+    def fock_jk(self, Ds, validate: bool = True, fp32: bool = False, deterministic: bool = False):
         if self._screen is None:
             self.schwarz()
         D = self.pack(Ds)
         J, K = np.zeros_like(D), np.zeros_like(D)
         st = Stats()
-        flags = (0 if validate else QCG_JK_SKIP_VALIDATION) | (QCG_JK_FP32 if fp32 else 0)
+        flags = ((0 if validate else QCG_JK_SKIP_VALIDATION) | (QCG_JK_FP32 if fp32 else 0) |
+                 (QCG_JK_DETERMINISTIC if deterministic else 0))
         self._check(lib().qcg_fock_jk(self._h, _p(D), _p(J), _p(K), flags, ctypes.byref(st)))
         return self.unpack(J), self.unpack(K), st
 

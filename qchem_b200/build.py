@@ -75,6 +75,14 @@ def _team_mask() -> int:
     return sum(1 << k for k in TEAM_CLASSES)
 
 
+# classes whose direct J/K build runs in the team form by default (QCG_JK_TEAM_MASK selects others at run time)
+JK_TEAM_CLASSES = ()
+
+
+def _jk_team_mask() -> int:
+    return sum(1 << k for k in JK_TEAM_CLASSES)
+
+
 def _jobs():
     core = _headers(["md_core.cuh", "qcg_internal.h"])
     jobs = []
@@ -92,15 +100,17 @@ def _jobs():
     for k in range(NCLASS):
         defs = [f"-DQCG_CLASS={k}"]
         parts = [_read(team_src), _read(os.path.join(GEN, f"md_team_{k}.cuh"))]
-        key = _hash(parts + core + _headers(["eri_kernels.cuh", "eri_team.cuh", "eri_team_iface.h", "smem_attr.h"])
+        key = _hash(parts + core + _headers(["eri_kernels.cuh", "eri_team.cuh", "eri_team_iface.h", "team_sync.cuh", "smem_attr.h"])
                     + FLAGS + defs)
         jobs.append((team_src, defs, os.path.join(BUILD, f"eri_team_{k}_{key}.o")))
     extra = {"runtime.cu": _headers(["boys_table.h", "eri_team_iface.h"]) + [_read(os.path.join(INCLUDE, "qchem_b200.h"))],
              "registry.cu": _headers(["eri_team_iface.h"]),
+             "fock_kernels.cu": _headers(["team_sync.cuh"]),
              "mlp.cu": [_read(os.path.join(INCLUDE, "qchem_b200.h"))]}
     for name in ("registry.cu", "fock_kernels.cu", "runtime.cu", "mlp.cu"):
         s = os.path.join(CSRC, name)
-        defs = HOST_OMP + [f"-DQCG_TEAM_DEFAULT_MASK={_team_mask():#x}u"] if name == "runtime.cu" else []
+        defs = HOST_OMP + [f"-DQCG_TEAM_DEFAULT_MASK={_team_mask():#x}u",
+                           f"-DQCG_JK_TEAM_DEFAULT_MASK={_jk_team_mask():#x}u"] if name == "runtime.cu" else []
         key = _hash([_read(s)] + core + extra.get(name, []) + FLAGS + defs)
         jobs.append((s, defs, os.path.join(BUILD, f"{name[:-3]}_{key}.o")))
     return jobs

@@ -103,11 +103,13 @@ constexpr size_t kSmem = Cls::kRShared ? (size_t)kThreads * Cls::kRSize * sizeof
 // the Schwarz diagonals are always FP64
 constexpr size_t kSmem64 = Cls::kRShared ? (size_t)kThreads * Cls::kRSize * sizeof(double) : 0;
 
-template <class KernelPtr>
-void prepare(KernelPtr k, size_t smem = kSmem)
+// keyed on the kernel itself: instantiations that differ only in a template flag share a pointer TYPE, and
+// each needs its own attribute
+template <auto Kernel>
+void prepare(size_t smem = kSmem)
 {
     static std::atomic<unsigned long long> ready{0};
-    ensure_smem(k, smem, ready);
+    ensure_smem(Kernel, smem, ready);
 }
 
 long long grid_for(long long work, int nsm)
@@ -153,24 +155,26 @@ void QCG_NAME(launch_eri_batch)(const BasisDev& bs, const int4* q, const int* or
     else
     {
         auto k = eri_batch_kernel<Cls, kThreads, Real>;
-        prepare(k);
+        prepare<eri_batch_kernel<Cls, kThreads, Real>>();
         k<<<(unsigned)grid_for(nq, nsm), kThreads, kSmem, st>>>(bs, q, order, nq, out, boys);
     }
 }
 
-void QCG_NAME(launch_jk)(const JKWorkDev& w, const PairListDev& bra, const PairListDev& ket, const PrimPairsDev& P,
-                         const int* f0, const double* D, double* J, double* K, int n, const double* boys,
-                         cudaStream_t st, int nsm)
+namespace {
+// DET: the deterministic accumulation (JKWorkDev::det_lo, FP64 objects only)
+template <bool DET>
+void launch_jk_form(const JKWorkDev& w, const PairListDev& bra, const PairListDev& ket, const PrimPairsDev& P,
+                    const int* f0, const double* D, double* J, double* K, int n, const double* boys,
+                    cudaStream_t st, int nsm)
 {
     const long long span = w.gend - w.gbeg;
-    if (span <= 0) return;
     if constexpr (Cls::kChunked)
     {
         // at most one block of quartets per SM: a plain launch would leave most of the GPU idle while each
         // lane runs a whole quartet's code, so the quartets' ket-component chunks go to separate warps
         if (span <= (long long)nsm * kThreads)
         {
-            auto ks = jk_split_kernel<Cls, kThreads, Real>;
+            auto ks = jk_split_kernel<Cls, kThreads, Real, DET>;
             static std::atomic<unsigned long long> split_ready{0};
             ensure_smem(ks, kSmem, split_ready);
             const long long items = ((span + 31) & ~31LL) * Cls::kNChunk;
@@ -179,8 +183,8 @@ void QCG_NAME(launch_jk)(const JKWorkDev& w, const PairListDev& bra, const PairL
             return;
         }
     }
-    auto k = jk_kernel<Cls, kThreads, Real>;
-    prepare(k);
+    auto k = jk_kernel<Cls, kThreads, Real, DET>;
+    prepare<jk_kernel<Cls, kThreads, Real, DET>>();
     // quartets per lane run: enough threads for the whole GPU first, longer runs only for large builds
     // (unless the autotuner chose the run and the grid cap)
     long long run = span / ((long long)nsm * 1024);
@@ -194,6 +198,22 @@ void QCG_NAME(launch_jk)(const JKWorkDev& w, const PairListDev& bra, const PairL
         if (blocks > (long long)nsm * w.cap) blocks = (long long)nsm * w.cap;
     }
     k<<<(unsigned)blocks, kThreads, kSmem, st>>>(w, bra, ket, P, f0, D, J, K, n, boys, (int)run);
+}
+}   // namespace
+
+void QCG_NAME(launch_jk)(const JKWorkDev& w, const PairListDev& bra, const PairListDev& ket, const PrimPairsDev& P,
+                         const int* f0, const double* D, double* J, double* K, int n, const double* boys,
+                         cudaStream_t st, int nsm)
+{
+    if (w.gend - w.gbeg <= 0) return;
+#if QCG_PREC == 64
+    if (w.det_lo)
+    {
+        launch_jk_form<true>(w, bra, ket, P, f0, D, J, K, n, boys, st, nsm);
+        return;
+    }
+#endif
+    launch_jk_form<false>(w, bra, ket, P, f0, D, J, K, n, boys, st, nsm);
 }
 
 #if QCG_PREC == 64
@@ -219,7 +239,7 @@ void QCG_CAT(launch_schwarz_, QCG_CLASS)(const PairListDev& pl, const PrimPairsD
             }
         }
         auto k = schwarz_kernel<Cls, kThreads>;
-        prepare(k, kSmem64);
+        prepare<schwarz_kernel<Cls, kThreads>>(kSmem64);
         k<<<(pl.n + kThreads - 1) / kThreads, kThreads, kSmem64, st>>>(pl, P, Q, boys);
     }
 }

@@ -288,7 +288,7 @@ __global__ void __launch_bounds__(THREADS) schwarz_split_kernel(PairListDev pl, 
 // and J = J' + J'^T, K = K' + K'^T afterwards.  Partial sums are kept in registers along the
 // component loops; what leaves the thread goes to the L2-resident J'/K' with red.global.add.f64.
 // ------------------------------------------------------------------------------------------------
-template <class RT, int LA, int LB, int LC, int LD>
+template <class RT, int LA, int LB, int LC, int LD, bool DET = false>
 struct JKSink
 {
     static constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD), NAB = NA * NB;
@@ -297,6 +297,14 @@ struct JKSink
     double* __restrict__ K;
     int n, fa, fb, fc, fd;
     double s;
+    long long det_lo = 0;   // DET: offset of the accumulator pairs' low words (JKWorkDev::det_lo)
+    // DET: exact integer accumulator pairs (fixed_add); else FP64 atomics.  A template parameter, so that the
+    // FP64 kernels carry no trace of the deterministic mode.
+    __device__ __forceinline__ void acc(double* M, size_t k, double v)
+    {
+        if constexpr (DET) fixed_add(M, k, det_lo, v);
+        else atomicAdd(M + k, v);
+    }
     double jab[NAB];
     double kac[NA], kbc[NB], kad[NA], kbd[NB];
     double dls, jcd;
@@ -349,17 +357,17 @@ struct JKSink
     __device__ __forceinline__ void ket_end(int ic, int id)
     {
         const int la = fc + ic, si = fd + id;
-        atomicAdd(J + (size_t)la * n + si, 2.0 * jcd);
+        acc(J, (size_t)la * n + si, 2.0 * jcd);
 #pragma unroll
-        for (int k = 0; k < NA; ++k) atomicAdd(K + (size_t)(fa + k) * n + si, kad[k]);
+        for (int k = 0; k < NA; ++k) acc(K, (size_t)(fa + k) * n + si, kad[k]);
 #pragma unroll
-        for (int k = 0; k < NB; ++k) atomicAdd(K + (size_t)(fb + k) * n + si, kbd[k]);
+        for (int k = 0; k < NB; ++k) acc(K, (size_t)(fb + k) * n + si, kbd[k]);
         if (id == ND - 1)
         {
 #pragma unroll
-            for (int k = 0; k < NA; ++k) { atomicAdd(K + (size_t)(fa + k) * n + la, kac[k]); kac[k] = 0.0; }
+            for (int k = 0; k < NA; ++k) { acc(K, (size_t)(fa + k) * n + la, kac[k]); kac[k] = 0.0; }
 #pragma unroll
-            for (int k = 0; k < NB; ++k) { atomicAdd(K + (size_t)(fb + k) * n + la, kbc[k]); kbc[k] = 0.0; }
+            for (int k = 0; k < NB; ++k) { acc(K, (size_t)(fb + k) * n + la, kbc[k]); kbc[k] = 0.0; }
             row_la = -1;
         }
     }
@@ -368,10 +376,22 @@ struct JKSink
     {
         if (row_la < 0) return;
 #pragma unroll
-        for (int k = 0; k < NA; ++k) { atomicAdd(K + (size_t)(fa + k) * n + row_la, kac[k]); kac[k] = 0.0; }
+        for (int k = 0; k < NA; ++k) { acc(K, (size_t)(fa + k) * n + row_la, kac[k]); kac[k] = 0.0; }
 #pragma unroll
-        for (int k = 0; k < NB; ++k) { atomicAdd(K + (size_t)(fb + k) * n + row_la, kbc[k]); kbc[k] = 0.0; }
+        for (int k = 0; k < NB; ++k) { acc(K, (size_t)(fb + k) * n + row_la, kbc[k]); kbc[k] = 0.0; }
         row_la = -1;
+    }
+    // the end of one quartet: in the deterministic mode J'[a b] leaves the registers after every quartet, so
+    // that each quartet's contribution is rounded alone and the integer sums do not depend on how many
+    // quartets a lane runs (the launch shape); the FP64 mode keeps summing over the lane's run
+    __device__ __forceinline__ void quartet_end()
+    {
+        if constexpr (DET)
+        {
+            flush_bra();
+#pragma unroll
+            for (int k = 0; k < NAB; ++k) jab[k] = 0.0;
+        }
     }
     // the bra pair is done (or the lane's run ends): flush J'[a b]
     __device__ __forceinline__ void flush_bra()
@@ -382,7 +402,7 @@ struct JKSink
             for (int ib = 0; ib < NB; ++ib)
             {
                 const double x = jab[ia * NB + ib];
-                if (x != 0.0) atomicAdd(J + (size_t)(fa + ia) * n + fb + ib, 2.0 * x);
+                if (x != 0.0) acc(J, (size_t)(fa + ia) * n + fb + ib, 2.0 * x);
             }
     }
 };
@@ -420,7 +440,7 @@ __device__ __forceinline__ bool jk_skip(const JKWorkDev& w, const PairListDev& b
 // RT is the arithmetic type of the ERI evaluation; a launch takes the quartets whose bound (Q_ab Q_cd, times
 // the density maximum when density screening is on) lies in [w.lo, w.hi), so that an FP64 and an FP32
 // launch split one build between them.
-template <class Cls, int THREADS, class RT>
+template <class Cls, int THREADS, class RT, bool DET = false>
 __global__ void __launch_bounds__(THREADS) jk_kernel(JKWorkDev w, PairListDev bra, PairListDev ket, PrimPairsDev P,
                                                      const int* __restrict__ shell_f0, const double* __restrict__ D,
                                                      double* __restrict__ J, double* __restrict__ K, int n,
@@ -444,8 +464,9 @@ __global__ void __launch_bounds__(THREADS) jk_kernel(JKWorkDev w, PairListDev br
         }
         int i = lo;
         long long next = w.offs[i + 1];
-        JKSink<RT, Cls::LA, Cls::LB, Cls::LC, Cls::LD> sink;
+        JKSink<RT, Cls::LA, Cls::LB, Cls::LC, Cls::LD, DET> sink;
         sink.D = D; sink.J = J; sink.K = K; sink.n = n;
+        if constexpr (DET) sink.det_lo = w.det_lo;
         // several molecules: the bra pair's molecule selects the packed blocks and their dimension
         auto bind = [&](int ii) {
             if (bra.mol)
@@ -493,6 +514,7 @@ __global__ void __launch_bounds__(THREADS) jk_kernel(JKWorkDev w, PairListDev br
                     Cls::template quartet<RT>(ab, cd, boys_table, rs, THREADS, sink);
                 }
             }
+            sink.quartet_end();
         }
         sink.flush_bra();
     }
@@ -503,7 +525,7 @@ __global__ void __launch_bounds__(THREADS) jk_kernel(JKWorkDev w, PairListDev br
 // w.gbeg + q.  A warp's lanes share the chunk, and the chunks of one quartet run on different warps at the
 // same time, so the launch takes about one chunk's time instead of one whole quartet's.  Each item
 // rebuilds Boys and R and digests its chunk's outputs like jk_kernel (the digestion is linear).
-template <class Cls, int THREADS, class RT>
+template <class Cls, int THREADS, class RT, bool DET = false>
 __global__ void __launch_bounds__(THREADS) jk_split_kernel(JKWorkDev w, PairListDev bra, PairListDev ket,
                                                            PrimPairsDev P, const int* __restrict__ shell_f0,
                                                            const double* __restrict__ D, double* __restrict__ J,
@@ -532,8 +554,9 @@ __global__ void __launch_bounds__(THREADS) jk_split_kernel(JKWorkDev w, PairList
         const int j = (w.kbase ? w.kbase[i] : 0) + (int)(g - w.offs[i]);
         const int sa = bra.sa[i], sb = bra.sb[i], sc = ket.sa[j], sd = ket.sb[j];
         if (jk_skip(w, bra, ket, i, j, sa, sb, sc, sd)) continue;
-        JKSink<RT, Cls::LA, Cls::LB, Cls::LC, Cls::LD> sink;
+        JKSink<RT, Cls::LA, Cls::LB, Cls::LC, Cls::LD, DET> sink;
         sink.D = D; sink.J = J; sink.K = K; sink.n = n;
+        if constexpr (DET) sink.det_lo = w.det_lo;
         if (bra.mol)
         {
             const int m = bra.mol[i];

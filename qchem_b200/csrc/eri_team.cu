@@ -97,7 +97,8 @@ TeamShape QCG_CAT(team_shape_, QCG_CLASS)(int nsm)
     sh.grid = nsm * per_sm;
     sh.threads = kThreads;
     sh.slot_doubles = (long long)Cls::kStage * 32;
-    sh.hrr_doubles = (long long)(Cls::kNE * Cls::kNF + Cls::kNE * kNCD) * 32;
+    // [e0|f0], [e0|cd] and, for the J/K form, (ab|cd): lane-minor blocks of the group's 32 quartets
+    sh.hrr_doubles = (long long)(Cls::kNE * Cls::kNF + Cls::kNE * kNCD + ncart(Cls::LA) * ncart(Cls::LB) * kNCD) * 32;
     return sh;
 }
 
@@ -112,6 +113,22 @@ void QCG_CAT(launch_eri_team_, QCG_CLASS)(const BasisDev& bs, const int4* q, con
     const long long ngroups = (nq + 31) / 32;
     const long long blocks = ngroups < sh.grid ? ngroups : sh.grid;
     k<<<(unsigned)blocks, kThreads, kSmem, st>>>(bs, q, order, nq, out, boys, scr);
+}
+
+// the team form of the direct J/K build of this class (jk_team_kernel); the scratch has room for sh.grid CTAs
+void QCG_CAT(launch_jk_team_, QCG_CLASS)(const JKWorkDev& w, const PairListDev& bra, const PairListDev& ket,
+                                         const PrimPairsDev& P, const int* f0, const double* D, double* J,
+                                         double* K, int n, const double* boys, const TeamScratchDev& scr,
+                                         const TeamShape& sh, cudaStream_t st)
+{
+    const long long span = w.gend - w.gbeg;
+    if (span <= 0) return;
+    auto k = w.det_lo ? jk_team_kernel<Cls, true> : jk_team_kernel<Cls, false>;
+    static std::atomic<unsigned long long> ready{0}, ready_det{0};
+    ensure_smem(k, kSmem, w.det_lo ? ready_det : ready);
+    const long long ngroups = (span + 31) / 32;
+    const long long blocks = ngroups < sh.grid ? ngroups : sh.grid;
+    k<<<(unsigned)blocks, kThreads, kSmem, st>>>(w, bra, ket, P, f0, D, J, K, n, boys, scr);
 }
 
 }   // namespace qcg

@@ -34,67 +34,11 @@
 
 #include "eri_team_iface.h"
 #include "md_core.cuh"
+#include "team_sync.cuh"
 
 namespace qcg {
 
 extern __shared__ __align__(128) double qcg_team_smem[];
-
-namespace team {
-
-// a wait for a bulk copy gives up after this many polls (each poll may suspend the thread for a while)
-constexpr long long kWaitPolls = 1ll << 24;
-
-__device__ __forceinline__ uint32_t smem_addr(const void* p)
-{
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
-}
-
-__device__ __forceinline__ void mbar_init_fence()
-{
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-
-// bulk copy of `bytes` (a multiple of 16; both addresses 16-byte aligned) from global to shared memory,
-// completing a phase of `bar`
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
-                 : "memory");
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-            smem_addr(dst)),
-        "l"(src), "r"(bytes), "r"(smem_addr(bar))
-        : "memory");
-}
-
-// bounded wait for phase `parity` of `bar`; false when it gave up
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
-{
-    for (long long n = 0; n < kWaitPolls; ++n)
-    {
-        uint32_t done;
-        asm volatile(
-            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
-            : "=r"(done)
-            : "r"(smem_addr(bar)), "r"(parity)
-            : "memory");
-        if (done) return true;
-    }
-    return false;
-}
-
-// this thread's generic-proxy writes to global memory become visible to later bulk copies (async proxy)
-__device__ __forceinline__ void fence_async_global()
-{
-    asm volatile("fence.proxy.async.global;" ::: "memory");
-}
-
-}   // namespace team
 
 template <class Cls>
 __global__ void __launch_bounds__(Cls::kNW * 32, 1)
@@ -122,7 +66,6 @@ __global__ void __launch_bounds__(Cls::kNW * 32, 1)
     double* const hA = scr.hrr + (long long)blockIdx.x * (NE * NF + NE * NCD) * 32;
     double* const hB = hA + NE * NF * 32;
     unsigned long long G = 0;   // steps streamed so far: step G uses stage G % 3, phase (G / 3) & 1
-    bool ok = true;             // the leader's waits all completed
     const long long ngroups = (nq + 31) >> 5;
     for (long long g = blockIdx.x; g < ngroups; g += gridDim.x)
     {
@@ -180,8 +123,19 @@ __global__ void __launch_bounds__(Cls::kNW * 32, 1)
             for (int i = 0; i < Kg; ++i)
             {
                 const unsigned long long gs = G + i;
-                if (leader) ok = team::mbar_wait(&full[gs % 3], (uint32_t)((gs / 3) & 1)) && ok;
-                __syncthreads();   // stage i is in shared memory; every warp has left step i - 1
+                bool late = false;
+                if (leader) late = !team::mbar_wait(&full[gs % 3], (uint32_t)((gs / 3) & 1));
+                // stage i is in shared memory; every warp has left step i - 1
+                if (__syncthreads_or(late))
+                {
+                    // a copy did not arrive: let the ones in flight land, record it and end the CTA
+                    if (leader)
+                    {
+                        team::drain(full, G, i, Kg);
+                        atomicOr(scr.err, 1);
+                    }
+                    return;
+                }
                 if (leader && i + 2 < Kg) issue(i + 2);   // into the stage step i - 1 used
                 if (jf < NF && i < K)
                 {
@@ -226,7 +180,200 @@ __global__ void __launch_bounds__(Cls::kNW * 32, 1)
         }
         __syncthreads();   // the scratch and the R cache are free for the next group
     }
-    if (leader && !ok) atomicOr(scr.err, 1);
+}
+
+// ------------------------------------------------------------------------------------------------
+// The team form of the direct J/K build.  The same three phases on 32 quartets of a class's screened work
+// list at a time (lane l: quartet gbeg + 32 g + l, its bra pair found by binary search, its kets from the
+// Q-sorted list), the stages built from the primitive-pair table; the bra recurrence writes (ab|cd) into a
+// third lane-minor block of the CTA's scratch, and a fourth phase digests it into J' and K' with the
+// thread-per-quartet kernel's sink (JKSink: the eight permutational images, symmetry weights, registers for
+// the partial sums, atomics or the deterministic integer pairs), warp w taking ket components w, w + nwarps,
+// ....  This replaces qchem's MakeDirect/MakeExchange + ERI4::MatMul (Molecule/IrrepBasisSet.C:138-183,
+// Internal/Imp/ERI4.C:10-17) without storing the integrals.
+// ------------------------------------------------------------------------------------------------
+template <class Cls, bool DET>
+__global__ void __launch_bounds__(Cls::kNW * 32, 1)
+    jk_team_kernel(JKWorkDev w, PairListDev bra, PairListDev ket, PrimPairsDev P, const int* __restrict__ shell_f0,
+                   const double* __restrict__ D, double* __restrict__ J, double* __restrict__ K, int n,
+                   const double* __restrict__ boys_table, TeamScratchDev scr)
+{
+    constexpr int NW = Cls::kNW;
+    constexpr int NF = Cls::kNF, NE = Cls::kNE, NH = Cls::kNH;
+    constexpr int NPASS = (NF + NW - 1) / NW;
+    constexpr int STAGE = Cls::kStage * 32;
+    constexpr uint32_t STAGE_BYTES = STAGE * sizeof(double);
+    constexpr int NB = ncart(Cls::LB), ND = ncart(Cls::LD);
+    constexpr int NAB = ncart(Cls::LA) * NB, NCD = ncart(Cls::LC) * ND;
+    static_assert(NE <= NAB && NF <= NCD, "[e0|f0] fits the blocks");
+    __shared__ uint64_t full[3];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const bool leader = threadIdx.x == 0;
+    if (leader)
+    {
+        for (int s = 0; s < 3; ++s) team::mbar_init(&full[s]);
+        team::mbar_init_fence();
+    }
+    __syncthreads();
+    double* const rc = scr.rcache + (long long)blockIdx.x * scr.kmax * STAGE;
+    double* const hA = scr.hrr + (long long)blockIdx.x * (NE * NF + NE * NCD + NAB * NCD) * 32;
+    double* const hB = hA + NE * NF * 32;
+    double* const hC = hB + NE * NCD * 32;
+    unsigned long long G = 0;
+    const long long ngroups = (w.gend - w.gbeg + 31) >> 5;
+    for (long long g = blockIdx.x; g < ngroups; g += gridDim.x)
+    {
+        const long long gq = w.gbeg + g * 32 + lane;
+        bool valid = gq < w.gend;
+        int i = 0, j = 0, sa = 0, sb = 0, sc = 0, sd = 0;
+        if (valid)
+        {
+            int lo = 0, hi = bra.n;   // bra pair i: offs[i] <= gq < offs[i+1]
+            while (hi - lo > 1)
+            {
+                const int mid = (lo + hi) >> 1;
+                if (w.offs[mid] <= gq) lo = mid;
+                else hi = mid;
+            }
+            i = lo;
+            j = (w.kbase ? w.kbase[i] : 0) + (int)(gq - w.offs[i]);
+            sa = bra.sa[i];
+            sb = bra.sb[i];
+            sc = ket.sa[j];
+            sd = ket.sb[j];
+            if (w.mol_active && bra.mol && !w.mol_active[bra.mol[i]]) valid = false;
+            else if (jk_skip(w, bra, ket, i, j, sa, sb, sc, sd)) valid = false;
+        }
+        const int Kab = valid ? bra.npp[i] : 0, Kcd = valid ? ket.npp[j] : 0, Kq = Kab * Kcd;
+        const int Kg = __reduce_max_sync(0xffffffffu, Kq);   // CTA-uniform: every warp sees the same lanes
+        if (Kg == 0) continue;                               // every quartet of the group skipped
+        if (Kg > scr.kmax)
+        {
+            if (leader) atomicOr(scr.err, 2);
+            continue;
+        }
+        // 1. stage tables, from the primitive-pair table
+        for (int x = warp; x < Kg; x += NW)
+            if (x < Kq)
+            {
+                const int ij = x / Kcd, kl = x - ij * Kcd;
+                const PrimPairData ab = load_pp(P, bra.ppo[i] + ij);
+                const PrimPairData cd = load_pp(P, ket.ppo[j] + kl);
+                Cls::produce(rc + (long long)x * STAGE + lane, ab, cd, boys_table, kl == Kcd - 1);
+            }
+        team::fence_async_global();
+        __syncthreads();
+        // 2. contraction (as in eri_batch_team_kernel)
+        for (int pass = 0; pass < NPASS; ++pass)
+        {
+            const int jf = pass * NW + warp;
+            auto issue = [&](int x) {
+                const unsigned long long gs = G + x;
+                team::bulk_load(qcg_team_smem + (gs % 3) * STAGE, rc + (long long)x * STAGE, STAGE_BYTES,
+                                &full[gs % 3]);
+            };
+            if (leader)
+            {
+                issue(0);
+                if (Kg > 1) issue(1);
+            }
+            double Y[NH], acc[NE];
+#pragma unroll
+            for (int h = 0; h < NH; ++h) Y[h] = 0.0;
+#pragma unroll
+            for (int e = 0; e < NE; ++e) acc[e] = 0.0;
+            int kl = 0;
+            for (int x = 0; x < Kg; ++x)
+            {
+                const unsigned long long gs = G + x;
+                bool late = false;
+                if (leader) late = !team::mbar_wait(&full[gs % 3], (uint32_t)((gs / 3) & 1));
+                if (__syncthreads_or(late))
+                {
+                    if (leader)
+                    {
+                        team::drain(full, G, x, Kg);
+                        atomicOr(scr.err, 1);
+                    }
+                    return;
+                }
+                if (leader && x + 2 < Kg) issue(x + 2);
+                if (jf < NF && x < Kq)
+                {
+                    const double* st = qcg_team_smem + (gs % 3) * STAGE + lane;
+                    Cls::ket(jf, st, Y);
+                    if (kl == Kcd - 1)
+                    {
+                        Cls::bra(st, Y, acc);
+#pragma unroll
+                        for (int h = 0; h < NH; ++h) Y[h] = 0.0;
+                        kl = 0;
+                    }
+                    else
+                        ++kl;
+                }
+            }
+            G += Kg;
+            if (jf < NF)
+            {
+#pragma unroll
+                for (int e = 0; e < NE; ++e) hA[(e * NF + jf) * 32 + lane] = acc[e];
+            }
+            __syncthreads();
+        }
+        // 3. recurrences into the scratch: [e0|cd] in hB, (ab|cd) in hC (lane-minor)
+        // C - D = (P - D) - (P - C) and A - B = (P - B) - (P - A), from the shell pairs' first primitive pairs
+        if (valid)
+        {
+            const PrimPairData cd0 = load_pp(P, ket.ppo[j]);
+            const double CDx = cd0.PBx - cd0.PAx, CDy = cd0.PBy - cd0.PAy, CDz = cd0.PBz - cd0.PAz;
+            for (int e = warp; e < NE; e += NW)
+                Cls::hrr_ket(hA + e * NF * 32 + lane, hB + e * NCD * 32 + lane, CDx, CDy, CDz);
+        }
+        __syncthreads();
+        if (valid)
+        {
+            const PrimPairData ab0 = load_pp(P, bra.ppo[i]);
+            const double ABx = ab0.PBx - ab0.PAx, ABy = ab0.PBy - ab0.PAy, ABz = ab0.PBz - ab0.PAz;
+            for (int cd = warp; cd < NCD; cd += NW)
+                Cls::hrr_bra(hB + cd * 32 + lane, hC + cd * 32 + lane, NCD * 32, ABx, ABy, ABz);
+        }
+        __syncthreads();
+        // 4. digestion of this lane's quartet, ket components cd = warp, warp + NW, ...
+        if (valid)
+        {
+            JKSink<double, Cls::LA, Cls::LB, Cls::LC, Cls::LD, DET> sink;
+            sink.D = D;
+            sink.J = J;
+            sink.K = K;
+            sink.n = n;
+            if constexpr (DET) sink.det_lo = w.det_lo;
+            if (bra.mol)
+            {
+                const int m = bra.mol[i];
+                const long long o = w.mols.off[m];
+                sink.D = D + o;
+                sink.J = J + o;
+                sink.K = K + o;
+                sink.n = w.mols.n[m];
+            }
+            sink.set_bra(shell_f0[sa], shell_f0[sb]);
+            sink.fc = shell_f0[sc];
+            sink.fd = shell_f0[sd];
+            sink.s = (sa == sb ? 0.5 : 1.0) * (sc == sd ? 0.5 : 1.0) * ((w.same_class && i == j) ? 0.5 : 1.0);
+            for (int cd = warp; cd < NCD; cd += NW)
+            {
+                const int ic = cd / ND, id = cd - ic * ND;
+                sink.ket_begin(ic, id);
+#pragma unroll
+                for (int ab = 0; ab < NAB; ++ab) sink(ab / NB, ab % NB, ic, id, hC[(ab * NCD + cd) * 32 + lane]);
+                sink.ket_end(ic, id);
+                sink.flush_k_row();
+            }
+            sink.flush_bra();
+        }
+        __syncthreads();   // the scratch and the R cache are free for the next group
+    }
 }
 
 }   // namespace qcg

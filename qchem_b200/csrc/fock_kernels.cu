@@ -4,6 +4,7 @@
 
 #include "md_core.cuh"
 #include "qcg_internal.h"
+#include "team_sync.cuh"
 
 namespace qcg {
 
@@ -158,6 +159,34 @@ void launch_symmetrize(const double* Jp, const double* Kp, double* J, double* K,
                        const MolLayoutDev& ml, int* flag, cudaStream_t st, int nsm)
 {
     symmetrize_kernel<<<nsm * 4, 256, 0, st>>>(Jp, Kp, J, K, total, n, ml, flag);
+}
+
+// The same from deterministic accumulator pairs (JKWorkDev::det_lo): the element's and its transpose's
+// words are added as integers (exactly), then scaled back, so the result is the same for every order of
+// the atomic updates
+__global__ void symmetrize_fixed_kernel(const unsigned long long* __restrict__ Jp,
+                                        const unsigned long long* __restrict__ Kp, double* __restrict__ J,
+                                        double* __restrict__ K, long long total, int n, MolLayoutDev ml, int* flag)
+{
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total; k += (long long)gridDim.x * blockDim.x)
+    {
+        const long long t = elem_index(k, n, ml).t;
+        const long long jh = (long long)(Jp[k] + Jp[t]), jl = (long long)(Jp[k + total] + Jp[t + total]);
+        const long long kh = (long long)(Kp[k] + Kp[t]), kl = (long long)(Kp[k + total] + Kp[t + total]);
+        const double jv = (double)jh * 0x1p-30 + (double)jl * 0x1p-70;
+        const double kv = (double)kh * 0x1p-30 + (double)kl * 0x1p-70;
+        J[k] = jv;
+        K[k] = kv;
+        if (!isfinite(jv) || !isfinite(kv)) atomicOr(flag, 1);
+    }
+}
+
+void launch_symmetrize_fixed(const double* Jp, const double* Kp, double* J, double* K, long long total, int n,
+                             const MolLayoutDev& ml, int* flag, cudaStream_t st, int nsm)
+{
+    symmetrize_fixed_kernel<<<nsm * 4, 256, 0, st>>>(reinterpret_cast<const unsigned long long*>(Jp),
+                                                    reinterpret_cast<const unsigned long long*>(Kp), J, K, total,
+                                                    n, ml, flag);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -390,5 +419,24 @@ void launch_dfma_peak(double* out, int blocks, int threads, int iters, cudaStrea
 void launch_ffma_peak(float* out, int blocks, int threads, int iters, cudaStream_t st)
 {
     fma_peak_kernel<float><<<blocks, threads, 0, st>>>(out, iters, 0.999999f, 1e-7f);
+}
+
+// The team kernels' bounded wait, run on its own: one thread initialises an mbarrier that expects one
+// arrival and waits for its first phase.  With `arrive` the arrival comes first and the wait completes; without
+// it nothing ever arrives, and the wait must give up after `polls` polls and say so in err (bit 0).
+__global__ void bounded_wait_selftest_kernel(long long polls, int arrive, int* err)
+{
+    __shared__ uint64_t bar;
+    if (threadIdx.x != 0) return;
+    team::mbar_init(&bar);
+    team::mbar_init_fence();
+    if (arrive) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(team::smem_addr(&bar)) : "memory");
+    if (!team::mbar_wait(&bar, 0, polls)) atomicOr(err, 1);
+    team::mbar_inval(&bar);
+}
+
+void launch_bounded_wait_selftest(long long polls, int arrive, int* err, cudaStream_t st)
+{
+    bounded_wait_selftest_kernel<<<1, 32, 0, st>>>(polls, arrive, err);
 }
 }   // namespace qcg

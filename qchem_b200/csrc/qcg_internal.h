@@ -82,7 +82,25 @@ struct JKWorkDev
     // a subset of shell pairs (qcg_set_pair_subset): a quartet is evaluated only when pmask[a * nshell + b]
     // and pmask[c * nshell + d] are both set (the mask is symmetric); null: every quartet
     const unsigned char* pmask;
+    // deterministic accumulation (QCG_JK_DETERMINISTIC): J' and K' are pairs of 64-bit integer words, the
+    // high word at element k (units of 2^-30) and the low word at k + det_lo (units of 2^-70), summed with
+    // integer atomics, so that the result does not depend on their order; 0: FP64 atomics
+    long long det_lo;
 };
+
+// One contribution v to a deterministic accumulator pair (hi word at p[k], lo word at p[k + lo]).  v is split
+// exactly: hi = round(v 2^30), the remainder r = v - hi 2^-30 is exact (|r| <= 2^-31) and lo = round(r 2^70),
+// so a contribution is represented to 2^-71 and the two integer sums are exact for |J'|, |K'| < 2^33 and
+// fewer than 2^24 contributions per element.
+__device__ __forceinline__ void fixed_add(double* p, size_t k, long long lo_off, double v)
+{
+    const long long hi = __double2ll_rn(v * 0x1p30);
+    const double r = v - (double)hi * 0x1p-30;
+    const long long lo = __double2ll_rn(r * 0x1p70);
+    unsigned long long* w = reinterpret_cast<unsigned long long*>(p);
+    atomicAdd(w + k, (unsigned long long)hi);
+    atomicAdd(w + k + lo_off, (unsigned long long)lo);
+}
 
 void launch_block_max(const double* D, const int* shell_f0, const int* shell_L, int nshell, int n, double* dmax,
                       cudaStream_t st, int nsm);

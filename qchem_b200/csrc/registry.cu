@@ -17,7 +17,10 @@ namespace qcg {
                          const double*, double*, double*, int, const double*, cudaStream_t, int);                    \
     void launch_eri_team_##k(const BasisDev&, const int4*, const int*, long long, double*, const double*,            \
                              const TeamScratchDev&, const TeamShape&, cudaStream_t);                                 \
-    TeamShape team_shape_##k(int);
+    TeamShape team_shape_##k(int);                                                                                  \
+    void launch_jk_team_##k(const JKWorkDev&, const PairListDev&, const PairListDev&, const PrimPairsDev&,          \
+                            const int*, const double*, double*, double*, int, const double*, const TeamScratchDev&, \
+                            const TeamShape&, cudaStream_t);
 QCG_DECL(0) QCG_DECL(1) QCG_DECL(2) QCG_DECL(3) QCG_DECL(4) QCG_DECL(5) QCG_DECL(6) QCG_DECL(7) QCG_DECL(8)
 QCG_DECL(9) QCG_DECL(10) QCG_DECL(11) QCG_DECL(12) QCG_DECL(13) QCG_DECL(14) QCG_DECL(15) QCG_DECL(16)
 QCG_DECL(17) QCG_DECL(18) QCG_DECL(19) QCG_DECL(20)
@@ -33,6 +36,12 @@ const EriTeamShapeFn kEriTeamShapes[kNumQuartetClasses] = {
     team_shape_0,  team_shape_1,  team_shape_2,  team_shape_3,  team_shape_4,  team_shape_5,  team_shape_6,
     team_shape_7,  team_shape_8,  team_shape_9,  team_shape_10, team_shape_11, team_shape_12, team_shape_13,
     team_shape_14, team_shape_15, team_shape_16, team_shape_17, team_shape_18, team_shape_19, team_shape_20};
+const JKTeamLauncher kJKTeamLaunchers[kNumQuartetClasses] = {
+    launch_jk_team_0,  launch_jk_team_1,  launch_jk_team_2,  launch_jk_team_3,  launch_jk_team_4,
+    launch_jk_team_5,  launch_jk_team_6,  launch_jk_team_7,  launch_jk_team_8,  launch_jk_team_9,
+    launch_jk_team_10, launch_jk_team_11, launch_jk_team_12, launch_jk_team_13, launch_jk_team_14,
+    launch_jk_team_15, launch_jk_team_16, launch_jk_team_17, launch_jk_team_18, launch_jk_team_19,
+    launch_jk_team_20};
 const EriTeamLauncher kEriTeamLaunchers[kNumQuartetClasses] = {
     launch_eri_team_0,  launch_eri_team_1,  launch_eri_team_2,  launch_eri_team_3,  launch_eri_team_4,
     launch_eri_team_5,  launch_eri_team_6,  launch_eri_team_7,  launch_eri_team_8,  launch_eri_team_9,

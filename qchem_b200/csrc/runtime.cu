@@ -34,12 +34,15 @@ void launch_validate(const double* D, long long total, int n, const MolLayoutDev
                      cudaStream_t st, int nsm);
 void launch_symmetrize(const double* Jp, const double* Kp, double* J, double* K, long long total, int n,
                        const MolLayoutDev& ml, int* flag, cudaStream_t st, int nsm);
+void launch_symmetrize_fixed(const double* Jp, const double* Kp, double* J, double* K, long long total, int n,
+                             const MolLayoutDev& ml, int* flag, cudaStream_t st, int nsm);
 void launch_one_electron(const BasisDev& bs, const int* f0, int n, int natom, const double* Z, const double* R,
                          double* S, double* T, double* V, const double* boys, cudaStream_t st, int nsm,
                          const int2* pairs = nullptr, long long npair_list = 0, const int* shell_mol = nullptr,
                          const MolLayoutDev& ml = MolLayoutDev{1, nullptr, nullptr}, const int* atom0 = nullptr,
                          const int* natoms = nullptr);
 void launch_dfma_peak(double* out, int blocks, int threads, int iters, cudaStream_t st);
+void launch_bounded_wait_selftest(long long polls, int arrive, int* err, cudaStream_t st);
 void launch_ffma_peak(float* out, int blocks, int threads, int iters, cudaStream_t st);
 }   // namespace qcg
 
@@ -345,6 +348,7 @@ struct qcg_handle
     double* d_team = nullptr;
     long long team_cap = 0;   // doubles
     int* d_team_err = nullptr;
+    bool team_pending = false;   // a team kernel ran since the error word was last read
     unsigned char* d_pmask = nullptr;   // qcg_set_pair_subset (null: every quartet)
     int maxnp[kMaxL + 1] = {};   // largest contraction length per angular momentum (0: not yet computed)
 
@@ -366,7 +370,8 @@ struct qcg_handle
     cudaEvent_t fork = nullptr, join[kSide] = {};
     // J/K builds replayed as CUDA graphs, keyed by their arguments and the screening generation
     bool use_graphs = false;
-    long long team_mask = -1;   // qcg_set_eri_team_classes; -1: the process default (eri_team_mask)
+    long long team_mask = -1;      // qcg_set_eri_team_classes; -1: the process default (eri_team_mask)
+    long long jk_team_mask = -1;   // qcg_set_jk_team_classes; -1: the process default (jk_team_mask)
     int screen_gen = 0;
     QcgGraphKey last_key{};
     std::vector<std::pair<QcgGraphKey, cudaGraphExec_t>> graphs;
@@ -1658,8 +1663,9 @@ void ensure_jk_buffers(qcg_handle* h)
     if (h->d_Jp) return;
     const size_t nn = (size_t)h->packed;
     h->d_D = h->alloc<double>(nn);
-    h->d_Jp = h->alloc<double>(nn);
-    h->d_Kp = h->alloc<double>(nn);
+    // room for the deterministic mode's low words (QCG_JK_DETERMINISTIC): J' and K' are 2 nn words each
+    h->d_Jp = h->alloc<double>(2 * nn);
+    h->d_Kp = h->alloc<double>(2 * nn);
     h->d_J = h->alloc<double>(nn);
     h->d_K = h->alloc<double>(nn);
     h->d_flag = h->alloc<int>(1);
@@ -1906,6 +1912,9 @@ void build_screening(qcg_handle* h, double thresh)
 // quartet digests) is below it are evaluated in FP32 (FP64 accumulation); 0 = all FP64, HUGE_VAL = all
 // FP32.  The weighting is what makes FP32 safe: the FP32 error of a quartet's contribution to J and K is
 // about 3e-7 of its bound.  dmax (the density maxima of dD) is computed here when the caller has none.
+bool team_scratch(qcg_handle* h, int k, TeamScratchDev& scr, TeamShape& sh);
+unsigned jk_team_mask_default();
+
 void jk_device(qcg_handle* h, const double* dD, double* dJ, double* dK, int flags, qcg_stats* stats,
                const double* dmax = nullptr, double dthr = 0.0, double fp32_below = 0.0)
 {
@@ -1941,9 +1950,24 @@ void jk_device(qcg_handle* h, const double* dD, double* dJ, double* dK, int flag
     ensure_side_streams(h);
     // the build: zero J'/K', class kernels over the side streams, symmetrisation (timing events only
     // when the build is not a graph)
+    // classes built in the team form (FP64 band only); their scratch is sized here, before any capture, and
+    // their launches share it, so they run one after another on the first side stream
+    const unsigned jk_mask = h->jk_team_mask >= 0 ? (unsigned)h->jk_team_mask : jk_team_mask_default();
+    bool team_k[kNumQuartetClasses] = {};
+    TeamScratchDev team_scr[kNumQuartetClasses]{};
+    TeamShape team_sh[kNumQuartetClasses]{};
+    for (int k = 0; k < kNumQuartetClasses; ++k)
+        if (((jk_mask >> k) & 1u) && h->work[k].total > 0) team_k[k] = team_scratch(h, k, team_scr[k], team_sh[k]);
+    for (int k = 0; k < kNumQuartetClasses; ++k)   // the buffer may have grown after an earlier class's lookup
+        if (team_k[k]) team_scratch(h, k, team_scr[k], team_sh[k]);
+    // QCG_JK_DETERMINISTIC: J' and K' as integer accumulator pairs (the low words after the nn high ones),
+    // every quartet in FP64
+    const bool det = (flags & QCG_JK_DETERMINISTIC) != 0;
+    require(!det || fp32_below <= 0, "the deterministic J/K build evaluates every quartet in FP64 (no FP32 band)");
+    const size_t nacc = det ? 2 * nn : nn;
     auto enqueue = [&](bool timed) {
-        CK(cudaMemsetAsync(h->d_Jp, 0, nn * sizeof(double), h->stream));
-        CK(cudaMemsetAsync(h->d_Kp, 0, nn * sizeof(double), h->stream));
+        CK(cudaMemsetAsync(h->d_Jp, 0, nacc * sizeof(double), h->stream));
+        CK(cudaMemsetAsync(h->d_Kp, 0, nacc * sizeof(double), h->stream));
         if (timed) CK(cudaEventRecord(h->ev1, h->stream));
         CK(cudaEventRecord(h->fork, h->stream));
         for (int s = 0; s < qcg_handle::kSide; ++s) CK(cudaStreamWaitEvent(h->side[s], h->fork, 0));
@@ -1967,13 +1991,20 @@ void jk_device(qcg_handle* h, const double* dD, double* dJ, double* dK, int flag
             wk.nshell = h->nshell;
             wk.dthr = dthr;
             wk.pmask = h->d_pmask;
+            wk.det_lo = det ? (long long)nn : 0;
             if (fp32_below < HUGE_VAL)
             {
                 wk.lo = fp32_below;
                 wk.hi = HUGE_VAL;
-                kJKLaunchers[k](wk, h->pl_dev[X], h->pl_dev[Y], h->pp_dev, h->d_f0, dD, h->d_Jp, h->d_Kp, n,
-                                h->d_boys, h->side[slot], h->nsm);
-                slot = (slot + 1) % qcg_handle::kSide;
+                if (team_k[k])
+                    kJKTeamLaunchers[k](wk, h->pl_dev[X], h->pl_dev[Y], h->pp_dev, h->d_f0, dD, h->d_Jp, h->d_Kp, n,
+                                        h->d_boys, team_scr[k], team_sh[k], h->side[0]);
+                else
+                {
+                    kJKLaunchers[k](wk, h->pl_dev[X], h->pl_dev[Y], h->pp_dev, h->d_f0, dD, h->d_Jp, h->d_Kp, n,
+                                    h->d_boys, h->side[slot], h->nsm);
+                    slot = (slot + 1) % qcg_handle::kSide;
+                }
             }
             if (fp32_below > 0)
             {
@@ -1991,7 +2022,11 @@ void jk_device(qcg_handle* h, const double* dD, double* dJ, double* dK, int flag
             CK(cudaStreamWaitEvent(h->stream, h->join[s], 0));
         }
         if (timed) CK(cudaEventRecord(h->ev2, h->stream));
-        launch_symmetrize(h->d_Jp, h->d_Kp, dJ, dK, (long long)nn, n, h->mols(), h->d_flag, h->stream, h->nsm);
+        if (det)
+            launch_symmetrize_fixed(h->d_Jp, h->d_Kp, dJ, dK, (long long)nn, n, h->mols(), h->d_flag, h->stream,
+                                    h->nsm);
+        else
+            launch_symmetrize(h->d_Jp, h->d_Kp, dJ, dK, (long long)nn, n, h->mols(), h->d_flag, h->stream, h->nsm);
         CK(cudaGetLastError());
     };
     // With graphs enabled (qcg_set_graphs), a build whose arguments repeat (the SCF's builds into the
@@ -2000,7 +2035,8 @@ void jk_device(qcg_handle* h, const double* dD, double* dJ, double* dK, int flag
     // so replay saves little, and capture plus instantiation costs more than a 10-25 iteration SCF recovers.
     const QcgGraphKey key{dD, dJ, dK, dmax, dthr, fp32_below, h->screen_gen};
     cudaGraphExec_t exec = nullptr;
-    if ((flags & QCG_JK_SKIP_VALIDATION) && h->use_graphs && h->stream != nullptr)   // no capture on the legacy stream
+    if ((flags & QCG_JK_SKIP_VALIDATION) && !(flags & QCG_JK_DETERMINISTIC) && h->use_graphs &&
+        h->stream != nullptr)   // no capture on the legacy stream; deterministic builds are never recorded
     {
         for (auto& g : h->graphs)
             if (g.first == key) exec = g.second;
@@ -2329,6 +2365,7 @@ bool team_scratch(qcg_handle* h, int k, TeamScratchDev& scr, TeamShape& sh)
     scr.kmax = (int)kmax;
     scr.hrr = h->d_team + (long long)sh.grid * kmax * sh.slot_doubles;
     scr.err = h->d_team_err;
+    h->team_pending = true;
     return true;
 }
 
@@ -2336,13 +2373,29 @@ bool team_scratch(qcg_handle* h, int k, TeamScratchDev& scr, TeamShape& sh)
 // read after a synchronising call, then cleared
 void check_team_error(qcg_handle* h)
 {
-    if (!h->d_team_err) return;
+    if (!h->d_team_err || !h->team_pending) return;
+    h->team_pending = false;
     int e = 0;
     CK(cudaMemcpy(&e, h->d_team_err, sizeof(int), cudaMemcpyDeviceToHost));
     if (!e) return;
     CK(cudaMemset(h->d_team_err, 0, sizeof(int)));
-    throw Error{QCG_ERR_CUDA, e & 1 ? "ERI batch: a bulk-copy wait gave up; the results are not valid"
-                                    : "ERI batch: a primitive loop longer than the stage slots"};
+    throw Error{QCG_ERR_CUDA, e & 1 ? "team kernel: a bulk-copy wait gave up; the results are not valid"
+                                    : "team kernel: a primitive loop longer than the stage slots"};
+}
+
+#ifndef QCG_JK_TEAM_DEFAULT_MASK
+#define QCG_JK_TEAM_DEFAULT_MASK 0u
+#endif
+// The classes whose direct J/K build runs in the team form: the build's choice (QCG_JK_TEAM_DEFAULT_MASK),
+// unless QCG_JK_TEAM_MASK in the environment names others (read once per process).
+unsigned jk_team_mask_default()
+{
+    static const unsigned mask = [] {
+        const char* e = std::getenv("QCG_JK_TEAM_MASK");
+        if (!e || !*e) return (unsigned)(QCG_JK_TEAM_DEFAULT_MASK);
+        return (unsigned)std::strtoul(e, nullptr, 0);
+    }();
+    return mask;
 }
 
 template <class T>
@@ -2697,6 +2750,16 @@ int qcg_set_pair_subset(qcg_handle* h, const unsigned char* mask)
     });
 }
 
+int qcg_set_jk_team_classes(qcg_handle* h, long long mask)
+{
+    if (!h) return QCG_ERR_ARG;
+    return guarded(h, [&] {
+        require(mask >= -1 && mask < (1LL << kNumQuartetClasses), "mask must be -1 or a 21-bit class mask");
+        h->jk_team_mask = mask;
+        ++h->screen_gen;   // recorded builds (CUDA graphs) no longer apply
+    });
+}
+
 int qcg_set_eri_team_classes(qcg_handle* h, long long mask)
 {
     if (!h) return QCG_ERR_ARG;
@@ -2748,6 +2811,7 @@ int qcg_fock_jk(qcg_handle* h, const double* D, double* J, double* K, int flags,
         int flag = 0;
         CK(cudaMemcpyAsync(&flag, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
+        check_team_error(h);
         if (flag & 1) throw Error{QCG_ERR_NONFINITE, "non-finite J/K result"};
     });
 }
@@ -3041,6 +3105,7 @@ int qcg_rhf(qcg_handle* h, int natom, const double* Z, const double* R, int nele
             CK(cudaMemcpyAsync(Jpin.p, h->d_J, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
             CK(cudaMemcpyAsync(Kpin.p, h->d_K, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
             CK(cudaStreamSynchronize(h->stream));
+            check_team_error(h);
             std::copy(Jpin.p, Jpin.p + nn, J.begin());
             std::copy(Kpin.p, Kpin.p + nn, K.begin());
             const auto c2 = clk::now();
@@ -3262,6 +3327,40 @@ int qcg_measure_fp32_peak(int reps, double* tflops, double* ms_per_launch)
     return measure_fma_peak<float>(reps, tflops, ms_per_launch, launch_ffma_peak);
 }
 
+int qcg_selftest_bounded_wait(long long polls, int arrive, int* gave_up, double* ms)
+{
+    if (!gave_up || polls <= 0) return QCG_ERR_ARG;
+    int* err = nullptr;
+    cudaEvent_t a = nullptr, b = nullptr;
+    int rc = QCG_OK;
+    try
+    {
+        CK(cudaMalloc(&err, sizeof(int)));
+        CK(cudaMemset(err, 0, sizeof(int)));
+        CK(cudaEventCreate(&a));
+        CK(cudaEventCreate(&b));
+        CK(cudaEventRecord(a, nullptr));
+        launch_bounded_wait_selftest(polls, arrive ? 1 : 0, err, nullptr);
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(b, nullptr));
+        CK(cudaEventSynchronize(b));
+        float t = 0;
+        CK(cudaEventElapsedTime(&t, a, b));
+        int e = 0;
+        CK(cudaMemcpy(&e, err, sizeof(int), cudaMemcpyDeviceToHost));
+        *gave_up = e & 1;
+        if (ms) *ms = t;
+    }
+    catch (const Error& e)
+    {
+        rc = e.code;
+    }
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    if (err) cudaFree(err);
+    return rc;
+}
+
 // Several closed-shell SCFs advanced together (one handle from qcg_basis_create_batch): every iteration is
 // ONE J/K build over all molecules (the class kernels take every molecule's quartets), then each molecule's
 // host step (Fock matrix, energy, DIIS, diagonalisation) runs in parallel over the molecules.  A molecule
@@ -3363,6 +3462,7 @@ int qcg_rhf_batch(qcg_handle* h, const int* mol_natom, const double* Z, const do
             CK(cudaMemcpyAsync(J, h->d_J, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
             CK(cudaMemcpyAsync(K, h->d_K, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
             CK(cudaStreamSynchronize(h->stream));
+            check_team_error(h);
             fock_ms += st.ms_total;
 #pragma omp parallel for schedule(dynamic)
             for (int m = 0; m < nmol; ++m)

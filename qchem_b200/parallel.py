@@ -62,15 +62,16 @@ def reduce_jk(J, K):
     return J, K
 
 
-def sharded_fock_jk(engine, dD: int, dJ: int, dK: int, J, K, rank: int = None, world: int = None):
+def sharded_fock_jk(engine, dD: int, dJ: int, dK: int, J, K, rank: int = None, world: int = None,
+                    deterministic: bool = False):
     """One J/K build split over the ranks of the process group: this rank's slice into the device buffers
     dJ/dK (the data pointers of the torch tensors J and K), then the sum over ranks in place.  rank/world
-    default to the process group's."""
+    default to the process group's; deterministic=True accumulates each slice in exact integer pairs."""
     import torch.distributed as dist
     if rank is None or world is None:
         on = dist.is_available() and dist.is_initialized()
         rank, world = (dist.get_rank(), dist.get_world_size()) if on else (0, 1)
     engine.set_shard(rank, world)
-    st = engine.fock_jk_device(dD, dJ, dK)
+    st = engine.fock_jk_device(dD, dJ, dK, deterministic=deterministic)
     reduce_jk(J, K)
     return st

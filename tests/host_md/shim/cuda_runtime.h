@@ -45,6 +45,16 @@ inline float atomicAdd(float* p, float v)
     *p = o + v;
     return o;
 }
+inline unsigned long long atomicAdd(unsigned long long* p, unsigned long long v)
+{
+    const unsigned long long o = *p;
+    *p = o + v;
+    return o;
+}
+inline long long __double2ll_rn(double x)
+{
+    return (long long)__builtin_llrint(x);
+}
 inline int atomicMax(int* p, int v)
 {
     const int o = *p;

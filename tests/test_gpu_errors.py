@@ -1,7 +1,9 @@
 """Failure handling through the C ABI: bad inputs come back as status codes, never as a crash.
 
 All faults are injected on the host (bad matrices, bad arguments, a device-memory cap); no GPU fault,
-trap or hang is provoked.
+trap or hang is provoked.  The one device-side wait the library has (the team kernels' mbarrier waits for
+their bulk copies) is bounded; its give-up path is run on a barrier that nothing completes, with a short
+limit, and must come back as a status while the context stays usable.
 """
 import numpy as np
 import pytest
@@ -94,3 +96,21 @@ def test_odd_electron_count_rejected():
     with pytest.raises(api.QcgError) as e:
         api.Engine(B.even_tempered(mol)).rhf(mol)
     assert e.value.code == api.QCG_ERR_ARG
+
+
+def test_bounded_wait_completes_when_the_arrival_comes():
+    gave_up, _ = api.selftest_bounded_wait(polls=1000, arrive=True)
+    assert not gave_up
+
+
+def test_bounded_wait_gives_up_and_the_context_stays_usable(eng):
+    gave_up, ms = api.selftest_bounded_wait(polls=1000, arrive=False)
+    assert gave_up
+    assert ms < 1000.0   # 1000 polls, each suspending for at most a few microseconds
+    # the GPU still answers: a J/K build right after matches one made before
+    D = _density(eng.nbf)
+    J1, K1, _ = eng.fock_jk(D)
+    gave_up, _ = api.selftest_bounded_wait(polls=1000, arrive=False)
+    assert gave_up
+    J2, K2, _ = eng.fock_jk(D)
+    assert np.abs(J1 - J2).max() < 1e-12 and np.abs(K1 - K2).max() < 1e-12

@@ -182,7 +182,8 @@ def test_orbital_hf_ibs_face_fuses_j_and_k(oracle_mod):
     assert ibs.AODimension() == B.nbf(sh)
 
 
-def test_jk_deterministic_to_rounding(oracle_mod):
+def test_jk_fp64_atomics_agree_to_rounding(oracle_mod):
+    """The default build sums with FP64 atomics, whose order varies: repeated builds agree to rounding."""
     mol = W.water()
     sh = B.even_tempered(mol)
     D = oracle_mod.OracleBasis(sh).rhf(mol)["D"]
@@ -190,3 +191,30 @@ def test_jk_deterministic_to_rounding(oracle_mod):
     J1, K1, _ = eng.fock_jk(D)
     J2, K2, _ = eng.fock_jk(D)
     assert np.abs(J1 - J2).max() <= 1e-13 and np.abs(K1 - K2).max() <= 1e-13
+
+
+@pytest.mark.parametrize("nw", [1, 4])
+def test_jk_deterministic_is_bitwise_repeatable(nw, oracle_mod):
+    """QCG_JK_DETERMINISTIC: exact integer accumulation, so repeated builds -- including on another handle with
+    other launch shapes (the autotuner's choices) -- give the same bits, and match the oracle at the Fock
+    tolerance.  Checked on water and a water cluster (more quartets, so more atomic interleavings)."""
+    mol = W.water() if nw == 1 else W.water_cluster(nx=2, ny=2, nz=1, seed=W.SEED0 + 3600)
+    sh = B.even_tempered(mol)
+    ob = oracle_mod.OracleBasis(sh)
+    D = W.cluster_density(ob.nbf, nocc=5 * nw)
+    eng = api.Engine(sh)
+    J1, K1, _ = eng.fock_jk(D, deterministic=True)
+    for _ in range(3):
+        J2, K2, _ = eng.fock_jk(D, deterministic=True)
+        assert np.array_equal(J1, J2) and np.array_equal(K1, K2)
+    eng2 = api.Engine(sh)
+    eng2.schwarz(1e-10)
+    import torch
+    dD = torch.tensor(D, device="cuda")
+    eng2.autotune_jk(dD.data_ptr())
+    J3, K3, _ = eng2.fock_jk(D, deterministic=True)
+    assert np.array_equal(J1, J3) and np.array_equal(K1, K3)
+    Jr, Kr, _ = ob.jk_direct(D)
+    assert np.abs(J1 - Jr).max() <= FOCK_TOL and np.abs(K1 - Kr).max() <= FOCK_TOL
+    Jf, Kf, _ = eng.fock_jk(D)
+    assert np.abs(J1 - Jf).max() <= 1e-12 and np.abs(K1 - Kf).max() <= 1e-12
