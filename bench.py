@@ -9,7 +9,8 @@ Inputs are synthetic and seeded.  Every step reads inputs and writes outputs lar
 
 value  = device-resident throughput (quartets/s, all ranks), CUDA events on the launching stream,
 e2e    = one step of the same workload through the C ABI's host-buffer call qcg_eri_batch (pinned host
-         memory, H2D of the quartet list and D2H of every ERI block inside the timed region),
+         memory, H2D of the quartet list and D2H of every ERI block inside the timed region; each call
+         takes as many quartets as fill a 2 GiB output buffer),
 roofline = the dominant class kernel against the FP64 FMA peak measured here by the library's probe,
 cpu_baseline = the CPU oracle (a port of the reference's arithmetic) on a bounded sample, all host cores.
 --impl reference times the CPU oracle alone (the reference itself cannot be built here).
@@ -32,7 +33,7 @@ sys.path.insert(0, REPO)
 
 Q_PER_CLASS = 10_000_000
 CHUNK = 1_000_000
-E2E_CHUNK = 200_000      # quartets per host-buffer call in the e2e leg (2 GB of pinned output at (dd|dd))
+E2E_BYTES = 2 << 30      # pinned host output per host-buffer call in the e2e leg (207 126 (dd|dd) quartets)
 NPOOL = 32768
 METRIC = "ERI quartets/s (21 (s,p,d) classes, contraction 1-3, FP64 Cartesian)"
 UNIT = "quartets/s"
@@ -340,7 +341,9 @@ def main():
     # end to end through the host-buffer C ABI call (pinned host memory, copies inside the timed region)
     e2e = None
     if not args.no_e2e:
-        h_out = torch.empty(min(E2E_CHUNK, nq_cls) * max_blk, dtype=torch.float64).pin_memory()
+        # each call takes as many quartets as fill the 2 GiB pinned output buffer (a caller's memory budget)
+        per_call = lambda cls: max(1, min(nq_cls, E2E_BYTES // (8 * class_block(cls))))
+        h_out = torch.empty(max(per_call(c) * class_block(c) for c in classes), dtype=torch.float64).pin_memory()
         eng_h = api.Engine(pool)
         lib = api.lib()
         import ctypes
@@ -348,8 +351,8 @@ def main():
         def e2e_step():
             h2d = d2h = 0
             for k, cls in enumerate(classes):
-                for c0 in range(0, nq_cls, E2E_CHUNK):
-                    m = min(E2E_CHUNK, nq_cls - c0)
+                for c0 in range(0, nq_cls, per_call(cls)):
+                    m = min(per_call(cls), nq_cls - c0)
                     qptr = ctypes.cast(h_q[k].data_ptr() + 16 * c0, ctypes.POINTER(ctypes.c_int))
                     optr = ctypes.cast(h_out.data_ptr(), ctypes.POINTER(ctypes.c_double))
                     rc = lib.qcg_eri_batch(eng_h._h, *cls, m, qptr, optr)
@@ -362,7 +365,7 @@ def main():
         # warm-up: one call per class on a slice; then ONE full step (the device-resident leg above has
         # already shown the step-to-step spread; a host-buffer step moves ~283 GB across PCIe)
         for k, cls in enumerate(classes):
-            m = min(E2E_CHUNK, nq_cls)
+            m = min(per_call(cls), nq_cls, 200_000)
             rc = lib.qcg_eri_batch(eng_h._h, *cls, m, ctypes.cast(h_q[k].data_ptr(), ctypes.POINTER(ctypes.c_int)),
                                    ctypes.cast(h_out.data_ptr(), ctypes.POINTER(ctypes.c_double)))
             if rc != 0:

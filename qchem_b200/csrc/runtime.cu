@@ -2398,6 +2398,17 @@ unsigned jk_team_mask_default()
     return mask;
 }
 
+// output bytes per chunk of a host-buffer ERI batch: 512 MiB, or QCG_BATCH_CHUNK_MB (read once)
+long long batch_chunk_bytes()
+{
+    static const long long bytes = [] {
+        const char* e = std::getenv("QCG_BATCH_CHUNK_MB");
+        const long long mb = (e && *e) ? std::strtoll(e, nullptr, 10) : 0;
+        return mb > 0 ? mb << 20 : (1LL << 29);
+    }();
+    return bytes;
+}
+
 template <class T>
 void eri_batch_launch(qcg_handle* h, int k, const int* dq, long long m, T* dout)
 {
@@ -2485,10 +2496,12 @@ void eri_batch_run(qcg_handle* h, int la, int lb, int lc, int ld, long long nq, 
     {
         const int k = class_index(la, lb, lc, ld);
         const long long blk = (long long)ncart(la) * ncart(lb) * ncart(lc) * ncart(ld);
-        // two device buffers of at most 512 MiB of output each, kept by the handle between calls: the
-        // copy of one chunk back to the host overlaps the evaluation of the next
+        // two device buffers of at most batch_chunk_bytes() of output each, kept by the handle between
+        // calls: the copy of one chunk back to the host overlaps the evaluation of the next.  The chunks
+        // ramp up (1/8, 1/4, 1/2 of the full size, then full), so that the copy engine starts early: the
+        // evaluation of the first chunk is the one part of the call that nothing overlaps.
         const long long chunk =
-            std::max<long long>(1, std::min<long long>(nq, (1LL << 29) / (long long)sizeof(T) / blk));
+            std::max<long long>(1, std::min<long long>(nq, batch_chunk_bytes() / (long long)sizeof(T) / blk));
         const size_t qbytes = (size_t)4 * chunk * sizeof(int), obytes = (size_t)chunk * blk * sizeof(T);
         if (!h->copy_stream)
         {
@@ -2516,9 +2529,10 @@ void eri_batch_run(qcg_handle* h, int la, int lb, int lc, int ld, long long nq, 
             CK(cudaEventRecord(h->hb_free[b], h->copy_stream));   // both buffers start free
         }
         int b = 0;
-        for (long long q0 = 0; q0 < nq; q0 += chunk, b ^= 1)
+        long long step = std::max<long long>(1, chunk / 8);
+        for (long long q0 = 0, m = 0; q0 < nq; q0 += m, b ^= 1, step = std::min(chunk, 2 * step))
         {
-            const long long m = std::min(chunk, nq - q0);
+            m = std::min(step, nq - q0);
             int* dq = (int*)h->hb_q[b];
             T* dout = (T*)h->hb_out[b];
             CK(cudaStreamWaitEvent(h->stream, h->hb_free[b], 0));   // the buffer's previous copy-out is done
