@@ -182,8 +182,10 @@ int qcg_set_graphs(qcg_handle* h, int enable);
 int qcg_set_eri_team_classes(qcg_handle* h, long long mask);
 /* The same choice for the direct J/K build (bit k: class k of the work lists): the team kernel, whose CTAs
  * digest each group's integral blocks into J and K, or the thread-per-quartet kernel; -1 (default): the
- * library's choice, or QCG_JK_TEAM_MASK in the environment.  Same J and K to rounding (bit for bit under
- * QCG_JK_DETERMINISTIC only within one form).  No reference counterpart. */
+ * library's choice -- the team form for the (dd|xx), (dp|dp) and (dp|pp) classes of a build with at least
+ * 2^20 quartets in the class -- or QCG_JK_TEAM_MASK in the environment (a mask set here or there applies at
+ * any size).  Same J and K to rounding (bit for bit under QCG_JK_DETERMINISTIC only within one form).  No
+ * reference counterpart. */
 int qcg_set_jk_team_classes(qcg_handle* h, long long mask);
 /* Restrict later J/K builds to a subset of shell pairs: mask (nshell x nshell bytes, row-major; pair (a,b) is
  * in the subset when mask[a*nshell+b] or mask[b*nshell+a] is non-zero) selects the pairs, and a quartet

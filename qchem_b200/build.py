@@ -75,8 +75,11 @@ def _team_mask() -> int:
     return sum(1 << k for k in TEAM_CLASSES)
 
 
-# classes whose direct J/K build runs in the team form by default (QCG_JK_TEAM_MASK selects others at run time)
-JK_TEAM_CLASSES = ()
+# classes whose direct J/K build runs in the team form by default (QCG_JK_TEAM_MASK selects others at run time):
+# (dd|dd), (dd|dp), (dd|ds), (dd|pp), (dd|ps), (dp|dp), (dp|pp).  Measured class by class on a B200 on the
+# uncontracted 32-water build (1824 functions), the team form took 0.48-0.91x the thread-per-quartet kernel's
+# time on these seven ((dd|dd) 43 vs 89 ms, (dp|dp) 529 vs 823 ms); on the others it took 1.07-4.7x.
+JK_TEAM_CLASSES = (12, 14, 16, 17, 18, 19, 20)
 
 
 def _jk_team_mask() -> int:

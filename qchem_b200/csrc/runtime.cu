@@ -1908,13 +1908,16 @@ void build_screening(qcg_handle* h, double thresh)
     h->screened = true;
 }
 
+bool team_scratch(qcg_handle* h, int k, TeamScratchDev& scr, TeamShape& sh);
+unsigned jk_team_mask_default(bool* forced);
+// smallest per-rank quartet count of a class for the build's default team form (2^20: ~220 groups of 32
+// quartets per CTA on 148 SMs)
+constexpr long long kJKTeamMinQuartets = 1LL << 20;
+
 // fp32_below: quartets whose density-weighted bound Q_ab Q_cd max|D| (max over the six D blocks the
 // quartet digests) is below it are evaluated in FP32 (FP64 accumulation); 0 = all FP64, HUGE_VAL = all
 // FP32.  The weighting is what makes FP32 safe: the FP32 error of a quartet's contribution to J and K is
 // about 3e-7 of its bound.  dmax (the density maxima of dD) is computed here when the caller has none.
-bool team_scratch(qcg_handle* h, int k, TeamScratchDev& scr, TeamShape& sh);
-unsigned jk_team_mask_default();
-
 void jk_device(qcg_handle* h, const double* dD, double* dJ, double* dK, int flags, qcg_stats* stats,
                const double* dmax = nullptr, double dthr = 0.0, double fp32_below = 0.0)
 {
@@ -1952,12 +1955,21 @@ void jk_device(qcg_handle* h, const double* dD, double* dJ, double* dK, int flag
     // when the build is not a graph)
     // classes built in the team form (FP64 band only); their scratch is sized here, before any capture, and
     // their launches share it, so they run one after another on the first side stream
-    const unsigned jk_mask = h->jk_team_mask >= 0 ? (unsigned)h->jk_team_mask : jk_team_mask_default();
+    // The build's default applies to a class only when its slice has at least kJKTeamMinQuartets quartets:
+    // the team form is a throughput design (a CTA per SM streaming groups of 32 quartets), and on a small
+    // build (a 57-function water) its classes took 3x the thread-per-quartet kernels' time.  A mask set by
+    // qcg_set_jk_team_classes or QCG_JK_TEAM_MASK applies whatever the size.
+    bool jk_forced = h->jk_team_mask >= 0;
+    unsigned jk_mask = jk_forced ? (unsigned)h->jk_team_mask : jk_team_mask_default(&jk_forced);
     bool team_k[kNumQuartetClasses] = {};
     TeamScratchDev team_scr[kNumQuartetClasses]{};
     TeamShape team_sh[kNumQuartetClasses]{};
     for (int k = 0; k < kNumQuartetClasses; ++k)
-        if (((jk_mask >> k) & 1u) && h->work[k].total > 0) team_k[k] = team_scratch(h, k, team_scr[k], team_sh[k]);
+    {
+        const long long span = h->work[k].total / h->shard_world;
+        if (((jk_mask >> k) & 1u) && h->work[k].total > 0 && (jk_forced || span >= kJKTeamMinQuartets))
+            team_k[k] = team_scratch(h, k, team_scr[k], team_sh[k]);
+    }
     for (int k = 0; k < kNumQuartetClasses; ++k)   // the buffer may have grown after an earlier class's lookup
         if (team_k[k]) team_scratch(h, k, team_scr[k], team_sh[k]);
     // QCG_JK_DETERMINISTIC: J' and K' as integer accumulator pairs (the low words after the nn high ones),
@@ -2387,14 +2399,13 @@ void check_team_error(qcg_handle* h)
 #define QCG_JK_TEAM_DEFAULT_MASK 0u
 #endif
 // The classes whose direct J/K build runs in the team form: the build's choice (QCG_JK_TEAM_DEFAULT_MASK),
-// unless QCG_JK_TEAM_MASK in the environment names others (read once per process).
-unsigned jk_team_mask_default()
+// unless QCG_JK_TEAM_MASK in the environment names others (read once per process; *forced then true).
+unsigned jk_team_mask_default(bool* forced)
 {
-    static const unsigned mask = [] {
-        const char* e = std::getenv("QCG_JK_TEAM_MASK");
-        if (!e || !*e) return (unsigned)(QCG_JK_TEAM_DEFAULT_MASK);
-        return (unsigned)std::strtoul(e, nullptr, 0);
-    }();
+    static const char* const env = std::getenv("QCG_JK_TEAM_MASK");
+    static const bool from_env = env && *env;
+    static const unsigned mask = from_env ? (unsigned)std::strtoul(env, nullptr, 0) : (unsigned)(QCG_JK_TEAM_DEFAULT_MASK);
+    if (forced) *forced = from_env;
     return mask;
 }
 
