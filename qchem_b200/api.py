@@ -127,6 +127,7 @@ def lib():
     L.qcg_scf_default_params.restype = None
     L.qcg_rhf.argtypes = [vp, i32, P(f64), P(f64), i32, P(ScfParams), P(ScfResult), P(f64)]
     L.qcg_internal_syev.argtypes = [i32, P(f64), P(f64), P(f64)]
+    L.qcg_internal_gemm_bf16.argtypes = [i32, i32, i32, i32, i32, vp, i32, vp, i32, vp, i32, vp, i32]
     L.qcg_internal_syev_lowest.argtypes = [i32, P(f64), i32, P(f64), P(f64)]
     L.qcg_internal_orthogonaliser.argtypes = [i32, P(f64), P(f64)]
     L.qcg_measure_fp64_peak.argtypes = [i32, P(f64), P(f64)]

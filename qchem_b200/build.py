@@ -109,7 +109,7 @@ def _jobs():
     extra = {"runtime.cu": _headers(["boys_table.h", "eri_team_iface.h"]) + [_read(os.path.join(INCLUDE, "qchem_b200.h"))],
              "registry.cu": _headers(["eri_team_iface.h"]),
              "fock_kernels.cu": _headers(["team_sync.cuh"]),
-             "mlp.cu": [_read(os.path.join(INCLUDE, "qchem_b200.h"))]}
+             "mlp.cu": [_read(os.path.join(INCLUDE, "qchem_b200.h"))] + _headers(["smem_attr.h", "team_sync.cuh"])}
     for name in ("registry.cu", "fock_kernels.cu", "runtime.cu", "mlp.cu"):
         s = os.path.join(CSRC, name)
         defs = HOST_OMP + [f"-DQCG_TEAM_DEFAULT_MASK={_team_mask():#x}u",

@@ -4,13 +4,12 @@
 // pair geometry features to density-matrix blocks; it has no counterpart in the reference, whose SCF
 // always starts from the core Hamiltonian (src/SCFIterator/Imp/Seed.C:70-80).
 //
-// Matrix products are SIMT tiles (64 x 64 outputs per 256-thread block, 4 x 4 per thread, k-slices of 16
-// staged in shared memory): the whole network is ~0.4 M parameters and a training step over 10^4 rows
-// is a few GFLOP, far below anything the SCF spends, so tensor-core tiles would not change a measurable
-// time here.
+// Matrix products run on the tensor cores (tcgen05.mma, accumulators in tensor memory; see tc::gemm_kernel).
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <random>
@@ -19,6 +18,8 @@
 #include <vector>
 
 #include "../../include/qchem_b200.h"
+#include "smem_attr.h"
+#include "team_sync.cuh"
 
 namespace {
 
@@ -35,79 +36,263 @@ struct MlpError
         if (e_ != cudaSuccess) throw MlpError{QCG_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)}; \
     } while (0)
 
-__device__ __forceinline__ float bf16r(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
+// ------------------------------------------------------------------------------------------------
+// Matrix products on the 5th-generation tensor cores (tcgen05), one 128 x 128 output tile per CTA:
+//   C[m][n] (+)= sum_k A(m,k) B(k,n) (+ bias[n]);  A(m,k) = TA ? A[k*lda+m] : A[m*lda+k],
+//   B(k,n) = TB ? B[n*ldb+k] : B[k*ldb+n].
+// The 128 threads stage a 128 x 64 slice of A and of B^T into shared memory per step, rounded to BF16, in
+// the K-major canonical layout without swizzle (8-row x 16-byte core matrices; rows 16 B apart, 8-row
+// groups 128 B apart, the 8-element K halves of one MMA R*16 B apart for an R-row tile); one thread issues
+// four tcgen05.mma (kind::f16, M = 128, N = 128, K = 16) per step with the FP32 accumulator in tensor
+// memory (128 columns), and commits them to the step's mbarrier, which frees that stage two steps later.
+// The epilogue reads the accumulator back with tcgen05.ld (warp w: lanes, i.e. rows, 32w..32w+31).  Long
+// K (the weight gradients, K = rows) is split over CTAs, whose partial tiles are added with FP32 atomics.
+// Every wait is bounded: a wait that gives up sets the error word, waits (bounded) for the MMAs in flight
+// and frees the tensor memory before the CTA returns.
+namespace tc {
+constexpr int BM = 128, BN = 128, BK = 64, THREADS = 128, NSTAGE = 2;
+constexpr uint32_t A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2, STAGE_BYTES = A_BYTES + B_BYTES;
+// two stages need 64 KB; the allocation is 96 KB so that every address a descriptor of these tiles can
+// form, read either way round (LBO and SBO), stays inside it
+constexpr size_t SMEM = 96 * 1024;
+// instruction descriptor: FP32 accumulator (bits 4-5 = 1), A and B BF16 (bits 7-9, 10-12 = 1), both
+// K-major (bits 15, 16 = 0), N >> 3 at bit 17, M >> 4 at bit 24
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                            ((uint32_t)(BM >> 4) << 24);
 
-// C[m][n] (+)= sum_k A(m,k) B(k,n) (+ bias[n]); A(m,k) = TA ? A[k*lda+m] : A[m*lda+k],
-// B(k,n) = TB ? B[n*ldb+k] : B[k*ldb+n].  Operands rounded to BF16, FP32 accumulation.
-constexpr int TM = 64, TN = 64, TK = 16;
-template <bool TA, bool TB>
-__global__ void __launch_bounds__(256) gemm_bf16_kernel(int M, int N, int K, const float* __restrict__ A, int lda,
-                                                        const float* __restrict__ B, int ldb, float* __restrict__ C,
-                                                        int ldc, const float* __restrict__ bias, int accumulate)
+// shared-memory matrix descriptor: start address, leading-dimension byte offset (between the K core
+// matrices), stride byte offset (between 8-row groups), all in 16-byte units; version 1 (bits 46-47);
+// base offset, LBO mode and layout type (no swizzle) zero
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo)
 {
-    __shared__ float As[TK][TM + 4];
-    __shared__ float Bs[TK][TN + 4];
-    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-    const int m0 = blockIdx.y * TM, n0 = blockIdx.x * TN;
-    float acc[4][4] = {};
-    for (int k0 = 0; k0 < K; k0 += TK)
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ void mma(uint32_t tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc)
+{
+    asm volatile(
+        "{ .reg .pred p; setp.ne.b32 p, %4, 0; tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p; }" ::"r"(tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc)
+        : "memory");
+}
+
+__device__ __forceinline__ void commit(uint64_t* bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     qcg::team::smem_addr(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// 16 consecutive FP32 columns of this thread's lane
+__device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t (&r)[16])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(addr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// Rows [r0, r0 + R) x k [k0, k0 + BK) of an operand whose element (r, k) is X[r*ld + k] (KMAJ) or
+// X[k*ld + r], zero outside [0, nrows) x [0, K), rounded to BF16 into the canonical layout at dst: the
+// 16-byte chunk (r, c) (k = 8c..8c+7) at byte c*R*16 + r*16.  Consecutive threads take consecutive rows, so
+// that the shared-memory stores do not conflict and the loads of a non-K-major operand coalesce.
+template <bool KMAJ, int R>
+__device__ __forceinline__ void stage(const float* __restrict__ X, int ld, int nrows, int K, int r0, int k0,
+                                      uint8_t* dst)
+{
+    for (int e = threadIdx.x; e < R * (BK / 8); e += THREADS)
     {
-        for (int e = threadIdx.x; e < TK * TM; e += 256)
+        const int r = e % R, c = e / R;
+        const int gr = r0 + r, gk = k0 + 8 * c;
+        float v[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
         {
-            const int kk = e / TM, mm = e % TM;
-            const int m = m0 + mm, k = k0 + kk;
-            float v = 0.f;
-            if (m < M && k < K) v = TA ? A[(size_t)k * lda + m] : A[(size_t)m * lda + k];
-            As[kk][mm] = bf16r(v);
+            v[j] = 0.f;
+            if (gr < nrows && gk + j < K)
+                v[j] = KMAJ ? __ldg(X + (size_t)gr * ld + gk + j) : __ldg(X + (size_t)(gk + j) * ld + gr);
         }
-        for (int e = threadIdx.x; e < TK * TN; e += 256)
-        {
-            const int kk = e / TN, nn = e % TN;
-            const int n = n0 + nn, k = k0 + kk;
-            float v = 0.f;
-            if (n < N && k < K) v = TB ? B[(size_t)n * ldb + k] : B[(size_t)k * ldb + n];
-            Bs[kk][nn] = bf16r(v);
-        }
-        __syncthreads();
-#pragma unroll
-        for (int kk = 0; kk < TK; ++kk)
-        {
-            float a[4], b[4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) a[i] = As[kk][ty * 4 + i];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx * 4 + j];
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
-        }
-        __syncthreads();
-    }
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-    {
-        const int m = m0 + ty * 4 + i;
-        if (m >= M) continue;
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-        {
-            const int n = n0 + tx * 4 + j;
-            if (n >= N) continue;
-            float v = acc[i][j] + (bias ? bias[n] : 0.f);
-            float* c = C + (size_t)m * ldc + n;
-            *c = accumulate ? *c + v : v;
-        }
+        uint4 u;
+        __nv_bfloat162 h;
+        h = __floats2bfloat162_rn(v[0], v[1]);
+        u.x = *reinterpret_cast<uint32_t*>(&h);
+        h = __floats2bfloat162_rn(v[2], v[3]);
+        u.y = *reinterpret_cast<uint32_t*>(&h);
+        h = __floats2bfloat162_rn(v[4], v[5]);
+        u.z = *reinterpret_cast<uint32_t*>(&h);
+        h = __floats2bfloat162_rn(v[6], v[7]);
+        u.w = *reinterpret_cast<uint32_t*>(&h);
+        *reinterpret_cast<uint4*>(dst + (size_t)c * R * 16 + (size_t)r * 16) = u;
     }
 }
+
+// mode 0: C = AB + bias; 1: C += AB + bias; 2: atomicAdd (split K; bias from the first split)
+template <bool TA, bool TB>
+__global__ void __launch_bounds__(THREADS) gemm_kernel(int M, int N, int K, const float* __restrict__ A, int lda,
+                                                       const float* __restrict__ B, int ldb, float* __restrict__ C,
+                                                       int ldc, const float* __restrict__ bias, int mode,
+                                                       int chunks_per_split, int* __restrict__ err)
+{
+    extern __shared__ __align__(128) uint8_t tc_smem[];
+    __shared__ uint64_t bar[NSTAGE];
+    __shared__ uint32_t tmem_base;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    const int nchunks = (K + BK - 1) / BK > 0 ? (K + BK - 1) / BK : 1;
+    const int kc0 = blockIdx.z * chunks_per_split;
+    const int nk = min(kc0 + chunks_per_split, nchunks) - kc0;   // >= 1: the host launches no empty split
+    if (threadIdx.x == 0)
+    {
+        for (int s = 0; s < NSTAGE; ++s) qcg::team::mbar_init(&bar[s]);
+        qcg::team::mbar_init_fence();
+    }
+    if (warp == 0)
+    {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         qcg::team::smem_addr(&tmem_base)),
+                     "r"(BN)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = tmem_base;
+    bool ok = true;
+    int issued = 0;   // steps whose MMAs were committed
+    for (int i = 0; i < nk; ++i)
+    {
+        const int s = i % NSTAGE;
+        uint8_t* sa = tc_smem + s * STAGE_BYTES;
+        uint8_t* sb = sa + A_BYTES;
+        if (i >= NSTAGE)
+        {
+            // the MMAs of step i - NSTAGE read this stage
+            bool late = false;
+            if (threadIdx.x == 0) late = !qcg::team::mbar_wait(&bar[s], (uint32_t)(((i - NSTAGE) / NSTAGE) & 1));
+            if (__syncthreads_or(late))
+            {
+                ok = false;
+                break;
+            }
+        }
+        const int k0 = (kc0 + i) * BK;
+        stage<!TA, BM>(A, lda, M, K, m0, k0, sa);
+        stage<TB, BN>(B, ldb, N, K, n0, k0, sb);
+        // the generic-proxy stores become visible to the tensor cores (async proxy)
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (threadIdx.x == 0)
+        {
+            fence_after();
+            const uint32_t a0 = qcg::team::smem_addr(sa), b0 = qcg::team::smem_addr(sb);
+#pragma unroll
+            for (int kk = 0; kk < BK / 16; ++kk)
+                mma(tmem, smem_desc(a0 + kk * 2 * BM * 16, BM * 16, 128), smem_desc(b0 + kk * 2 * BN * 16, BN * 16, 128),
+                    kIdesc, (i > 0 || kk > 0) ? 1u : 0u);
+            commit(&bar[s]);
+        }
+        issued = i + 1;
+    }
+    if (ok)
+    {
+        // the last commit covers every MMA this thread issued
+        bool late = false;
+        if (threadIdx.x == 0)
+            late = !qcg::team::mbar_wait(&bar[(nk - 1) % NSTAGE], (uint32_t)(((nk - 1) / NSTAGE) & 1));
+        ok = !__syncthreads_or(late);
+    }
+    else if (threadIdx.x == 0 && issued > 0)
+        qcg::team::mbar_wait(&bar[(issued - 1) % NSTAGE], (uint32_t)(((issued - 1) / NSTAGE) & 1));
+    fence_after();
+    if (ok)
+    {
+        const int row = m0 + 32 * warp + lane;
+        const bool add_bias = bias && blockIdx.z == 0;
+        for (int c = 0; c < BN; c += 16)
+        {
+            uint32_t r[16];
+            tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c, r);
+            if (row < M)
+            {
+                float* crow = C + (size_t)row * ldc;
+#pragma unroll
+                for (int j = 0; j < 16; ++j)
+                {
+                    const int n = n0 + c + j;
+                    if (n >= N) continue;
+                    const float v = __uint_as_float(r[j]) + (add_bias ? bias[n] : 0.f);
+                    if (mode == 2) atomicAdd(crow + n, v);
+                    else if (mode == 1) crow[n] += v;
+                    else crow[n] = v;
+                }
+            }
+        }
+    }
+    else if (threadIdx.x == 0)
+        atomicOr(err, 1);
+    fence_before();
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN) : "memory");
+}
+
+__global__ void zero_2d_kernel(float* __restrict__ C, int M, int N, int ldc)
+{
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < (long long)M * N) C[(e / N) * ldc + e % N] = 0.f;
+}
+}   // namespace tc
+
+// the error word of the tensor-core products (bit 0: a wait for an MMA gave up); read and cleared by the
+// calls that synchronise
+__device__ int g_mlp_err;
 
 template <bool TA, bool TB>
 void gemm(int M, int N, int K, const float* A, int lda, const float* B, int ldb, float* C, int ldc, const float* bias,
           bool accumulate, cudaStream_t st)
 {
     if (M <= 0 || N <= 0) return;
-    dim3 grid((N + TN - 1) / TN, (M + TM - 1) / TM);
-    gemm_bf16_kernel<TA, TB><<<grid, 256, 0, st>>>(M, N, K, A, lda, B, ldb, C, ldc, bias, accumulate ? 1 : 0);
+    static std::atomic<unsigned long long> ready{0};
+    qcg::ensure_smem(tc::gemm_kernel<TA, TB>, tc::SMEM, ready);
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int tm = (M + tc::BM - 1) / tc::BM, tn = (N + tc::BN - 1) / tc::BN;
+    const int nchunks = std::max(1, (K + tc::BK - 1) / tc::BK);
+    // split K until about two CTAs per SM are busy, keeping at least 4 steps per split
+    int splits = std::min(std::max(1, nchunks / 4), std::max(1, 2 * nsm / (tm * tn)));
+    const int per = (nchunks + splits - 1) / splits;
+    splits = (nchunks + per - 1) / per;   // no empty split
+    int mode = accumulate ? 1 : 0;
+    if (splits > 1)
+    {
+        mode = 2;
+        if (!accumulate)
+            tc::zero_2d_kernel<<<(unsigned)(((long long)M * N + 255) / 256), 256, 0, st>>>(C, M, N, ldc);
+    }
+    int* err = nullptr;
+    MCK(cudaGetSymbolAddress((void**)&err, g_mlp_err));
+    dim3 grid(tn, tm, splits);
+    tc::gemm_kernel<TA, TB><<<grid, tc::THREADS, tc::SMEM, st>>>(M, N, K, A, lda, B, ldb, C, ldc, bias, mode, per, err);
+}
+
+// reads (after the caller synchronised the stream) and clears the tensor-core error word
+void check_mlp_err()
+{
+    int e = 0;
+    MCK(cudaMemcpyFromSymbol(&e, g_mlp_err, sizeof(int)));
+    if (!e) return;
+    const int zero = 0;
+    MCK(cudaMemcpyToSymbol(g_mlp_err, &zero, sizeof(int)));
+    throw MlpError{QCG_ERR_CUDA, "MLP matrix product: a wait for the tensor cores gave up; the results are not valid"};
 }
 
 __device__ __forceinline__ float sigmoid(float z) { return 1.f / (1.f + __expf(-z)); }
@@ -418,6 +603,7 @@ int qcg_mlp_loss_grad(qcg_mlp* m, int rows, const float* d_x, const float* d_t, 
         if (grad_host)
             MCK(cudaMemcpyAsync(grad_host, m->d_g, m->nparam * sizeof(float), cudaMemcpyDeviceToHost, m->stream));
         MCK(cudaStreamSynchronize(m->stream));
+        check_mlp_err();
         if (loss) *loss = acc[0];
     });
 }
@@ -433,6 +619,30 @@ int qcg_mlp_adam(qcg_mlp* m, float lr, float beta1, float beta2, float eps, floa
                                                                 beta2, eps, weight_decay, c1, c2);
         MCK(cudaGetLastError());
     });
+}
+
+// test hook (not part of the public header): C (+)= op(A) op(B) (+ bias) on device pointers through the
+// tensor-core product above, synchronous; ta/tb select the transposed operand forms
+int qcg_internal_gemm_bf16(int ta, int tb, int M, int N, int K, const float* A, int lda, const float* B, int ldb,
+                           float* C, int ldc, const float* bias, int accumulate)
+{
+    try
+    {
+        if (M < 0 || N < 0 || K < 0 || (K > 0 && (!A || !B)) || (M > 0 && N > 0 && !C)) return QCG_ERR_ARG;
+        const bool acc = accumulate != 0;
+        if (ta && tb) gemm<true, true>(M, N, K, A, lda, B, ldb, C, ldc, bias, acc, nullptr);
+        else if (ta) gemm<true, false>(M, N, K, A, lda, B, ldb, C, ldc, bias, acc, nullptr);
+        else if (tb) gemm<false, true>(M, N, K, A, lda, B, ldb, C, ldc, bias, acc, nullptr);
+        else gemm<false, false>(M, N, K, A, lda, B, ldb, C, ldc, bias, acc, nullptr);
+        MCK(cudaGetLastError());
+        MCK(cudaDeviceSynchronize());
+        check_mlp_err();
+        return QCG_OK;
+    }
+    catch (const MlpError& e)
+    {
+        return e.code;
+    }
 }
 
 }   // extern "C"

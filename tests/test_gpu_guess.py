@@ -22,6 +22,40 @@ def _problem(widths, rows, seed):
     return x, t, mask
 
 
+def _gemm_case(ta, tb, M, N, K, bias, accumulate, seed):
+    """C (+)= op(A) op(B) (+ bias) through the tensor-core product, against float64 products of the same
+    BF16-rounded operands."""
+    g = torch.Generator().manual_seed(seed)
+    A = torch.randn((K, M) if ta else (M, K), generator=g)
+    B = torch.randn((N, K) if tb else (K, N), generator=g)
+    C0 = torch.randn((M, N), generator=g)
+    b = torch.randn(N, generator=g) if bias else None
+    dA, dB, dC = A.cuda(), B.cuda(), C0.clone().cuda()
+    db = b.cuda() if bias else None
+    rc = api.lib().qcg_internal_gemm_bf16(int(ta), int(tb), M, N, K, dA.data_ptr(), A.shape[1], dB.data_ptr(),
+                                          B.shape[1], dC.data_ptr(), N, db.data_ptr() if bias else None,
+                                          int(accumulate))
+    assert rc == 0
+    r = lambda x: x.to(torch.bfloat16).to(torch.float64)
+    opA = r(A).T if ta else r(A)
+    opB = r(B).T if tb else r(B)
+    ref = opA @ opB + (b.double() if bias else 0.0) + (C0.double() if accumulate else 0.0)
+    scale = (opA.abs() @ opB.abs()).max().item() + 1.0
+    return (dC.cpu().double() - ref).abs().max().item() / scale
+
+
+@pytest.mark.parametrize("ta,tb", [(False, False), (False, True), (True, False), (True, True)])
+@pytest.mark.parametrize("M,N,K", [(1, 1, 1), (127, 129, 65), (300, 256, 256), (256, 1225, 256), (256, 256, 9000),
+                                   (64, 16, 0)])
+def test_tensor_core_product_matches_float64(ta, tb, M, N, K):
+    """The MLP's matrix product on the tensor cores (tcgen05.mma, accumulator in tensor memory): every
+    operand form, ragged tiles, long K (split over CTAs, atomics), K = 0, with and without bias and
+    accumulation.  BF16 products are exact in FP32; only the FP32 summation order differs."""
+    for bias, acc in ((False, False), (True, False), (True, True)):
+        err = _gemm_case(ta, tb, M, N, K, bias, acc, seed=M * 7 + N * 3 + K + 2 * ta + tb)
+        assert err < 2e-6, (bias, acc, err)
+
+
 def test_mlp_forward_matches_oracle():
     widths = [23, 256, 256, 256, 300]
     net = api.Mlp(widths, seed=5)
