@@ -1,5 +1,6 @@
 """Batched SCF (several molecules in one handle, one J/K build over all of them per iteration): every
-molecule's J, K and converged energy must equal those of its own single-molecule handle."""
+molecule's J, K and converged energy must equal those of its own single-molecule handle, and those of the
+CPU oracle (the oracle's direct J/K build and its plain SCF, which takes the same DIIS steps)."""
 import numpy as np
 import pytest
 
@@ -22,7 +23,7 @@ def mols():
     return ms
 
 
-def test_batch_jk_equals_single_builds(mols):
+def test_batch_jk_equals_single_builds(mols, oracle_mod):
     shells = [B.even_tempered(m) for m in mols]
     be = api.BatchEngine(shells)
     assert be.nmol == len(mols) and be.mol_nbf == [B.nbf(s) for s in shells]
@@ -32,11 +33,13 @@ def test_batch_jk_equals_single_builds(mols):
     for k, (s, D) in enumerate(zip(shells, Ds)):
         Js, Ks, sts = api.Engine(s).fock_jk(D)
         assert np.abs(J[k] - Js).max() <= FOCK_TOL and np.abs(K[k] - Ks).max() <= FOCK_TOL, k
+        Jo, Ko, _ = oracle_mod.OracleBasis(s).jk_direct(D, 1e-10)
+        assert np.abs(J[k] - Jo).max() <= FOCK_TOL and np.abs(K[k] - Ko).max() <= FOCK_TOL, k
         total += sts.quartets
     assert st.quartets == total
 
 
-def test_batch_rhf_equals_single_rhf(mols):
+def test_batch_rhf_equals_single_rhf(mols, oracle_mod):
     shells = [B.even_tempered(m) for m in mols]
     res = api.BatchEngine(shells).rhf(mols)
     for m, s, r in zip(mols, shells, res):
@@ -45,6 +48,11 @@ def test_batch_rhf_equals_single_rhf(mols):
         if ref["converged"]:
             assert abs(r["energy"] - ref["energy"]) <= E_TOL
             assert abs(r["iterations"] - ref["iterations"]) <= 1   # same trajectory up to summation order
+        orc = oracle_mod.OracleBasis(s).rhf(m)
+        assert r["converged"] == orc["converged"]
+        if orc["converged"]:
+            assert abs(r["energy"] - orc["energy"]) <= E_TOL
+            assert abs(r["iterations"] - orc["iterations"]) <= 1
 
 
 def test_batch_rejects_single_molecule_only_calls(mols):

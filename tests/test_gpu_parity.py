@@ -40,6 +40,26 @@ def test_eri_batch_class(k, pool_engines):
     assert err <= ERI_TOL, f"class {cls}: max abs error {err:.3e} (max |eri| {np.abs(ref).max():.3e})"
 
 
+@pytest.fixture(scope="module")
+def bench_engines(oracle_mod):
+    shells = W.shell_pool(512, seed=W.SEED0 + 4000)
+    return api.Engine(shells), oracle_mod.OracleBasis(shells)
+
+
+@pytest.mark.parametrize("k", range(21))
+def test_eri_batch_default_form_on_1e4_benchmark_quartets(k, bench_engines):
+    """Each class in the form the library picks for it (the team form for 15 classes, thread-per-quartet for
+    the (xx|ss) classes) on 10^4 quartets drawn like the ERI benchmark: contraction 1-3 per shell, exponents
+    log-uniform in [0.05, 50], centres in a 12-bohr box."""
+    eng, ob = bench_engines
+    cls = W.quartet_classes()[k]
+    q = W.eri_class_batch(cls, 10_000, 512, seed=W.SEED0 + 4300 + k)
+    got = eng.eri_batch(cls, q)
+    ref = ob.eri_batch(q)
+    err = np.abs(got - ref).max()
+    assert err <= ERI_TOL, f"class {cls}: max abs error {err:.3e} (max |eri| {np.abs(ref).max():.3e})"
+
+
 def test_eri_batch_matches_fourc_elements(pool_engines):
     """Spot-check single elements against the reference's per-component route (FourC)."""
     eng, ob = pool_engines
