@@ -194,11 +194,17 @@ int qcg_set_jk_team_classes(qcg_handle* h, long long mask);
  * build against the CPU oracle; no reference counterpart. */
 int qcg_set_pair_subset(qcg_handle* h, const unsigned char* mask);
 /* Several GPUs on one J/K build: with (rank, world) set, later qcg_fock_jk* calls evaluate only this rank's
- * contiguous slice (1/world of the screened quartets of every class) and return the rank's PARTIAL J and K;
+ * contiguous slice of every class's screened quartets (1/world of its primitive quartets, see
+ * qcg_shard_work) and return the rank's PARTIAL J and K;
  * the sum over ranks (one all-reduce) is the full J and K.  (0, 1), the default, is the whole build.  The
  * qcg_stats figures still describe the whole build.  No reference counterpart (the reference is one
  * process). */
 int qcg_set_shard(qcg_handle* h, int rank, int world);
+/* The work of share `rank` of `world` under qcg_set_shard: its screened shell quartets and primitive quartets.
+ * The shares are cut at equal fractions of every class's primitive quartets (a contracted quartet costs its
+ * primitive-quartet count), so their primitive counts are equal to within one quartet per class while their
+ * quartet counts may differ.  Needs qcg_schwarz first.  No reference counterpart. */
+int qcg_shard_work(qcg_handle* h, int rank, int world, long long* quartets, long long* prim_quartets);
 /* Autotuner of the J/K launch shapes.  For every quartet class it times the class kernel on up to 2^20 of
  * the handle's screened quartets (density d_D, `reps` timed launches per candidate) for each candidate
  * (quartets per lane 1, 2, 4, 8, 16) x (blocks per SM 8, 16) and keeps the fastest for later builds of this

@@ -43,7 +43,7 @@ EXPORTS = ["qcg_basis_create", "qcg_destroy", "qcg_last_error", "qcg_set_stream"
            "qcg_mlp_adam", "qcg_basis_create_batch", "qcg_nmol", "qcg_mol_nbf", "qcg_one_electron_batch",
            "qcg_rhf_batch", "qcg_set_graphs", "qcg_set_shard", "qcg_autotune_jk", "qcg_eri3_batch",
            "qcg_nbf_spherical", "qcg_spherical_transform", "qcg_fock_jk_spherical", "qcg_release_cache",
-           "qcg_set_eri_team_classes", "qcg_set_pair_subset", "qcg_set_jk_team_classes", "qcg_selftest_bounded_wait"]
+           "qcg_set_eri_team_classes", "qcg_set_pair_subset", "qcg_set_jk_team_classes", "qcg_selftest_bounded_wait", "qcg_shard_work"]
 
 
 class QcgError(RuntimeError):
@@ -118,6 +118,7 @@ def lib():
     L.qcg_set_fp32_bound.argtypes = [vp, f64]
     L.qcg_set_graphs.argtypes = [vp, i32]
     L.qcg_set_shard.argtypes = [vp, i32, i32]
+    L.qcg_shard_work.argtypes = [vp, i32, i32, P(i64), P(i64)]
     L.qcg_autotune_jk.argtypes = [vp, vp, i32, P(i32), P(i32)]
     L.qcg_schwarz.argtypes = [vp, f64, P(f64)]
     L.qcg_fock_jk.argtypes = [vp, P(f64), P(f64), P(f64), i32, P(Stats)]
@@ -327,9 +328,17 @@ class Engine:
         self._check(f(self._h, la, lb, lc, ld, int(nq), ctypes.c_void_p(d_quartets_ptr), ctypes.c_void_p(d_out_ptr)))
 
     def set_shard(self, rank: int, world: int):
-        """Later J/K builds evaluate this rank's 1/world slice of the quartets and return partial J and K
-        (summed over ranks they are the full build)."""
+        """Later J/K builds evaluate this rank's slice of the quartets (1/world of every class's primitive
+        quartets) and return partial J and K (summed over ranks they are the full build)."""
         self._check(lib().qcg_set_shard(self._h, int(rank), int(world)))
+
+    def shard_work(self, rank: int, world: int):
+        """(screened quartets, primitive quartets) of share `rank` of `world` under set_shard."""
+        if self._screen is None:
+            self.schwarz()
+        nq, npq = ctypes.c_longlong(), ctypes.c_longlong()
+        self._check(lib().qcg_shard_work(self._h, int(rank), int(world), ctypes.byref(nq), ctypes.byref(npq)))
+        return nq.value, npq.value
 
     def autotune_jk(self, d_D: int, reps: int = 1):
         """Tune the J/K launch shape of every class on the density at device pointer d_D; returns the chosen

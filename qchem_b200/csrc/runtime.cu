@@ -330,6 +330,12 @@ struct qcg_handle
     PairListDev pl_dev[kNumPairClasses]{};
     PrimPairsDev pp_dev{};
     JKWorkDev work[kNumQuartetClasses]{};
+    // host copies of the work lists for the shard boundaries: per class, the quartet offsets and ket bases
+    // of the bra pairs and the prefix sums of their primitive quartets; per pair class, the prefix sums of
+    // the primitive-pair counts
+    std::vector<long long> wh_offs[kNumQuartetClasses], wh_cum[kNumQuartetClasses];
+    std::vector<int> wh_kbase[kNumQuartetClasses];
+    std::vector<long long> pl_nppsum[kNumPairClasses];
     double fp32_below = 0;   // qcg_set_fp32_bound: quartets with a smaller bound are evaluated in FP32
     int shard_rank = 0, shard_world = 1;   // qcg_set_shard: this handle's slice of every J/K build
     std::shared_ptr<void> sph;             // the spherical map, built on first use
@@ -1865,8 +1871,10 @@ void build_screening(qcg_handle* h, double thresh)
             std::vector<long long> offs(qx.size() + 1, 0);
             std::vector<int> kbase(qx.size(), 0);
             // prefix sums of ket primitive-pair counts for the primitive-quartet tally
-            std::vector<long long> nppy(qy.size() + 1, 0);
+            std::vector<long long>& nppy = h->pl_nppsum[Y];
+            nppy.assign(qy.size() + 1, 0);
             for (size_t j = 0; j < qy.size(); ++j) nppy[j + 1] = nppy[j] + h->pl_npp[Y][j];
+            std::vector<long long> cum(qx.size() + 1, 0);
             long long pq = 0;
             for (size_t i = 0; i < qx.size(); ++i)
             {
@@ -1886,6 +1894,7 @@ void build_screening(qcg_handle* h, double thresh)
                 kbase[i] = jb;
                 offs[i + 1] = offs[i] + cnt;
                 pq += (long long)h->pl_npp[X][i] * (nppy[jb + cnt] - nppy[jb]);
+                cum[i + 1] = pq;
             }
             h->work[k].total = offs.back();
             h->work[k].gbeg = 0;
@@ -1894,6 +1903,7 @@ void build_screening(qcg_handle* h, double thresh)
             h->work[k].cap = 0;
             h->work[k].offs = h->upload(offs);
             h->work[k].kbase = h->nmol > 1 ? h->upload(kbase) : nullptr;
+
             h->work[k].mols = h->mols();
             h->work[k].same_class = (X == Y);
             h->work[k].lo = 0.0;
@@ -1901,11 +1911,53 @@ void build_screening(qcg_handle* h, double thresh)
             h->work_quartets += offs.back();
             h->work_prim_quartets += pq;
             h->work_flops += (double)pq * class_flops(kPairLA[X], kPairLB[X], kPairLA[Y], kPairLB[Y]);
+            h->wh_offs[k] = std::move(offs);   // offs, kbase and cum are not used after this
+            h->wh_kbase[k] = std::move(kbase);
+            h->wh_cum[k] = std::move(cum);
         }
     h->flush_uploads();
     CK(cudaStreamSynchronize(h->stream));
     h->thresh = thresh;
     h->screened = true;
+}
+
+// The first quartet of share r (of w) of class k's work list: the cut lies where the primitive quartets
+// before it (the ERI work: a contracted quartet costs its primitive-quartet count) reach r/w of the class's
+// total, so that ranks get equal work rather than equal quartet counts.  Within the bra pair that holds the
+// cut, the kets' primitive-pair prefix sums place it to the quartet.
+long long shard_cut(const qcg_handle* h, int k, long long r, long long w)
+{
+    const std::vector<long long>& offs = h->wh_offs[k];
+    const std::vector<long long>& cum = h->wh_cum[k];
+    const long long total = offs.empty() ? 0 : offs.back();
+    if (r <= 0) return 0;
+    if (r >= w || cum.empty() || cum.back() <= 0) return r >= w ? total : total * r / w;
+    const long long target = (long long)((long double)cum.back() * r / w);
+    // bra pair i with cum[i] <= target < cum[i + 1]
+    const size_t i = (size_t)(std::upper_bound(cum.begin(), cum.end(), target) - cum.begin()) - 1;
+    if (i + 1 >= cum.size()) return total;
+    int X = 0;
+    while ((X + 1) * (X + 2) / 2 <= k) ++X;
+    const int Y = k - X * (X + 1) / 2;
+    const long long np = h->pl_npp[X][i];
+    const std::vector<long long>& nppy = h->pl_nppsum[Y];
+    const long long jb = h->wh_kbase[k][i], len = offs[i + 1] - offs[i];
+    // smallest c in [0, len] with np * (nppy[jb + c] - nppy[jb]) >= target - cum[i]
+    long long lo = 0, hi = len;
+    while (lo < hi)
+    {
+        const long long mid = (lo + hi) / 2;
+        if (np * (nppy[jb + mid] - nppy[jb]) >= target - cum[i]) hi = mid;
+        else lo = mid + 1;
+    }
+    return offs[i] + lo;
+}
+
+// this handle's slice [gbeg, gend) of class k under qcg_set_shard
+void shard_range(const qcg_handle* h, int k, long long& gbeg, long long& gend)
+{
+    gbeg = shard_cut(h, k, h->shard_rank, h->shard_world);
+    gend = shard_cut(h, k, h->shard_rank + 1, h->shard_world);
 }
 
 bool team_scratch(qcg_handle* h, int k, TeamScratchDev& scr, TeamShape& sh);
@@ -1966,7 +2018,9 @@ void jk_device(qcg_handle* h, const double* dD, double* dJ, double* dK, int flag
     TeamShape team_sh[kNumQuartetClasses]{};
     for (int k = 0; k < kNumQuartetClasses; ++k)
     {
-        const long long span = h->work[k].total / h->shard_world;
+        long long gb = 0, ge = 0;
+        shard_range(h, k, gb, ge);
+        const long long span = ge - gb;
         if (((jk_mask >> k) & 1u) && h->work[k].total > 0 && (jk_forced || span >= kJKTeamMinQuartets))
             team_k[k] = team_scratch(h, k, team_scr[k], team_sh[k]);
     }
@@ -1995,9 +2049,8 @@ void jk_device(qcg_handle* h, const double* dD, double* dJ, double* dK, int flag
             wk.run = h->tuned_run[k];
             wk.cap = h->tuned_cap[k];
             wk.mol_active = h->d_mol_active;
-            // this rank's contiguous slice of the class's quartets
-            wk.gbeg = wk.total * h->shard_rank / h->shard_world;
-            wk.gend = wk.total * (h->shard_rank + 1) / h->shard_world;
+            // this rank's contiguous slice of the class's quartets (equal shares of its primitive quartets)
+            shard_range(h, k, wk.gbeg, wk.gend);
             if (wk.gend <= wk.gbeg) continue;
             wk.dmax = dmax;
             wk.nshell = h->nshell;
@@ -2742,6 +2795,38 @@ int qcg_set_shard(qcg_handle* h, int rank, int world)
     });
 }
 
+int qcg_shard_work(qcg_handle* h, int rank, int world, long long* quartets, long long* prim_quartets)
+{
+    if (!h) return QCG_ERR_ARG;
+    return guarded(h, [&] {
+        require(world >= 1 && rank >= 0 && rank < world, "need 0 <= rank < world");
+        require(quartets && prim_quartets, "null argument");
+        require(h->screened, "qcg_schwarz must be called first", QCG_ERR_STATE);
+        long long nq = 0, npq = 0;
+        for (int k = 0; k < kNumQuartetClasses; ++k)
+        {
+            const long long gb = shard_cut(h, k, rank, world), ge = shard_cut(h, k, rank + 1, world);
+            nq += ge - gb;
+            // primitive quartets of [gb, ge): the bra pairs' prefix sums, with partial bra pairs at both ends
+            auto prim_before = [&](long long g) {
+                const std::vector<long long>& offs = h->wh_offs[k];
+                if (offs.empty() || g <= 0) return 0LL;
+                const size_t i = (size_t)(std::upper_bound(offs.begin(), offs.end(), g) - offs.begin()) - 1;
+                if (i + 1 >= offs.size()) return h->wh_cum[k].back();
+                int X = 0;
+                while ((X + 1) * (X + 2) / 2 <= k) ++X;
+                const int Y = k - X * (X + 1) / 2;
+                const std::vector<long long>& nppy = h->pl_nppsum[Y];
+                const long long jb = h->wh_kbase[k][i];
+                return h->wh_cum[k][i] + (long long)h->pl_npp[X][i] * (nppy[jb + (g - offs[i])] - nppy[jb]);
+            };
+            npq += prim_before(ge) - prim_before(gb);
+        }
+        *quartets = nq;
+        *prim_quartets = npq;
+    });
+}
+
 int qcg_set_graphs(qcg_handle* h, int enable)
 {
     if (!h) return QCG_ERR_ARG;
@@ -3285,8 +3370,7 @@ extern "C" int qcg_fock_jk_device_noalloc(qcg_handle* h, const double* d_D, doub
             wk.run = h->tuned_run[k];
             wk.cap = h->tuned_cap[k];
             wk.mol_active = h->d_mol_active;
-            wk.gbeg = wk.total * h->shard_rank / h->shard_world;
-            wk.gend = wk.total * (h->shard_rank + 1) / h->shard_world;
+            shard_range(h, k, wk.gbeg, wk.gend);
             if (wk.gend <= wk.gbeg) continue;
             wk.nshell = h->nshell;
             wk.pmask = h->d_pmask;
