@@ -279,6 +279,19 @@ int qcg_mlp_loss_grad(qcg_mlp* m, int rows, const float* d_x, const float* d_tar
 /* one Adam step with decoupled weight decay on the last gradient */
 int qcg_mlp_adam(qcg_mlp* m, float lr, float beta1, float beta2, float eps, float weight_decay);
 
+/* ---- symmetry-adapted (SALC) blocks ----------------------------------------------------------- */
+/* qchem's WholeSystemFock_IBS face of a symmetry-adapted basis (src/BasisSet/Orbital_HF_IBS.C:75-87,
+ * src/BasisSet/Imp/SymmetryAdapted_IBS.C:45-70): one irrep block is m functions, the columns of O (nbf x m,
+ * row-major, over the handle's Cartesian AO functions).  J and K are linear in D, so the whole system's J
+ * and K come from ONE AO build of the summed density: each block folds its density up (qcg_salc_fold), the
+ * AO build runs once (qcg_fock_jk), and each block slices its part out (qcg_salc_slice).  Both products run
+ * on the GPU (cuBLAS, the handle's stream); the results are symmetrised, as the reference's SymCopy does.
+ * Host buffers, synchronous; single-molecule handles. */
+/* Dao (nbf x nbf) += sym(O D O^T), D (m x m) the block's density */
+int qcg_salc_fold(qcg_handle* h, int m, const double* O, const double* D, double* Dao);
+/* Fab (m x m) += sym(O^T Fao O), Fao (nbf x nbf) an AO matrix (J, K or a Fock matrix) */
+int qcg_salc_slice(qcg_handle* h, int m, const double* O, const double* Fao, double* Fab);
+
 /* ---- measurement ----------------------------------------------------------------------------- */
 /* FP64 fused-multiply-add throughput of the current device (TFLOP/s) from a pure-DFMA kernel timed over
  * `reps` launches: the roofline denominator of the ERI kernels.  No reference counterpart. */

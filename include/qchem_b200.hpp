@@ -11,6 +11,8 @@
 // engine builds J and K together in one GPU pass and keeps them for the density it last saw, so the
 // second call costs nothing.  Status codes from the C ABI become qcg::Error exceptions here, the way the
 // reference's own substrate throws std::runtime_error (Internal/Imp/Orbital_ERI4_IBS.C:19-32).
+// qcg::SalcBlock adds the symmetry-adapted faces (src/BasisSet/Imp/SymmetryAdapted_IBS.C:45-140): one irrep
+// block of SALC columns over a FockEngine, sharing its one AO build.
 #pragma once
 #include <cstring>
 #include <stdexcept>
@@ -110,7 +112,7 @@ public:
         if (nonzero(Di)) add(Kj, Di, true);
     }
 
-    qcg_handle* handle() { return h_; }
+    qcg_handle* handle() const { return h_; }
 
 private:
     void check(int rc)
@@ -146,6 +148,89 @@ private:
     qcg_handle* h_ = nullptr;
     int n_ = 0;
     std::vector<double> D_, J_, K_;
+};
+
+// One irrep block of a symmetry-adapted (SALC) basis over an AO FockEngine: qchem's SymmetryAdapted_IBS
+// (src/BasisSet/Imp/SymmetryAdapted_IBS.C:45-140).  The block is m functions, the columns of O (AODimension()
+// x m, row-major).  J and K are linear in D, so every block shares ONE AO build: the partner block folds its
+// density up (AddAODensity, Dao += sym(O D O^T)), the engine builds J or K of Dao (MakeAOFock), and this
+// block slices its part out (SliceAOFock, Fab += sym(O^T Fao O)).  The folds and slices run on the GPU.
+class SalcBlock
+{
+public:
+    SalcBlock(FockEngine& ao, std::vector<double> O, int m) : ao_(ao), O_(std::move(O)), m_(m)
+    {
+        if (m < 1 || (size_t)m > ao.AODimension() || O_.size() != ao.AODimension() * (size_t)m)
+            throw Error(QCG_ERR_ARG, "O must be AODimension() x m with 1 <= m <= AODimension()");
+    }
+    size_t Dimension() const { return (size_t)m_; }
+
+    // WholeSystemFock_IBS<double>
+    size_t AODimension() const { return ao_.AODimension(); }
+    void AddAODensity(double* Dao, const double* D) const
+    {
+        check(qcg_salc_fold(ao_.handle(), m_, O_.data(), D, Dao));
+    }
+    void MakeAOFock(const double* Dao, bool exchange, double* out) const
+    {
+        const size_t nn = AODimension() * AODimension();
+        if (!nonzero(Dao, nn))   // the reference's pre-screen: an empty density builds nothing
+        {
+            std::memset(out, 0, nn * sizeof(double));
+            return;
+        }
+        ao_.MakeAOFock(Dao, exchange, out);
+    }
+    void SliceAOFock(double* Fab, const double* Fao) const
+    {
+        check(qcg_salc_slice(ao_.handle(), m_, O_.data(), Fao, Fab));
+    }
+    // sym(O^T M O) of an AO matrix (overlap, kinetic, nuclear), into out (m x m)
+    void Transform(const double* M, double* out) const
+    {
+        std::memset(out, 0, (size_t)m_ * m_ * sizeof(double));
+        SliceAOFock(out, M);
+    }
+
+    // Orbital_HF_IBS<double>: the partner cd folds its block's density up, one AO build, this block slices
+    void AccumulateDirect(double* Jab, const double* Dcd, const SalcBlock* cd) const { pair(Jab, Dcd, cd, false); }
+    void AccumulateExchange(double* Kab, const double* Dcd, const SalcBlock* cd) const { pair(Kab, Dcd, cd, true); }
+    void AccumulateDirectBoth(double* Ji, double* Jj, const double* Di, const double* Dj, const SalcBlock* cd) const
+    {
+        if (nonzero(Dj, cd->Dimension() * cd->Dimension())) AccumulateDirect(Ji, Dj, cd);
+        if (nonzero(Di, Dimension() * Dimension())) cd->AccumulateDirect(Jj, Di, this);
+    }
+    void AccumulateExchangeBoth(double* Ki, double* Kj, const double* Di, const double* Dj, const SalcBlock* cd) const
+    {
+        if (nonzero(Dj, cd->Dimension() * cd->Dimension())) AccumulateExchange(Ki, Dj, cd);
+        if (nonzero(Di, Dimension() * Dimension())) cd->AccumulateExchange(Kj, Di, this);
+    }
+
+private:
+    void check(int rc) const
+    {
+        if (rc != QCG_OK) throw Error(rc, qcg_last_error(ao_.handle()));
+    }
+    static bool nonzero(const double* X, size_t n)
+    {
+        for (size_t k = 0; k < n; ++k)
+            if (X[k] != 0.0) return true;
+        return false;
+    }
+    void pair(double* S, const double* Dcd, const SalcBlock* cd, bool exchange) const
+    {
+        if (!cd) throw Error(QCG_ERR_ARG, "the partner block is needed to fold its density");
+        if (&cd->ao_ != &ao_) throw Error(QCG_ERR_ARG, "the partner block belongs to another AO engine");
+        const size_t nn = AODimension() * AODimension();
+        std::vector<double> Dao(nn, 0.0), F(nn);
+        cd->AddAODensity(Dao.data(), Dcd);
+        MakeAOFock(Dao.data(), exchange, F.data());
+        SliceAOFock(S, F.data());
+    }
+
+    FockEngine& ao_;
+    std::vector<double> O_;
+    int m_;
 };
 
 // Frees the device slabs, pinned staging, streams and events that destroyed engines left for reuse by the

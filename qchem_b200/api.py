@@ -43,7 +43,8 @@ EXPORTS = ["qcg_basis_create", "qcg_destroy", "qcg_last_error", "qcg_set_stream"
            "qcg_mlp_adam", "qcg_basis_create_batch", "qcg_nmol", "qcg_mol_nbf", "qcg_one_electron_batch",
            "qcg_rhf_batch", "qcg_set_graphs", "qcg_set_shard", "qcg_autotune_jk", "qcg_eri3_batch",
            "qcg_nbf_spherical", "qcg_spherical_transform", "qcg_fock_jk_spherical", "qcg_release_cache",
-           "qcg_set_eri_team_classes", "qcg_set_pair_subset", "qcg_set_jk_team_classes", "qcg_selftest_bounded_wait", "qcg_shard_work"]
+           "qcg_set_eri_team_classes", "qcg_set_pair_subset", "qcg_set_jk_team_classes", "qcg_selftest_bounded_wait", "qcg_shard_work",
+           "qcg_salc_fold", "qcg_salc_slice"]
 
 
 class QcgError(RuntimeError):
@@ -119,6 +120,8 @@ def lib():
     L.qcg_set_graphs.argtypes = [vp, i32]
     L.qcg_set_shard.argtypes = [vp, i32, i32]
     L.qcg_shard_work.argtypes = [vp, i32, i32, P(i64), P(i64)]
+    L.qcg_salc_fold.argtypes = [vp, i32, P(f64), P(f64), P(f64)]
+    L.qcg_salc_slice.argtypes = [vp, i32, P(f64), P(f64), P(f64)]
     L.qcg_autotune_jk.argtypes = [vp, vp, i32, P(i32), P(i32)]
     L.qcg_schwarz.argtypes = [vp, f64, P(f64)]
     L.qcg_fock_jk.argtypes = [vp, P(f64), P(f64), P(f64), i32, P(Stats)]
@@ -665,3 +668,84 @@ class OrbitalHFIBS:
 
     def SliceAOFock(self, Fab, Fao):
         Fab += Fao
+
+
+class SymmetryAdaptedIBS:
+    """One irrep block of a symmetry-adapted (SALC) basis over the AO engine: qchem's SymmetryAdapted_IBS
+    (src/BasisSet/Imp/SymmetryAdapted_IBS.C:45-140).  The block is m functions, the columns of O
+    (nbf x m, over the engine's Cartesian AO functions); `ao` is the whole-molecule HF face (OrbitalHFIBS)
+    whose one AO build every block shares.
+
+    WholeSystemFock_IBS:  AODimension(); AddAODensity(Dao, D): Dao += sym(O D O^T);
+                          MakeAOFock(Dao, exchange): the AO J or K of Dao (one build, memoised on Dao);
+                          SliceAOFock(Fab, Fao): Fab += sym(O^T Fao O).
+    Orbital_HF_IBS:       AccumulateDirect(Jab, Dcd, bs_cd): the partner bs_cd folds its block's density up,
+                          one AO build, this block slices (PairAOFock); AccumulateExchange likewise;
+                          the ...Both forms serve the pair as two slices, skipping a zero density.
+    Transform(M):         sym(O^T M O) of an AO matrix (overlap, kinetic, nuclear).
+    The folds and slices run on the GPU (qcg_salc_fold / qcg_salc_slice).
+    """
+
+    def __init__(self, ao: "OrbitalHFIBS", O, label: str = ""):
+        self.ao = ao
+        self.O = np.ascontiguousarray(O, dtype=np.float64)
+        n = ao.engine.nbf
+        if self.O.ndim != 2 or self.O.shape[0] != n or not 1 <= self.O.shape[1] <= n:
+            raise QcgError(QCG_ERR_ARG, f"O must be nbf x m with 1 <= m <= nbf (nbf = {n})")
+        self.m = self.O.shape[1]
+        self.label = label
+
+    def _h(self):
+        return self.ao.engine._h
+
+    # WholeSystemFock_IBS<double>
+    def AODimension(self) -> int:
+        return self.ao.engine.nbf
+
+    def AddAODensity(self, Dao, D):
+        D = _f64(D)
+        if Dao.dtype != np.float64 or not Dao.flags.c_contiguous:
+            raise QcgError(QCG_ERR_ARG, "Dao must be a C-contiguous float64 array")
+        self.ao.engine._check(lib().qcg_salc_fold(self._h(), self.m, _p(self.O), _p(D), _p(Dao)))
+
+    def MakeAOFock(self, Dao, exchange: bool):
+        if not np.any(Dao):
+            return np.zeros_like(_f64(Dao))   # the reference's pre-screen: an empty density builds nothing
+        return self.ao.MakeAOFock(Dao, exchange)
+
+    def SliceAOFock(self, Fab, Fao):
+        Fao = _f64(Fao)
+        if Fab.dtype != np.float64 or not Fab.flags.c_contiguous:
+            raise QcgError(QCG_ERR_ARG, "Fab must be a C-contiguous float64 array")
+        self.ao.engine._check(lib().qcg_salc_slice(self._h(), self.m, _p(self.O), _p(Fao), _p(Fab)))
+
+    def Transform(self, M):
+        out = np.zeros((self.m, self.m))
+        self.SliceAOFock(out, M)
+        return out
+
+    # Orbital_HF_IBS<double>
+    def PairAOFock(self, Dcd, bs_cd: "SymmetryAdaptedIBS", exchange: bool):
+        if not isinstance(bs_cd, SymmetryAdaptedIBS):
+            raise QcgError(QCG_ERR_ARG, "the HF partner basis has no whole-system Fock face")
+        Dao = np.zeros((self.AODimension(), self.AODimension()))
+        bs_cd.AddAODensity(Dao, Dcd)   # the partner folds with its own columns
+        return self.MakeAOFock(Dao, exchange)
+
+    def AccumulateDirect(self, Jab, Dcd, bs_cd):
+        self.SliceAOFock(Jab, self.PairAOFock(Dcd, bs_cd, False))
+
+    def AccumulateExchange(self, Kab, Dcd, bs_cd):
+        self.SliceAOFock(Kab, self.PairAOFock(Dcd, bs_cd, True))
+
+    def AccumulateDirectBoth(self, Ji, Jj, Di, Dj, cd):
+        if np.any(Dj):
+            self.AccumulateDirect(Ji, Dj, cd)
+        if np.any(Di):
+            cd.AccumulateDirect(Jj, Di, self)
+
+    def AccumulateExchangeBoth(self, Ki, Kj, Di, Dj, cd):
+        if np.any(Dj):
+            self.AccumulateExchange(Ki, Dj, cd)
+        if np.any(Di):
+            cd.AccumulateExchange(Kj, Di, self)

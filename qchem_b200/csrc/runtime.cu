@@ -339,6 +339,7 @@ struct qcg_handle
     double fp32_below = 0;   // qcg_set_fp32_bound: quartets with a smaller bound are evaluated in FP32
     int shard_rank = 0, shard_world = 1;   // qcg_set_shard: this handle's slice of every J/K build
     std::shared_ptr<void> sph;             // the spherical map, built on first use
+    std::shared_ptr<void> salc;            // cuBLAS handle and buffers of the symmetry-adapted faces
     int tuned_run[kNumQuartetClasses] = {}, tuned_cap[kNumQuartetClasses] = {};   // qcg_autotune_jk (0: default)
     double* d_dmaxD = nullptr;   // per shell-pair max |D| of a full build's density (mixed precision)
     long long work_quartets = 0, work_prim_quartets = 0;
@@ -2981,6 +2982,100 @@ const SphericalMap& spherical_map(qcg_handle* h)
 }
 }
 }   // namespace
+
+extern "C++" {
+namespace {
+// Device products of the symmetry-adapted (SALC) faces: one cuBLAS handle per qcg handle, on its stream,
+// and grow-only device buffers for O, the square operand, the intermediate and the result.
+struct SalcWork
+{
+    cublasHandle_t blas = nullptr;
+    double* buf[4] = {};
+    size_t cap[4] = {};
+    ~SalcWork()
+    {
+        for (double* p : buf) cudaFree(p);
+        if (blas) cublasDestroy(blas);
+    }
+    double* get(int i, size_t n)
+    {
+        if (n > cap[i])
+        {
+            cudaFree(buf[i]);
+            buf[i] = nullptr;
+            cap[i] = 0;
+            CK(cudaMalloc(&buf[i], n * sizeof(double)));
+            cap[i] = n;
+        }
+        return buf[i];
+    }
+};
+
+SalcWork& salc_work(qcg_handle* h)
+{
+    if (!h->salc)
+    {
+        auto w = std::make_shared<SalcWork>();
+        if (cublasCreate(&w->blas) != CUBLAS_STATUS_SUCCESS) throw Error{QCG_ERR_CUDA, "cublasCreate failed"};
+        h->salc = w;
+    }
+    SalcWork& w = *static_cast<SalcWork*>(h->salc.get());
+    cublasSetStream(w.blas, h->stream);
+    return w;
+}
+
+// fold (Dao += sym(O X O^T), X m x m) or slice (Out += sym(O^T X O), X n x n); O is n x m row-major, which
+// cuBLAS (column-major) sees as Oc = O^T, m x n
+void salc_product(qcg_handle* h, bool fold, int m, const double* O, const double* X, double* Out)
+{
+    const int n = h->nbf;
+    require(h->nmol == 1, "the symmetry-adapted faces take a single-molecule handle");
+    require(m >= 1 && m <= n, "need 1 <= m <= nbf columns");
+    require(O && X && Out, "null argument");
+    SalcWork& w = salc_work(h);
+    const size_t nm = (size_t)n * m, nx = fold ? (size_t)m * m : (size_t)n * n, no = fold ? (size_t)n * n : (size_t)m * m;
+    double* dO = w.get(0, nm);
+    double* dX = w.get(1, nx);
+    double* dT = w.get(2, nm);
+    double* dR = w.get(3, no);
+    CK(cudaMemcpyAsync(dO, O, nm * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(dX, X, nx * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    const double one = 1.0, zero = 0.0;
+    cublasStatus_t a, b;
+    if (fold)
+    {
+        // T = X Oc (m x n) = X O^T;  R = Oc^T T (n x n) = O X O^T
+        a = cublasDgemm(w.blas, CUBLAS_OP_N, CUBLAS_OP_N, m, n, m, &one, dX, m, dO, m, &zero, dT, m);
+        b = cublasDgemm(w.blas, CUBLAS_OP_T, CUBLAS_OP_N, n, n, m, &one, dO, m, dT, m, &zero, dR, n);
+    }
+    else
+    {
+        // T = X Oc^T (n x m) = X O;  R = Oc T (m x m) = O^T X O
+        a = cublasDgemm(w.blas, CUBLAS_OP_N, CUBLAS_OP_T, n, m, n, &one, dX, n, dO, m, &zero, dT, n);
+        b = cublasDgemm(w.blas, CUBLAS_OP_N, CUBLAS_OP_N, m, m, n, &one, dO, m, dT, n, &zero, dR, m);
+    }
+    if (a != CUBLAS_STATUS_SUCCESS || b != CUBLAS_STATUS_SUCCESS) throw Error{QCG_ERR_CUDA, "cublasDgemm failed"};
+    std::vector<double> R(no);
+    CK(cudaMemcpyAsync(R.data(), dR, no * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    const int k = fold ? n : m;
+    for (int i = 0; i < k; ++i)
+        for (int j = 0; j < k; ++j) Out[(size_t)i * k + j] += 0.5 * (R[(size_t)i * k + j] + R[(size_t)j * k + i]);
+}
+}   // namespace
+}   // extern "C++"
+
+int qcg_salc_fold(qcg_handle* h, int m, const double* O, const double* D, double* Dao)
+{
+    if (!h) return QCG_ERR_ARG;
+    return guarded(h, [&] { salc_product(h, true, m, O, D, Dao); });
+}
+
+int qcg_salc_slice(qcg_handle* h, int m, const double* O, const double* Fao, double* Fab)
+{
+    if (!h) return QCG_ERR_ARG;
+    return guarded(h, [&] { salc_product(h, false, m, O, Fao, Fab); });
+}
 
 int qcg_spherical_transform(qcg_handle* h, double* T)
 {
