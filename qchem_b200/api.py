@@ -44,7 +44,7 @@ EXPORTS = ["qcg_basis_create", "qcg_destroy", "qcg_last_error", "qcg_set_stream"
            "qcg_rhf_batch", "qcg_set_graphs", "qcg_set_shard", "qcg_autotune_jk", "qcg_eri3_batch",
            "qcg_nbf_spherical", "qcg_spherical_transform", "qcg_fock_jk_spherical", "qcg_release_cache",
            "qcg_set_eri_team_classes", "qcg_set_pair_subset", "qcg_set_jk_team_classes", "qcg_selftest_bounded_wait", "qcg_shard_work",
-           "qcg_salc_fold", "qcg_salc_slice"]
+           "qcg_salc_fold", "qcg_salc_slice", "qcg_set_jk_warp_classes"]
 
 
 class QcgError(RuntimeError):
@@ -103,6 +103,7 @@ def lib():
     L.qcg_set_stream.argtypes = [vp, vp]
     L.qcg_set_eri_team_classes.argtypes = [vp, i64]
     L.qcg_set_jk_team_classes.argtypes = [vp, i64]
+    L.qcg_set_jk_warp_classes.argtypes = [vp, i64]
     L.qcg_set_pair_subset.argtypes = [vp, vp]
     L.qcg_set_memory_limit.argtypes = [vp, i64]
     L.qcg_nbf.argtypes = [vp, P(i32)]
@@ -364,6 +365,11 @@ class Engine:
     def set_jk_team_classes(self, mask: int):
         """J/K-build classes (bit k: class k) run by the team kernel; -1 restores the default."""
         self._check(lib().qcg_set_jk_team_classes(self._h, ctypes.c_longlong(mask)))
+
+    def set_jk_warp_classes(self, mask: int):
+        """J/K-build classes (bit k: class k) run in the warp-shared form (the team form takes precedence);
+        -1 restores the default."""
+        self._check(lib().qcg_set_jk_warp_classes(self._h, ctypes.c_longlong(mask)))
 
     def set_pair_subset(self, mask):
         """Later J/K builds evaluate only quartets whose two shell pairs are both in the subset (mask: nshell x

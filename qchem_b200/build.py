@@ -86,6 +86,18 @@ def _jk_team_mask() -> int:
     return sum(1 << k for k in JK_TEAM_CLASSES)
 
 
+# classes whose direct J/K build runs in the warp-shared form by default (QCG_JK_WARP_MASK selects others):
+# (ps|ss), (ps|ps), (pp|ss), (pp|ps), (ds|ss), (ds|ps), (ds|pp), (ds|ds), (dp|ss), (dp|ps).  Measured class
+# by class on a B200 on the uncontracted 32-water build, the warp-shared form took 0.49-0.98x the
+# thread-per-quartet kernel's time on these ten ((ds|ps) 209 vs 428 ms, (dp|ps) 354 vs 511 ms); on (ss|ss),
+# (pp|pp), (dp|ds) and (dd|ss) it took 1.06-1.26x.
+JK_WARP_CLASSES = (1, 2, 3, 4, 6, 7, 8, 9, 10, 11)
+
+
+def _jk_warp_mask() -> int:
+    return sum(1 << k for k in JK_WARP_CLASSES)
+
+
 def _jobs():
     core = _headers(["md_core.cuh", "qcg_internal.h"])
     jobs = []
@@ -113,7 +125,8 @@ def _jobs():
     for name in ("registry.cu", "fock_kernels.cu", "runtime.cu", "mlp.cu"):
         s = os.path.join(CSRC, name)
         defs = HOST_OMP + [f"-DQCG_TEAM_DEFAULT_MASK={_team_mask():#x}u",
-                           f"-DQCG_JK_TEAM_DEFAULT_MASK={_jk_team_mask():#x}u"] if name == "runtime.cu" else []
+                           f"-DQCG_JK_TEAM_DEFAULT_MASK={_jk_team_mask():#x}u",
+                           f"-DQCG_JK_WARP_DEFAULT_MASK={_jk_warp_mask():#x}u"] if name == "runtime.cu" else []
         key = _hash([_read(s)] + core + extra.get(name, []) + FLAGS + defs)
         jobs.append((s, defs, os.path.join(BUILD, f"{name[:-3]}_{key}.o")))
     return jobs

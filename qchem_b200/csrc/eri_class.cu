@@ -217,6 +217,19 @@ void QCG_NAME(launch_jk)(const JKWorkDev& w, const PairListDev& bra, const PairL
 }
 
 #if QCG_PREC == 64
+// the warp-shared form of the J/K build (jk_warp_kernel): one warp per work item, grid-stride
+void QCG_CAT(launch_jk_warp_, QCG_CLASS)(const JKWorkDev& w, const PairListDev& bra, const PairListDev& ket,
+                                          const PrimPairsDev& P, const int* f0, const double* D, double* J, double* K,
+                                          int n, const double* boys, const int* gbra, const int4* items,
+                                          long long nitems, cudaStream_t st, int nsm)
+{
+    if (nitems <= 0) return;
+    auto k = jk_warp_kernel<Cls, kThreads>;
+    prepare<jk_warp_kernel<Cls, kThreads>>();
+    k<<<(unsigned)grid_for(nitems * 32, nsm), kThreads, kSmem, st>>>(w, bra, ket, P, f0, D, J, K, n, boys, gbra,
+                                                                      items, nitems);
+}
+
 // Schwarz diagonals exist only for the diagonal classes (X == Y)
 void QCG_CAT(launch_schwarz_, QCG_CLASS)(const PairListDev& pl, const PrimPairsDev& P, double* Q, const double* boys,
                                          cudaStream_t st, int nsm)

@@ -520,6 +520,222 @@ __global__ void __launch_bounds__(THREADS) jk_kernel(JKWorkDev w, PairListDev br
     }
 }
 
+// ------------------------------------------------------------------------------------------------
+// The warp-shared form of the direct J/K build.  A warp takes up to 32 bra pairs (a b_l) that share their
+// first shell a -- lane l holds (a b_l) -- against one ket pair (c d) at a time.  Of the six digestion
+// targets of a quartet, three are then the same for every lane: J'(c d), K'(a c) and K'(a d).  Their lane
+// partial sums are added across the warp by shuffles and written by one lane each, so an L2 atomic per
+// lane becomes one per warp; only K'(b c) and K'(b d) stay per lane, and J'(a b) stays in registers over the
+// whole run of kets.  The ket's pair data and its density rows D(a, .) are the same for every lane (one
+// broadcast load each).  Lanes whose quartet is absent (past their bra pair's screened ket prefix, skipped
+// by jk_skip, or past the end of a short warp set) evaluate a valid quartet with weight 0, so that every
+// lane reaches the shuffles.  This replaces the same arithmetic as JKSink (qchem's MakeDirect /
+// MakeExchange, Molecule/IrrepBasisSet.C:138-183) with fewer memory operations.
+// ------------------------------------------------------------------------------------------------
+
+// Sum P values (P a power of two, <= 32) over the 32 lanes of a warp: in log2 P exchange steps each lane
+// keeps half of its values and adds its partner's copy of them, then the rest is a plain butterfly.  On
+// return every lane holds the warp's total of value (lane >> (5 - log2 P)); the lanes with
+// lane % (32 / P) == 0 are one writer per value.
+template <int P>
+__device__ __forceinline__ double warp_transpose_sum(double (&v)[P], int lane)
+{
+#pragma unroll
+    for (int m = P, o = 16; m > 1; m >>= 1, o >>= 1)
+    {
+        const bool up = (lane & o) != 0;
+#pragma unroll
+        for (int k = 0; k < m / 2; ++k)
+        {
+            const double send = up ? v[k] : v[k + m / 2];
+            const double keep = up ? v[k + m / 2] : v[k];
+            v[k] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+        }
+    }
+    double x = v[0];
+#pragma unroll
+    for (int o = 16 / P; o >= 1; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    return x;
+}
+
+constexpr int pow2_at_least(int v) { return v <= 1 ? 1 : 2 * pow2_at_least((v + 1) / 2); }
+
+template <int LA, int LB, int LC, int LD>
+struct WarpJKSink
+{
+    static constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD), NAB = NA * NB;
+    const double* __restrict__ D;
+    double* __restrict__ J;
+    double* __restrict__ K;
+    int n, fa, fb, fc, fd, lane;
+    double s;   // symmetry weight of this lane's quartet, 0 for an absent quartet
+    double jab[NAB];
+    double dls, jcd;
+    double das[NA], dal[NA], dbs[NB], dbl[NB];
+    double kac[NA], kad[NA], kbc[NB], kbd[NB];
+
+    __device__ __forceinline__ void set_bra(int fa_, int fb_)
+    {
+        fa = fa_;
+        fb = fb_;
+#pragma unroll
+        for (int k = 0; k < NAB; ++k) jab[k] = 0.0;
+    }
+    __device__ __forceinline__ void ket_begin(int ic, int id)
+    {
+        const int la = fc + ic, si = fd + id;
+        dls = __ldg(D + (size_t)la * n + si);
+        jcd = 0.0;
+#pragma unroll
+        for (int k = 0; k < NA; ++k)
+        {
+            das[k] = __ldg(D + (size_t)(fa + k) * n + si);
+            dal[k] = __ldg(D + (size_t)(fa + k) * n + la);
+            kad[k] = 0.0;
+            if (id == 0) kac[k] = 0.0;
+        }
+#pragma unroll
+        for (int k = 0; k < NB; ++k)
+        {
+            dbs[k] = __ldg(D + (size_t)(fb + k) * n + si);
+            dbl[k] = __ldg(D + (size_t)(fb + k) * n + la);
+            kbd[k] = 0.0;
+            if (id == 0) kbc[k] = 0.0;
+        }
+    }
+    __device__ __forceinline__ void operator()(int ia, int ib, int, int, double v)
+    {
+        const double w = s * v;
+        jab[ia * NB + ib] += w * dls;
+        jcd += w * __ldg(D + (size_t)(fa + ia) * n + fb + ib);
+        kac[ia] += w * dbs[ib];
+        kbc[ib] += w * das[ia];
+        kad[ia] += w * dbl[ib];
+        kbd[ib] += w * dal[ia];
+    }
+    // the shared targets of this ket component (and of its ket row at the row's end) across the warp
+    template <int V>
+    __device__ __forceinline__ void flush_shared(int la, int si)
+    {
+        constexpr int P = pow2_at_least(V);
+        constexpr int SHIFT = (P == 1 ? 5 : P == 2 ? 4 : P == 4 ? 3 : P == 8 ? 2 : P == 16 ? 1 : 0);
+        double v[P];
+        v[0] = jcd;
+#pragma unroll
+        for (int k = 0; k < NA; ++k) v[1 + k] = kad[k];
+        if constexpr (V > 1 + NA)
+        {
+#pragma unroll
+            for (int k = 0; k < NA; ++k) v[1 + NA + k] = kac[k];
+        }
+#pragma unroll
+        for (int k = V; k < P; ++k) v[k] = 0.0;
+        const double x = warp_transpose_sum<P>(v, lane);
+        const int idx = lane >> SHIFT;
+        if ((lane & ((1 << SHIFT) - 1)) != 0 || idx >= V || x == 0.0) return;
+        if (idx == 0) atomicAdd(J + (size_t)la * n + si, 2.0 * x);
+        else if (idx <= NA) atomicAdd(K + (size_t)(fa + idx - 1) * n + si, x);
+        else atomicAdd(K + (size_t)(fa + idx - 1 - NA) * n + la, x);
+    }
+    __device__ __forceinline__ void ket_end(int ic, int id)
+    {
+        const int la = fc + ic, si = fd + id;
+#pragma unroll
+        for (int k = 0; k < NB; ++k)
+            if (kbd[k] != 0.0) atomicAdd(K + (size_t)(fb + k) * n + si, kbd[k]);
+        if (id == ND - 1)
+        {
+#pragma unroll
+            for (int k = 0; k < NB; ++k)
+                if (kbc[k] != 0.0) atomicAdd(K + (size_t)(fb + k) * n + la, kbc[k]);
+            flush_shared<1 + 2 * NA>(la, si);
+        }
+        else
+            flush_shared<1 + NA>(la, si);
+    }
+    __device__ __forceinline__ void flush_bra()
+    {
+#pragma unroll
+        for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+            for (int ib = 0; ib < NB; ++ib)
+            {
+                const double x = jab[ia * NB + ib];
+                if (x != 0.0) atomicAdd(J + (size_t)(fa + ia) * n + fb + ib, 2.0 * x);
+            }
+    }
+};
+
+// items[t] = {first entry of the warp set in gbra, its lane count (<= 32), first ket, end ket}: the warp set
+// is gbra[x .. x + y), bra pairs sharing their first shell; the kets are positions [z, w) of every lane's
+// ket list (its molecule's part of the ket class, from kbase), each lane stopping at its own screened prefix
+template <class Cls, int THREADS>
+__global__ void __launch_bounds__(THREADS) jk_warp_kernel(JKWorkDev w, PairListDev bra, PairListDev ket,
+                                                          PrimPairsDev P, const int* __restrict__ shell_f0,
+                                                          const double* __restrict__ D, double* __restrict__ J,
+                                                          double* __restrict__ K, int n,
+                                                          const double* __restrict__ boys_table,
+                                                          const int* __restrict__ gbra, const int4* __restrict__ items,
+                                                          long long nitems)
+{
+    double* rs = r_slice<double>();
+    const int lane = threadIdx.x & 31;
+    const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const long long nwarp = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long t = warp; t < nitems; t += nwarp)
+    {
+        const int4 it = items[t];
+        const bool real = lane < it.y;
+        const int i = gbra[it.x + (real ? lane : 0)];
+        const int prefix = real ? (int)(w.offs[i + 1] - w.offs[i]) : 0;
+        const int jb = w.kbase ? w.kbase[i] : 0;   // the same for the whole set: one molecule
+        const int sa = bra.sa[i], sb = bra.sb[i];
+        WarpJKSink<Cls::LA, Cls::LB, Cls::LC, Cls::LD> sink;
+        sink.D = D;
+        sink.J = J;
+        sink.K = K;
+        sink.n = n;
+        sink.lane = lane;
+        bool on = true;
+        if (bra.mol)
+        {
+            const int m = bra.mol[i];
+            const long long o = w.mols.off[m];
+            sink.D = D + o;
+            sink.J = J + o;
+            sink.K = K + o;
+            sink.n = w.mols.n[m];
+            on = !(w.mol_active && !w.mol_active[m]);
+        }
+        sink.set_bra(shell_f0[sa], shell_f0[sb]);
+        const int oi = bra.ppo[i], ni = bra.npp[i];
+        const int nimax = __reduce_max_sync(0xffffffffu, ni);
+        for (int jj = it.z; jj < it.w; ++jj)
+        {
+            const int j = jb + jj;
+            const int sc = ket.sa[j], sd = ket.sb[j];
+            const bool act = real && on && jj < prefix && !jk_skip(w, bra, ket, i, j, sa, sb, sc, sd);
+            if (!__any_sync(0xffffffffu, act)) continue;
+            sink.fc = shell_f0[sc];
+            sink.fd = shell_f0[sd];
+            const double s =
+                (sa == sb ? 0.5 : 1.0) * (sc == sd ? 0.5 : 1.0) * ((w.same_class && i == j) ? 0.5 : 1.0);
+            const int oj = ket.ppo[j], nj = ket.npp[j];
+            for (int x = 0; x < nimax; ++x)
+            {
+                const PrimPairData ab = load_pp(P, oi + (x < ni ? x : ni - 1));
+                sink.s = (act && x < ni) ? s : 0.0;
+                for (int y = 0; y < nj; ++y)
+                {
+                    const PrimPairData cd = load_pp(P, oj + y);
+                    Cls::template quartet<double>(ab, cd, boys_table, rs, THREADS, sink);
+                }
+            }
+        }
+        sink.flush_bra();
+    }
+}
+
 // Launches of the chunked classes with too few quartets to fill the GPU: work item t = c * span32 + q
 // (span32 = the quartet count rounded up to a multiple of 32) runs ket-component chunk c of quartet
 // w.gbeg + q.  A warp's lanes share the chunk, and the chunks of one quartet run on different warps at the

@@ -111,6 +111,12 @@ using EriBatchLauncher = void (*)(const BasisDev&, const int4*, const int*, long
                                   cudaStream_t, int);
 using JKLauncher = void (*)(const JKWorkDev&, const PairListDev&, const PairListDev&, const PrimPairsDev&, const int*,
                             const double*, double*, double*, int, const double*, cudaStream_t, int);
+// the warp-shared J/K form (FP64): gbra = bra pairs grouped by first shell, items = {gbra start, lanes,
+// first ket, end ket}
+using JKWarpLauncher = void (*)(const JKWorkDev&, const PairListDev&, const PairListDev&, const PrimPairsDev&,
+                                const int*, const double*, double*, double*, int, const double*, const int*,
+                                const int4*, long long, cudaStream_t, int);
+extern const JKWarpLauncher kJKWarpLaunchers[kNumQuartetClasses];
 using SchwarzLauncher = void (*)(const PairListDev&, const PrimPairsDev&, double*, const double*, cudaStream_t, int);
 
 using EriBatch32Launcher = void (*)(const BasisDev&, const int4*, const int*, long long, float*, const double*,

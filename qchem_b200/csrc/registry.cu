@@ -1,5 +1,6 @@
 // registry.cu -- tables of the per-class launchers compiled in the 42 eri_class objects (21 classes x FP64/FP32)
-// and the 21 eri_team objects (the team form of the FP64 ERI batches).
+// and the 21 eri_team objects (the team form of the FP64 ERI batches); the warp-shared J/K form is in the
+// FP64 eri_class objects.
 #include "eri_team_iface.h"
 #include "qcg_internal.h"
 
@@ -20,7 +21,10 @@ namespace qcg {
     TeamShape team_shape_##k(int);                                                                                  \
     void launch_jk_team_##k(const JKWorkDev&, const PairListDev&, const PairListDev&, const PrimPairsDev&,          \
                             const int*, const double*, double*, double*, int, const double*, const TeamScratchDev&, \
-                            const TeamShape&, cudaStream_t);
+                            const TeamShape&, cudaStream_t);                                                        \
+    void launch_jk_warp_##k(const JKWorkDev&, const PairListDev&, const PairListDev&, const PrimPairsDev&,          \
+                            const int*, const double*, double*, double*, int, const double*, const int*,            \
+                            const int4*, long long, cudaStream_t, int);
 QCG_DECL(0) QCG_DECL(1) QCG_DECL(2) QCG_DECL(3) QCG_DECL(4) QCG_DECL(5) QCG_DECL(6) QCG_DECL(7) QCG_DECL(8)
 QCG_DECL(9) QCG_DECL(10) QCG_DECL(11) QCG_DECL(12) QCG_DECL(13) QCG_DECL(14) QCG_DECL(15) QCG_DECL(16)
 QCG_DECL(17) QCG_DECL(18) QCG_DECL(19) QCG_DECL(20)
@@ -42,6 +46,12 @@ const JKTeamLauncher kJKTeamLaunchers[kNumQuartetClasses] = {
     launch_jk_team_10, launch_jk_team_11, launch_jk_team_12, launch_jk_team_13, launch_jk_team_14,
     launch_jk_team_15, launch_jk_team_16, launch_jk_team_17, launch_jk_team_18, launch_jk_team_19,
     launch_jk_team_20};
+const JKWarpLauncher kJKWarpLaunchers[kNumQuartetClasses] = {
+    launch_jk_warp_0,  launch_jk_warp_1,  launch_jk_warp_2,  launch_jk_warp_3,  launch_jk_warp_4,
+    launch_jk_warp_5,  launch_jk_warp_6,  launch_jk_warp_7,  launch_jk_warp_8,  launch_jk_warp_9,
+    launch_jk_warp_10, launch_jk_warp_11, launch_jk_warp_12, launch_jk_warp_13, launch_jk_warp_14,
+    launch_jk_warp_15, launch_jk_warp_16, launch_jk_warp_17, launch_jk_warp_18, launch_jk_warp_19,
+    launch_jk_warp_20};
 const EriTeamLauncher kEriTeamLaunchers[kNumQuartetClasses] = {
     launch_eri_team_0,  launch_eri_team_1,  launch_eri_team_2,  launch_eri_team_3,  launch_eri_team_4,
     launch_eri_team_5,  launch_eri_team_6,  launch_eri_team_7,  launch_eri_team_8,  launch_eri_team_9,

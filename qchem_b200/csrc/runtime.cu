@@ -336,6 +336,13 @@ struct qcg_handle
     std::vector<long long> wh_offs[kNumQuartetClasses], wh_cum[kNumQuartetClasses];
     std::vector<int> wh_kbase[kNumQuartetClasses];
     std::vector<long long> pl_nppsum[kNumPairClasses];
+    // the warp-shared J/K form (jk_warp_kernel), per class, built on first use after each screening: bra pairs
+    // grouped by first shell and the work items over them
+    int* d_wgbra[kNumQuartetClasses] = {};
+    int4* d_witems[kNumQuartetClasses] = {};
+    long long nwitems[kNumQuartetClasses] = {};
+    bool witems_ready[kNumQuartetClasses] = {};
+    long long jk_warp_mask = -1;   // qcg_set_jk_warp_classes; -1: the process default
     double fp32_below = 0;   // qcg_set_fp32_bound: quartets with a smaller bound are evaluated in FP32
     int shard_rank = 0, shard_world = 1;   // qcg_set_shard: this handle's slice of every J/K build
     std::shared_ptr<void> sph;             // the spherical map, built on first use
@@ -1961,6 +1968,60 @@ void shard_range(const qcg_handle* h, int k, long long& gbeg, long long& gend)
     gend = shard_cut(h, k, h->shard_rank + 1, h->shard_world);
 }
 
+// kets per work item of the warp-shared form: J'(a b) leaves the registers once per item
+constexpr int kWarpItemKets = 256;
+
+// The warp-shared form's work of class k: the class's bra pairs that have quartets, grouped by first shell
+// (one shell belongs to one molecule; within a group the pair list's order, Q descending, so that a warp's
+// lanes have similar screened ket prefixes), cut into warp sets of up to 32 pairs, and each set's kets
+// [0, its longest prefix) cut into items of kWarpItemKets.  Built once per screening, before any capture.
+void warp_items(qcg_handle* h, int k)
+{
+    if (h->witems_ready[k]) return;
+    int X = 0;
+    while ((X + 1) * (X + 2) / 2 <= k) ++X;
+    const std::vector<long long>& offs = h->wh_offs[k];
+    const std::vector<int>& sa = h->pl_sa[X];
+    std::vector<int> ord;
+    for (int i = 0; i + 1 < (int)offs.size(); ++i)
+        if (offs[i + 1] > offs[i]) ord.push_back(i);
+    std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return sa[x] < sa[y]; });
+    std::vector<int4> items;
+    for (size_t g0 = 0; g0 < ord.size();)
+    {
+        size_t g1 = g0;
+        while (g1 < ord.size() && sa[ord[g1]] == sa[ord[g0]]) ++g1;
+        for (size_t s0 = g0; s0 < g1; s0 += 32)
+        {
+            const int cnt = (int)std::min<size_t>(32, g1 - s0);
+            long long maxp = 0;
+            for (int l = 0; l < cnt; ++l) maxp = std::max(maxp, offs[ord[s0 + l] + 1] - offs[ord[s0 + l]]);
+            for (long long j0 = 0; j0 < maxp; j0 += kWarpItemKets)
+                items.push_back(make_int4((int)s0, cnt, (int)j0, (int)std::min<long long>(maxp, j0 + kWarpItemKets)));
+        }
+        g0 = g1;
+    }
+    h->d_wgbra[k] = ord.empty() ? nullptr : h->upload(ord);
+    h->d_witems[k] = items.empty() ? nullptr : h->upload(items);
+    h->nwitems[k] = (long long)items.size();
+    h->witems_ready[k] = true;
+}
+
+#ifndef QCG_JK_WARP_DEFAULT_MASK
+#define QCG_JK_WARP_DEFAULT_MASK 0u
+#endif
+// The classes whose direct J/K build runs in the warp-shared form: the build's choice
+// (QCG_JK_WARP_DEFAULT_MASK), unless QCG_JK_WARP_MASK in the environment names others (read once; *forced
+// then true).
+unsigned jk_warp_mask_default(bool* forced)
+{
+    static const char* const env = std::getenv("QCG_JK_WARP_MASK");
+    static const bool from_env = env && *env;
+    static const unsigned mask = from_env ? (unsigned)std::strtoul(env, nullptr, 0) : (unsigned)(QCG_JK_WARP_DEFAULT_MASK);
+    if (forced) *forced = from_env;
+    return mask;
+}
+
 bool team_scratch(qcg_handle* h, int k, TeamScratchDev& scr, TeamShape& sh);
 unsigned jk_team_mask_default(bool* forced);
 // smallest per-rank quartet count of a class for the build's default team form (2^20: ~220 groups of 32
@@ -2027,6 +2088,23 @@ void jk_device(qcg_handle* h, const double* dD, double* dJ, double* dK, int flag
     }
     for (int k = 0; k < kNumQuartetClasses; ++k)   // the buffer may have grown after an earlier class's lookup
         if (team_k[k]) team_scratch(h, k, team_scr[k], team_sh[k]);
+    // classes in the warp-shared form (FP64 band, one rank, not deterministic; the team form comes first);
+    // their work items are built here, before any capture.  The build's default applies to full builds of
+    // classes with at least kJKTeamMinQuartets quartets: under density screening a warp evaluates every
+    // quartet that one of its lanes needs, where the thread-per-quartet form skips each one alone.  A mask
+    // set by qcg_set_jk_warp_classes or QCG_JK_WARP_MASK applies to every build.
+    bool warp_forced = h->jk_warp_mask >= 0;
+    const unsigned warp_mask =
+        warp_forced ? (unsigned)h->jk_warp_mask : jk_warp_mask_default(&warp_forced);
+    bool warp_k[kNumQuartetClasses] = {};
+    for (int k = 0; k < kNumQuartetClasses; ++k)
+        if (((warp_mask >> k) & 1u) && !team_k[k] && h->work[k].total > 0 && h->shard_world == 1 &&
+            !(flags & QCG_JK_DETERMINISTIC) &&
+            (warp_forced || (dmax == nullptr && dthr <= 0.0 && h->work[k].total >= kJKTeamMinQuartets)))
+        {
+            warp_items(h, k);
+            warp_k[k] = h->nwitems[k] > 0;
+        }
     // QCG_JK_DETERMINISTIC: J' and K' as integer accumulator pairs (the low words after the nn high ones),
     // every quartet in FP64
     const bool det = (flags & QCG_JK_DETERMINISTIC) != 0;
@@ -2065,6 +2143,13 @@ void jk_device(qcg_handle* h, const double* dD, double* dJ, double* dK, int flag
                 if (team_k[k])
                     kJKTeamLaunchers[k](wk, h->pl_dev[X], h->pl_dev[Y], h->pp_dev, h->d_f0, dD, h->d_Jp, h->d_Kp, n,
                                         h->d_boys, team_scr[k], team_sh[k], h->side[0]);
+                else if (warp_k[k])
+                {
+                    kJKWarpLaunchers[k](wk, h->pl_dev[X], h->pl_dev[Y], h->pp_dev, h->d_f0, dD, h->d_Jp, h->d_Kp, n,
+                                        h->d_boys, h->d_wgbra[k], h->d_witems[k], h->nwitems[k], h->side[slot],
+                                        h->nsm);
+                    slot = (slot + 1) % qcg_handle::kSide;
+                }
                 else
                 {
                     kJKLaunchers[k](wk, h->pl_dev[X], h->pl_dev[Y], h->pp_dev, h->d_f0, dD, h->d_Jp, h->d_Kp, n,
@@ -2698,6 +2783,12 @@ int qcg_schwarz(qcg_handle* h, double thresh, double* Q)
                 {
                     h->release((void*)h->work[k].offs);
                     if (h->work[k].kbase) h->release((void*)h->work[k].kbase);
+                    if (h->d_wgbra[k]) h->release(h->d_wgbra[k]);
+                    if (h->d_witems[k]) h->release(h->d_witems[k]);
+                    h->d_wgbra[k] = nullptr;
+                    h->d_witems[k] = nullptr;
+                    h->nwitems[k] = 0;
+                    h->witems_ready[k] = false;
                 }
                 h->screened = false;
             }
@@ -2825,6 +2916,16 @@ int qcg_shard_work(qcg_handle* h, int rank, int world, long long* quartets, long
         }
         *quartets = nq;
         *prim_quartets = npq;
+    });
+}
+
+int qcg_set_jk_warp_classes(qcg_handle* h, long long mask)
+{
+    if (!h) return QCG_ERR_ARG;
+    return guarded(h, [&] {
+        require(mask >= -1 && mask < (1LL << kNumQuartetClasses), "mask: -1 or bits of the 21 classes");
+        h->jk_warp_mask = mask;
+        h->drop_graphs();
     });
 }
 
