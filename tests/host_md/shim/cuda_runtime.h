@@ -74,3 +74,9 @@ inline long long __double_as_longlong(double d)
     return r;
 }
 inline void __syncthreads() {}
+// Warp collectives for a warp of one lane (the host harness runs one thread): the shuffle returns the
+// lane's own value and the votes and reductions see that lane alone.  Only the warp-shared J/K kernel uses
+// them, and the harness compiles it without running it.
+inline double __shfl_xor_sync(unsigned, double v, int) { return v; }
+inline int __reduce_max_sync(unsigned, int v) { return v; }
+inline int __any_sync(unsigned, int p) { return p != 0; }
