@@ -182,7 +182,7 @@ int qcg_set_graphs(qcg_handle* h, int enable);
 int qcg_set_eri_team_classes(qcg_handle* h, long long mask);
 /* The same choice for the direct J/K build (bit k: class k of the work lists): the team kernel, whose CTAs
  * digest each group's integral blocks into J and K, or the thread-per-quartet kernel; -1 (default): the
- * library's choice -- the team form for the (dd|xx), (dp|dp) and (dp|pp) classes of a build with at least
+ * library's choice -- the team form for the (dd|xx) classes except (dd|ss), and (dp|dp), of a build with at least
  * 2^20 quartets in the class -- or QCG_JK_TEAM_MASK in the environment (a mask set here or there applies at
  * any size).  Same J and K to rounding (bit for bit under QCG_JK_DETERMINISTIC only within one form).  No
  * reference counterpart. */
@@ -192,7 +192,7 @@ int qcg_set_jk_team_classes(qcg_handle* h, long long mask);
  * pair at a time, so that the J'(cd), K'(ac) and K'(ad) contributions of its lanes are added by warp
  * shuffles and written once per warp instead of once per lane.  FP64 builds of one rank (not with
  * qcg_set_shard or QCG_JK_DETERMINISTIC).  -1 (default): the library's choice -- the (ps|ss), (ps|ps),
- * (pp|ss), (pp|ps), (ds|xx), (dp|ss) and (dp|ps) classes of full builds with at least 2^20 quartets in the
+ * (pp|ss), (pp|ps), (ds|xx), (dp|ss), (dp|ps) and (dp|pp) classes of full builds with at least 2^20 quartets in the
  * class -- or QCG_JK_WARP_MASK in the environment (a mask set here or there applies to every build).  Same J
  * and K to rounding.  No reference counterpart. */
 int qcg_set_jk_warp_classes(qcg_handle* h, long long mask);

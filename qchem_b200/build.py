@@ -76,10 +76,12 @@ def _team_mask() -> int:
 
 
 # classes whose direct J/K build runs in the team form by default (QCG_JK_TEAM_MASK selects others at run time):
-# (dd|dd), (dd|dp), (dd|ds), (dd|pp), (dd|ps), (dp|dp), (dp|pp).  Measured class by class on a B200 on the
-# uncontracted 32-water build (1824 functions), the team form took 0.48-0.91x the thread-per-quartet kernel's
-# time on these seven ((dd|dd) 43 vs 89 ms, (dp|dp) 529 vs 823 ms); on the others it took 1.07-4.7x.
-JK_TEAM_CLASSES = (12, 14, 16, 17, 18, 19, 20)
+# (dd|dd), (dd|dp), (dd|ds), (dd|pp), (dd|ps), (dp|dp).  Measured class by class on a B200 on the
+# uncontracted 32-water build (1824 functions), the team form took 0.47-0.93x the thread-per-quartet kernel's
+# time on these six ((dd|dd) 43 vs 92 ms, (dp|dp) 528 vs 826 ms) and 0.31-0.76x the warp-shared form's; on
+# (dp|pp) the warp-shared form is faster still (999 vs 1231 ms), and on the others the team form took
+# 1.07-4.7x the thread-per-quartet time.
+JK_TEAM_CLASSES = (14, 16, 17, 18, 19, 20)
 
 
 def _jk_team_mask() -> int:
@@ -87,11 +89,12 @@ def _jk_team_mask() -> int:
 
 
 # classes whose direct J/K build runs in the warp-shared form by default (QCG_JK_WARP_MASK selects others):
-# (ps|ss), (ps|ps), (pp|ss), (pp|ps), (ds|ss), (ds|ps), (ds|pp), (ds|ds), (dp|ss), (dp|ps).  Measured class
-# by class on a B200 on the uncontracted 32-water build, the warp-shared form took 0.49-0.98x the
-# thread-per-quartet kernel's time on these ten ((ds|ps) 209 vs 428 ms, (dp|ps) 354 vs 511 ms); on (ss|ss),
-# (pp|pp), (dp|ds) and (dd|ss) it took 1.06-1.26x.
-JK_WARP_CLASSES = (1, 2, 3, 4, 6, 7, 8, 9, 10, 11)
+# (ps|ss), (ps|ps), (pp|ss), (pp|ps), (ds|ss), (ds|ps), (ds|pp), (ds|ds), (dp|ss), (dp|ps), (dp|pp).
+# Measured class by class on a B200 on the uncontracted 32-water build, the warp-shared form took 0.49-0.98x
+# the thread-per-quartet kernel's time on these eleven ((ds|ps) 209 vs 428 ms, (dp|ps) 354 vs 511 ms,
+# (dp|pp) 999 vs 1345 ms, where the team form took 1231 ms); on (ss|ss), (pp|pp), (dp|ds) and (dd|ss) it took
+# 1.06-1.26x.
+JK_WARP_CLASSES = (1, 2, 3, 4, 6, 7, 8, 9, 10, 11, 12)
 
 
 def _jk_warp_mask() -> int:
