@@ -71,8 +71,10 @@ typedef struct qcg_scf_params {
     double diis_svtol;        /* default 5e-9 */
     int incremental;          /* 0 (default): full FP64 J/K every iteration.  1: after a full build, build
                                  J[D_k - D_k-1], K[...] with density-weighted Schwarz screening and add them
-                                 to the previous J, K; full rebuild every rebuild_every iterations and once
-                                 more on convergence (the reported energy is from a full build) */
+                                 to the previous J, K; full rebuild every rebuild_every iterations, for every
+                                 iteration once |dE| < 1000 de_tol (each screened build adds its own small
+                                 error), and once more on convergence (the reported energy is from a full
+                                 build) */
     double inc_thresh;        /* skip a quartet of an incremental build when Q_ab Q_cd max|dD| < inc_thresh
                                  (default 1e-11) */
     int rebuild_every;        /* default 8 */

@@ -3350,6 +3350,10 @@ int qcg_rhf(qcg_handle* h, int natom, const double* Z, const double* R, int nele
         const bool inc = prm.incremental != 0;
         int since_full = 0, nfull = 0, ninc = 0, n32 = 0;
         bool force_full = true;
+        // the final phase of an incremental SCF: full builds once |dE| is within 1000x the tolerance.  Each
+        // density-screened build adds its own small error (skipped quartets below inc_thresh), about 1e-8 Eh
+        // at 456 functions of this even-tempered basis, which would keep |dE| above de_tol for good.
+        bool inc_final = false;
         // precision schedule: until the DIIS error first falls below fp32_switch, quartets whose density-
         // weighted bound is below fp32_scale * (previous DIIS error) are FP32; then FP64 (quartets below
         // fp32_below still FP32).  The build that confirms convergence is always all-FP64.  A quartet's FP32
@@ -3379,7 +3383,7 @@ int qcg_rhf(qcg_handle* h, int natom, const double* Z, const double* R, int nele
         {
             const auto c0 = clk::now();
             qcg_stats st{};
-            const bool full = !inc || force_full || since_full >= prm.rebuild_every || exact_next;
+            const bool full = !inc || inc_final || force_full || since_full >= prm.rebuild_every || exact_next;
             const double band = exact_next ? 0.0 : (fp32_phase ? fp32_scale * En_prev : prm.fp32_below);
             exact_next = false;
             if (band > 0) ++n32;
@@ -3460,6 +3464,11 @@ int qcg_rhf(qcg_handle* h, int natom, const double* Z, const double* R, int nele
                 std::fprintf(stderr, "qcg_rhf it %3d  E %.12f  dE %+.3e  [F,D] %.3e  %s  fp32 below %.2e\n", it, sc.E,
                              sc.E - sc.Eold, sc.En, full ? "full" : "incr", band);
             En_prev = sc.En;
+            if (inc && !inc_final && it > 1 && std::fabs(sc.E - sc.Eold) < 1e3 * prm.de_tol)
+            {
+                inc_final = true;
+                force_full = true;
+            }
             if (fp32_phase && it > 1 && sc.En < prm.fp32_switch)
             {
                 fp32_phase = false;   // FP64 from here on, starting from a full rebuild

@@ -43,3 +43,18 @@ def test_incremental_rebuild_every_iteration_equals_plain_trajectory():
     b = api.Engine(sh).rhf(mol, incremental=True, rebuild_every=0)
     assert b["incremental_builds"] == 0 and b["iterations"] == a["iterations"]
     assert abs(a["energy"] - b["energy"]) < 1e-12
+
+
+@pytest.mark.parametrize("open_diis", [False, True])
+def test_incremental_scf_converges_on_the_water8_cluster(open_diis):
+    """456 functions: every density-screened build adds an error of about 1e-8 Eh, more than the 1e-10 Eh
+    convergence test allows, so the incremental SCF must finish on full builds (once |dE| < 1000 de_tol) and
+    reach the plain SCF's energy instead of wandering until the iteration limit."""
+    mol = W.water_cluster(nx=2, ny=2, nz=2, seed=W.SEED0 + 3650)
+    sh = B.even_tempered(mol)
+    kw = {"diis_fdmax": 1e6} if open_diis else {}
+    plain = api.Engine(sh).rhf(mol)
+    inc = api.Engine(sh).rhf(mol, incremental=True, **kw)
+    assert plain["converged"] and inc["converged"]
+    assert inc["incremental_builds"] > 0
+    assert abs(plain["energy"] - inc["energy"]) <= E_TOL, (plain["energy"], inc["energy"])
