@@ -45,6 +45,11 @@ def lib():
         L.orc_rhf.argtypes = [vp, i32, P(f64), P(f64), i32, i32, f64, f64, i32, i32, P(f64), P(i32), P(f64),
                               P(f64)]
         L.orc_rhf.restype = i32
+        L.orc_rhf2.argtypes = [vp, i32, P(f64), P(f64), i32, i32, f64, f64, i32, i32, f64, P(f64), P(i32), P(f64),
+                               P(f64)]
+        L.orc_rhf2.restype = i32
+        L.orc_null_modes.argtypes = [i32, P(f64)]
+        L.orc_null_modes.restype = i32
         _lib = L
     return _lib
 
@@ -163,14 +168,23 @@ class OracleBasis:
         lib().orc_jk_eri4(self.h, _p(D), _p(J), _p(K))
         return J, K
 
-    def rhf(self, mol, jk_mode=0, thresh=1e-10, dE_tol=1e-10, maxiter=100, nthreads=0):
+    def rhf(self, mol, jk_mode=0, thresh=1e-10, dE_tol=1e-10, maxiter=100, nthreads=0, diis_fdmax=0.0):
+        """diis_fdmax > 0 replaces the reference's DIIS switch-on bound (the GPU SCF's diis_fdmax)"""
         Z = np.ascontiguousarray(mol.Z, dtype=np.float64)
         R = np.ascontiguousarray(mol.R, dtype=np.float64).reshape(-1)
         E = np.zeros(1)
         it = np.zeros(1, dtype=np.int32)
         D = np.zeros((self.nbf, self.nbf))
-        st = np.zeros(4)
-        rc = lib().orc_rhf(self.h, len(Z), _p(Z), _p(R), int(mol.nelec), int(jk_mode), float(thresh),
-                           float(dE_tol), int(maxiter), int(nthreads), _p(E), _p(it, ctypes.c_int), _p(D), _p(st))
+        st = np.zeros(5)
+        rc = lib().orc_rhf2(self.h, len(Z), _p(Z), _p(R), int(mol.nelec), int(jk_mode), float(thresh),
+                            float(dE_tol), int(maxiter), int(nthreads), float(diis_fdmax), _p(E),
+                            _p(it, ctypes.c_int), _p(D), _p(st))
         return {"energy": float(E[0]), "iterations": int(it[0]), "converged": rc == 0, "D": D,
-                "wall_s": float(st[0]), "jk_s": float(st[1]), "fd_error": float(st[2]), "e_nn": float(st[3])}
+                "wall_s": float(st[0]), "jk_s": float(st[1]), "fd_error": float(st[2]), "e_nn": float(st[3]),
+                "dropped_modes": int(st[4])}
+
+
+def null_modes(w) -> int:
+    """overlap modes the reference's automatic orthogonaliser drops, for ascending eigenvalues w"""
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    return int(lib().orc_null_modes(len(w), _p(w)))

@@ -484,8 +484,50 @@ void orc_jk_eri4(void* h, const double* D, double* J, double* K)
 
 // RHF with core guess + DIIS.  jk_mode 0 = direct (OpenMP), 1 = ERI4 supermatrix (serial).
 // stats[0]=wall seconds total, [1]=seconds in J/K builds, [2]=final ||[F',D']||, [3]=nuclear repulsion
+// Near-null overlap modes to drop, by the rule of the reference's default orthogonaliser (LASolverAuto with
+// the gap-detection tolerance, LASolver/Internal/Imp/LASolverLapack.C:32-62, 385-402), on ascending overlap
+// eigenvalues w: the leading non-positive ones always; then, among the eigenvalues below 1e-3 of the largest,
+// the largest ratio between neighbours -- above 30 it is a clean gap and everything below it goes; without a
+// clean gap, every eigenvalue below the absolute floor 1e-8 goes.  0: S is kept whole (Cholesky there).
+int null_modes(int n, const double* w)
+{
+    if (n <= 0) return 0;
+    int k = 0;
+    while (k < n && w[k] <= 0.0) ++k;
+    int cut = k;
+    double best = 1.0;
+    for (int i = k; i + 1 < n && w[i] < 1e-3 * w[n - 1]; ++i)
+        if (w[i + 1] / w[i] > best)
+        {
+            best = w[i + 1] / w[i];
+            cut = i + 1;
+        }
+    if (best > 30.0) return cut;
+    int m = k;
+    while (m < n && w[m] < 1e-8) ++m;
+    return m;
+}
+int orc_null_modes(int n, const double* w) { return null_modes(n, w); }
+
+int orc_rhf2(void* h, int natom, const double* Z, const double* R, int nelec, int jk_mode, double thresh,
+             double dE_tol, int maxiter, int nthreads, double fdmax, double* E_out, int* iters, double* D_out,
+             double* stats);
+
 int orc_rhf(void* h, int natom, const double* Z, const double* R, int nelec, int jk_mode, double thresh,
             double dE_tol, int maxiter, int nthreads, double* E_out, int* iters, double* D_out, double* stats)
+{
+    double st5[5] = {};
+    const int rc = orc_rhf2(h, natom, Z, R, nelec, jk_mode, thresh, dE_tol, maxiter, nthreads, 0.0, E_out, iters,
+                            D_out, st5);
+    if (stats) std::copy(st5, st5 + 4, stats);
+    return rc;
+}
+
+// fdmax > 0 replaces the DIIS switch-on bound Z^2 * 0.1 / 32 (the GPU SCF's diis_fdmax); stats[4] = the
+// number of overlap modes dropped
+int orc_rhf2(void* h, int natom, const double* Z, const double* R, int nelec, int jk_mode, double thresh,
+             double dE_tol, int maxiter, int nthreads, double fdmax, double* E_out, int* iters, double* D_out,
+             double* stats)
 {
     double t0 = now(), tjk = 0;
     auto* o = (OBasis*)h;
@@ -499,15 +541,21 @@ int orc_rhf(void* h, int natom, const double* Z, const double* R, int nelec, int
     std::vector<double> H(n * n);
     for (int i = 0; i < n * n; ++i) H[i] = T[i] + V[i];
     const double Enn = nuclear_repulsion(atoms);
-    // canonical orthogonalisation X = U s^-1/2 (LASolverLapack.C LASolverEigen, no truncation)
+    // canonical orthogonalisation X = U s^-1/2 (LASolverLapack.C LASolverEigen); the near-null modes of the
+    // reference's automatic rule (null_modes) are dropped: their columns of X are zero and X^T F X gets a
+    // large diagonal shift on them, so that the eigenproblem is that of the kept modes and a dropped mode is
+    // never occupied.  Without dropped modes the reference uses Cholesky, which differs from this X by a
+    // rotation that leaves densities and energies unchanged.
     std::vector<double> sw(n), U(n * n), X(n * n);
     jacobi_eigen(n, S.data(), sw.data(), U.data());
+    const int ndrop = null_modes(n, sw.data());
     for (int i = 0; i < n; ++i)
-        for (int j = 0; j < n; ++j) X[i * n + j] = U[i * n + j] / std::sqrt(sw[j]);
+        for (int j = 0; j < n; ++j) X[i * n + j] = j < ndrop ? 0.0 : U[i * n + j] / std::sqrt(sw[j]);
     auto ortho = [&](const std::vector<double>& F) {   // X^T F X
         std::vector<double> t(n * n), r(n * n);
         matmul(n, n, n, F.data(), false, X.data(), false, t.data());
         matmul(n, n, n, X.data(), true, t.data(), false, r.data());
+        for (int j = 0; j < ndrop; ++j) r[j * n + j] += 1e6;
         return r;
     };
     std::vector<double> Dp(n * n, 0.0), D(n * n, 0.0), w(n), Up(n * n);
@@ -527,7 +575,7 @@ int orc_rhf(void* h, int natom, const double* Z, const double* R, int nelec, int
     diag_fill(ortho(H));   // core guess: static terms only (Seed.C:70-80, HamiltonianImp.C:58-63)
     if (o->Q.empty() && jk_mode == 0) o->Q = schwarz(bs);
     const int Nproj = 4;
-    const double FDMax = Ztot * Ztot * 0.1 / 32, SVTol = 5e-9;
+    const double FDMax = fdmax > 0 ? fdmax : Ztot * Ztot * 0.1 / 32, SVTol = 5e-9;
     std::deque<std::vector<double>> Es, Fps;
     std::vector<double> J(n * n), K(n * n), F(n * n);
     double E = 0, Eold = 0, En = 0;
@@ -602,7 +650,7 @@ int orc_rhf(void* h, int natom, const double* Z, const double* R, int nelec, int
     *E_out = E;
     *iters = conv ? it : maxiter;   // iterations run (the loop exits at maxiter + 1)
     if (D_out) std::copy(D.begin(), D.end(), D_out);
-    if (stats) { stats[0] = now() - t0; stats[1] = tjk; stats[2] = En; stats[3] = Enn; }
+    if (stats) { stats[0] = now() - t0; stats[1] = tjk; stats[2] = En; stats[3] = Enn; stats[4] = ndrop; }
     return conv ? 0 : 1;
 }
 

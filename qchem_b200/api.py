@@ -135,6 +135,7 @@ def lib():
     L.qcg_internal_gemm_bf16.argtypes = [i32, i32, i32, i32, i32, vp, i32, vp, i32, vp, i32, vp, i32]
     L.qcg_internal_syev_lowest.argtypes = [i32, P(f64), i32, P(f64), P(f64)]
     L.qcg_internal_orthogonaliser.argtypes = [i32, P(f64), P(f64)]
+    L.qcg_internal_null_modes.argtypes = [i32, P(f64)]
     L.qcg_measure_fp64_peak.argtypes = [i32, P(f64), P(f64)]
     L.qcg_measure_fp32_peak.argtypes = [i32, P(f64), P(f64)]
     L.qcg_selftest_bounded_wait.argtypes = [ctypes.c_longlong, i32, P(i32), P(f64)]
@@ -199,6 +200,13 @@ def release_cache() -> None:
     """Free the idle device slabs, pinned staging buffers, streams and events that destroyed handles left
     for reuse (qcg_release_cache)."""
     lib().qcg_release_cache()
+
+
+def null_modes(w) -> int:
+    """overlap modes the SCF's orthogonaliser drops, for ascending overlap eigenvalues w (the reference's
+    automatic rule: a clean spectral gap, else the eigenvalues below 1e-8)"""
+    w = _f64(w)
+    return int(lib().qcg_internal_null_modes(len(w), _p(w)))
 
 
 def measure_fp64_peak(reps: int = 20):

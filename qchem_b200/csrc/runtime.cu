@@ -1420,9 +1420,37 @@ struct SphericalMap
 // Host state of one closed-shell SCF (SCFIterator.C:283-362, SCFAcceleratorDIIS.C:35-238): canonical
 // orthogonaliser X = U s^{-1/2}, density, Fock matrix in the orthonormal basis and the DIIS subspace.
 // ------------------------------------------------------------------------------------------------
+// Near-null overlap modes to drop, by the rule of the reference's default orthogonaliser (LASolverAuto with
+// the gap-detection tolerance, LASolver/Internal/Imp/LASolverLapack.C:32-62, 385-402), on ascending overlap
+// eigenvalues w: the leading non-positive ones always; then, among the eigenvalues below 1e-3 of the largest,
+// the largest ratio between neighbours -- above 30 it is a clean gap and everything below it goes; without a
+// clean gap, every eigenvalue below the absolute floor 1e-8 goes.  0: the overlap is kept whole.
+int overlap_null_modes(int n, const double* w)
+{
+    if (n <= 0) return 0;
+    int k = 0;
+    while (k < n && w[k] <= 0.0) ++k;
+    int cut = k;
+    double best = 1.0;
+    for (int i = k; i + 1 < n && w[i] < 1e-3 * w[n - 1]; ++i)
+        if (w[i + 1] / w[i] > best)
+        {
+            best = w[i + 1] / w[i];
+            cut = i + 1;
+        }
+    if (best > 30.0) return cut;
+    int m = k;
+    while (m < n && w[m] < 1e-8) ++m;
+    return m;
+}
+
+// diagonal shift of the dropped modes in X^T F X: far above every orbital energy, so never occupied
+constexpr double kDroppedShift = 1e6;
+
 struct ScfCore
 {
     int n = 0, nocc = 0;
+    int ndrop = 0;   // overlap modes dropped by the orthogonaliser (overlap_null_modes)
     double fdmax = 0, Enn = 0;
     std::vector<double> S, H, X, Xt, D, Dp, F, Fp, Err, tmp, Up, w, a, b, Cocc;
     std::deque<std::vector<double>> Es, Fps;
@@ -1451,17 +1479,25 @@ struct ScfCore
         S = std::move(S_);
         H = std::move(H_);
         X.assign(nn, 0.0);
-        // orthogonaliser X with X^T S X = 1.  On the host: X = L^{-T} from the Cholesky factor S = L L^T
-        // (n^3/3 against the eigendecomposition's ~6 n^3); every such X differs from the canonical U s^{-1/2}
-        // by an orthogonal rotation, which leaves the DIIS error norms, the aufbau density and the energy
-        // unchanged.  On the GPU, and if the factorisation meets a non-positive pivot: X = U s^{-1/2}.
-        if (gl || !cholesky_orthogonaliser(n, S.data(), X.data()))
+        // orthogonaliser X with X^T S X = 1 on the kept modes, chosen as the reference's default does
+        // (LASolverAuto): the overlap's eigenvalues decide whether near-null modes are dropped.  None dropped:
+        // on the host X = L^{-T} from the Cholesky factor S = L L^T, which differs from the canonical
+        // U s^{-1/2} by a rotation that leaves the DIIS error norms, the aufbau density and the energy
+        // unchanged; on the GPU X = U s^{-1/2}.  Modes dropped: the canonical X with their columns zero, and
+        // X^T F X shifted by kDroppedShift on them (ortho), so that the eigenproblem is the kept modes' one.
         {
             std::vector<double> sw(n), U(nn);
             xsyev(S.data(), sw.data(), U.data());
-            require(sw[0] > 0, "overlap matrix is not positive definite");
-            for (int i = 0; i < n; ++i)
-                for (int j = 0; j < n; ++j) X[(size_t)i * n + j] = U[(size_t)i * n + j] / std::sqrt(sw[j]);
+            ndrop = overlap_null_modes(n, sw.data());
+            require(ndrop < n, "the overlap matrix has no mode to keep");
+            if (gl || ndrop > 0 || !cholesky_orthogonaliser(n, S.data(), X.data()))
+            {
+                require(sw[ndrop] > 0, "overlap matrix is not positive definite");
+                for (int i = 0; i < n; ++i)
+                    for (int j = 0; j < n; ++j)
+                        X[(size_t)i * n + j] = j < ndrop ? 0.0 : U[(size_t)i * n + j] / std::sqrt(sw[j]);
+            }
+            require(n - ndrop >= nocc, "more occupied orbitals than kept basis modes");
         }
         Xt.assign(nn, 0.0);
         for (int i = 0; i < n; ++i)
@@ -1503,6 +1539,7 @@ struct ScfCore
         xgemm(M.data(), false, X.data(), false, tmp.data());
         if (gl) xgemm(X.data(), true, tmp.data(), false, out.data());
         else gemm(n, Xt.data(), false, tmp.data(), false, out.data());   // X^T kept from set-up
+        for (int j = 0; j < ndrop; ++j) out[(size_t)j * n + j] += kDroppedShift;
     }
     // aufbau density of an orthonormal-basis Fock matrix, back in the AO basis (exactly symmetric)
     void diag_fill(const std::vector<double>& Fo)
@@ -3852,6 +3889,12 @@ int qcg_internal_syev(int n, const double* A, double* w, double* V)
     {
         return e.code;
     }
+}
+
+// test hook: the overlap modes the SCF's orthogonaliser drops, for ascending eigenvalues w
+int qcg_internal_null_modes(int n, const double* w)
+{
+    return overlap_null_modes(n, w);
 }
 
 // test hook: the host SCF's Cholesky orthogonaliser (1: X written; 0: S is not positive definite)

@@ -280,3 +280,25 @@ def test_oracle_pair_subset_of_every_pair_is_the_direct_build(oracle_mod):
     m[::2, :] = True
     _, _, cnt_half = ob.jk_direct_subset(D, m)
     assert 0 < cnt_half < cnt
+
+
+def test_overlap_null_mode_rule_product_and_oracle_agree(oracle_mod):
+    """The orthogonaliser's choice of dropped overlap modes (the reference's automatic rule, LASolverAuto): the
+    product's host code and the oracle give the same count on synthetic spectra -- a clean gap (a ratio above
+    30 below 1e-3 of the largest eigenvalue), a smooth ramp (the absolute floor 1e-8), none -- and on the
+    overlaps of real molecules: none for the config-1 water, one (a clean gap) for molecule 34 of the
+    random-molecule set, three for the 32-water cluster."""
+    from qchem_b200 import api
+    from oracle import oracle as O
+    cases = [([1e-10, 1e-9, 1e-2, 0.5, 1.0, 2.0, 1e4], 2),
+             ([3e-9, 6e-9, 2e-8, 5e-8, 2e-7, 1e-6, 1e-5, 1e-4, 1e-3, 1e-2, 0.1, 1.0, 50.0], 2),
+             ([1e-6, 1e-5, 1e-4, 1e-3, 1e-2, 0.1, 1.0], 0),
+             ([-1e-12, 0.5, 1.0, 2.0], 1), ([-1e-12, 1e-3, 1.0, 2.0], 2)]
+    for w, want in cases:
+        assert O.null_modes(np.array(w)) == want, w
+        assert api.null_modes(np.array(w)) == want, w
+    mols = {"water": (W.water(), 0), "random34": (W.random_molecules(256)[34], 1), "water32": (W.water_cluster(), 3)}
+    for name, (mol, want) in mols.items():
+        ob = oracle_mod.OracleBasis(B.even_tempered(mol))
+        w = np.linalg.eigvalsh(ob.one_electron(mol)[0])
+        assert O.null_modes(w) == want and api.null_modes(w) == want, name
