@@ -133,7 +133,10 @@ class LearnedGuess:
         return ((self._x(mols) - self.x_mu) / self.x_sd).astype(np.float32)
 
     def fit(self, mols: Sequence[_basis.Molecule], densities: Sequence[np.ndarray], steps: int = 3000,
-            batch_molecules: int = 128, lr: float = 2e-3, seed: int = 0, device: str = "cuda") -> dict:
+            batch_molecules: int = 128, lr: float = 2e-3, seed: int = 0, device: str = "cuda",
+            y_floor: float = 1e-8) -> dict:
+        """y_floor: the smallest spread an output entry is standardised by; entries that vary less are not
+        amplified into the loss (1e-8: every entry counts)"""
         import torch
         P = len(self.layout.pairs)
         X = self._x(mols)
@@ -141,7 +144,7 @@ class LearnedGuess:
         self.x_sd = X.std(axis=0) + 1e-6
         Y = np.stack([self.layout.blocks(D) for D in densities])          # (nmol, P, nout)
         self.y_mu = Y.mean(axis=0)
-        self.y_sd = Y.std(axis=0) + 1e-8
+        self.y_sd = np.maximum(Y.std(axis=0), y_floor) + 1e-8
         mask = self.layout.mask()
         Yn = ((Y - self.y_mu) / self.y_sd * mask).astype(np.float32).reshape(-1, self.layout.nout)
         Xn = ((X - self.x_mu) / self.x_sd).astype(np.float32)
@@ -225,6 +228,28 @@ def plain_scf_dataset(mols: Sequence[_basis.Molecule], shells_of=_basis.even_tem
         Es.append(r["energy"])
         its.append(r["iterations"])
         walls.append(r["wall_s"])
+    return Ds, np.array(Es), np.array(its), np.array(walls), kept
+
+
+def plain_scf_dataset_batched(mols: Sequence[_basis.Molecule], chunk: int = 500, shells_of=_basis.even_tempered,
+                              **rhf_kw):
+    """plain_scf_dataset through the batched SCF: `chunk` conformers per batch handle, every SCF with the
+    plain settings (core guess, the reference's DIIS rules), one J/K build per iteration over the chunk.
+    The returned walls are each chunk's wall time per molecule."""
+    Ds, Es, its, walls, kept = [], [], [], [], []
+    for c0 in range(0, len(mols), chunk):
+        part = list(mols[c0:c0 + chunk])
+        t0 = time.perf_counter()
+        res = api.BatchEngine([shells_of(m) for m in part]).rhf(part, want_density=True, **rhf_kw)
+        per = (time.perf_counter() - t0) / len(part)
+        for k, r in enumerate(res):
+            if not r["converged"]:
+                continue
+            kept.append(c0 + k)
+            Ds.append(r["D"])
+            Es.append(r["energy"])
+            its.append(r["iterations"])
+            walls.append(per)
     return Ds, np.array(Es), np.array(its), np.array(walls), kept
 
 
