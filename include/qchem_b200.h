@@ -90,6 +90,11 @@ typedef struct qcg_scf_params {
     int autotune;             /* 1: qcg_autotune_jk on the first density before the first build; default 0 */
     int spherical;            /* 1: the SCF in real solid-harmonic functions (qcg_spherical_transform); D_guess
                                  and D_out are then spherical; needs incremental = 0; default 0 */
+    int deterministic;        /* 1: every J/K build with QCG_JK_DETERMINISTIC (exact integer accumulation), so
+                                 that the trajectory, the iteration count and the energy repeat bit for bit from
+                                 run to run -- near-degenerate SCFs otherwise follow the rounding of the FP64
+                                 atomics; each build costs about 1.9x; not with fp32_early or fp32_below > 0;
+                                 default 0 */
 } qcg_scf_params;
 
 typedef struct qcg_scf_result {

@@ -64,7 +64,8 @@ class ScfParams(ctypes.Structure):
                 ("diis_svtol", ctypes.c_double), ("incremental", ctypes.c_int), ("inc_thresh", ctypes.c_double),
                 ("rebuild_every", ctypes.c_int), ("fp32_early", ctypes.c_int), ("fp32_switch", ctypes.c_double),
                 ("fp32_scale", ctypes.c_double), ("fp32_below", ctypes.c_double),
-                ("D_guess", ctypes.POINTER(ctypes.c_double)), ("autotune", ctypes.c_int), ("spherical", ctypes.c_int)]
+                ("D_guess", ctypes.POINTER(ctypes.c_double)), ("autotune", ctypes.c_int), ("spherical", ctypes.c_int),
+                ("deterministic", ctypes.c_int)]
 
 
 class ScfResult(ctypes.Structure):
@@ -439,7 +440,7 @@ class Engine:
     def rhf(self, mol: _basis.Molecule, max_iter=100, de_tol=1e-10, fd_tol=1e-5, schwarz_thresh=1e-10,
             want_density=False, incremental=False, inc_thresh=1e-11, rebuild_every=8, fp32_early=False,
             fp32_switch=1e-5, fp32_scale=0.0, fp32_below=0.0, guess=None, diis_nproj=4, diis_fdmax=0.0,
-            autotune=False, spherical=False):
+            autotune=False, spherical=False, deterministic=False):
         """RHF to convergence.  incremental=True: density-difference J/K builds with density-weighted
         screening between full builds (the energy on exit is always from a full build).  fp32_early=True:
         until the DIIS error drops below fp32_switch, quartets whose density-weighted bound is below
@@ -455,6 +456,7 @@ class Engine:
         prm.diis_nproj, prm.diis_fdmax = int(diis_nproj), float(diis_fdmax)
         prm.autotune = int(bool(autotune))
         prm.spherical = int(bool(spherical))
+        prm.deterministic = int(bool(deterministic))
         nw = self.nbf_spherical if spherical else self.nbf
         if guess is not None:
             guess = _f64(guess)
@@ -528,7 +530,7 @@ class BatchEngine(Engine):
         self._screen = thresh
 
     def rhf(self, mols: Sequence[_basis.Molecule], max_iter=100, de_tol=1e-10, fd_tol=1e-5, schwarz_thresh=1e-10,
-            want_density=False, diis_nproj=4, diis_fdmax=0.0, autotune=False, guesses=None):
+            want_density=False, diis_nproj=4, diis_fdmax=0.0, autotune=False, guesses=None, deterministic=False):
         """guesses: optional list of per-molecule initial densities (None entries are not allowed; omit the
         argument for the core guess everywhere)."""
         prm = ScfParams()
@@ -536,6 +538,7 @@ class BatchEngine(Engine):
         prm.max_iter, prm.de_tol, prm.fd_tol, prm.schwarz_thresh = max_iter, de_tol, fd_tol, schwarz_thresh
         prm.diis_nproj, prm.diis_fdmax = int(diis_nproj), float(diis_fdmax)
         prm.autotune = int(bool(autotune))
+        prm.deterministic = int(bool(deterministic))
         Dg = None
         if guesses is not None:
             if len(guesses) != len(mols):

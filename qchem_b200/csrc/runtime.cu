@@ -3314,6 +3314,7 @@ void qcg_scf_default_params(qcg_scf_params* p)
     p->D_guess = nullptr;
     p->autotune = 0;
     p->spherical = 0;
+    p->deterministic = 0;
 }
 
 // Closed-shell SCF (SCFIterator.C:283-362 loop; DIIS gating/pruning per SCFAcceleratorDIIS.C:35-238)
@@ -3329,6 +3330,9 @@ int qcg_rhf(qcg_handle* h, int natom, const double* Z, const double* R, int nele
         if (params) prm = *params;
         require(result != nullptr, "null result");
         require(h->nmol == 1, "qcg_rhf takes a single-molecule handle (qcg_rhf_batch for several)");
+        require(!prm.deterministic || (!prm.fp32_early && prm.fp32_below <= 0),
+                "the deterministic SCF builds every quartet in FP64 (no fp32_early, no fp32_below)");
+        const int jk_flags = QCG_JK_SKIP_VALIDATION | (prm.deterministic ? QCG_JK_DETERMINISTIC : 0);
         require(natom > 0 && Z && R, "bad nuclei");
         require(nelec > 0 && nelec % 2 == 0, "closed-shell RHF needs a positive even electron count");
         const int n = h->nbf, nocc = nelec / 2;
@@ -3439,14 +3443,14 @@ int qcg_rhf(qcg_handle* h, int natom, const double* Z, const double* R, int nele
                     const int e = qcg_autotune_jk(h, h->d_D, 1, nullptr, nullptr);
                     if (e != QCG_OK) throw Error{e, h->last_error};
                 }
-                jk_device(h, h->d_D, h->d_J, h->d_K, QCG_JK_SKIP_VALIDATION, &st, nullptr, 0.0, band);
+                jk_device(h, h->d_D, h->d_J, h->d_K, jk_flags, &st, nullptr, 0.0, band);
             }
             else
             {
                 for (size_t k = 0; k < nn; ++k) Dpin.p[k] = D[k] - Dprev[k];
                 CK(cudaMemcpyAsync(h->d_D, Dpin.p, nn * sizeof(double), cudaMemcpyHostToDevice, h->stream));
                 launch_block_max(h->d_D, h->d_f0, h->bs.L, h->nshell, n, d_dmax, h->stream, h->nsm);
-                jk_device(h, h->d_D, h->d_J, h->d_K, QCG_JK_SKIP_VALIDATION, &st, d_dmax, prm.inc_thresh, band);
+                jk_device(h, h->d_D, h->d_J, h->d_K, jk_flags, &st, d_dmax, prm.inc_thresh, band);
             }
             const auto c1 = clk::now();
             CK(cudaMemcpyAsync(Jpin.p, h->d_J, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
@@ -3809,7 +3813,8 @@ int qcg_rhf_batch(qcg_handle* h, const int* mol_natom, const double* Z, const do
                 const int e = qcg_autotune_jk(h, h->d_D, 1, nullptr, nullptr);
                 if (e != QCG_OK) throw Error{e, h->last_error};
             }
-            jk_device(h, h->d_D, h->d_J, h->d_K, QCG_JK_SKIP_VALIDATION, &st);
+            jk_device(h, h->d_D, h->d_J, h->d_K,
+                      QCG_JK_SKIP_VALIDATION | (prm.deterministic ? QCG_JK_DETERMINISTIC : 0), &st);
             CK(cudaMemcpyAsync(J, h->d_J, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
             CK(cudaMemcpyAsync(K, h->d_K, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
             CK(cudaStreamSynchronize(h->stream));

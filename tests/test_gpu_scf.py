@@ -58,3 +58,24 @@ def test_incremental_scf_converges_on_the_water8_cluster(open_diis):
     assert plain["converged"] and inc["converged"]
     assert inc["incremental_builds"] > 0
     assert abs(plain["energy"] - inc["energy"]) <= E_TOL, (plain["energy"], inc["energy"])
+
+
+def test_deterministic_scf_repeats_bit_for_bit():
+    """With deterministic J/K builds (exact integer accumulation) the SCF's trajectory repeats: the 456-function
+    water cluster, whose iteration count otherwise moves between runs with the FP64 atomics' rounding, gives the
+    same energy bits and iteration count twice, and the plain SCF's energy to 1e-8 Eh; a batch handle does too."""
+    mol = W.water_cluster(nx=2, ny=2, nz=2, seed=W.SEED0 + 3650)
+    sh = B.even_tempered(mol)
+    a = api.Engine(sh).rhf(mol, diis_fdmax=1e6, deterministic=True)
+    b = api.Engine(sh).rhf(mol, diis_fdmax=1e6, deterministic=True)
+    assert a["converged"] and b["converged"]
+    assert a["energy"] == b["energy"] and a["iterations"] == b["iterations"]
+    plain = api.Engine(sh).rhf(mol)
+    assert abs(a["energy"] - plain["energy"]) <= E_TOL
+    mols = [W.water(), W.water_cluster(nx=2, ny=1, nz=1, seed=W.SEED0 + 3300)]
+    shells = [B.even_tempered(m) for m in mols]
+    r1 = api.BatchEngine(shells).rhf(mols, diis_fdmax=1e6, deterministic=True)
+    r2 = api.BatchEngine(shells).rhf(mols, diis_fdmax=1e6, deterministic=True)
+    assert [r["energy"] for r in r1] == [r["energy"] for r in r2]
+    with pytest.raises(api.QcgError):
+        api.Engine(sh).rhf(mol, deterministic=True, fp32_below=1e-7)
