@@ -521,27 +521,30 @@ __global__ void __launch_bounds__(THREADS) jk_kernel(JKWorkDev w, PairListDev br
 }
 
 // ------------------------------------------------------------------------------------------------
-// The warp-shared form of the direct J/K build.  A warp takes up to 32 bra pairs (a b_l) that share their
-// first shell a -- lane l holds (a b_l) -- against one ket pair (c d) at a time.  Of the six digestion
-// targets of a quartet, three are then the same for every lane: J'(c d), K'(a c) and K'(a d).  Their lane
-// partial sums are added across the warp by shuffles and written by one lane each, so an L2 atomic per
-// lane becomes one per warp; only K'(b c) and K'(b d) stay per lane, and J'(a b) stays in registers over the
-// whole run of kets.  The ket's pair data and its density rows D(a, .) are the same for every lane (one
-// broadcast load each).  Lanes whose quartet is absent (past their bra pair's screened ket prefix, skipped
-// by jk_skip, or past the end of a short warp set) evaluate a valid quartet with weight 0, so that every
-// lane reaches the shuffles.  This replaces the same arithmetic as JKSink (qchem's MakeDirect /
-// MakeExchange, Molecule/IrrepBasisSet.C:138-183) with fewer memory operations.
+// The warp-shared form of the direct J/K build.  Each half of a warp takes up to 16 bra pairs (a b_l) that
+// share their first shell a -- lane l holds (a b_l) -- against one ket pair (c d) at a time.  Of the six
+// digestion targets of a quartet, three are then the same for every lane of a half: J'(c d), K'(a c) and
+// K'(a d).  Their lane partial sums are added across the half by shuffles and written by one lane each, so
+// an L2 atomic per lane becomes one per half warp; only K'(b c) and K'(b d) stay per lane, and J'(a b)
+// stays in registers over the whole run of kets.  The ket's pair data and its density rows D(a, .) are the
+// same for every lane of a half (one broadcast load each).  Lanes whose quartet is absent (past their bra
+// pair's screened ket prefix, skipped by jk_skip, past the end of a short set, or past a shorter primitive
+// loop) evaluate a valid quartet with weight 0, so that every lane reaches the shuffles.  Half-warp sets
+// rather than whole-warp ones keep more lanes busy: a shell's partner list rarely fills a multiple of 32,
+// and 16 neighbours in Q order have closer ket prefixes.  This replaces the same arithmetic as JKSink
+// (qchem's MakeDirect / MakeExchange, Molecule/IrrepBasisSet.C:138-183) with fewer memory operations.
 // ------------------------------------------------------------------------------------------------
 
-// Sum P values (P a power of two, <= 32) over the 32 lanes of a warp: in log2 P exchange steps each lane
-// keeps half of its values and adds its partner's copy of them, then the rest is a plain butterfly.  On
-// return every lane holds the warp's total of value (lane >> (5 - log2 P)); the lanes with
-// lane % (32 / P) == 0 are one writer per value.
+// Sum P values (P a power of two, <= 16) over the 16 lanes of each half of a warp (lanes 0-15 and 16-31
+// are separate sets): in log2 P exchange steps each lane keeps half of its values and adds its partner's
+// copy of them, then the rest is a plain butterfly, every shuffle within the half.  On return every lane
+// holds its half's total of value ((lane & 15) >> (4 - log2 P)); the lanes with lane % (16 / P) == 0 are one
+// writer per value and half.
 template <int P>
-__device__ __forceinline__ double warp_transpose_sum(double (&v)[P], int lane)
+__device__ __forceinline__ double half_warp_transpose_sum(double (&v)[P], int lane)
 {
 #pragma unroll
-    for (int m = P, o = 16; m > 1; m >>= 1, o >>= 1)
+    for (int m = P, o = 8; m > 1; m >>= 1, o >>= 1)
     {
         const bool up = (lane & o) != 0;
 #pragma unroll
@@ -554,7 +557,7 @@ __device__ __forceinline__ double warp_transpose_sum(double (&v)[P], int lane)
     }
     double x = v[0];
 #pragma unroll
-    for (int o = 16 / P; o >= 1; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    for (int o = 8 / P; o >= 1; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
     return x;
 }
 
@@ -618,7 +621,8 @@ struct WarpJKSink
     __device__ __forceinline__ void flush_shared(int la, int si)
     {
         constexpr int P = pow2_at_least(V);
-        constexpr int SHIFT = (P == 1 ? 5 : P == 2 ? 4 : P == 4 ? 3 : P == 8 ? 2 : P == 16 ? 1 : 0);
+        static_assert(P <= 16, "at most 16 shared values per half warp");
+        constexpr int SHIFT = (P == 1 ? 4 : P == 2 ? 3 : P == 4 ? 2 : P == 8 ? 1 : 0);
         double v[P];
         v[0] = jcd;
 #pragma unroll
@@ -630,8 +634,8 @@ struct WarpJKSink
         }
 #pragma unroll
         for (int k = V; k < P; ++k) v[k] = 0.0;
-        const double x = warp_transpose_sum<P>(v, lane);
-        const int idx = lane >> SHIFT;
+        const double x = half_warp_transpose_sum<P>(v, lane);
+        const int idx = (lane & 15) >> SHIFT;
         if ((lane & ((1 << SHIFT) - 1)) != 0 || idx >= V || x == 0.0) return;
         if (idx == 0) atomicAdd(J + (size_t)la * n + si, 2.0 * x);
         else if (idx <= NA) atomicAdd(K + (size_t)(fa + idx - 1) * n + si, x);
@@ -666,9 +670,12 @@ struct WarpJKSink
     }
 };
 
-// items[t] = {first entry of the warp set in gbra, its lane count (<= 32), first ket, end ket}: the warp set
-// is gbra[x .. x + y), bra pairs sharing their first shell; the kets are positions [z, w) of every lane's
-// ket list (its molecule's part of the ket class, from kbase), each lane stopping at its own screened prefix
+// Work item t is two half-warp sets: items[2t] for lanes 0-15 and items[2t + 1] for lanes 16-31, each
+// {first entry of its set in gbra, its lane count (<= 16), first ket, end ket}.  A set is gbra[x .. x + y),
+// bra pairs sharing their first shell; its kets are positions [z, w) of each lane's ket list (its molecule's
+// part of the ket class, from kbase), each lane stopping at its own screened prefix.  The two sets of an
+// item have the same first ket, so the warp walks one ket loop for both; the primitive loops run to the
+// warp's longest, with weight 0 beyond a lane's own, so that every lane reaches every shuffle.
 template <class Cls, int THREADS>
 __global__ void __launch_bounds__(THREADS) jk_warp_kernel(JKWorkDev w, PairListDev bra, PairListDev ket,
                                                           PrimPairsDev P, const int* __restrict__ shell_f0,
@@ -684,11 +691,13 @@ __global__ void __launch_bounds__(THREADS) jk_warp_kernel(JKWorkDev w, PairListD
     const long long nwarp = ((long long)gridDim.x * blockDim.x) >> 5;
     for (long long t = warp; t < nitems; t += nwarp)
     {
-        const int4 it = items[t];
-        const bool real = lane < it.y;
-        const int i = gbra[it.x + (real ? lane : 0)];
+        const int4 it = items[2 * t + (lane >> 4)];
+        const int4 other = items[2 * t + 1 - (lane >> 4)];
+        const bool real = (lane & 15) < it.y;
+        // an empty half (an odd set count) borrows the other half's first bra pair, with weight 0
+        const int i = real ? gbra[it.x + (lane & 15)] : gbra[it.y > 0 ? it.x : other.x];
         const int prefix = real ? (int)(w.offs[i + 1] - w.offs[i]) : 0;
-        const int jb = w.kbase ? w.kbase[i] : 0;   // the same for the whole set: one molecule
+        const int jb = w.kbase ? w.kbase[i] : 0;   // the same within a half: one molecule per set
         const int sa = bra.sa[i], sb = bra.sb[i];
         WarpJKSink<Cls::LA, Cls::LB, Cls::LC, Cls::LD> sink;
         sink.D = D;
@@ -710,24 +719,27 @@ __global__ void __launch_bounds__(THREADS) jk_warp_kernel(JKWorkDev w, PairListD
         sink.set_bra(shell_f0[sa], shell_f0[sb]);
         const int oi = bra.ppo[i], ni = bra.npp[i];
         const int nimax = __reduce_max_sync(0xffffffffu, ni);
-        for (int jj = it.z; jj < it.w; ++jj)
+        const int jend = it.w > other.w ? it.w : other.w;   // both halves start at it.z == other.z
+        for (int jj = it.z; jj < jend; ++jj)
         {
-            const int j = jb + jj;
+            // a half past its own end repeats its last ket with weight 0
+            const int j = jb + (jj < it.w ? jj : (it.w > it.z ? it.w - 1 : it.z));
             const int sc = ket.sa[j], sd = ket.sb[j];
-            const bool act = real && on && jj < prefix && !jk_skip(w, bra, ket, i, j, sa, sb, sc, sd);
+            const bool act = real && on && jj < it.w && jj < prefix && !jk_skip(w, bra, ket, i, j, sa, sb, sc, sd);
             if (!__any_sync(0xffffffffu, act)) continue;
             sink.fc = shell_f0[sc];
             sink.fd = shell_f0[sd];
             const double s =
                 (sa == sb ? 0.5 : 1.0) * (sc == sd ? 0.5 : 1.0) * ((w.same_class && i == j) ? 0.5 : 1.0);
             const int oj = ket.ppo[j], nj = ket.npp[j];
+            const int njmax = __reduce_max_sync(0xffffffffu, nj);
             for (int x = 0; x < nimax; ++x)
             {
                 const PrimPairData ab = load_pp(P, oi + (x < ni ? x : ni - 1));
-                sink.s = (act && x < ni) ? s : 0.0;
-                for (int y = 0; y < nj; ++y)
+                for (int y = 0; y < njmax; ++y)
                 {
-                    const PrimPairData cd = load_pp(P, oj + y);
+                    const PrimPairData cd = load_pp(P, oj + (y < nj ? y : nj - 1));
+                    sink.s = (act && x < ni && y < nj) ? s : 0.0;
                     Cls::template quartet<double>(ab, cd, boys_table, rs, THREADS, sink);
                 }
             }

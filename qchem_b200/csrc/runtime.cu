@@ -2009,9 +2009,11 @@ void shard_range(const qcg_handle* h, int k, long long& gbeg, long long& gend)
 constexpr int kWarpItemKets = 256;
 
 // The warp-shared form's work of class k: the class's bra pairs that have quartets, grouped by first shell
-// (one shell belongs to one molecule; within a group the pair list's order, Q descending, so that a warp's
-// lanes have similar screened ket prefixes), cut into warp sets of up to 32 pairs, and each set's kets
-// [0, its longest prefix) cut into items of kWarpItemKets.  Built once per screening, before any capture.
+// (one shell belongs to one molecule; within a group the pair list's order, Q descending, so that a set's
+// lanes have similar screened ket prefixes), cut into half-warp sets of up to 16 pairs.  The sets, ordered by
+// their longest prefix, are paired two to a warp; each pair's kets [0, its longer prefix) are cut into items
+// of kWarpItemKets, one int4 per half (a half past its own prefix gets an empty entry).  Built once per
+// screening, before any capture.
 void warp_items(qcg_handle* h, int k)
 {
     if (h->witems_ready[k]) return;
@@ -2023,24 +2025,45 @@ void warp_items(qcg_handle* h, int k)
     for (int i = 0; i + 1 < (int)offs.size(); ++i)
         if (offs[i + 1] > offs[i]) ord.push_back(i);
     std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return sa[x] < sa[y]; });
-    std::vector<int4> items;
+    struct Set
+    {
+        long long maxp;
+        int start, cnt;
+    };
+    std::vector<Set> sets;
     for (size_t g0 = 0; g0 < ord.size();)
     {
         size_t g1 = g0;
         while (g1 < ord.size() && sa[ord[g1]] == sa[ord[g0]]) ++g1;
-        for (size_t s0 = g0; s0 < g1; s0 += 32)
+        for (size_t s0 = g0; s0 < g1; s0 += 16)
         {
-            const int cnt = (int)std::min<size_t>(32, g1 - s0);
+            const int cnt = (int)std::min<size_t>(16, g1 - s0);
             long long maxp = 0;
             for (int l = 0; l < cnt; ++l) maxp = std::max(maxp, offs[ord[s0 + l] + 1] - offs[ord[s0 + l]]);
-            for (long long j0 = 0; j0 < maxp; j0 += kWarpItemKets)
-                items.push_back(make_int4((int)s0, cnt, (int)j0, (int)std::min<long long>(maxp, j0 + kWarpItemKets)));
+            sets.push_back({maxp, (int)s0, cnt});
         }
         g0 = g1;
     }
+    std::stable_sort(sets.begin(), sets.end(), [](const Set& x, const Set& y) { return x.maxp > y.maxp; });
+    std::vector<int4> items;
+    for (size_t q = 0; q < sets.size(); q += 2)
+    {
+        const Set A = sets[q];
+        const Set B = q + 1 < sets.size() ? sets[q + 1] : Set{0, A.start, 0};
+        const long long m = std::max(A.maxp, B.maxp);
+        for (long long j0 = 0; j0 < m; j0 += kWarpItemKets)
+            for (const Set& S : {A, B})
+            {
+                if (j0 < S.maxp)
+                    items.push_back(
+                        make_int4(S.start, S.cnt, (int)j0, (int)std::min<long long>(S.maxp, j0 + kWarpItemKets)));
+                else
+                    items.push_back(make_int4(S.start, 0, (int)j0, (int)j0));
+            }
+    }
     h->d_wgbra[k] = ord.empty() ? nullptr : h->upload(ord);
     h->d_witems[k] = items.empty() ? nullptr : h->upload(items);
-    h->nwitems[k] = (long long)items.size();
+    h->nwitems[k] = (long long)items.size() / 2;   // warp items: two half-warp entries each
     h->witems_ready[k] = true;
 }
 
