@@ -199,7 +199,7 @@ int qcg_set_jk_team_classes(qcg_handle* h, long long mask);
  * pair at a time, so that the J'(cd), K'(ac) and K'(ad) contributions of its lanes are added by warp
  * shuffles and written once per warp instead of once per lane.  FP64 builds of one rank (not with
  * qcg_set_shard or QCG_JK_DETERMINISTIC).  -1 (default): the library's choice -- the (ps|ss), (ps|ps),
- * (pp|ss), (pp|ps), (ds|xx), (dp|ss), (dp|ps) and (dp|pp) classes of full builds with at least 2^20 quartets in the
+ * (pp|ss), (pp|ps), (ds|xx), (dp|ss), (dp|ps), (dp|pp) and (dp|ds) classes of full builds with at least 2^20 quartets in the
  * class -- or QCG_JK_WARP_MASK in the environment (a mask set here or there applies to every build).  Same J
  * and K to rounding.  No reference counterpart. */
 int qcg_set_jk_warp_classes(qcg_handle* h, long long mask);

@@ -89,12 +89,12 @@ def _jk_team_mask() -> int:
 
 
 # classes whose direct J/K build runs in the warp-shared form by default (QCG_JK_WARP_MASK selects others):
-# (ps|ss), (ps|ps), (pp|ss), (pp|ps), (ds|ss), (ds|ps), (ds|pp), (ds|ds), (dp|ss), (dp|ps), (dp|pp).
-# Measured class by class on a B200 on the uncontracted 32-water build, the warp-shared form took 0.49-0.98x
-# the thread-per-quartet kernel's time on these eleven ((ds|ps) 209 vs 428 ms, (dp|ps) 354 vs 511 ms,
-# (dp|pp) 999 vs 1345 ms, where the team form took 1231 ms); on (ss|ss), (pp|pp), (dp|ds) and (dd|ss) it took
-# 1.06-1.26x.
-JK_WARP_CLASSES = (1, 2, 3, 4, 6, 7, 8, 9, 10, 11, 12)
+# (ps|ss), (ps|ps), (pp|ss), (pp|ps), (ds|ss), (ds|ps), (ds|pp), (ds|ds), (dp|ss), (dp|ps), (dp|pp), (dp|ds).
+# Measured class by class on a B200 on the uncontracted 32-water build (half-warp sets), the warp-shared form
+# took 0.51-0.82x the thread-per-quartet kernel's time on these twelve ((ds|ps) 219 vs 428 ms, (dp|ds) 625
+# vs 872 ms, (dp|pp) 994 vs 1345 ms, where the team form took 1231 ms); on (ss|ss), (pp|pp) and (dd|ss) it
+# was level (1.00-1.02x), and those stay thread-per-quartet.
+JK_WARP_CLASSES = (1, 2, 3, 4, 6, 7, 8, 9, 10, 11, 12, 13)
 
 
 def _jk_warp_mask() -> int:
