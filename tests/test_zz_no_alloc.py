@@ -65,7 +65,7 @@ def test_noalloc_matches_allocating_entry_point_twice():
         for i, (J, K) in enumerate(bufs):
             if i == 1:
                 # the first call on the device looks up the array's address, and with lazy module loading
-                # the driver materialises the library's static array then; from here on free memory must
+                # the CUDA driver materialises the library's static array then; from here on free memory must
                 # not move
                 free0 = torch.cuda.mem_get_info()[0]
             rc = f(eng._h, ctypes.c_void_p(D.data_ptr()), ctypes.c_void_p(J.data_ptr()), ctypes.c_void_p(K.data_ptr()))
