@@ -266,3 +266,25 @@ def test_hrr_class_selection(monkeypatch):
     assert all(qb._eri_hrr(k) for k in range(21))
     monkeypatch.setenv("QCG_ERI_HRR", "0")
     assert not any(qb._eri_hrr(k) for k in range(21))
+
+
+def test_bench_reference_arm_prints_the_contract_line():
+    """`bench.py --impl reference` (the CPU oracle's rate on the ERI microbenchmark's class mix) runs without
+    a GPU and prints one JSON line with the keys the benchmark contract needs, the same metric and unit as the
+    GPU arm, and a cpu_baseline and e2e block describing itself."""
+    import json
+    import subprocess
+    import sys
+    from tests.conftest import REPO
+    r = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--steps", "1", "--warmup", "1",
+                        "--ref-sample", "40"], cwd=REPO, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "scaling",
+                "dtype", "data", "config", "cpu_baseline", "e2e"):
+        assert key in line, key
+    assert line["impl"] == "reference" and line["value"] > 0 and line["higher_is_better"] is True
+    assert line["unit"] == "quartets/s" and line["metric"].startswith("ERI quartets/s")
+    cb = line["cpu_baseline"]
+    assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == line["value"] and cb["sample"]
+    assert line["e2e"]["value"] == line["value"] and line["e2e"]["h2d_bytes_per_step"] == 0
