@@ -195,12 +195,13 @@ int qcg_set_eri_team_classes(qcg_handle* h, long long mask);
  * reference counterpart. */
 int qcg_set_jk_team_classes(qcg_handle* h, long long mask);
 /* The warp-shared form of the direct J/K build for the classes in mask (bit k: class k; the team form takes
- * precedence where both are set): a warp takes up to 32 bra pairs sharing their first shell against one ket
- * pair at a time, so that the J'(cd), K'(ac) and K'(ad) contributions of its lanes are added by warp
- * shuffles and written once per warp instead of once per lane.  FP64 builds of one rank (not with
- * qcg_set_shard or QCG_JK_DETERMINISTIC).  -1 (default): the library's choice -- the (ps|ss), (ps|ps),
- * (pp|ss), (pp|ps), (ds|xx), (dp|ss), (dp|ps), (dp|pp) and (dp|ds) classes of full builds with at least 2^20 quartets in the
- * class -- or QCG_JK_WARP_MASK in the environment (a mask set here or there applies to every build).  Same J
+ * precedence where both are set): each half of a warp takes up to 16 bra pairs sharing their first shell
+ * against one ket pair at a time, so that the J'(cd), K'(ac) and K'(ad) contributions of its lanes are added
+ * by warp shuffles and written once per half warp instead of once per lane.  FP64 builds of one rank (not
+ * with qcg_set_shard or QCG_JK_DETERMINISTIC).  -1 (default): the library's choice -- the (ps|ss), (ps|ps),
+ * (pp|ss), (pp|ps), (ds|xx), (dp|ss), (dp|ps), (dp|pp) and (dp|ds) classes of full builds with at least 2^20
+ * quartets in the class -- or QCG_JK_WARP_MASK in the environment (a mask set here or there applies to every
+ * build).  Same J
  * and K to rounding.  No reference counterpart. */
 int qcg_set_jk_warp_classes(qcg_handle* h, long long mask);
 /* Restrict later J/K builds to a subset of shell pairs: mask (nshell x nshell bytes, row-major; pair (a,b) is
