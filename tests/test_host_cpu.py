@@ -288,3 +288,41 @@ def test_bench_reference_arm_prints_the_contract_line():
     cb = line["cpu_baseline"]
     assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == line["value"] and cb["sample"]
     assert line["e2e"]["value"] == line["value"] and line["e2e"]["h2d_bytes_per_step"] == 0
+
+
+def test_cpp_salc_block_compiles_and_links(tmp_path):
+    """qcg::SalcBlock (the symmetry-adapted faces) compiles against include/qchem_b200.hpp and links against
+    qcg_salc_fold / qcg_salc_slice; without a GPU the AO engine's constructor throws QCG_ERR_CUDA first."""
+    import shutil
+    import subprocess
+    import torch
+    if shutil.which("g++") is None:
+        pytest.skip("no g++")
+    src = tmp_path / "s.cpp"
+    src.write_text('#include "qchem_b200.hpp"\nint main(){std::vector<qcg::ShellSpec> s{{0,{0,0,0},{1.0},{1.0}}};\n'
+                   'int rc;\n'
+                   'try { qcg::FockEngine e(s); qcg::SalcBlock b(e, std::vector<double>{1.0}, 1);\n'
+                   '  double D[1] = {1.0}, Dao[1] = {0.0}, F[1] = {0.0}, J[1] = {0.0};\n'
+                   '  b.AddAODensity(Dao, D); b.SliceAOFock(F, Dao); b.AccumulateDirect(J, D, &b);\n'
+                   '  rc = (Dao[0] == 1.0 && F[0] == 1.0 && J[0] > 0.0) ? 0 : 3; }\n'
+                   'catch (const qcg::Error& err) { rc = err.code == QCG_ERR_CUDA ? 10 : 11; }\n'
+                   'qcg::release_cache(); return rc; }\n')
+    libdir = os.path.dirname(api.library_path())
+    exe = tmp_path / "s"
+    subprocess.run(["g++", "-std=c++17", "-I", os.path.join(REPO, "include"), str(src), "-L", libdir, "-lqchem_b200",
+                    f"-Wl,-rpath,{libdir}", "-o", str(exe)], check=True)
+    rc = subprocess.run([str(exe)]).returncode
+    assert rc == (0 if torch.cuda.is_available() else 10)
+
+
+def test_default_jk_forms_do_not_overlap():
+    """The build's default J/K class sets: the team form for the high-L classes, the warp-shared form for
+    twelve others; no class is in both (the team form would take precedence), and (ss|ss), (pp|pp) and
+    (dd|ss) stay thread-per-quartet."""
+    from qchem_b200 import build as qb
+    team, warp = set(qb.JK_TEAM_CLASSES), set(qb.JK_WARP_CLASSES)
+    assert not team & warp
+    assert len(team) == 6 and len(warp) == 12
+    names = ["".join("spd"[l] for l in c) for c in W.quartet_classes()]
+    assert {names[k] for k in set(range(21)) - team - warp} == {"ssss", "pppp", "ddss"}
+    assert qb._jk_team_mask() & qb._jk_warp_mask() == 0
