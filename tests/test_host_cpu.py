@@ -256,8 +256,9 @@ def test_cpp_adapter_builds_and_fails_loudly_without_a_device(tmp_path):
 
 
 def test_hrr_class_selection(monkeypatch):
-    """The FP64 ERI batches use the horizontal-recurrence form for (dp|dp), (dd|pp), (dd|dp) and (dd|dd) by
-    default; QCG_ERI_HRR=1 / =0 switch every class."""
+    """Where an FP64 ERI batch runs thread-per-quartet (the team form switched off for the class), the
+    horizontal-recurrence form serves (dp|dp), (dd|pp), (dd|dp) and (dd|dd) by default; QCG_ERI_HRR=1 / =0
+    switch every class."""
     from qchem_b200 import build as qb
     monkeypatch.delenv("QCG_ERI_HRR", raising=False)
     picked = [W.quartet_classes()[k] for k in range(21) if qb._eri_hrr(k)]
